@@ -1,0 +1,331 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 path-tracing hot path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload rays|cornell|ggx] [--impl ours|reference]
+
+Default workload (the ray-query configuration): 2^22 FP32 rays, origins uniform in the scene
+box and directions uniform on the sphere (seeded), against a 1,310,720-triangle displaced
+icosphere (level 8, radius 10, 4-octave value noise of amplitude 0.1); closest hit through the
+8-wide quantised BVH. A step = one closest-hit launch over all rays; the metric is Mrays/s.
+
+One JSON line on rank 0. `value`: device-timed (CUDA events) throughput with rays resident in
+HBM; `e2e`: the same rays through the host-buffer C-ABI entry point rbr_trace_host (pinned
+host rays in, hits out, copies inside the timed region); `roofline`: algorithmic bytes of the
+traversal kernel (rays + hits + nodes and leaf records the traversal fetches, counted by
+rbr_trace_counts) per launch over its event-timed duration, against the measured HBM copy
+bandwidth; `cpu_baseline`: the reference's own BVH (oracle/_ref, built from the reference
+sources) on the host cores over a bounded sample of the same rays.
+
+With --impl reference the reference's CPU implementation is timed instead (rank 0 only).
+Multi-GPU: every rank traces its own 2^22 rays (weak scaling, no data-path collective).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO / "ray-based-rendering_b200"))
+
+RAYS_LOG2 = 22
+ICO_LEVEL = 8
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--workload", choices=["rays"], default="rays")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=8.0, help="target length of the CPU-baseline sample")
+    return p.parse_args()
+
+
+# ------------------------------------------------------------------------------------------
+def measured_peaks():
+    f = REPO / "MEASURED_PEAKS.json"
+    if f.exists():
+        d = json.loads(f.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clock and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self):
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self, gpu_indices=None):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        for line in Path(self.path).read_text().splitlines():
+            c = [x.strip() for x in line.split(",")]
+            if len(c) < 9:
+                continue
+            try:
+                idx, sm, smax = int(c[0]), float(c[1]), float(c[2])
+            except ValueError:
+                continue
+            if gpu_indices is not None and idx not in gpu_indices:
+                continue
+            rows.append((idx, sm, smax, c[5:9]))
+        os.unlink(self.path)
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i, v in enumerate(r[3]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[1] for r in rows), "sm_max_mhz": max(r[2] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def visible_gpu_indices(local_rank):
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        try:
+            return [int(vis.split(",")[local_rank])]
+        except (ValueError, IndexError):
+            return None
+    return [local_rank]
+
+
+# ------------------------------------------------------------------------------------------
+def workload(rank):
+    from rbr_b200 import scenes
+
+    scene = scenes.ray_query_scene(level=ICO_LEVEL, radius=10.0, seed=0)
+    lo, hi = scenes.scene_bounds(scene)
+    rays = scenes.uniform_rays(1 << RAYS_LOG2, lo, hi, seed=rank)
+    return scene, rays
+
+
+def cpu_baseline(scene, rays, target_s):
+    """The reference BVH (oracle/_ref) over a bounded sample of the rays, all host threads."""
+    sys.path.insert(0, str(REPO / "oracle"))
+    from oracle import Reference, have_reference
+
+    if not have_reference():
+        return None
+    ref = Reference()
+    h = ref.scene(scene)
+    threads = ref.max_threads()
+    n = 1 << 14
+    t0 = time.perf_counter()
+    ref.trace_closest(h, rays[:n], threads=threads)
+    dt = max(time.perf_counter() - t0, 1e-4)
+    n = int(min(len(rays), max(1 << 15, n / dt * target_s)))
+    t0 = time.perf_counter()
+    ref.trace_closest(h, rays[:n], threads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": n / dt / 1e6, "unit": "Mrays/s", "cores": threads, "kind": "reference",
+            "sample": f"first {n} of the 2^22 rays, reference BVH::intersect (src/acceleration/bvh.cpp) "
+                      f"in an OpenMP loop, {dt:.1f} s; BVH build not timed"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    sys.path.insert(0, str(REPO / "oracle"))
+    from oracle import Reference, have_reference
+
+    if not have_reference():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/librbr_ref.so was not built"}))
+        return
+    scene, rays = workload(0)
+    ref = Reference()
+    h = ref.scene(scene)
+    threads = ref.max_threads()
+    n = 1 << 14
+    t0 = time.perf_counter()
+    ref.trace_closest(h, rays[:n], threads=threads)
+    rate = n / max(time.perf_counter() - t0, 1e-4)
+    # each step: a bounded sample so that the whole run stays within a few minutes
+    n = int(min(len(rays), max(1 << 15, rate * 120.0 / max(1, args.steps + args.warmup))))
+    for i in range(args.warmup):
+        ref.trace_closest(h, rays[:n], threads=threads)
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        ref.trace_closest(h, rays[:n], threads=threads)
+    dt = time.perf_counter() - t0
+    value = n * args.steps / dt / 1e6
+    sample = f"{n} of the 2^22 rays per step, reference BVH::intersect in an OpenMP loop over {threads} threads"
+    print(json.dumps({
+        "impl": "reference", "metric": "Mrays/s traversal (closest hit)", "value": value, "unit": "Mrays/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": config_block(),
+        "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": threads, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def config_block():
+    return {"workload": "ray-query: 2^22 rays (origins uniform in the scene box, directions uniform on the sphere, "
+                        "seed 0) vs a 1,310,720-triangle displaced icosphere (level 8, radius 10, 4-octave value "
+                        "noise, amplitude 0.1); closest hit",
+            "rays_per_step": 1 << RAYS_LOG2, "triangles": 20 * 4 ** ICO_LEVEL,
+            "l2": "inputs larger than L2: 134 MB of rays per step (the 70 MB BVH stays L2-resident by design)",
+            "parallelism": "replicas (each GPU its own rays)"}
+
+
+# ------------------------------------------------------------------------------------------
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local_rank)
+
+    from rbr_b200 import Context, abi
+
+    scene, rays = workload(rank)
+    ctx = Context(local_rank)
+    stats = ctx.upload(scene)
+    n = len(rays)
+    d_rays = torch.from_numpy(rays.view(np.uint8)).to(f"cuda:{local_rank}")
+    d_hits = torch.empty(n * 8, dtype=torch.uint8, device=f"cuda:{local_rank}")
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+
+    def step():
+        ctx.trace_closest_dev(d_rays.data_ptr(), n, d_hits.data_ptr(), sp)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    clocks = Clocks() if rank == 0 else None
+    if clocks:
+        clocks.start()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    evs[0].record(stream)
+    for k in range(args.steps):
+        step()
+        evs[k + 1].record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    launch_ms = [evs[k].elapsed_time(evs[k + 1]) for k in range(args.steps)]
+    total_ms = evs[0].elapsed_time(evs[-1])
+    if dist:
+        t = torch.tensor([total_ms], device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    clk = clocks.stop(visible_gpu_indices(local_rank)) if clocks else None
+
+    # algorithmic traffic of one launch
+    nodes, recs = ctx.trace_counts_dev(d_rays.data_ptr(), n)
+    alg_bytes = n * (32 + 8) + nodes * 80 + recs * 48
+    avg_launch_s = statistics.mean(launch_ms) / 1e3
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / avg_launch_s / 1e9
+    traffic = None
+    tf = REPO / "profiles" / "traffic.json"
+    if tf.exists():
+        traffic = json.loads(tf.read_text()).get("trace_closest_icosphere8")
+
+    # end to end through the host-buffer entry point
+    host_rays = torch.from_numpy(rays.view(np.uint8)).pin_memory()
+    host_hits = torch.empty(n * 8, dtype=torch.uint8).pin_memory()
+    hr = host_rays.numpy().view(abi.RAY_DTYPE)
+    hh = host_hits.numpy().view(abi.HIT_DTYPE)
+    for _ in range(2):
+        ctx.trace_host(hr, out=hh)
+    e2e_steps = max(3, min(args.steps, 10))
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        ctx.trace_host(hr, out=hh)
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    got = d_hits.cpu().numpy().view(abi.HIT_DTYPE)
+    assert np.array_equal(got["prim"], hh["prim"]), "device and host entry points disagree"
+
+    base = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        base = cpu_baseline(scene, rays, args.cpu_seconds)
+
+    if rank == 0:
+        value = n * world * args.steps / (total_ms / 1e3) / 1e6
+        line = {
+            "metric": "Mrays/s traversal (closest hit)", "value": value, "unit": "Mrays/s", "n_gpus": world,
+            "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded)", "config": config_block(),
+            "e2e": {"value": n * world * e2e_steps / e2e_s / 1e6, "unit": "Mrays/s",
+                    "h2d_bytes_per_step": n * 32, "d2h_bytes_per_step": n * 8,
+                    "path": "rbr_trace_host: pinned host rays -> device, closest hit, hits -> pinned host"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": f"{peak_kind} HBM copy bandwidth",
+                         "algorithmic_bytes_per_launch": alg_bytes,
+                         "per_ray": {"nodes": nodes / n, "leaf_records": recs / n,
+                                     "bytes": alg_bytes / n},
+                         "kernel": "k_trace_closest", "avg_launch_ms": avg_launch_s * 1e3},
+            "cpu_baseline": base,
+            "clocks": clk,
+            "gpu_launches": args.steps,
+            "bvh": {"wide_nodes": stats.num_wide_nodes, "leaf_records": stats.num_leaf_records,
+                    "depth": stats.max_depth, "build_s": stats.build_seconds,
+                    "device_mb": stats.device_bytes / 1e6},
+        }
+        print(json.dumps(line))
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

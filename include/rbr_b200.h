@@ -1,0 +1,251 @@
+/*
+ * rbr_b200.h — C ABI of the B200 path-tracing library (librbr_b200.so).
+ *
+ * The library is the GPU side of two drop-ins for the Ray-Based-Rendering C++17 API:
+ *   - an Accelerator   (include/render/acceleration/accelerator.h:19-34) selected with `-a gpubvh`,
+ *   - an Integrator    (include/render/renderers/integrator.h:37-73)     selected with `-i gpupt`.
+ * The C++ adapters that derive from those classes (adapters/gpu_accelerator.h,
+ * adapters/gpu_integrator.h) flatten a render::Scene into the plain arrays below and call
+ * these entry points. Nothing here uses C++ or CUDA types: streams are passed as `void*`
+ * (a cudaStream_t, NULL = the legacy default stream) and every buffer is a plain pointer.
+ *
+ * Conventions
+ *   - Every entry point returns an rbr_status; on failure rbr_last_error() holds a message.
+ *   - A context owns all of its device memory (scene, BVH, queues, film, cache). Calls on one
+ *     context are not re-entrant: callers that share a context across threads serialise them.
+ *   - "device pointer" arguments must point to memory of the context's device;
+ *     "host pointer" arguments may be pageable or pinned host memory.
+ *   - There is no CPU fallback: without a usable CUDA device rbr_ctx_create fails.
+ */
+#ifndef RBR_B200_H
+#define RBR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RBR_ABI_VERSION 1u
+
+typedef enum rbr_status {
+    RBR_OK = 0,
+    RBR_ERR_INVALID_ARGUMENT = 1, /* bad pointer, size, index or NaN in a descriptor */
+    RBR_ERR_CUDA = 2,             /* a CUDA runtime call failed (message has the CUDA error) */
+    RBR_ERR_OUT_OF_MEMORY = 3,    /* device or pinned-host allocation failed */
+    RBR_ERR_NO_SCENE = 4,         /* a trace/render call before rbr_scene_upload */
+    RBR_ERR_UNSUPPORTED = 5,      /* input the GPU path does not implement (reported, never emulated) */
+    RBR_ERR_DEVICE_TIMEOUT = 6,   /* a bounded device-side wait ran out; the context stays usable */
+    RBR_ERR_INTERNAL = 7          /* a device-side consistency check failed (e.g. stack overflow) */
+} rbr_status;
+
+/* Marks "no primitive" in rbr_hit.prim. */
+#define RBR_MISS 0xFFFFFFFFu
+
+typedef struct rbr_ctx rbr_ctx;
+
+/* ------------------------------------------------------------------------------------------
+ * Scene description. Mirrors what render::Scene holds (include/render/scene/scene.h:92-95):
+ * primitives with a material each, the six-parameter materials, lights and a background.
+ * Primitive ids: the index of the primitive in Scene::primitives(); the per-type `*_ids`
+ * arrays give it. When an ids array is NULL the ids of that type follow one another in the
+ * order triangles, spheres, quads, planes (so an all-NULL scene numbers them in that order).
+ * ids must be a permutation of 0..N-1 over all primitives of the scene.
+ * ------------------------------------------------------------------------------------------ */
+
+/* render::Material's six public parameters (include/render/materials/material.h:28-36). */
+typedef struct rbr_material {
+    float base_color[3];
+    float metallic;
+    float roughness;
+    float ior;
+    float transmission;
+    float emission[3];
+} rbr_material;
+
+enum { RBR_LIGHT_AREA = 0, RBR_LIGHT_POINT = 1 };
+
+/* render::AreaLight (include/render/lighting/area_light.h:16-27: centre `position`, edges u, v)
+ * or render::PointLight (include/render/lighting/point_light.h:13-20; u, v unused). */
+typedef struct rbr_light {
+    uint32_t type;        /* RBR_LIGHT_AREA or RBR_LIGHT_POINT */
+    float position[3];
+    float u[3];
+    float v[3];
+    float color[3];
+    float intensity;
+} rbr_light;
+
+typedef struct rbr_scene_desc {
+    /* render::Triangle (include/render/geometry/triangle.h:13-52): v0, v1, v2 per triangle. */
+    uint32_t num_triangles;
+    const float* triangle_vertices;     /* [num_triangles][9] */
+    const float* triangle_normals;      /* optional [num_triangles][9] unit n0, n1, n2, or NULL */
+    const uint32_t* triangle_materials; /* [num_triangles] */
+    const uint32_t* triangle_ids;       /* optional */
+    /* render::Sphere (include/render/geometry/sphere.h:13-19): centre, radius. */
+    uint32_t num_spheres;
+    const float* spheres;               /* [num_spheres][4] */
+    const uint32_t* sphere_materials;
+    const uint32_t* sphere_ids;
+    /* render::Quad (include/render/geometry/quad.h:13-19): corner `origin`, edges u, v. */
+    uint32_t num_quads;
+    const float* quads;                 /* [num_quads][9] */
+    const uint32_t* quad_materials;
+    const uint32_t* quad_ids;
+    /* render::Plane (include/render/geometry/plane.h:13-19): unit normal and d (n.p + d = 0). */
+    uint32_t num_planes;
+    const float* planes;                /* [num_planes][4] */
+    const uint32_t* plane_materials;
+    const uint32_t* plane_ids;
+    uint32_t num_materials;
+    const rbr_material* materials;
+    uint32_t num_lights;                /* in Scene::lights() order */
+    const rbr_light* lights;
+    float background[3];                /* Scene::backgroundColor */
+} rbr_scene_desc;
+
+/* Sizes of what rbr_scene_upload built. */
+typedef struct rbr_scene_stats {
+    uint32_t num_primitives;      /* all primitives */
+    uint32_t num_bounded;         /* primitives inside the BVH */
+    uint32_t num_unbounded;       /* planes, tested outside the BVH */
+    uint32_t num_wide_nodes;      /* 8-wide nodes (80 B each) */
+    uint32_t num_leaf_records;    /* leaf primitive records (48 B each) */
+    uint32_t max_depth;           /* depth of the wide tree */
+    uint64_t device_bytes;        /* device memory held by the scene */
+    double build_seconds;         /* host SAH build + collapse + quantisation */
+} rbr_scene_stats;
+
+/* ------------------------------------------------------------------------------------------
+ * Ray queries. render::Ray (include/render/core/ray.h:10-35): origin, unit direction, tMax;
+ * the implicit tMin is the primitives' EPSILON = 1e-4 (include/render/core/common.h:22).
+ * Directions are used exactly as given (render::Ray normalises in its constructor, so a
+ * caller passes the already-normalised direction of its Ray).
+ * ------------------------------------------------------------------------------------------ */
+typedef struct rbr_ray {
+    float origin[3];
+    float tmax;
+    float direction[3];
+    float pad;
+} rbr_ray; /* 32 B, two 16 B loads */
+
+typedef struct rbr_hit {
+    uint32_t prim; /* primitive id, RBR_MISS if nothing was hit */
+    float t;       /* SurfaceInteraction::t of the closest hit */
+} rbr_hit;
+
+/* ------------------------------------------------------------------------------------------
+ * Camera and integrator parameters.
+ * ------------------------------------------------------------------------------------------ */
+
+enum { RBR_CAMERA_PINHOLE = 0, RBR_CAMERA_THIN_LENS = 1 };
+
+/* A PinholeCamera or a ThinLensCamera: CameraExtrinsics
+ * (include/render/camera/camera_extrinsics.h:16-21) + PerspectiveIntrinsics
+ * (include/render/camera/perspective_intrinsics.h:21-24) + thin-lens parameters
+ * (include/render/camera/thin_lens_camera.h:15-16). */
+typedef struct rbr_camera {
+    int32_t width, height;
+    uint32_t model;          /* RBR_CAMERA_PINHOLE or RBR_CAMERA_THIN_LENS */
+    float position[3];
+    float forward[3];
+    float right[3];
+    float up[3];
+    float fx, fy, cx, cy;
+    float lens_radius;
+    float focal_distance;
+} rbr_camera;
+
+/* Flags of rbr_render_params.flags. */
+enum {
+    /* Adds the BSDF-sampled hit of emissive geometry with the matching MIS weight instead of
+     * discarding it (the reference's estimator drops it: path_tracing_integrator.cpp:130-133).
+     * Off by default so that images converge to what the reference converges to. */
+    RBR_RENDER_CORRECTED_MIS = 1u << 0,
+    /* Also return per-pixel sums of squared sample values (for Monte-Carlo error bars). */
+    RBR_RENDER_SECOND_MOMENT = 1u << 1
+};
+
+/* IntegratorConfig (include/render/renderers/integrator.h:22-28). */
+typedef struct rbr_render_params {
+    int32_t samples_per_pixel;
+    int32_t max_depth;
+    int32_t use_nee;
+    int32_t use_mis;
+    uint64_t seed;            /* key of the counter-based RNG */
+    uint32_t sample_offset;   /* index of the first sample (independent batches use disjoint ranges) */
+    uint32_t flags;           /* RBR_RENDER_* */
+} rbr_render_params;
+
+/* Timings and counters of the last rbr_render call. */
+typedef struct rbr_render_stats {
+    uint64_t paths;           /* camera samples traced */
+    uint64_t extension_rays;  /* closest-hit rays */
+    uint64_t shadow_rays;     /* any-hit rays */
+    uint32_t waves;           /* path chunks processed */
+    uint32_t launches;        /* kernels launched */
+    float milliseconds;       /* device time of the whole render (CUDA events) */
+} rbr_render_stats;
+
+/* ------------------------------------------------------------------------------------------
+ * Entry points.
+ * ------------------------------------------------------------------------------------------ */
+
+uint32_t rbr_abi_version(void);
+/* sizeof() of a struct of this header by name ("rbr_ray", ...), 0 for an unknown name; lets
+ * bindings check their struct mirrors against the compiled library. */
+size_t rbr_struct_size(const char* name);
+
+/* Creates a context on CUDA device `device`. */
+rbr_status rbr_ctx_create(int device, rbr_ctx** out);
+void rbr_ctx_destroy(rbr_ctx* ctx);
+const char* rbr_last_error(const rbr_ctx* ctx);
+
+/* Replaces the context's scene: validates the description, builds the SAH BVH on the host,
+ * collapses it into the 8-wide quantised layout and uploads everything.
+ * Replaces: Scene::buildAccelerator / Accelerator::build (src/scene/scene.cpp:22-28,
+ * include/render/acceleration/accelerator.h:25). A rebuild drops the previous contents. */
+rbr_status rbr_scene_upload(rbr_ctx* ctx, const rbr_scene_desc* desc);
+rbr_status rbr_scene_stats_get(const rbr_ctx* ctx, rbr_scene_stats* out);
+/* World bounds of the bounded primitives (Accelerator::worldBounds, accelerator.h:33).
+ * An empty scene gives min = +FLT_MAX, max = -FLT_MAX (an empty BoundingBox). */
+rbr_status rbr_world_bounds(const rbr_ctx* ctx, float out_min[3], float out_max[3]);
+
+/* Closest hit for n rays (device pointers), asynchronous on `stream`.
+ * Replaces: Accelerator::intersect / BVH::intersect (accelerator.h:28, src/acceleration/bvh.cpp:33-36). */
+rbr_status rbr_trace_closest(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, rbr_hit* hits, void* stream);
+/* Any hit (occluded[i] = 1 if something lies in [EPSILON, tmax]), device pointers, asynchronous.
+ * Replaces: Accelerator::intersectP / BVH::intersectP (accelerator.h:31, bvh.cpp:38-41). */
+rbr_status rbr_trace_any(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, uint8_t* occluded, void* stream);
+/* The same two queries on host buffers: copies the rays in, traces, copies the answers out and
+ * waits. `out` is rbr_hit[n] when any_hit == 0, uint8_t[n] otherwise. */
+rbr_status rbr_trace_host(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any_hit, void* out);
+
+/* Diagnostic: replays the traversal of n rays (device pointer) and returns the total number of
+ * 8-wide nodes fetched (out[0]) and leaf records tested (out[1]); waits for the result.
+ * The traversal order of a ray is deterministic, so these are its algorithmic node and leaf
+ * traffic (80 B per node, 48 B per record) for roofline accounting. No reference counterpart. */
+rbr_status rbr_trace_counts(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any_hit, uint64_t out[2]);
+
+/* Renders the scene with the wavefront path tracer.
+ * film_mean: device pointer, width*height*3 floats, receives the per-pixel mean over the
+ * samples, as Film::addSample(x, y, sum / spp) stores it (src/renderers/integrator.cpp:36).
+ * film_m2: device pointer or NULL; with RBR_RENDER_SECOND_MOMENT it receives per-pixel sums
+ * of squared sample values (width*height*3 floats). Asynchronous on `stream`.
+ * Replaces: Integrator::render with PathTracingIntegrator::Li (src/renderers/integrator.cpp:7-50,
+ * src/renderers/path_tracing_integrator.cpp:5-138). */
+rbr_status rbr_render(rbr_ctx* ctx, const rbr_camera* camera, const rbr_render_params* params,
+                      float* film_mean, float* film_m2, void* stream);
+/* The same on host buffers (film_mean required, film_m2 optional); waits for the result. */
+rbr_status rbr_render_host(rbr_ctx* ctx, const rbr_camera* camera, const rbr_render_params* params,
+                           float* film_mean, float* film_m2);
+/* Counters and device time of the last render (waits for it). */
+rbr_status rbr_render_stats_get(rbr_ctx* ctx, rbr_render_stats* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RBR_B200_H */

@@ -1,0 +1,383 @@
+// Host BVH construction for the GPU traversal kernels.
+//
+// 1. Binary tree, binned SAH (32 bins on each of the three axes, centroid binning), leaves of
+//    at most 3 primitives. The reference's own builder (src/acceleration/bvh.cpp:47-209) bins
+//    12 buckets on the single axis of largest centroid extent and stops at 4 primitives; its
+//    tree shape does not enter any result here: closest-hit answers are defined by the
+//    primitives alone (smallest t, ties to the highest primitive id, as a brute-force loop in
+//    primitive order gives), so the GPU tree is free to be a better one.
+// 2. Collapse into 8-wide nodes: starting from a node's two children, the child with the
+//    largest surface area is replaced by its two children until 8 slots are full.
+// 3. Quantise each node's child boxes to 8-bit coordinates on a per-axis power-of-two grid,
+//    rounded outwards, after growing every box by `pad`.
+#include "bvh_build.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <thread>
+
+#include "rbr_layout.h"
+
+namespace rbr {
+namespace {
+
+constexpr int kBins = 32;
+constexpr int kForceMedianDepth = 40;     // below this depth splits become plain median splits
+constexpr uint32_t kParallelMin = 32768;  // subtrees at least this large may get their own thread
+constexpr float kTraversalCost = 1.0f;
+constexpr float kIntersectCost = 1.0f;
+
+struct BNode {
+    Box box;
+    uint32_t left = 0, right = 0;
+    uint32_t begin = 0, count = 0;  // count > 0: leaf over refs[begin, begin + count)
+};
+
+inline Box empty_box() {
+    Box b;
+    for (int a = 0; a < 3; ++a) {
+        b.lo[a] = FLT_MAX;
+        b.hi[a] = -FLT_MAX;
+    }
+    return b;
+}
+
+inline void grow(Box& b, const Box& o) {
+    for (int a = 0; a < 3; ++a) {
+        b.lo[a] = std::min(b.lo[a], o.lo[a]);
+        b.hi[a] = std::max(b.hi[a], o.hi[a]);
+    }
+}
+
+inline float half_area(const Box& b) {
+    const float dx = b.hi[0] - b.lo[0], dy = b.hi[1] - b.lo[1], dz = b.hi[2] - b.lo[2];
+    if (dx < 0.0f || dy < 0.0f || dz < 0.0f) return 0.0f;
+    return dx * dy + dy * dz + dz * dx;
+}
+
+struct Builder {
+    const std::vector<Box>& boxes;
+    std::vector<float> cen;
+    std::vector<uint32_t> refs;
+    std::vector<BNode> nodes;
+    std::atomic<uint32_t> next_node{1};
+    std::atomic<int> threads_left{0};
+    std::atomic<uint32_t> depth_seen{0};
+
+    explicit Builder(const std::vector<Box>& b) : boxes(b) {}
+
+    int bin_of(float c, float cmin, float scale) const {
+        int k = static_cast<int>((c - cmin) * scale);
+        return std::min(kBins - 1, std::max(0, k));
+    }
+
+    void build(uint32_t ni, uint32_t begin, uint32_t end, uint32_t depth) {
+        uint32_t seen = depth_seen.load(std::memory_order_relaxed);
+        while (depth > seen && !depth_seen.compare_exchange_weak(seen, depth)) {
+        }
+        Box b = empty_box(), cb = empty_box();
+        for (uint32_t i = begin; i < end; ++i) {
+            const uint32_t r = refs[i];
+            grow(b, boxes[r]);
+            for (int a = 0; a < 3; ++a) {
+                cb.lo[a] = std::min(cb.lo[a], cen[3 * r + a]);
+                cb.hi[a] = std::max(cb.hi[a], cen[3 * r + a]);
+            }
+        }
+        BNode& node = nodes[ni];
+        node.box = b;
+        const uint32_t n = end - begin;
+        if (n <= 1) {
+            node.begin = begin;
+            node.count = n;
+            return;
+        }
+        uint32_t mid = begin;
+        bool split = false;
+        if (depth < kForceMedianDepth) {
+            // binned SAH over the three axes
+            float best = FLT_MAX;
+            int best_axis = -1, best_bin = -1;
+            float scale[3];
+            struct Bin {
+                Box box;
+                uint32_t count;
+            } bins[3][kBins];
+            for (int a = 0; a < 3; ++a) {
+                const float ext = cb.hi[a] - cb.lo[a];
+                scale[a] = ext > 0.0f ? (kBins * (1.0f - 1e-6f)) / ext : 0.0f;
+                for (int k = 0; k < kBins; ++k) {
+                    bins[a][k].box = empty_box();
+                    bins[a][k].count = 0;
+                }
+            }
+            for (uint32_t i = begin; i < end; ++i) {
+                const uint32_t r = refs[i];
+                for (int a = 0; a < 3; ++a) {
+                    if (scale[a] == 0.0f) continue;
+                    Bin& bin = bins[a][bin_of(cen[3 * r + a], cb.lo[a], scale[a])];
+                    grow(bin.box, boxes[r]);
+                    bin.count++;
+                }
+            }
+            for (int a = 0; a < 3; ++a) {
+                if (scale[a] == 0.0f) continue;
+                float rarea[kBins];
+                uint32_t rcount[kBins];
+                Box acc = empty_box();
+                uint32_t cnt = 0;
+                for (int k = kBins - 1; k >= 0; --k) {
+                    grow(acc, bins[a][k].box);
+                    cnt += bins[a][k].count;
+                    rarea[k] = half_area(acc);
+                    rcount[k] = cnt;
+                }
+                acc = empty_box();
+                cnt = 0;
+                for (int k = 0; k < kBins - 1; ++k) {
+                    grow(acc, bins[a][k].box);
+                    cnt += bins[a][k].count;
+                    if (cnt == 0 || rcount[k + 1] == 0) continue;
+                    const float cost = half_area(acc) * cnt + rarea[k + 1] * rcount[k + 1];
+                    if (cost < best) {
+                        best = cost;
+                        best_axis = a;
+                        best_bin = k;
+                    }
+                }
+            }
+            const float area = half_area(b);
+            const float leaf_cost = kIntersectCost * n * area;
+            const float split_cost = kTraversalCost * area + kIntersectCost * best;
+            if (n <= static_cast<uint32_t>(kMaxLeafPrims) && (best_axis < 0 || leaf_cost <= split_cost)) {
+                node.begin = begin;
+                node.count = n;
+                return;
+            }
+            if (best_axis >= 0) {
+                const int a = best_axis;
+                const float cmin = cb.lo[a], sc = scale[a];
+                uint32_t* m = std::partition(refs.data() + begin, refs.data() + end, [&](uint32_t r) {
+                    return bin_of(cen[3 * r + a], cmin, sc) <= best_bin;
+                });
+                mid = static_cast<uint32_t>(m - refs.data());
+                split = mid > begin && mid < end;
+            }
+        }
+        if (!split) {
+            if (n <= static_cast<uint32_t>(kMaxLeafPrims)) {
+                node.begin = begin;
+                node.count = n;
+                return;
+            }
+            int a = 0;
+            float ext = -1.0f;
+            for (int k = 0; k < 3; ++k) {
+                const float e = cb.hi[k] - cb.lo[k];
+                if (e > ext) {
+                    ext = e;
+                    a = k;
+                }
+            }
+            mid = begin + n / 2;
+            std::nth_element(refs.data() + begin, refs.data() + mid, refs.data() + end,
+                             [&](uint32_t x, uint32_t y) { return cen[3 * x + a] < cen[3 * y + a]; });
+        }
+        const uint32_t c = next_node.fetch_add(2);
+        nodes[ni].left = c;
+        nodes[ni].right = c + 1;
+        if (n >= kParallelMin && threads_left.fetch_sub(1) > 0) {
+            std::thread t([=] { build(c, begin, mid, depth + 1); });
+            build(c + 1, mid, end, depth + 1);
+            t.join();
+        } else {
+            build(c, begin, mid, depth + 1);
+            build(c + 1, mid, end, depth + 1);
+        }
+    }
+};
+
+inline float nudge_down(double x) {
+    float f = static_cast<float>(x);
+    if (static_cast<double>(f) > x) f = std::nextafter(f, -FLT_MAX);
+    return f;
+}
+
+struct ChildRef {
+    uint32_t bnode;
+    bool leaf;
+};
+
+}  // namespace
+
+WideBVH build_wide_bvh(const std::vector<Box>& boxes, float pad, int threads) {
+    WideBVH out;
+    const uint32_t n = static_cast<uint32_t>(boxes.size());
+    if (n == 0) return out;
+
+    Builder B(boxes);
+    B.cen.resize(3 * static_cast<size_t>(n));
+    B.refs.resize(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        B.refs[i] = i;
+        for (int a = 0; a < 3; ++a) B.cen[3 * i + a] = 0.5f * (boxes[i].lo[a] + boxes[i].hi[a]);
+    }
+    B.nodes.resize(2 * static_cast<size_t>(n));
+    B.threads_left = std::max(0, threads - 1);
+    B.build(0, 0, n, 1);
+    out.binary_nodes = B.next_node.load();
+
+    // Collapse to 8-wide nodes, breadth first.
+    struct Item {
+        uint32_t wide;
+        uint32_t bnode;
+        uint32_t depth;
+    };
+    std::vector<Item> queue;
+    queue.push_back({0, 0, 1});
+    out.nodes.assign(kNodeWords, 0u);
+    out.leaf_order.reserve(n);
+    for (size_t head = 0; head < queue.size(); ++head) {
+        const Item item = queue[head];
+        out.max_depth = std::max(out.max_depth, item.depth);
+        ChildRef ch[8];
+        int k = 0;
+        const BNode& root = B.nodes[item.bnode];
+        if (root.count > 0) {
+            ch[k++] = {item.bnode, true};
+        } else {
+            ch[k++] = {root.left, B.nodes[root.left].count > 0};
+            ch[k++] = {root.right, B.nodes[root.right].count > 0};
+            while (k < 8) {
+                int pick = -1;
+                float best = -1.0f;
+                for (int i = 0; i < k; ++i) {
+                    if (ch[i].leaf) continue;
+                    const float a = half_area(B.nodes[ch[i].bnode].box);
+                    if (a > best) {
+                        best = a;
+                        pick = i;
+                    }
+                }
+                if (pick < 0) break;
+                const BNode& bn = B.nodes[ch[pick].bnode];
+                ch[pick] = {bn.left, B.nodes[bn.left].count > 0};
+                ch[k++] = {bn.right, B.nodes[bn.right].count > 0};
+            }
+        }
+        // padded child boxes in double precision
+        double clo[8][3], chi[8][3], nlo[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, nhi[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+        for (int i = 0; i < k; ++i) {
+            const Box& bx = B.nodes[ch[i].bnode].box;
+            for (int a = 0; a < 3; ++a) {
+                clo[i][a] = static_cast<double>(bx.lo[a]) - pad;
+                chi[i][a] = static_cast<double>(bx.hi[a]) + pad;
+                nlo[a] = std::min(nlo[a], clo[i][a]);
+                nhi[a] = std::max(nhi[a], chi[i][a]);
+            }
+        }
+        // slots: child i goes to the slot whose octant direction its centre points to most
+        int slot_child[8];
+        for (int s = 0; s < 8; ++s) slot_child[s] = -1;
+        {
+            double score[8][8];
+            for (int i = 0; i < k; ++i) {
+                for (int s = 0; s < 8; ++s) {
+                    double v = 0.0;
+                    for (int a = 0; a < 3; ++a) {
+                        const double d = 0.5 * (clo[i][a] + chi[i][a]) - 0.5 * (nlo[a] + nhi[a]);
+                        v += ((s >> a) & 1) ? -d : d;
+                    }
+                    score[i][s] = v;
+                }
+            }
+            bool child_used[8] = {}, slot_used[8] = {};
+            for (int it = 0; it < k; ++it) {
+                double best = -DBL_MAX;
+                int bi = -1, bs = -1;
+                for (int i = 0; i < k; ++i) {
+                    if (child_used[i]) continue;
+                    for (int s = 0; s < 8; ++s) {
+                        if (slot_used[s]) continue;
+                        if (score[i][s] > best) {
+                            best = score[i][s];
+                            bi = i;
+                            bs = s;
+                        }
+                    }
+                }
+                child_used[bi] = slot_used[bs] = true;
+                slot_child[bs] = bi;
+            }
+        }
+        // quantisation grid
+        uint32_t* w = &out.nodes[static_cast<size_t>(item.wide) * kNodeWords];
+        float p[3];
+        double scale[3];
+        uint32_t ebits = 0;
+        for (int a = 0; a < 3; ++a) {
+            p[a] = nudge_down(nlo[a]);
+            const double ext = nhi[a] - static_cast<double>(p[a]);
+            int e = -100;
+            if (ext > 0.0) {
+                e = static_cast<int>(std::ceil(std::log2(ext / 255.0)));
+                while (std::ldexp(255.0, e) < ext) ++e;
+                while (e > -126 && std::ldexp(255.0, e - 1) >= ext) --e;
+            }
+            e = std::max(-126, std::min(127, e));
+            scale[a] = std::ldexp(1.0, e);
+            ebits |= static_cast<uint32_t>(e + 127) << (8 * a);
+            std::memcpy(&w[a], &p[a], 4);
+        }
+        uint8_t meta[8] = {}, qlo[3][8], qhi[3][8];
+        uint32_t imask = 0;
+        const uint32_t child_base = static_cast<uint32_t>(out.nodes.size() / kNodeWords);
+        const uint32_t prim_base = static_cast<uint32_t>(out.leaf_order.size());
+        uint32_t internal_rank = 0, prim_offset = 0;
+        for (int s = 0; s < 8; ++s) {
+            const int i = slot_child[s];
+            if (i < 0) {
+                for (int a = 0; a < 3; ++a) {
+                    qlo[a][s] = 255;  // inverted box: never hit
+                    qhi[a][s] = 0;
+                }
+                continue;
+            }
+            for (int a = 0; a < 3; ++a) {
+                const double lo = std::floor((clo[i][a] - p[a]) / scale[a]);
+                const double hi = std::ceil((chi[i][a] - p[a]) / scale[a]);
+                qlo[a][s] = static_cast<uint8_t>(std::max(0.0, std::min(255.0, lo)));
+                qhi[a][s] = static_cast<uint8_t>(std::max(0.0, std::min(255.0, hi)));
+            }
+            const BNode& bn = B.nodes[ch[i].bnode];
+            if (ch[i].leaf) {
+                meta[s] = static_cast<uint8_t>((bn.count << 5) | prim_offset);
+                for (uint32_t j = 0; j < bn.count; ++j) out.leaf_order.push_back(B.refs[bn.begin + j]);
+                prim_offset += bn.count;
+            } else {
+                imask |= 1u << s;
+                queue.push_back({child_base + internal_rank, ch[i].bnode, item.depth + 1});
+                ++internal_rank;
+            }
+        }
+        out.nodes.resize(out.nodes.size() + static_cast<size_t>(internal_rank) * kNodeWords, 0u);
+        w = &out.nodes[static_cast<size_t>(item.wide) * kNodeWords];  // may have moved
+        for (int a = 0; a < 3; ++a) std::memcpy(&w[a], &p[a], 4);
+        w[3] = ebits | (imask << 24);
+        w[4] = internal_rank ? child_base : 0u;
+        w[5] = prim_base;
+        std::memcpy(&w[6], meta, 8);
+        std::memcpy(&w[8], qlo[0], 8);
+        std::memcpy(&w[10], qlo[1], 8);
+        std::memcpy(&w[12], qlo[2], 8);
+        std::memcpy(&w[14], qhi[0], 8);
+        std::memcpy(&w[16], qhi[1], 8);
+        std::memcpy(&w[18], qhi[2], 8);
+    }
+    return out;
+}
+
+}  // namespace rbr

@@ -1,0 +1,255 @@
+// The C ABI of include/rbr_b200.h.
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "rbr_context.h"
+
+namespace rbr {
+
+rbr_status fail(rbr_ctx* ctx, rbr_status code, const std::string& msg) {
+    if (ctx) ctx->error = msg;
+    return code;
+}
+
+rbr_status cuda_fail(rbr_ctx* ctx, cudaError_t e, const char* what) {
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        return fail(ctx, RBR_ERR_OUT_OF_MEMORY, std::string(what) + ": " + cudaGetErrorString(e));
+    }
+    return fail(ctx, RBR_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+void release(DevBuf& b) {
+    if (b.ptr) cudaFree(b.ptr);
+    b.ptr = nullptr;
+    b.bytes = 0;
+}
+
+rbr_status ensure(rbr_ctx* ctx, DevBuf& b, size_t bytes, const char* what) {
+    if (b.bytes >= bytes && b.ptr) return RBR_OK;
+    release(b);
+    if (bytes == 0) return RBR_OK;
+    cudaError_t e = cudaMalloc(&b.ptr, bytes);
+    if (e != cudaSuccess) {
+        b.ptr = nullptr;
+        cudaGetLastError();
+        return fail(ctx, RBR_ERR_OUT_OF_MEMORY, std::string("cudaMalloc for ") + what + " (" + std::to_string(bytes) +
+                                                    " B): " + cudaGetErrorString(e));
+    }
+    b.bytes = bytes;
+    return RBR_OK;
+}
+
+// Reads (and clears) the device error word after the work on `stream` has finished.
+rbr_status check_device_error(rbr_ctx* ctx, cudaStream_t stream) {
+    int h = 0;
+    cudaError_t e = cudaMemcpyAsync(&h, ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "reading the device error word");
+    if (h == 0) return RBR_OK;
+    cudaMemsetAsync(ctx->d_error, 0, sizeof(int), stream);
+    cudaStreamSynchronize(stream);
+    std::string what;
+    if (h & kErrStackOverflow) what += " traversal-stack overflow;";
+    if (h & kErrQueueOverflow) what += " queue overflow;";
+    return fail(ctx, RBR_ERR_INTERNAL, "device check failed:" + what);
+}
+
+}  // namespace rbr
+
+using namespace rbr;
+
+extern "C" {
+
+uint32_t rbr_abi_version(void) { return RBR_ABI_VERSION; }
+
+size_t rbr_struct_size(const char* name) {
+    if (!name) return 0;
+    const std::string n(name);
+    if (n == "rbr_material") return sizeof(rbr_material);
+    if (n == "rbr_light") return sizeof(rbr_light);
+    if (n == "rbr_scene_desc") return sizeof(rbr_scene_desc);
+    if (n == "rbr_scene_stats") return sizeof(rbr_scene_stats);
+    if (n == "rbr_ray") return sizeof(rbr_ray);
+    if (n == "rbr_hit") return sizeof(rbr_hit);
+    if (n == "rbr_camera") return sizeof(rbr_camera);
+    if (n == "rbr_render_params") return sizeof(rbr_render_params);
+    if (n == "rbr_render_stats") return sizeof(rbr_render_stats);
+    return 0;
+}
+
+rbr_status rbr_ctx_create(int device, rbr_ctx** out) {
+    if (!out) return RBR_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return RBR_ERR_CUDA;  // no usable device: there is no CPU fallback
+    }
+    if (device < 0 || device >= count) return RBR_ERR_INVALID_ARGUMENT;
+    rbr_ctx* ctx = new (std::nothrow) rbr_ctx();
+    if (!ctx) return RBR_ERR_OUT_OF_MEMORY;
+    ctx->device = device;
+    if ((e = cudaSetDevice(device)) != cudaSuccess ||
+        (e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaMalloc(reinterpret_cast<void**>(&ctx->d_error), sizeof(int))) != cudaSuccess ||
+        (e = cudaMemset(ctx->d_error, 0, sizeof(int))) != cudaSuccess ||
+        (e = cudaEventCreate(&ctx->ev_start)) != cudaSuccess || (e = cudaEventCreate(&ctx->ev_stop)) != cudaSuccess) {
+        cudaGetLastError();
+        rbr_ctx_destroy(ctx);
+        return RBR_ERR_CUDA;
+    }
+    *out = ctx;
+    return RBR_OK;
+}
+
+void rbr_ctx_destroy(rbr_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    cudaDeviceSynchronize();
+    free_scene(ctx);
+    free_path_buffers(ctx);
+    release(ctx->stage_in);
+    release(ctx->stage_out);
+    if (ctx->d_error) cudaFree(ctx->d_error);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
+    if (ctx->ev_stop) cudaEventDestroy(ctx->ev_stop);
+    delete ctx;
+}
+
+const char* rbr_last_error(const rbr_ctx* ctx) { return ctx ? ctx->error.c_str() : "no context"; }
+
+rbr_status rbr_scene_upload(rbr_ctx* ctx, const rbr_scene_desc* desc) {
+    if (!ctx) return RBR_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(ctx->device);
+    cudaDeviceSynchronize();  // nothing may still read the scene being replaced
+    return upload_scene(ctx, desc);
+}
+
+rbr_status rbr_scene_stats_get(const rbr_ctx* ctx, rbr_scene_stats* out) {
+    if (!ctx || !out) return RBR_ERR_INVALID_ARGUMENT;
+    if (!ctx->has_scene) return RBR_ERR_NO_SCENE;
+    *out = ctx->stats;
+    return RBR_OK;
+}
+
+rbr_status rbr_world_bounds(const rbr_ctx* ctx, float out_min[3], float out_max[3]) {
+    if (!ctx || !out_min || !out_max) return RBR_ERR_INVALID_ARGUMENT;
+    if (!ctx->has_scene) return RBR_ERR_NO_SCENE;
+    for (int a = 0; a < 3; ++a) {
+        out_min[a] = ctx->bounds_lo[a];
+        out_max[a] = ctx->bounds_hi[a];
+    }
+    return RBR_OK;
+}
+
+rbr_status rbr_trace_closest(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, rbr_hit* hits, void* stream) {
+    if (!ctx) return RBR_ERR_INVALID_ARGUMENT;
+    if (!ctx->has_scene) return fail(ctx, RBR_ERR_NO_SCENE, "rbr_trace_closest before rbr_scene_upload");
+    if (n && (!rays || !hits)) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "rays or hits is NULL");
+    cudaSetDevice(ctx->device);
+    const cudaError_t e = launch_trace_closest(ctx->scene, rays, n, hits, ctx->d_error, ctx->num_sms,
+                                               static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? RBR_OK : cuda_fail(ctx, e, "closest-hit launch");
+}
+
+rbr_status rbr_trace_any(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, uint8_t* occluded, void* stream) {
+    if (!ctx) return RBR_ERR_INVALID_ARGUMENT;
+    if (!ctx->has_scene) return fail(ctx, RBR_ERR_NO_SCENE, "rbr_trace_any before rbr_scene_upload");
+    if (n && (!rays || !occluded)) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "rays or occluded is NULL");
+    cudaSetDevice(ctx->device);
+    const cudaError_t e = launch_trace_any(ctx->scene, rays, n, occluded, ctx->d_error, ctx->num_sms,
+                                           static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? RBR_OK : cuda_fail(ctx, e, "any-hit launch");
+}
+
+rbr_status rbr_trace_host(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any_hit, void* out) {
+    if (!ctx) return RBR_ERR_INVALID_ARGUMENT;
+    if (!ctx->has_scene) return fail(ctx, RBR_ERR_NO_SCENE, "rbr_trace_host before rbr_scene_upload");
+    if (n == 0) return RBR_OK;
+    if (!rays || !out) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "rays or out is NULL");
+    cudaSetDevice(ctx->device);
+    const size_t in_bytes = size_t(n) * sizeof(rbr_ray);
+    const size_t out_bytes = size_t(n) * (any_hit ? 1 : sizeof(rbr_hit));
+    rbr_status st;
+    if ((st = ensure(ctx, ctx->stage_in, in_bytes, "ray staging")) != RBR_OK) return st;
+    if ((st = ensure(ctx, ctx->stage_out, out_bytes, "hit staging")) != RBR_OK) return st;
+    cudaStream_t s = ctx->stream;
+    cudaError_t e = cudaMemcpyAsync(ctx->stage_in.ptr, rays, in_bytes, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "ray upload");
+    if (any_hit)
+        e = launch_trace_any(ctx->scene, static_cast<const rbr_ray*>(ctx->stage_in.ptr), n,
+                             static_cast<uint8_t*>(ctx->stage_out.ptr), ctx->d_error, ctx->num_sms, s);
+    else
+        e = launch_trace_closest(ctx->scene, static_cast<const rbr_ray*>(ctx->stage_in.ptr), n,
+                                 static_cast<rbr_hit*>(ctx->stage_out.ptr), ctx->d_error, ctx->num_sms, s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "trace launch");
+    e = cudaMemcpyAsync(out, ctx->stage_out.ptr, out_bytes, cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "hit download");
+    return check_device_error(ctx, s);
+}
+
+rbr_status rbr_trace_counts(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any_hit, uint64_t out[2]) {
+    if (!ctx || !out) return RBR_ERR_INVALID_ARGUMENT;
+    if (!ctx->has_scene) return fail(ctx, RBR_ERR_NO_SCENE, "rbr_trace_counts before rbr_scene_upload");
+    if (n && !rays) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "rays is NULL");
+    cudaSetDevice(ctx->device);
+    rbr_status st = ensure(ctx, ctx->stage_out, 2 * sizeof(unsigned long long), "count totals");
+    if (st != RBR_OK) return st;
+    auto* d = static_cast<unsigned long long*>(ctx->stage_out.ptr);
+    cudaError_t e = cudaMemsetAsync(d, 0, 2 * sizeof(unsigned long long), ctx->stream);
+    if (e == cudaSuccess) e = launch_trace_counts(ctx->scene, rays, n, any_hit, d, ctx->d_error, ctx->stream);
+    unsigned long long h[2] = {0, 0};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "counting traversal");
+    st = check_device_error(ctx, ctx->stream);
+    out[0] = h[0];
+    out[1] = h[1];
+    return st;
+}
+
+rbr_status rbr_render(rbr_ctx* ctx, const rbr_camera* camera, const rbr_render_params* params, float* film_mean,
+                      float* film_m2, void* stream) {
+    if (!ctx) return RBR_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(ctx->device);
+    return render(ctx, camera, params, film_mean, film_m2, static_cast<cudaStream_t>(stream));
+}
+
+rbr_status rbr_render_host(rbr_ctx* ctx, const rbr_camera* camera, const rbr_render_params* params, float* film_mean,
+                           float* film_m2) {
+    if (!ctx) return RBR_ERR_INVALID_ARGUMENT;
+    if (!camera || !film_mean) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "camera or film_mean is NULL");
+    if (camera->width <= 0 || camera->height <= 0) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "empty image");
+    cudaSetDevice(ctx->device);
+    const size_t bytes = size_t(camera->width) * camera->height * 3 * sizeof(float);
+    rbr_status st;
+    if ((st = ensure(ctx, ctx->stage_out, 2 * bytes, "film staging")) != RBR_OK) return st;
+    float* dmean = static_cast<float*>(ctx->stage_out.ptr);
+    float* dm2 = film_m2 ? dmean + size_t(camera->width) * camera->height * 3 : nullptr;
+    if ((st = render(ctx, camera, params, dmean, dm2, ctx->stream)) != RBR_OK) return st;
+    cudaError_t e = cudaMemcpyAsync(film_mean, dmean, bytes, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess && film_m2) e = cudaMemcpyAsync(film_m2, dm2, bytes, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "film download");
+    return check_device_error(ctx, ctx->stream);
+}
+
+rbr_status rbr_render_stats_get(rbr_ctx* ctx, rbr_render_stats* out) {
+    if (!ctx || !out) return RBR_ERR_INVALID_ARGUMENT;
+    if (ctx->render_pending) {
+        cudaSetDevice(ctx->device);
+        cudaError_t e = cudaEventSynchronize(ctx->ev_stop);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "waiting for the render");
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop);
+        ctx->last_render.milliseconds = ms;
+        ctx->render_pending = false;
+    }
+    *out = ctx->last_render;
+    return RBR_OK;
+}
+
+}  // extern "C"

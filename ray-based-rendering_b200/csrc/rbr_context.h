@@ -1,0 +1,83 @@
+// Internal definition of rbr_ctx and the host-side helpers shared by the library's files.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "rbr_b200.h"
+#include "rbr_scene_dev.h"
+#include "rbr_layout.h"
+
+namespace rbr {
+
+// A device allocation owned by the context.
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+};
+
+// Path-tracer working set (sized for one wave of paths).
+struct PathBuffers {
+    uint32_t capacity = 0;      // paths per wave
+    uint32_t shadow_capacity = 0;
+    DevBuf ray;                 // float4 x2 per path: (o, -), (d, -)
+    DevBuf thr;                 // float4 per path: throughput rgb, w = specular flag
+    DevBuf rad;                 // float4 per path: radiance rgb
+    DevBuf hit;                 // uint2 per path
+    DevBuf queue[2];            // active path indices (ping-pong)
+    DevBuf classq;              // material-class queues: kClasses x capacity
+    DevBuf shadow;              // 3 float4 per shadow ray
+    DevBuf counters;            // uint32 counters (see pt kernels)
+};
+
+}  // namespace rbr
+
+struct rbr_ctx {
+    int device = 0;
+    int num_sms = 0;
+    std::string error;
+    cudaStream_t stream = nullptr;  // internal stream for host-buffer calls
+    // scene
+    bool has_scene = false;
+    rbr::DeviceScene scene{};
+    std::vector<rbr::DevBuf> scene_bufs;
+    rbr_scene_stats stats{};
+    float bounds_lo[3] = {0, 0, 0}, bounds_hi[3] = {0, 0, 0};
+    // host-call staging
+    rbr::DevBuf stage_in, stage_out;
+    // device error word (rbr::kErr*)
+    int* d_error = nullptr;
+    // path tracer
+    rbr::PathBuffers pt;
+    rbr_render_stats last_render{};
+    cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+    bool render_pending = false;
+};
+
+namespace rbr {
+
+rbr_status fail(rbr_ctx* ctx, rbr_status code, const std::string& msg);
+rbr_status cuda_fail(rbr_ctx* ctx, cudaError_t e, const char* what);
+rbr_status ensure(rbr_ctx* ctx, DevBuf& b, size_t bytes, const char* what);
+void release(DevBuf& b);
+rbr_status check_device_error(rbr_ctx* ctx, cudaStream_t stream);
+
+rbr_status upload_scene(rbr_ctx* ctx, const rbr_scene_desc* desc);
+void free_scene(rbr_ctx* ctx);
+
+// kernels (trace.cu)
+cudaError_t launch_trace_closest(const DeviceScene& s, const rbr_ray* rays, uint32_t n, rbr_hit* hits, int* err,
+                                 int num_sms, cudaStream_t stream);
+cudaError_t launch_trace_any(const DeviceScene& s, const rbr_ray* rays, uint32_t n, uint8_t* occ, int* err,
+                             int num_sms, cudaStream_t stream);
+cudaError_t launch_trace_counts(const DeviceScene& s, const rbr_ray* rays, uint32_t n, int any_hit,
+                                unsigned long long* totals, int* err, cudaStream_t stream);
+
+// path tracer (pt.cu)
+rbr_status render(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_params* p, float* film_mean, float* film_m2,
+                  cudaStream_t stream);
+void free_path_buffers(rbr_ctx* ctx);
+
+}  // namespace rbr

@@ -1,0 +1,299 @@
+// Device-side scene view, exact float helpers and the 8-wide BVH traversal.
+//
+// Primitive tests restate the reference operation for operation with explicitly rounded
+// intrinsics (__fmul_rn/__fadd_rn/__fsub_rn/__fdiv_rn/__fsqrt_rn never fuse into an FMA), so
+// a GPU hit distance equals the reference's bit for bit:
+//   Triangle::intersect  src/geometry/triangle.cpp:6-24   (Moller-Trumbore, |a| < EPSILON cull)
+//   Sphere::intersect    src/geometry/sphere.cpp:6-19
+//   Quad::intersect      src/geometry/quad.cpp:12-28
+//   Plane::intersect     src/geometry/plane.cpp:12-20
+// Closest hit keeps the smallest t and, at equal t, the highest primitive id: exactly what a
+// loop over Scene::primitives() in order returns (a later primitive at t == tMax replaces an
+// earlier one because only t > tMax is rejected).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "rbr_layout.h"
+#include "rbr_scene_dev.h"
+
+namespace rbr {
+
+// ----------------------------------------------------------------------------------------
+// Exactly rounded float3 arithmetic (the reference's Vec3, include/render/core/vector.h)
+// ----------------------------------------------------------------------------------------
+struct f3 {
+    float x, y, z;
+};
+
+__device__ __forceinline__ f3 mk(float x, float y, float z) { return f3{x, y, z}; }
+__device__ __forceinline__ f3 xsub(f3 a, f3 b) { return mk(__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y), __fsub_rn(a.z, b.z)); }
+__device__ __forceinline__ f3 xadd(f3 a, f3 b) { return mk(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y), __fadd_rn(a.z, b.z)); }
+__device__ __forceinline__ f3 xmuls(f3 a, float s) { return mk(__fmul_rn(a.x, s), __fmul_rn(a.y, s), __fmul_rn(a.z, s)); }
+__device__ __forceinline__ f3 xmul(f3 a, f3 b) { return mk(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y), __fmul_rn(a.z, b.z)); }
+__device__ __forceinline__ f3 xneg(f3 a) { return mk(-a.x, -a.y, -a.z); }
+__device__ __forceinline__ float xdot(f3 a, f3 b) {
+    return __fadd_rn(__fadd_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)), __fmul_rn(a.z, b.z));
+}
+__device__ __forceinline__ f3 xcross(f3 a, f3 b) {
+    return mk(__fsub_rn(__fmul_rn(a.y, b.z), __fmul_rn(a.z, b.y)), __fsub_rn(__fmul_rn(a.z, b.x), __fmul_rn(a.x, b.z)),
+              __fsub_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x)));
+}
+// Vec3::operator/(float): multiply by the rounded reciprocal
+__device__ __forceinline__ f3 xdivs(f3 a, float s) { return xmuls(a, __fdiv_rn(1.0f, s)); }
+__device__ __forceinline__ float xlen(f3 a) { return __fsqrt_rn(xdot(a, a)); }
+__device__ __forceinline__ f3 xnorm(f3 a) {
+    const float l = xlen(a);
+    return l > 0.0f ? xdivs(a, l) : mk(0.0f, 0.0f, 0.0f);
+}
+__device__ __forceinline__ f3 ld3(const float* p) { return mk(p[0], p[1], p[2]); }
+
+// ----------------------------------------------------------------------------------------
+// Primitive tests. `tbest`/`best` hold the current closest hit (best = -1: none yet).
+// Each returns the candidate t (or a negative value for no hit); acceptance with the tie rule
+// happens in accept().
+// ----------------------------------------------------------------------------------------
+__device__ __forceinline__ bool accept(float t, uint32_t id, float tbest, int best) {
+    return t < tbest || (t == tbest && static_cast<int>(id) > best);
+}
+
+// Triangle::intersect (triangle.cpp:6-24). v0, e1 = v1 - v0, e2 = v2 - v0.
+__device__ __forceinline__ float hit_triangle(f3 o, f3 d, f3 v0, f3 e1, f3 e2, float tmax, float* pu = nullptr,
+                                              float* pv = nullptr) {
+    const f3 h = xcross(d, e2);
+    const float a = xdot(e1, h);
+    if (fabsf(a) < kEpsilon) return -1.0f;
+    const float f = __fdiv_rn(1.0f, a);
+    const f3 s = xsub(o, v0);
+    const float u = __fmul_rn(f, xdot(s, h));
+    if (u < 0.0f || u > 1.0f) return -1.0f;
+    const f3 q = xcross(s, e1);
+    const float v = __fmul_rn(f, xdot(d, q));
+    if (v < 0.0f || __fadd_rn(u, v) > 1.0f) return -1.0f;
+    const float t = __fmul_rn(f, xdot(e2, q));
+    if (t < kEpsilon || t > tmax) return -1.0f;
+    if (pu) {
+        *pu = u;
+        *pv = v;
+    }
+    return t;
+}
+
+// Sphere::intersect (sphere.cpp:6-19): near root, else far root, both within [EPSILON, tmax].
+__device__ __forceinline__ float hit_sphere(f3 o, f3 d, f3 c, float r2, float tmax) {
+    const f3 oc = xsub(o, c);
+    const float a = xdot(d, d);
+    const float halfB = xdot(oc, d);
+    const float cc = __fsub_rn(xdot(oc, oc), r2);
+    const float disc = __fsub_rn(__fmul_rn(halfB, halfB), __fmul_rn(a, cc));
+    if (disc < 0.0f) return -1.0f;
+    const float sq = __fsqrt_rn(disc);
+    float t = __fdiv_rn(__fsub_rn(-halfB, sq), a);
+    if (t < kEpsilon || t > tmax) {
+        t = __fdiv_rn(__fadd_rn(-halfB, sq), a);
+        if (t < kEpsilon || t > tmax) return -1.0f;
+    }
+    return t;
+}
+
+// Quad::intersect (quad.cpp:12-28); the normal is recomputed as the constructor computes it.
+__device__ __forceinline__ float hit_quad(f3 o, f3 d, f3 org, f3 u, f3 v, float ulen2, float vlen2, float tmax) {
+    const f3 n = xnorm(xcross(u, v));
+    const float denom = xdot(n, d);
+    if (fabsf(denom) < kEpsilon) return -1.0f;
+    const float t = __fdiv_rn(xdot(xsub(org, o), n), denom);
+    if (t < kEpsilon || t > tmax) return -1.0f;
+    const f3 hp = xadd(o, xmuls(d, t));
+    const f3 lp = xsub(hp, org);
+    const float uc = __fdiv_rn(xdot(lp, u), ulen2);
+    const float vc = __fdiv_rn(xdot(lp, v), vlen2);
+    if (uc < 0.0f || uc > 1.0f || vc < 0.0f || vc > 1.0f) return -1.0f;
+    return t;
+}
+
+// Plane::intersect (plane.cpp:12-20).
+__device__ __forceinline__ float hit_plane(f3 o, f3 d, f3 n, float pd, float tmax) {
+    const float denom = xdot(n, d);
+    if (fabsf(denom) < kEpsilon) return -1.0f;
+    const float t = __fdiv_rn(-__fadd_rn(xdot(n, o), pd), denom);
+    if (t < kEpsilon || t > tmax) return -1.0f;
+    return t;
+}
+
+// Tests leaf record `rec`; returns t or negative. `tag` receives the record's tag word.
+__device__ __forceinline__ float hit_record(const float4* __restrict__ records, uint32_t rec, f3 o, f3 d, float tmax,
+                                            uint32_t& tag) {
+    const float4 a = __ldg(records + 3 * rec);
+    const float4 b = __ldg(records + 3 * rec + 1);
+    const float4 c = __ldg(records + 3 * rec + 2);
+    tag = __float_as_uint(c.y);
+    const uint32_t type = tag >> kTypeShift;
+    if (type == kPrimTriangle) {
+        return hit_triangle(o, d, mk(a.x, a.y, a.z), mk(a.w, b.x, b.y), mk(b.z, b.w, c.x), tmax);
+    } else if (type == kPrimSphere) {
+        return hit_sphere(o, d, mk(a.x, a.y, a.z), b.x, tmax);
+    } else {
+        return hit_quad(o, d, mk(a.x, a.y, a.z), mk(a.w, b.x, b.y), mk(b.z, b.w, c.x), c.z, c.w, tmax);
+    }
+}
+
+// ----------------------------------------------------------------------------------------
+// 8-wide node test
+// ----------------------------------------------------------------------------------------
+struct RayCtx {
+    f3 o, d;
+    float ix, iy, iz;   // 1 / d
+    uint32_t oct;       // bit k set: d_k negative (visiting order)
+    bool nx, ny, nz;    // sign of 1/d per axis (near/far plane choice)
+};
+
+__device__ __forceinline__ RayCtx make_ctx(f3 o, f3 d) {
+    RayCtx r;
+    r.o = o;
+    r.d = d;
+    r.ix = __fdiv_rn(1.0f, d.x);
+    r.iy = __fdiv_rn(1.0f, d.y);
+    r.iz = __fdiv_rn(1.0f, d.z);
+    r.nx = signbit(r.ix);
+    r.ny = signbit(r.iy);
+    r.nz = signbit(r.iz);
+    r.oct = (r.nx ? 1u : 0u) | (r.ny ? 2u : 0u) | (r.nz ? 4u : 0u);
+    return r;
+}
+
+// byte i of a 64-bit pair, as an exact float
+__device__ __forceinline__ float qbyte(uint2 w, int i) {
+    const uint32_t word = (i < 4) ? w.x : w.y;
+    return __uint_as_float(__byte_perm(word, 0x4B000000u, 0x7650 | (i & 3))) - 8388608.0f;
+}
+
+// Relative widening of box intervals in t (2^-16): covers the rounding of the slab
+// arithmetic and of the primitive tests near a box face.
+constexpr float kTLo = 1.0f - 1.0f / 65536.0f;
+constexpr float kTHi = 1.0f + 1.0f / 65536.0f;
+
+// Tests the 8 children of node `idx`. ngroup = (child_base, hit bits << 24 | imask << 16),
+// pgroup = (prim_base, 24-bit mask of leaf records to test).
+__device__ __forceinline__ void intersect_node(const uint4* __restrict__ nodes, uint32_t idx, const RayCtx& r,
+                                               float tbest, uint2& ngroup, uint2& pgroup) {
+    const uint4* np = nodes + 5 * static_cast<size_t>(idx);
+    const uint4 w0 = __ldg(np);
+    const uint4 w1 = __ldg(np + 1);
+    const uint4 w2 = __ldg(np + 2);
+    const uint4 w3 = __ldg(np + 3);
+    const uint4 w4 = __ldg(np + 4);
+    const float sx = __uint_as_float((w0.w & 0xFFu) << 23);
+    const float sy = __uint_as_float(((w0.w >> 8) & 0xFFu) << 23);
+    const float sz = __uint_as_float(((w0.w >> 16) & 0xFFu) << 23);
+    const uint32_t imask = w0.w >> 24;
+    const float ax = sx * r.ix, ay = sy * r.iy, az = sz * r.iz;
+    const float bx = (__uint_as_float(w0.x) - r.o.x) * r.ix;
+    const float by = (__uint_as_float(w0.y) - r.o.y) * r.iy;
+    const float bz = (__uint_as_float(w0.z) - r.o.z) * r.iz;
+    const uint2 qlox = make_uint2(w2.x, w2.y), qloy = make_uint2(w2.z, w2.w), qloz = make_uint2(w3.x, w3.y);
+    const uint2 qhix = make_uint2(w3.z, w3.w), qhiy = make_uint2(w4.x, w4.y), qhiz = make_uint2(w4.z, w4.w);
+    const uint2 nearx = r.nx ? qhix : qlox, farx = r.nx ? qlox : qhix;
+    const uint2 neary = r.ny ? qhiy : qloy, fary = r.ny ? qloy : qhiy;
+    const uint2 nearz = r.nz ? qhiz : qloz, farz = r.nz ? qloz : qhiz;
+    uint32_t cbits = 0, pbits = 0;
+    const uint32_t meta_lo = w1.z, meta_hi = w1.w;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const float tnx = fmaf(qbyte(nearx, i), ax, bx);
+        const float tny = fmaf(qbyte(neary, i), ay, by);
+        const float tnz = fmaf(qbyte(nearz, i), az, bz);
+        const float tfx = fmaf(qbyte(farx, i), ax, bx);
+        const float tfy = fmaf(qbyte(fary, i), ay, by);
+        const float tfz = fmaf(qbyte(farz, i), az, bz);
+        const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f)) * kTLo;
+        const float tf = fminf(fminf(tfx, tfy), tfz) * kTHi;
+        if (tn <= tf && tn <= tbest) {
+            if ((imask >> i) & 1u) {
+                cbits |= 1u << (24 + (static_cast<uint32_t>(i) ^ r.oct));
+            } else {
+                const uint32_t meta = ((i < 4 ? meta_lo : meta_hi) >> (8 * (i & 3))) & 0xFFu;
+                const uint32_t cnt = meta >> 5;
+                pbits |= ((1u << cnt) - 1u) << (meta & 31u);
+            }
+        }
+    }
+    ngroup = make_uint2(w1.x, cbits | (imask << 16));
+    pgroup = make_uint2(w1.y, pbits);
+}
+
+// ----------------------------------------------------------------------------------------
+// Traversal. Closest hit: returns the primitive id (or RBR_MISS) and its t.
+// Any hit: returns 1 as soon as a primitive lies in [EPSILON, tmax].
+// ----------------------------------------------------------------------------------------
+// With kCount, `counts` receives the number of wide nodes fetched (x) and leaf records
+// tested (y) by this ray: the traversal is deterministic per ray, so these are the ray's
+// algorithmic node and record traffic.
+template <bool kAny, bool kCount = false>
+__device__ __forceinline__ uint32_t traverse(const DeviceScene& s, f3 o, f3 d, float tmax, float& thit, int* err,
+                                             uint2* counts = nullptr) {
+    float tbest = tmax;
+    int best = -1;
+    for (uint32_t i = 0; i < s.num_planes; ++i) {
+        const float4 pl = __ldg(s.planes + i);
+        const float t = hit_plane(o, d, mk(pl.x, pl.y, pl.z), pl.w, tbest);
+        if (t >= 0.0f) {
+            const uint32_t id = __ldg(s.plane_tags + i) & kIdMask;
+            if (kAny) return 1u;
+            if (accept(t, id, tbest, best)) {
+                tbest = t;
+                best = static_cast<int>(id);
+            }
+        }
+    }
+    if (s.num_nodes != 0) {
+        const RayCtx r = make_ctx(o, d);
+        uint2 stack[kStackSize];
+        int sp = 0;
+        uint2 ng, pg;
+        intersect_node(s.nodes, 0, r, tbest, ng, pg);
+        if (kCount) counts->x += 1;
+        while (true) {
+            while (pg.y != 0) {
+                const int i = __ffs(pg.y) - 1;
+                pg.y &= pg.y - 1;
+                if (kCount) counts->y += 1;
+                uint32_t tag;
+                const float t = hit_record(s.records, pg.x + i, o, d, tbest, tag);
+                if (t >= 0.0f) {
+                    if (kAny) return 1u;
+                    const uint32_t id = tag & kIdMask;
+                    if (accept(t, id, tbest, best)) {
+                        tbest = t;
+                        best = static_cast<int>(id);
+                    }
+                }
+            }
+            if (ng.y & 0xFF000000u) {
+                const int b = 31 - __clz(ng.y);
+                ng.y &= ~(1u << b);
+                const uint32_t slot = static_cast<uint32_t>(b - 24) ^ r.oct;
+                const uint32_t imask = (ng.y >> 16) & 0xFFu;
+                const uint32_t child = ng.x + __popc(imask & ((1u << slot) - 1u));
+                if (ng.y & 0xFF000000u) {
+                    if (sp < kStackSize) {
+                        stack[sp++] = ng;
+                    } else {
+                        atomicOr(err, kErrStackOverflow);
+                        break;
+                    }
+                }
+                intersect_node(s.nodes, child, r, tbest, ng, pg);
+                if (kCount) counts->x += 1;
+                continue;
+            }
+            if (sp == 0) break;
+            ng = stack[--sp];
+        }
+    }
+    if (kAny) return 0u;
+    thit = tbest;
+    return best < 0 ? 0xFFFFFFFFu : static_cast<uint32_t>(best);
+}
+
+}  // namespace rbr

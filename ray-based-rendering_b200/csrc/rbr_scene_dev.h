@@ -1,0 +1,42 @@
+// Plain structs describing a scene in device memory (usable from host C++ and from kernels).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace rbr {
+
+struct MaterialDev {
+    float base[3];
+    float metallic, roughness, ior, transmission;
+    float emission[3];
+};
+
+struct LightDev {
+    uint32_t type;
+    float position[3], u[3], v[3], color[3];
+    float intensity;
+    float normal[3];  // normalize(u x v), AreaLight::AreaLight
+    float area;       // |u x v|
+};
+
+// Everything a kernel needs to read a scene. Passed by value.
+struct DeviceScene {
+    const uint4* nodes;      // kNodeWords/4 uint4 per node
+    const float4* records;   // 3 float4 per leaf record
+    const float4* planes;    // per plane: (unit normal, d)
+    const uint32_t* plane_tags;
+    uint32_t num_nodes;
+    uint32_t num_planes;
+    // shading data, indexed by primitive id
+    const uint32_t* prim_record;   // leaf record index, or (plane index | 0x80000000)
+    const uint32_t* prim_material;
+    const float4* tri_normals;     // 3 float4 per leaf record of a triangle with normals, or null
+    const MaterialDev* materials;
+    const LightDev* lights;
+    uint32_t num_materials;
+    uint32_t num_lights;
+    float background[3];
+};
+
+}  // namespace rbr

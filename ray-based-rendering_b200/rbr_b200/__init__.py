@@ -1,0 +1,188 @@
+"""Python binding of librbr_b200.so, the B200 path-tracing hot path (C ABI: include/rbr_b200.h).
+
+The library is the GPU side of the reference framework's Accelerator / Integrator drop-ins;
+this module is a thin ctypes layer used by the tests and the benchmark. There is no CPU
+fallback: without the built library or without a CUDA device every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import re
+from pathlib import Path
+
+import numpy as np
+
+from . import abi
+from .abi import RAY_DTYPE, HIT_DTYPE
+
+LIB_PATH = Path(__file__).resolve().parent / "librbr_b200.so"
+HEADER = Path(__file__).resolve().parents[2] / "include" / "rbr_b200.h"
+
+_lib = None
+
+
+class RbrError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{abi.STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+def header_functions() -> list[str]:
+    """Names of the functions include/rbr_b200.h declares."""
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(rbr_[a-z_0-9]+)\s*\(", text)))
+
+
+def load_library() -> C.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with __graft_entry__.build() "
+                           "(python -m rbr_b200.build); there is no CPU fallback")
+    lib = C.CDLL(str(LIB_PATH))
+    P = C.c_void_p
+    sig = {
+        "rbr_abi_version": (C.c_uint32, []),
+        "rbr_struct_size": (C.c_size_t, [C.c_char_p]),
+        "rbr_ctx_create": (C.c_int, [C.c_int, C.POINTER(P)]),
+        "rbr_ctx_destroy": (None, [P]),
+        "rbr_last_error": (C.c_char_p, [P]),
+        "rbr_scene_upload": (C.c_int, [P, C.POINTER(abi.rbr_scene_desc)]),
+        "rbr_scene_stats_get": (C.c_int, [P, C.POINTER(abi.rbr_scene_stats)]),
+        "rbr_world_bounds": (C.c_int, [P, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+        "rbr_trace_closest": (C.c_int, [P, P, C.c_uint32, P, P]),
+        "rbr_trace_any": (C.c_int, [P, P, C.c_uint32, P, P]),
+        "rbr_trace_host": (C.c_int, [P, P, C.c_uint32, C.c_int, P]),
+        "rbr_trace_counts": (C.c_int, [P, P, C.c_uint32, C.c_int, C.POINTER(C.c_uint64)]),
+        "rbr_render": (C.c_int, [P, C.POINTER(abi.rbr_camera), C.POINTER(abi.rbr_render_params), P, P, P]),
+        "rbr_render_host": (C.c_int, [P, C.POINTER(abi.rbr_camera), C.POINTER(abi.rbr_render_params), P, P]),
+        "rbr_render_stats_get": (C.c_int, [P, C.POINTER(abi.rbr_render_stats)]),
+    }
+    for name, (res, args) in sig.items():
+        if hasattr(lib, name):
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def render_params(spp=16, max_depth=8, use_nee=True, use_mis=True, seed=0, sample_offset=0, flags=0):
+    p = abi.rbr_render_params()
+    p.samples_per_pixel = spp
+    p.max_depth = max_depth
+    p.use_nee = int(use_nee)
+    p.use_mis = int(use_mis)
+    p.seed = seed
+    p.sample_offset = sample_offset
+    p.flags = flags
+    return p
+
+
+class Context:
+    """One rbr_ctx: a device, a resident scene, and the path tracer's working memory."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load_library()
+        h = C.c_void_p()
+        st = self.lib.rbr_ctx_create(device, C.byref(h))
+        if st != abi.RBR_OK:
+            raise RbrError(st, f"rbr_ctx_create({device}) failed (no usable CUDA device?)")
+        self.h = h
+        self._scene_keep = None
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.rbr_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, st):
+        if st != abi.RBR_OK:
+            raise RbrError(st, self.lib.rbr_last_error(self.h).decode())
+
+    # scene ---------------------------------------------------------------------------------
+    def upload(self, scene) -> abi.rbr_scene_stats:
+        desc = scene.desc() if hasattr(scene, "desc") and callable(scene.desc) else scene
+        self._check(self.lib.rbr_scene_upload(self.h, C.byref(desc.desc)))
+        self._scene_keep = desc
+        return self.stats()
+
+    def upload_raw(self, desc: abi.rbr_scene_desc) -> int:
+        return self.lib.rbr_scene_upload(self.h, C.byref(desc))
+
+    def last_error(self) -> str:
+        return self.lib.rbr_last_error(self.h).decode()
+
+    def stats(self) -> abi.rbr_scene_stats:
+        s = abi.rbr_scene_stats()
+        self._check(self.lib.rbr_scene_stats_get(self.h, C.byref(s)))
+        return s
+
+    def world_bounds(self):
+        lo = (C.c_float * 3)()
+        hi = (C.c_float * 3)()
+        self._check(self.lib.rbr_world_bounds(self.h, lo, hi))
+        return np.array(lo[:], np.float32), np.array(hi[:], np.float32)
+
+    # ray queries ---------------------------------------------------------------------------
+    def trace_closest_dev(self, rays_ptr: int, n: int, hits_ptr: int, stream: int = 0):
+        self._check(self.lib.rbr_trace_closest(self.h, C.c_void_p(rays_ptr), n, C.c_void_p(hits_ptr),
+                                               C.c_void_p(stream)))
+
+    def trace_any_dev(self, rays_ptr: int, n: int, occ_ptr: int, stream: int = 0):
+        self._check(self.lib.rbr_trace_any(self.h, C.c_void_p(rays_ptr), n, C.c_void_p(occ_ptr),
+                                           C.c_void_p(stream)))
+
+    def trace_host(self, rays: np.ndarray, any_hit: bool = False, out: np.ndarray | None = None) -> np.ndarray:
+        rays = np.ascontiguousarray(rays, dtype=RAY_DTYPE)
+        n = len(rays)
+        if out is None:
+            out = np.zeros(n, dtype=np.uint8 if any_hit else HIT_DTYPE)
+        self._check(self.lib.rbr_trace_host(self.h, C.c_void_p(rays.ctypes.data), n, int(any_hit),
+                                            C.c_void_p(out.ctypes.data)))
+        return out
+
+    def trace_counts_dev(self, rays_ptr: int, n: int, any_hit: bool = False):
+        """(wide nodes fetched, leaf records tested) summed over the n rays."""
+        out = (C.c_uint64 * 2)()
+        self._check(self.lib.rbr_trace_counts(self.h, C.c_void_p(rays_ptr), n, int(any_hit), out))
+        return int(out[0]), int(out[1])
+
+    # rendering -----------------------------------------------------------------------------
+    def render_dev(self, camera, params, film_mean_ptr: int, film_m2_ptr: int = 0, stream: int = 0):
+        self._check(self.lib.rbr_render(self.h, C.byref(camera), C.byref(params), C.c_void_p(film_mean_ptr),
+                                        C.c_void_p(film_m2_ptr or None), C.c_void_p(stream)))
+
+    def render_host(self, camera, params, second_moment: bool = False):
+        W, H = camera.width, camera.height
+        mean = np.zeros((H, W, 3), np.float32)
+        m2 = np.zeros((H, W, 3), np.float32) if second_moment else None
+        if second_moment:
+            params.flags |= abi.RBR_RENDER_SECOND_MOMENT
+        self._check(self.lib.rbr_render_host(self.h, C.byref(camera), C.byref(params),
+                                             C.c_void_p(mean.ctypes.data),
+                                             C.c_void_p(m2.ctypes.data) if m2 is not None else None))
+        return (mean, m2) if second_moment else mean
+
+    def render_stats(self) -> abi.rbr_render_stats:
+        s = abi.rbr_render_stats()
+        self._check(self.lib.rbr_render_stats_get(self.h, C.byref(s)))
+        return s
+
+
+__all__ = ["Context", "RbrError", "load_library", "header_functions", "render_params", "abi", "RAY_DTYPE",
+           "HIT_DTYPE"]

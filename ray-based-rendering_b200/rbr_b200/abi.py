@@ -1,0 +1,174 @@
+"""ctypes mirror of include/rbr_b200.h (the C ABI of librbr_b200.so).
+
+Structures here must match the header field for field; tests/test_abi.py checks the sizes
+and offsets against the compiled library (rbr_abi_layout).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+RBR_OK = 0
+RBR_ERR_INVALID_ARGUMENT = 1
+RBR_ERR_CUDA = 2
+RBR_ERR_OUT_OF_MEMORY = 3
+RBR_ERR_NO_SCENE = 4
+RBR_ERR_UNSUPPORTED = 5
+RBR_ERR_DEVICE_TIMEOUT = 6
+RBR_ERR_INTERNAL = 7
+
+STATUS_NAMES = {
+    0: "RBR_OK",
+    1: "RBR_ERR_INVALID_ARGUMENT",
+    2: "RBR_ERR_CUDA",
+    3: "RBR_ERR_OUT_OF_MEMORY",
+    4: "RBR_ERR_NO_SCENE",
+    5: "RBR_ERR_UNSUPPORTED",
+    6: "RBR_ERR_DEVICE_TIMEOUT",
+    7: "RBR_ERR_INTERNAL",
+}
+
+RBR_MISS = 0xFFFFFFFF
+RBR_LIGHT_AREA = 0
+RBR_LIGHT_POINT = 1
+RBR_CAMERA_PINHOLE = 0
+RBR_CAMERA_THIN_LENS = 1
+RBR_RENDER_CORRECTED_MIS = 1 << 0
+RBR_RENDER_SECOND_MOMENT = 1 << 1
+
+_f3 = C.c_float * 3
+_u32p = C.POINTER(C.c_uint32)
+_f32p = C.POINTER(C.c_float)
+
+
+class rbr_material(C.Structure):
+    _fields_ = [
+        ("base_color", _f3),
+        ("metallic", C.c_float),
+        ("roughness", C.c_float),
+        ("ior", C.c_float),
+        ("transmission", C.c_float),
+        ("emission", _f3),
+    ]
+
+
+class rbr_light(C.Structure):
+    _fields_ = [
+        ("type", C.c_uint32),
+        ("position", _f3),
+        ("u", _f3),
+        ("v", _f3),
+        ("color", _f3),
+        ("intensity", C.c_float),
+    ]
+
+
+class rbr_scene_desc(C.Structure):
+    _fields_ = [
+        ("num_triangles", C.c_uint32),
+        ("triangle_vertices", _f32p),
+        ("triangle_normals", _f32p),
+        ("triangle_materials", _u32p),
+        ("triangle_ids", _u32p),
+        ("num_spheres", C.c_uint32),
+        ("spheres", _f32p),
+        ("sphere_materials", _u32p),
+        ("sphere_ids", _u32p),
+        ("num_quads", C.c_uint32),
+        ("quads", _f32p),
+        ("quad_materials", _u32p),
+        ("quad_ids", _u32p),
+        ("num_planes", C.c_uint32),
+        ("planes", _f32p),
+        ("plane_materials", _u32p),
+        ("plane_ids", _u32p),
+        ("num_materials", C.c_uint32),
+        ("materials", C.POINTER(rbr_material)),
+        ("num_lights", C.c_uint32),
+        ("lights", C.POINTER(rbr_light)),
+        ("background", _f3),
+    ]
+
+
+class rbr_scene_stats(C.Structure):
+    _fields_ = [
+        ("num_primitives", C.c_uint32),
+        ("num_bounded", C.c_uint32),
+        ("num_unbounded", C.c_uint32),
+        ("num_wide_nodes", C.c_uint32),
+        ("num_leaf_records", C.c_uint32),
+        ("max_depth", C.c_uint32),
+        ("device_bytes", C.c_uint64),
+        ("build_seconds", C.c_double),
+    ]
+
+
+class rbr_camera(C.Structure):
+    _fields_ = [
+        ("width", C.c_int32),
+        ("height", C.c_int32),
+        ("model", C.c_uint32),
+        ("position", _f3),
+        ("forward", _f3),
+        ("right", _f3),
+        ("up", _f3),
+        ("fx", C.c_float),
+        ("fy", C.c_float),
+        ("cx", C.c_float),
+        ("cy", C.c_float),
+        ("lens_radius", C.c_float),
+        ("focal_distance", C.c_float),
+    ]
+
+
+class rbr_render_params(C.Structure):
+    _fields_ = [
+        ("samples_per_pixel", C.c_int32),
+        ("max_depth", C.c_int32),
+        ("use_nee", C.c_int32),
+        ("use_mis", C.c_int32),
+        ("seed", C.c_uint64),
+        ("sample_offset", C.c_uint32),
+        ("flags", C.c_uint32),
+    ]
+
+
+class rbr_render_stats(C.Structure):
+    _fields_ = [
+        ("paths", C.c_uint64),
+        ("extension_rays", C.c_uint64),
+        ("shadow_rays", C.c_uint64),
+        ("waves", C.c_uint32),
+        ("launches", C.c_uint32),
+        ("milliseconds", C.c_float),
+    ]
+
+
+# numpy views of the ray / hit records
+RAY_DTYPE = np.dtype(
+    [("origin", np.float32, 3), ("tmax", np.float32), ("direction", np.float32, 3), ("pad", np.float32)]
+)
+HIT_DTYPE = np.dtype([("prim", np.uint32), ("t", np.float32)])
+assert RAY_DTYPE.itemsize == 32 and HIT_DTYPE.itemsize == 8
+
+
+def f3(v) -> "C.Array":
+    return _f3(*[float(x) for x in v])
+
+
+def make_rays(origins: np.ndarray, directions: np.ndarray, tmax=np.inf) -> np.ndarray:
+    """Packs origins/directions (n,3 float32) and tmax (scalar or n) into rbr_ray records."""
+    n = origins.shape[0]
+    rays = np.zeros(n, dtype=RAY_DTYPE)
+    rays["origin"] = origins.astype(np.float32)
+    rays["direction"] = directions.astype(np.float32)
+    rays["tmax"] = np.broadcast_to(np.asarray(tmax, dtype=np.float32), (n,))
+    return rays
+
+
+def ptr(a: np.ndarray | None, ctype):
+    if a is None:
+        return C.cast(None, C.POINTER(ctype))
+    assert a.flags["C_CONTIGUOUS"], "arrays passed to the C ABI must be C-contiguous"
+    return a.ctypes.data_as(C.POINTER(ctype))
