@@ -43,11 +43,12 @@ ICO_LEVEL = 8
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--steps", type=int, default=200)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["rays"], default="rays")
+    p.add_argument("--workload", choices=["rays", "cornell", "ggx"], default="rays")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true", help="skip the host-buffer measurement (profiling runs)")
     p.add_argument("--cpu-seconds", type=float, default=8.0, help="target length of the CPU-baseline sample")
     return p.parse_args()
 
@@ -78,7 +79,10 @@ class Clocks:
             os.close(fd)
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                                          "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+                                          "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+            t0 = time.time()  # wait until sampling is live so that it covers the timed region
+            while time.time() - t0 < 10 and Path(self.path).stat().st_size == 0:
+                time.sleep(0.05)
         except Exception:
             self.proc = None
 
@@ -202,6 +206,108 @@ def config_block():
 
 
 # ------------------------------------------------------------------------------------------
+# path-tracer workloads: a step = one rbr_render of the whole image
+RENDER_CONFIGS = {
+    "cornell": dict(spp=16, max_depth=8, desc="Cornell box (18 quads, quad light 0.5x0.5 emission (17,12,4), two "
+                                               "boxes rotated +-17 deg), pinhole fov 40, 256x256, 16 spp, max depth 8, "
+                                               "NEE+MIS, RR after depth 3, FP32 RGB film, seed 0"),
+    "ggx": dict(spp=64, max_depth=16, desc="GGX material scene: 256 spheres + 2M-triangle mound on a ground quad, "
+                                           "random per-object materials (20% glass), 2 quad area lights + 1 point "
+                                           "light, thin-lens camera, 1920x1080, 64 spp, max depth 16"),
+}
+
+
+def render_scene(which):
+    from rbr_b200 import scenes
+
+    return scenes.cornell_box() if which == "cornell" else scenes.ggx_scene()
+
+
+def run_render(args, rank, world, local_rank):
+    import torch
+
+    from rbr_b200 import Context, render_params
+
+    which = args.workload
+    cfg = RENDER_CONFIGS[which]
+    torch.cuda.set_device(local_rank)
+    scene = render_scene(which)
+    cam = scene.camera
+    W, H = cam.width, cam.height
+    ctx = Context(local_rank)
+    ctx.upload(scene)
+    film = torch.empty(W * H * 3, dtype=torch.float32, device=f"cuda:{local_rank}")
+    stream = torch.cuda.current_stream()
+    paths = W * H * cfg["spp"]
+
+    def step(k):
+        p = render_params(spp=cfg["spp"], max_depth=cfg["max_depth"], seed=rank * 1000003 + k)
+        ctx.render_dev(cam, p, film.data_ptr(), 0, stream.cuda_stream)
+
+    for k in range(max(3, args.warmup)):
+        step(k)
+    torch.cuda.synchronize()
+    clocks = Clocks() if rank == 0 else None
+    if clocks:
+        clocks.start()
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    evs[0].record(stream)
+    for k in range(args.steps):
+        step(1000 + k)
+    evs[1].record(stream)
+    torch.cuda.synchronize()
+    total_ms = evs[0].elapsed_time(evs[1])
+    st = ctx.render_stats()
+    clk = clocks.stop(visible_gpu_indices(local_rank)) if clocks else None
+    e2e = None
+    if not args.no_e2e:
+        t0 = time.perf_counter()
+        e2e_steps = max(3, min(args.steps, 5))
+        for k in range(e2e_steps):
+            ctx.render_host(cam, render_params(spp=cfg["spp"], max_depth=cfg["max_depth"], seed=k))
+        e2e_s = time.perf_counter() - t0
+        e2e = {"value": paths * e2e_steps / e2e_s / 1e6, "unit": "Mpaths/s", "h2d_bytes_per_step": 0,
+               "d2h_bytes_per_step": W * H * 12, "path": "rbr_render_host: render + film -> host"}
+    base = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sys.path.insert(0, str(REPO / "oracle"))
+        from oracle import Reference, have_reference
+
+        if have_reference():
+            ref = Reference()
+            h = ref.scene(scene)
+            # bounded sample: the same camera, the central band of about 1/8 of the rows
+            import ctypes
+
+            small = type(cam)()
+            ctypes.memmove(ctypes.byref(small), ctypes.byref(cam), ctypes.sizeof(cam))
+            small.height = max(8, H // 8)
+            small.cy = small.cy - (H - small.height) / 2.0
+            t0 = time.perf_counter()
+            ref.render(h, small, render_params(spp=cfg["spp"], max_depth=cfg["max_depth"]), threads=0)
+            dt = time.perf_counter() - t0
+            base = {"value": W * small.height * cfg["spp"] / dt / 1e6, "unit": "Mpaths/s",
+                    "cores": ref.max_threads(), "kind": "reference",
+                    "sample": f"central {W}x{small.height} band of the image, the reference's own "
+                              f"Integrator::render (OpenMP rows), {dt:.1f} s"}
+    if rank == 0:
+        print(json.dumps({
+            "metric": "Mpaths/s (camera samples per second), plain GPU path tracer", "value":
+                paths * world * args.steps / (total_ms / 1e3) / 1e6, "unit": "Mpaths/s", "n_gpus": world,
+            "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded)",
+            "config": {"workload": cfg["desc"], "paths_per_step": paths,
+                       "l2": "working set per wave (4M paths x ~100 B of state) larger than L2"},
+            "e2e": e2e, "cpu_baseline": base, "clocks": clk,
+            "gpu_launches": st.launches * args.steps,
+            "render": {"extension_rays_per_path": st.extension_rays / st.paths,
+                       "shadow_rays_per_path": st.shadow_rays / st.paths, "waves": st.waves,
+                       "launches_per_step": st.launches},
+        }))
+    ctx.close()
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -209,6 +315,8 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.workload != "rays":
+        return run_render(args, rank, world, local_rank)
 
     import torch
 
@@ -273,25 +381,30 @@ def main():
         traffic = json.loads(tf.read_text()).get("trace_closest_icosphere8")
 
     # end to end through the host-buffer entry point
-    host_rays = torch.from_numpy(rays.view(np.uint8)).pin_memory()
-    host_hits = torch.empty(n * 8, dtype=torch.uint8).pin_memory()
-    hr = host_rays.numpy().view(abi.RAY_DTYPE)
-    hh = host_hits.numpy().view(abi.HIT_DTYPE)
-    for _ in range(2):
-        ctx.trace_host(hr, out=hh)
-    e2e_steps = max(3, min(args.steps, 10))
-    if dist:
-        dist.barrier()
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        ctx.trace_host(hr, out=hh)
-    e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], device=f"cuda:{local_rank}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    got = d_hits.cpu().numpy().view(abi.HIT_DTYPE)
-    assert np.array_equal(got["prim"], hh["prim"]), "device and host entry points disagree"
+    e2e = None
+    if not args.no_e2e:
+        host_rays = torch.from_numpy(rays.view(np.uint8)).pin_memory()
+        host_hits = torch.empty(n * 8, dtype=torch.uint8).pin_memory()
+        hr = host_rays.numpy().view(abi.RAY_DTYPE)
+        hh = host_hits.numpy().view(abi.HIT_DTYPE)
+        for _ in range(2):
+            ctx.trace_host(hr, out=hh)
+        e2e_steps = max(3, min(args.steps, 20))
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            ctx.trace_host(hr, out=hh)
+        e2e_s = time.perf_counter() - t0
+        if dist:
+            t = torch.tensor([e2e_s], device=f"cuda:{local_rank}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        got = d_hits.cpu().numpy().view(abi.HIT_DTYPE)
+        assert np.array_equal(got["prim"], hh["prim"]), "device and host entry points disagree"
+        e2e = {"value": n * world * e2e_steps / e2e_s / 1e6, "unit": "Mrays/s",
+               "h2d_bytes_per_step": n * 32, "d2h_bytes_per_step": n * 8,
+               "path": "rbr_trace_host: pinned host rays -> device, closest hit, hits -> pinned host"}
 
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -304,9 +417,7 @@ def main():
             "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": total_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded)", "config": config_block(),
-            "e2e": {"value": n * world * e2e_steps / e2e_s / 1e6, "unit": "Mrays/s",
-                    "h2d_bytes_per_step": n * 32, "d2h_bytes_per_step": n * 8,
-                    "path": "rbr_trace_host: pinned host rays -> device, closest hit, hits -> pinned host"},
+            "e2e": e2e,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": f"{peak_kind} HBM copy bandwidth",

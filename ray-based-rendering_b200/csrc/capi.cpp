@@ -247,6 +247,8 @@ rbr_status rbr_render_stats_get(rbr_ctx* ctx, rbr_render_stats* out) {
         cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop);
         ctx->last_render.milliseconds = ms;
         ctx->render_pending = false;
+        const rbr_status st = read_render_counters(ctx);
+        if (st != RBR_OK) return st;
     }
     *out = ctx->last_render;
     return RBR_OK;

@@ -1,10 +1,375 @@
-// Wavefront path tracer (placeholder until the kernels land).
+// Wavefront path tracer: the GPU form of Integrator::render + PathTracingIntegrator::Li
+// (src/renderers/integrator.cpp:7-50, src/renderers/path_tracing_integrator.cpp:5-138).
+//
+// Paths are processed in waves of up to `capacity` camera samples; all samples of a pixel
+// belong to one wave, path k of a wave is sample (k % spp) of pixel (p0 + k / spp). Per wave:
+//   raygen                         camera rays for every path (counter-RNG jitter and lens)
+//   for depth = 0 .. maxDepth-1:
+//     begin    reset the per-depth queue counters
+//     extend   closest hit for the active queue; misses add background; hits are appended
+//              to one of four material-class queues (warp ballot + one atomic per warp)
+//     shade    per class queue: emission, next-event estimation over ALL lights (one shadow
+//              ray per light with a non-black BSDF value, appended to the shadow queue with
+//              its MIS-weighted contribution), BSDF sampling, Russian roulette after depth 3;
+//              surviving paths are appended to the next active queue
+//     shadow   any hit for the shadow queue; unoccluded contributions are added to the path
+//   film     per pixel, the sum of its samples' radiance in sample order / spp (what
+//            Film::addSample(x, y, sum / spp) stores), plus the sum of squares on request
+// The reference's estimator is reproduced, quirks included: emission only at depth 0 or after
+// a delta bounce, MIS weight on light samples without the BSDF-sampled emitter term, NEE over
+// every light, Russian roulette always on (q = max(0.05, 1 - max(T)) after depth 3). Its
+// BSDF-sampled "MIS" trace whose result is discarded (path_tracing_integrator.cpp:118-134)
+// changes nothing and is not traced.
+#include <algorithm>
+
+#include "rbr_bsdf.cuh"
 #include "rbr_context.h"
 
 namespace rbr {
 
-rbr_status render(rbr_ctx* ctx, const rbr_camera*, const rbr_render_params*, float*, float*, cudaStream_t) {
-    return fail(ctx, RBR_ERR_UNSUPPORTED, "rbr_render is not built yet");
+namespace {
+
+constexpr int kBlock = 128;
+constexpr uint32_t kDefaultCapacity = 1u << 22;  // paths per wave
+constexpr size_t kShadowBytesLimit = size_t(2) << 30;
+
+// counters (uint32 words)
+enum : int {
+    kCQ0 = 0,       // active queue counts, ping-pong by depth parity
+    kCClass = 2,    // kNumClasses class-queue counts
+    kCShadow = 6,   // shadow queue count
+    kCExt = 8,      // 64-bit: extension rays traced
+    kCSh = 10,      // 64-bit: shadow rays traced
+    kCWords = 16
+};
+
+struct Wave {
+    uint32_t p0;       // first pixel
+    uint32_t npaths;   // paths in this wave
+    uint32_t spp;
+    uint32_t sample_offset;
+    uint32_t width;
+    uint32_t max_depth;
+    uint32_t use_nee, use_mis;
+    uint64_t seed;
+};
+
+struct Paths {
+    float4* ray;      // 2 per path: (origin, -), (direction, -)
+    float4* thr;      // throughput rgb, w: 1 if the last bounce was a delta bounce
+    float4* rad;      // radiance rgb
+    uint2* hit;       // primitive id, t bits
+    uint32_t* q0;
+    uint32_t* q1;
+    uint32_t* classq; // kNumClasses x cap
+    float4* shadow;   // 3 per shadow ray: (origin, tmax), (direction, path index bits), (contribution, -)
+    uint32_t* counters;
+    uint32_t cap;
+    uint32_t shadow_cap;
+};
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Warp-aggregated append: every lane with `pred` gets a distinct slot of `queue`; one atomic
+// per warp (ballot + prefix count of the lanes below).
+__device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool pred) {
+    const uint32_t mask = __ballot_sync(0xFFFFFFFFu, pred);
+    if (mask == 0) return 0xFFFFFFFFu;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(mask) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(counter, __popc(mask));
+    base = __shfl_sync(0xFFFFFFFFu, base, leader);
+    return pred ? base + __popc(mask & lanemask_lt()) : 0xFFFFFFFFu;
+}
+
+__device__ __forceinline__ f3 ld_f3(float4 v) { return mk(v.x, v.y, v.z); }
+
+// ------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) k_raygen(CameraDev cam, Wave w, Paths P) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < w.npaths; k += stride) {
+        const uint32_t pixel = w.p0 + k / w.spp;
+        const uint32_t sample = w.sample_offset + k % w.spp;
+        const uint32_t x = pixel % w.width, y = pixel / w.width;
+        const float4 u = draw4(w.seed, pixel, sample, 0u, kRngCamera);
+        f3 o, d;
+        camera_ray(cam, fa(static_cast<float>(x), u.x), fa(static_cast<float>(y), u.y), u.z, u.w, o, d);
+        P.ray[2 * k] = make_float4(o.x, o.y, o.z, 0.0f);
+        P.ray[2 * k + 1] = make_float4(d.x, d.y, d.z, 0.0f);
+        P.thr[k] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);  // specularBounce starts true
+        P.rad[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        P.q0[k] = k;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) P.counters[kCQ0] = w.npaths;
+}
+
+// Resets the counters depth `d` appends to.
+__global__ void k_begin(Paths P, uint32_t d) {
+    uint32_t* c = P.counters;
+    c[kCQ0 + ((d + 1) & 1)] = 0;
+    for (int i = 0; i < kNumClasses; ++i) c[kCClass + i] = 0;
+    c[kCShadow] = 0;
+}
+
+__global__ void __launch_bounds__(kBlock) k_extend(DeviceScene s, Wave w, Paths P, uint32_t d, int* err) {
+    const uint32_t n = P.counters[kCQ0 + (d & 1)];
+    const uint32_t* q = (d & 1) ? P.q1 : P.q0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(reinterpret_cast<unsigned long long*>(P.counters + kCExt), n);
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {
+        const uint32_t j = base + threadIdx.x;
+        const bool valid = j < n;
+        uint32_t k = 0, cls = kNumClasses;
+        if (valid) {
+            k = q[j];
+            const float4 a = P.ray[2 * k], b = P.ray[2 * k + 1];
+            float t = 0.0f;
+            const uint32_t prim = traverse<false>(s, ld_f3(a), ld_f3(b), __int_as_float(0x7f800000), t, err);
+            P.hit[k] = make_uint2(prim, __float_as_uint(t));
+            if (prim == 0xFFFFFFFFu) {
+                const float4 T = P.thr[k];
+                float4 L = P.rad[k];
+                L.x = fa(L.x, fm(T.x, s.background[0]));
+                L.y = fa(L.y, fm(T.y, s.background[1]));
+                L.z = fa(L.z, fm(T.z, s.background[2]));
+                P.rad[k] = L;
+            } else {
+                cls = s.materials[s.prim_material[prim]].cls;
+            }
+        }
+#pragma unroll
+        for (uint32_t c = 0; c < kNumClasses; ++c) {
+            const uint32_t slot = warp_append(P.counters + kCClass + c, cls == c);
+            if (cls == c) P.classq[c * P.cap + slot] = k;
+        }
+    }
+}
+
+// Surface data of a hit, as the primitive's intersect() fills SurfaceInteraction.
+struct Hit {
+    f3 point;
+    f3 normal;   // faces the incoming ray (setFaceNormal)
+    f3 outward;  // outwardNormal()
+};
+
+__device__ __forceinline__ Hit surface(const DeviceScene& s, uint32_t prim, float t, f3 o, f3 d) {
+    Hit h;
+    h.point = xadd(o, xmuls(d, t));  // Ray::at
+    const uint32_t rec = s.prim_record[prim];
+    f3 outward;
+    if (rec & 0x80000000u) {  // plane
+        const float4 pl = s.planes[rec & 0x7FFFFFFFu];
+        outward = mk(pl.x, pl.y, pl.z);
+    } else {
+        const float4 a = s.records[3 * rec], b = s.records[3 * rec + 1], c = s.records[3 * rec + 2];
+        const uint32_t type = __float_as_uint(c.y) >> kTypeShift;
+        if (type == kPrimTriangle) {
+            const f3 v0 = mk(a.x, a.y, a.z), e1 = mk(a.w, b.x, b.y), e2 = mk(b.z, b.w, c.x);
+            const f3 geo = xnorm(xcross(e1, e2));
+            outward = geo;
+            if (s.tri_normals) {  // interpolated shading normal (triangle.cpp:40-46)
+                float u = 0.0f, v = 0.0f;
+                hit_triangle(o, d, v0, e1, e2, __int_as_float(0x7f800000), &u, &v);
+                const float wb = fs(fs(1.0f, u), v);
+                const float4 n0 = s.tri_normals[3 * rec], n1 = s.tri_normals[3 * rec + 1], n2 = s.tri_normals[3 * rec + 2];
+                f3 n = xnorm(xadd(xadd(xmuls(ld_f3(n0), wb), xmuls(ld_f3(n1), u)), xmuls(ld_f3(n2), v)));
+                if (xdot(n, geo) < 0.0f) n = xneg(n);
+                outward = n;
+            }
+        } else if (type == kPrimSphere) {
+            outward = xdivs(xsub(h.point, mk(a.x, a.y, a.z)), a.w);  // (hitPoint - center) / radius
+        } else {
+            outward = xnorm(xcross(mk(a.w, b.x, b.y), mk(b.z, b.w, c.x)));  // quad normal
+        }
+    }
+    const bool front = xdot(d, outward) < 0.0f;
+    h.normal = front ? outward : xneg(outward);
+    h.outward = outward;
+    return h;
+}
+
+// Interaction::spawnRay (interaction.h:22-29); the Ray constructor normalises the direction.
+__device__ __forceinline__ void spawn(const Hit& h, f3 dir, f3& o, f3& d) {
+    f3 off = xmuls(h.normal, kEpsilon);
+    if (xdot(dir, h.normal) < 0.0f) off = xneg(off);
+    o = xadd(h.point, off);
+    d = xnorm(dir);
+}
+
+__global__ void __launch_bounds__(kBlock) k_shade(DeviceScene s, Wave w, Paths P, uint32_t d) {
+    uint32_t cnt[kNumClasses + 1];
+    cnt[0] = 0;
+    for (int c = 0; c < kNumClasses; ++c) cnt[c + 1] = cnt[c] + P.counters[kCClass + c];
+    const uint32_t n = cnt[kNumClasses];
+    uint32_t* nextq = (d & 1) ? P.q0 : P.q1;
+    uint32_t* nextc = P.counters + kCQ0 + ((d + 1) & 1);
+    const bool last = d + 1 >= w.max_depth;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {
+        const uint32_t j = base + threadIdx.x;
+        const bool valid = j < n;
+        uint32_t k = 0;
+        bool alive = false, nee = false;
+        Hit h;
+        f3 T = mk(0.0f, 0.0f, 0.0f), wo = mk(0.0f, 0.0f, 0.0f);
+        Frame fr;
+        Bsdf bs;
+        bs.n = 0;
+        uint32_t pixel = 0, sample = 0;
+        if (valid) {
+            int c = 0;
+            while (j >= cnt[c + 1]) ++c;
+            k = P.classq[c * P.cap + (j - cnt[c])];
+            pixel = w.p0 + k / w.spp;
+            sample = w.sample_offset + k % w.spp;
+            const uint2 hv = P.hit[k];
+            const f3 ro = ld_f3(P.ray[2 * k]), rd = ld_f3(P.ray[2 * k + 1]);
+            const float4 t4 = P.thr[k];
+            T = mk(t4.x, t4.y, t4.z);
+            const bool specular = t4.w != 0.0f;
+            h = surface(s, hv.x, __uint_as_float(hv.y), ro, rd);
+            const MaterialDev& m = s.materials[s.prim_material[hv.x]];
+            if (m.emissive && (d == 0 || specular)) {
+                float4 L = P.rad[k];
+                L.x = fa(L.x, fm(T.x, m.emission[0]));
+                L.y = fa(L.y, fm(T.y, m.emission[1]));
+                L.z = fa(L.z, fm(T.z, m.emission[2]));
+                P.rad[k] = L;
+            }
+            bs = make_bsdf(m);
+            fr = make_frame(h.outward);
+            wo = to_local(fr, xneg(rd));  // isect.wo = -ray.direction
+            nee = w.use_nee && !bsdf_delta(bs);
+            alive = true;
+        }
+        // next-event estimation: one shadow ray per light (estimateDirectLighting)
+        for (uint32_t l = 0; l < s.num_lights; ++l) {
+            bool emit = false;
+            f3 contrib, so, sd;
+            float stmax = 0.0f;
+            if (valid && nee) {
+                const float4 u = draw4(w.seed, pixel, sample, d, kRngLights + ((l >> 1) << 8));
+                const LightDev& L = s.lights[l];
+                const LSample ls = light_sample(L, h.point, (l & 1) ? u.z : u.x, (l & 1) ? u.w : u.y);
+                if (ls.pdf > 0.0f && !black(ls.Li)) {
+                    const f3 wiL = to_local(fr, ls.wi);
+                    const f3 f = bsdf_eval(bs, wo, wiL);
+                    const float bpdf = bsdf_pdf(bs, wo, wiL);
+                    if (!black(f)) {
+                        spawn(h, ls.wi, so, sd);
+                        stmax = fs(ls.dist, kEpsilon);
+                        const float c = fabsf(xdot(ls.wi, h.normal));
+                        f3 ld;
+                        if (w.use_mis && !ls.delta) {
+                            const float wgt = power_heuristic(ls.pdf, bpdf);
+                            ld = xdivs(xmuls(xmuls(xmul(f, ls.Li), c), wgt), ls.pdf);
+                        } else {
+                            ld = xdivs(xmuls(xmul(f, ls.Li), c), ls.pdf);
+                        }
+                        contrib = xmul(T, ld);
+                        emit = true;
+                    }
+                }
+            }
+            const uint32_t slot = warp_append(P.counters + kCShadow, emit);
+            if (emit && slot < P.shadow_cap) {
+                float4* e = P.shadow + 3 * static_cast<size_t>(slot);
+                e[0] = make_float4(so.x, so.y, so.z, stmax);
+                e[1] = make_float4(sd.x, sd.y, sd.z, __uint_as_float(k));
+                e[2] = make_float4(contrib.x, contrib.y, contrib.z, 0.0f);
+            }
+        }
+        // BSDF sampling, throughput update, Russian roulette, next ray
+        bool cont = false;
+        if (valid && alive && !last) {
+            const float4 u = draw4(w.seed, pixel, sample, d, kRngBounce);
+            const BSample b = bsdf_sample(bs, wo, u.x, u.y);
+            if (b.pdf > 0.0f && !black(b.f)) {
+                const f3 wiW = to_world(fr, b.wi);
+                const float c = fabsf(xdot(wiW, h.normal));
+                T = xmul(T, xmuls(b.f, fd(c, b.pdf)));
+                cont = true;
+                if (d > 3) {
+                    const float q = omax(0.05f, fs(1.0f, maxc(T)));
+                    if (u.z < q) cont = false;
+                    else T = xdivs(T, fs(1.0f, q));
+                }
+                if (cont) {
+                    f3 no, nd;
+                    spawn(h, wiW, no, nd);
+                    P.ray[2 * k] = make_float4(no.x, no.y, no.z, 0.0f);
+                    P.ray[2 * k + 1] = make_float4(nd.x, nd.y, nd.z, 0.0f);
+                    P.thr[k] = make_float4(T.x, T.y, T.z, b.delta ? 1.0f : 0.0f);
+                }
+            }
+        }
+        const uint32_t slot = warp_append(nextc, cont);
+        if (cont) nextq[slot] = k;
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) k_shadow(DeviceScene s, Paths P, int* err) {
+    uint32_t n = P.counters[kCShadow];
+    if (n > P.shadow_cap) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(err, kErrQueueOverflow);
+        n = P.shadow_cap;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(reinterpret_cast<unsigned long long*>(P.counters + kCSh), n);
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
+        const float4* e = P.shadow + 3 * static_cast<size_t>(j);
+        const float4 a = e[0], b = e[1];
+        float t;
+        if (!traverse<true>(s, ld_f3(a), ld_f3(b), a.w, t, err)) {
+            const float4 c = e[2];
+            float4* L = P.rad + __float_as_uint(b.w);
+            atomicAdd(&L->x, c.x);
+            atomicAdd(&L->y, c.y);
+            atomicAdd(&L->z, c.z);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) k_film(Wave w, Paths P, float* film_mean, float* film_m2) {
+    const uint32_t npix = w.npaths / w.spp;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < npix; i += stride) {
+        f3 sum = mk(0.0f, 0.0f, 0.0f), sq = mk(0.0f, 0.0f, 0.0f);
+        for (uint32_t s = 0; s < w.spp; ++s) {
+            const f3 L = ld_f3(P.rad[i * w.spp + s]);
+            sum = xadd(sum, L);
+            sq = xadd(sq, xmul(L, L));
+        }
+        const f3 mean = xdivs(sum, static_cast<float>(w.spp));  // pixelColor / samplesPerPixel
+        float* o = film_mean + 3 * static_cast<size_t>(w.p0 + i);
+        o[0] = mean.x;
+        o[1] = mean.y;
+        o[2] = mean.z;
+        if (film_m2) {
+            float* q = film_m2 + 3 * static_cast<size_t>(w.p0 + i);
+            q[0] = sq.x;
+            q[1] = sq.y;
+            q[2] = sq.z;
+        }
+    }
+}
+
+}  // namespace
+
+rbr_status read_render_counters(rbr_ctx* ctx) {
+    if (!ctx->pt.counters.ptr) return RBR_OK;
+    unsigned long long h[2] = {0, 0};
+    const cudaError_t e = cudaMemcpy(h, static_cast<uint32_t*>(ctx->pt.counters.ptr) + kCExt, 16,
+                                     cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "reading the render counters");
+    ctx->last_render.extension_rays = h[0];
+    ctx->last_render.shadow_rays = h[1];
+    return RBR_OK;
 }
 
 void free_path_buffers(rbr_ctx* ctx) {
@@ -19,6 +384,123 @@ void free_path_buffers(rbr_ctx* ctx) {
     release(p.shadow);
     release(p.counters);
     p.capacity = 0;
+    p.shadow_capacity = 0;
+}
+
+static rbr_status ensure_paths(rbr_ctx* ctx, uint32_t cap, uint32_t shadow_cap) {
+    PathBuffers& p = ctx->pt;
+    if (p.capacity >= cap && p.shadow_capacity >= shadow_cap && p.counters.ptr) return RBR_OK;
+    free_path_buffers(ctx);
+    rbr_status st;
+    if ((st = ensure(ctx, p.ray, size_t(cap) * 32, "path rays")) != RBR_OK ||
+        (st = ensure(ctx, p.thr, size_t(cap) * 16, "path throughput")) != RBR_OK ||
+        (st = ensure(ctx, p.rad, size_t(cap) * 16, "path radiance")) != RBR_OK ||
+        (st = ensure(ctx, p.hit, size_t(cap) * 8, "path hits")) != RBR_OK ||
+        (st = ensure(ctx, p.queue[0], size_t(cap) * 4, "active queue")) != RBR_OK ||
+        (st = ensure(ctx, p.queue[1], size_t(cap) * 4, "active queue")) != RBR_OK ||
+        (st = ensure(ctx, p.classq, size_t(cap) * 4 * kNumClasses, "class queues")) != RBR_OK ||
+        (st = ensure(ctx, p.shadow, size_t(std::max(1u, shadow_cap)) * 48, "shadow queue")) != RBR_OK ||
+        (st = ensure(ctx, p.counters, kCWords * 4, "queue counters")) != RBR_OK) {
+        free_path_buffers(ctx);
+        return st;
+    }
+    p.capacity = cap;
+    p.shadow_capacity = shadow_cap;
+    return RBR_OK;
+}
+
+rbr_status render(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_params* p, float* film_mean, float* film_m2,
+                  cudaStream_t stream) {
+    if (!cam || !p || !film_mean) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "camera, params or film_mean is NULL");
+    if (!ctx->has_scene) return fail(ctx, RBR_ERR_NO_SCENE, "rbr_render before rbr_scene_upload");
+    if (cam->width <= 0 || cam->height <= 0 || p->samples_per_pixel <= 0 || p->max_depth < 0)
+        return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "image size, samples per pixel or max depth out of range");
+    if (cam->model != RBR_CAMERA_PINHOLE && cam->model != RBR_CAMERA_THIN_LENS)
+        return fail(ctx, RBR_ERR_UNSUPPORTED, "camera model " + std::to_string(cam->model));
+    if (p->flags & RBR_RENDER_CORRECTED_MIS)
+        return fail(ctx, RBR_ERR_UNSUPPORTED, "RBR_RENDER_CORRECTED_MIS is not implemented");
+    if ((p->flags & RBR_RENDER_SECOND_MOMENT) == 0) film_m2 = nullptr;
+    const uint64_t npix = uint64_t(cam->width) * cam->height;
+    const uint32_t spp = static_cast<uint32_t>(p->samples_per_pixel);
+    if (npix * spp > 0xFFFFFFFFull || spp > kDefaultCapacity)
+        return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "more than 2^32 camera samples in one render call");
+    const uint32_t nl = std::max(1u, ctx->scene.num_lights);
+    uint32_t cap = static_cast<uint32_t>(std::min<uint64_t>(npix * spp, kDefaultCapacity));
+    cap = std::min<uint64_t>(cap, kShadowBytesLimit / (48ull * nl));
+    cap = std::max(spp, cap / spp * spp);
+    rbr_status st = ensure_paths(ctx, cap, cap * nl);
+    if (st != RBR_OK) return st;
+
+    PathBuffers& pb = ctx->pt;
+    Paths P;
+    P.ray = static_cast<float4*>(pb.ray.ptr);
+    P.thr = static_cast<float4*>(pb.thr.ptr);
+    P.rad = static_cast<float4*>(pb.rad.ptr);
+    P.hit = static_cast<uint2*>(pb.hit.ptr);
+    P.q0 = static_cast<uint32_t*>(pb.queue[0].ptr);
+    P.q1 = static_cast<uint32_t*>(pb.queue[1].ptr);
+    P.classq = static_cast<uint32_t*>(pb.classq.ptr);
+    P.shadow = static_cast<float4*>(pb.shadow.ptr);
+    P.counters = static_cast<uint32_t*>(pb.counters.ptr);
+    P.cap = pb.capacity;
+    P.shadow_cap = pb.shadow_capacity;
+
+    CameraDev cd;
+    cd.width = cam->width;
+    cd.height = cam->height;
+    cd.model = cam->model;
+    for (int a = 0; a < 3; ++a) {
+        cd.position[a] = cam->position[a];
+        cd.forward[a] = cam->forward[a];
+        cd.right[a] = cam->right[a];
+        cd.up[a] = cam->up[a];
+    }
+    cd.fx = cam->fx;
+    cd.fy = cam->fy;
+    cd.cx = cam->cx;
+    cd.cy = cam->cy;
+    cd.lens_radius = cam->lens_radius;
+    cd.focal_distance = cam->focal_distance;
+
+    const int grid = ctx->num_sms * 8;
+    const uint32_t pix_per_wave = cap / spp;
+    uint32_t launches = 0, waves = 0;
+    cudaError_t e = cudaMemsetAsync(P.counters, 0, kCWords * 4, stream);
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_start, stream);
+    for (uint64_t p0 = 0; p0 < npix && e == cudaSuccess; p0 += pix_per_wave) {
+        Wave w;
+        w.p0 = static_cast<uint32_t>(p0);
+        w.npaths = static_cast<uint32_t>(std::min<uint64_t>(pix_per_wave, npix - p0)) * spp;
+        w.spp = spp;
+        w.sample_offset = p->sample_offset;
+        w.width = static_cast<uint32_t>(cam->width);
+        w.max_depth = static_cast<uint32_t>(p->max_depth);
+        w.use_nee = p->use_nee != 0;
+        w.use_mis = p->use_mis != 0;
+        w.seed = p->seed;
+        k_raygen<<<grid, kBlock, 0, stream>>>(cd, w, P);
+        ++launches;
+        for (uint32_t d = 0; d < w.max_depth; ++d) {
+            k_begin<<<1, 1, 0, stream>>>(P, d);
+            k_extend<<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d, ctx->d_error);
+            k_shade<<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d);
+            k_shadow<<<grid, kBlock, 0, stream>>>(ctx->scene, P, ctx->d_error);
+            launches += 4;
+        }
+        k_film<<<grid, kBlock, 0, stream>>>(w, P, film_mean, film_m2);
+        ++launches;
+        ++waves;
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_stop, stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "path tracer launch");
+    ctx->last_render.paths = npix * spp;
+    ctx->last_render.extension_rays = 0;  // read from the device by rbr_render_stats_get
+    ctx->last_render.shadow_rays = 0;
+    ctx->last_render.waves = waves;
+    ctx->last_render.launches = launches;
+    ctx->render_pending = true;
+    return RBR_OK;
 }
 
 }  // namespace rbr

@@ -1,0 +1,620 @@
+// Device materials, BSDF lobes, lights, camera rays and the counter-based RNG.
+//
+// Restates the reference operation for operation with exactly rounded intrinsics, so BSDF
+// values and densities equal the reference's bit for bit; only the sampling routines call
+// cosf/sinf (CUDA's accurate versions), whose results may differ from glibc's by an ulp.
+//   Material::createBSDF      src/materials/material.cpp:69-108
+//   MixtureBSDF               src/materials/mixture_bsdf.cpp:5-82
+//   LambertianBSDF            src/materials/lambertian_bsdf.cpp:5-28
+//   Specular{Reflection,Transmission}BSDF  src/materials/specular_bsdf.cpp:5-57
+//   GGXDistribution, Microfacet{Reflection,Transmission}BSDF  src/materials/microfacet_bsdf.cpp:9-179
+//   fresnelDielectric / fresnelSchlick     include/render/materials/fresnel.h:16-48
+//   AreaLight::sample / PointLight::sample src/lighting/area_light.cpp:13-39, point_light.cpp:5-19
+//   Camera rays               src/camera/camera.cpp:5-9, thin_lens_camera.cpp:6-23
+//   sampling::*               include/render/core/sampler.h:58-149
+#pragma once
+
+#include "rbr_b200.h"
+#include "rbr_device.cuh"
+
+namespace rbr {
+
+// ----------------------------------------------------------------------------------------
+// scalar helpers: exactly rounded arithmetic and std::min/max/clamp semantics
+// ----------------------------------------------------------------------------------------
+__device__ __forceinline__ float fm(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fa(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fs(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float fd(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ float fq(float a) { return __fsqrt_rn(a); }
+__device__ __forceinline__ float omax(float a, float b) { return (a < b) ? b : a; }
+__device__ __forceinline__ float omin(float a, float b) { return (b < a) ? b : a; }
+__device__ __forceinline__ float oclamp(float v, float lo, float hi) { return omax(lo, omin(hi, v)); }
+__device__ __forceinline__ bool black(f3 a) { return a.x <= 0.0f && a.y <= 0.0f && a.z <= 0.0f; }
+__device__ __forceinline__ float maxc(f3 a) {  // std::max({x, y, z})
+    float m = a.x;
+    if (m < a.y) m = a.y;
+    if (m < a.z) m = a.z;
+    return m;
+}
+
+constexpr float kPi = 3.14159265358979323846f;
+constexpr float kTwoPi = 2.0f * kPi;
+constexpr float kInvPi = 1.0f / kPi;
+
+// ----------------------------------------------------------------------------------------
+// Philox-4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11). Counter = (pixel, sample, depth,
+// purpose), key = seed. The same streams as the CPU restatement in oracle/rbr_oracle.c.
+// ----------------------------------------------------------------------------------------
+enum : uint32_t { kRngCamera = 0, kRngBounce = 1, kRngLights = 2 };
+
+__device__ __forceinline__ uint4 philox(uint4 c, uint2 k) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+        c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+        k.x += 0x9E3779B9u;
+        k.y += 0xBB67AE85u;
+    }
+    return c;
+}
+__device__ __forceinline__ float u01(uint32_t x) { return static_cast<float>(x >> 8) * (1.0f / 16777216.0f); }
+__device__ __forceinline__ float4 draw4(uint64_t seed, uint32_t pixel, uint32_t sample, uint32_t depth,
+                                        uint32_t purpose) {
+    const uint4 o = philox(make_uint4(pixel, sample, depth, purpose),
+                           make_uint2(static_cast<uint32_t>(seed), static_cast<uint32_t>(seed >> 32)));
+    return make_float4(u01(o.x), u01(o.y), u01(o.z), u01(o.w));
+}
+
+// ----------------------------------------------------------------------------------------
+// Frame (coordinateSystem, vector.h:282-289; sampling::Frame, sampler.h:104-118)
+// ----------------------------------------------------------------------------------------
+struct Frame {
+    f3 t, b, n;
+};
+__device__ __forceinline__ Frame make_frame(f3 n) {
+    Frame f;
+    f.n = n;
+    if (fabsf(n.x) > fabsf(n.y)) f.t = xnorm(mk(-n.z, 0.0f, n.x));
+    else f.t = xnorm(mk(0.0f, n.z, -n.y));
+    f.b = xcross(n, f.t);
+    return f;
+}
+__device__ __forceinline__ f3 to_world(const Frame& f, f3 l) {
+    return xadd(xadd(xmuls(f.t, l.x), xmuls(f.b, l.y)), xmuls(f.n, l.z));
+}
+__device__ __forceinline__ f3 to_local(const Frame& f, f3 w) { return mk(xdot(w, f.t), xdot(w, f.b), xdot(w, f.n)); }
+
+// ----------------------------------------------------------------------------------------
+// Fresnel
+// ----------------------------------------------------------------------------------------
+__device__ __forceinline__ float fresnel_dielectric(float c, float etaI, float etaT) {
+    c = oclamp(c, -1.0f, 1.0f);
+    if (c < 0.0f) {
+        const float tmp = etaI;
+        etaI = etaT;
+        etaT = tmp;
+        c = -c;
+    }
+    const float sinI = fq(omax(0.0f, fs(1.0f, fm(c, c))));
+    const float sinT = fm(fd(etaI, etaT), sinI);
+    if (sinT >= 1.0f) return 1.0f;
+    const float cosT = fq(omax(0.0f, fs(1.0f, fm(sinT, sinT))));
+    const float rParl = fd(fs(fm(etaT, c), fm(etaI, cosT)), fa(fm(etaT, c), fm(etaI, cosT)));
+    const float rPerp = fd(fs(fm(etaI, c), fm(etaT, cosT)), fa(fm(etaI, c), fm(etaT, cosT)));
+    return fm(0.5f, fa(fm(rParl, rParl), fm(rPerp, rPerp)));
+}
+__device__ __forceinline__ f3 fresnel_schlick(float c, f3 f0) {
+    const float m = fs(1.0f, oclamp(fabsf(c), 0.0f, 1.0f));
+    const float m2 = fm(m, m);
+    return xadd(f0, xmuls(xsub(mk(1.0f, 1.0f, 1.0f), f0), fm(fm(m2, m2), m)));
+}
+
+// ----------------------------------------------------------------------------------------
+// Lobes. A mixture is built from the six material parameters exactly as createBSDF does;
+// each lobe stores its kind and weight, everything else derives from the material.
+// ----------------------------------------------------------------------------------------
+enum : uint32_t {
+    kLambert = 0,
+    kCondSpec = 1,   // SpecularReflection, Schlick(baseColor)
+    kCondGGX = 2,    // MicrofacetReflection, Schlick(baseColor)
+    kDielSpec = 3,   // SpecularReflection, Dielectric(1, ior)
+    kDielGGX = 4,    // MicrofacetReflection, Dielectric(1, ior)
+    kTransSpec = 5,  // SpecularTransmission(baseColor, 1, ior)
+    kTransGGX = 6,   // MicrofacetTransmission(baseColor, 1, ior)
+    kPassSpec = 7    // SpecularTransmission(baseColor, 1, 1)
+};
+// BSDFType bits (include/render/materials/bsdf.h:10-24)
+enum : uint32_t { kTRefl = 1, kTTrans = 2, kTDiffuse = 4, kTGlossy = 8, kTSpecular = 16 };
+
+struct Bsdf {
+    f3 base;
+    float ior;
+    float alpha;       // GGXDistribution alpha: max(roughness^2, 1e-3)
+    bool has_sub;      // substrate Fresnel set (dielectric interface)
+    int n;
+    uint32_t kind[4];
+    float weight[4];
+    bool substrate[4];
+};
+
+__device__ __forceinline__ bool lobe_delta(uint32_t k) { return k == kCondSpec || k == kDielSpec || k == kTransSpec || k == kPassSpec; }
+
+__device__ __forceinline__ uint32_t lobe_type(uint32_t k) {
+    switch (k) {
+        case kLambert: return kTDiffuse | kTRefl;
+        case kCondSpec:
+        case kDielSpec: return kTSpecular | kTRefl;
+        case kCondGGX:
+        case kDielGGX: return kTGlossy | kTRefl;
+        case kTransGGX: return kTGlossy | kTTrans;
+        default: return kTSpecular | kTTrans;
+    }
+}
+
+__device__ __forceinline__ void add_lobe(Bsdf& b, uint32_t kind, float w, bool substrate) {
+    if (w <= 0.0f || b.n >= 4) return;
+    b.kind[b.n] = kind;
+    b.weight[b.n] = w;
+    b.substrate[b.n] = substrate;
+    ++b.n;
+}
+
+// Material::createBSDF (material.cpp:69-108)
+__device__ __forceinline__ Bsdf make_bsdf(const MaterialDev& m) {
+    Bsdf b;
+    b.base = mk(m.base[0], m.base[1], m.base[2]);
+    b.ior = m.ior;
+    b.alpha = omax(fm(m.roughness, m.roughness), 1e-3f);
+    b.has_sub = false;
+    b.n = 0;
+    const float met = oclamp(m.metallic, 0.0f, 1.0f);
+    const float t = oclamp(m.transmission, 0.0f, 1.0f);
+    const float diel = fs(1.0f, met);
+    const bool smooth = m.roughness < 0.03f;
+    const bool iface = fabsf(fs(m.ior, 1.0f)) > 1e-3f;
+    const bool tinted = !black(b.base);
+    if (met > 0.0f && tinted) add_lobe(b, smooth ? kCondSpec : kCondGGX, met, false);
+    if (diel > 0.0f) {
+        if (iface) {
+            add_lobe(b, smooth ? kDielSpec : kDielGGX, diel, false);
+            b.has_sub = true;
+            if (t > 0.0f && tinted) add_lobe(b, smooth ? kTransSpec : kTransGGX, fm(diel, t), false);
+            if (t < 1.0f && tinted) add_lobe(b, kLambert, fm(diel, fs(1.0f, t)), true);
+        } else {
+            if (t > 0.0f && tinted) add_lobe(b, kPassSpec, fm(diel, t), false);
+            if (t < 1.0f && tinted) add_lobe(b, kLambert, fm(diel, fs(1.0f, t)), false);
+        }
+    }
+    return b;
+}
+
+__device__ __forceinline__ bool bsdf_delta(const Bsdf& b) {
+    if (b.n == 0) return false;
+    for (int i = 0; i < b.n; ++i)
+        if (!lobe_delta(b.kind[i])) return false;
+    return true;
+}
+
+// Fresnel term of a reflection lobe (Schlick for conductors, dielectric for dielectrics)
+__device__ __forceinline__ f3 lobe_fresnel(const Bsdf& b, uint32_t k, float c) {
+    if (k == kCondSpec || k == kCondGGX) return fresnel_schlick(c, b.base);
+    const float v = fresnel_dielectric(c, 1.0f, b.ior);
+    return mk(v, v, v);
+}
+__device__ __forceinline__ float trans_eta_inside(const Bsdf& b, uint32_t k) { return k == kPassSpec ? 1.0f : b.ior; }
+
+// rho (BSDF::rho overrides)
+__device__ __forceinline__ f3 lobe_rho(const Bsdf& b, uint32_t k, f3 wo) {
+    switch (k) {
+        case kLambert: return b.base;
+        case kCondSpec:
+        case kCondGGX:
+        case kDielSpec:
+        case kDielGGX: return xmul(mk(1.0f, 1.0f, 1.0f), lobe_fresnel(b, k, wo.z));
+        default: return xmuls(b.base, fs(1.0f, fresnel_dielectric(wo.z, 1.0f, trans_eta_inside(b, k))));
+    }
+}
+
+// GGX distribution
+__device__ __forceinline__ float ggx_D(float alpha, f3 wh) {
+    const float cos2 = fm(wh.z, wh.z);
+    if (cos2 <= 0.0f) return 0.0f;
+    const float a2 = fm(alpha, alpha);
+    const float d = fa(fm(cos2, fs(a2, 1.0f)), 1.0f);
+    return fd(a2, fm(fm(kPi, d), d));
+}
+__device__ __forceinline__ float ggx_lambda(float alpha, f3 w) {
+    const float cos2 = fm(w.z, w.z);
+    if (cos2 <= 0.0f) return 0.0f;
+    const float tan2 = fd(omax(0.0f, fs(1.0f, cos2)), cos2);
+    return fm(0.5f, fs(fq(fa(1.0f, fm(fm(alpha, alpha), tan2))), 1.0f));
+}
+__device__ __forceinline__ float ggx_G1(float alpha, f3 w) { return fd(1.0f, fa(1.0f, ggx_lambda(alpha, w))); }
+__device__ __forceinline__ float ggx_G(float alpha, f3 wo, f3 wi) {
+    return fd(1.0f, fa(fa(1.0f, ggx_lambda(alpha, wo)), ggx_lambda(alpha, wi)));
+}
+__device__ __forceinline__ float ggx_pdf(float alpha, f3 wo, f3 wh) {
+    const float cosO = fabsf(wo.z);
+    if (cosO == 0.0f) return 0.0f;
+    return fd(fm(fm(ggx_D(alpha, wh), ggx_G1(alpha, wo)), fabsf(xdot(wo, wh))), cosO);
+}
+__device__ __forceinline__ f3 ggx_sample_wh(float alpha, f3 wo, float u1, float u2) {
+    const bool flip = wo.z < 0.0f;
+    const f3 v = flip ? xneg(wo) : wo;
+    const f3 vh = xnorm(mk(fm(alpha, v.x), fm(alpha, v.y), v.z));
+    const f3 t1 = vh.z < 0.9999f ? xnorm(xcross(mk(0.0f, 0.0f, 1.0f), vh)) : mk(1.0f, 0.0f, 0.0f);
+    const f3 t2 = xcross(vh, t1);
+    const float r = fq(u1);
+    const float phi = fm(kTwoPi, u2);
+    const float p1 = fm(r, cosf(phi));
+    float p2 = fm(r, sinf(phi));
+    const float s = fm(0.5f, fa(1.0f, vh.z));
+    p2 = fa(fm(fs(1.0f, s), fq(omax(0.0f, fs(1.0f, fm(p1, p1))))), fm(s, p2));
+    const f3 nh = xadd(xadd(xmuls(t1, p1), xmuls(t2, p2)), xmuls(vh, fq(omax(0.0f, fs(fs(1.0f, fm(p1, p1)), fm(p2, p2))))));
+    const f3 wh = xnorm(mk(fm(alpha, nh.x), fm(alpha, nh.y), omax(1e-6f, nh.z)));
+    return flip ? xneg(wh) : wh;
+}
+
+struct BSample {
+    f3 wi, f;
+    float pdf;
+    bool delta;
+};
+__device__ __forceinline__ BSample none() {
+    BSample s;
+    s.wi = mk(0.0f, 0.0f, 0.0f);
+    s.f = mk(0.0f, 0.0f, 0.0f);
+    s.pdf = 0.0f;
+    s.delta = false;
+    return s;
+}
+__device__ __forceinline__ bool same_hemi(f3 a, f3 b) { return fm(a.z, b.z) > 0.0f; }
+
+// MicrofacetReflectionBSDF
+__device__ __forceinline__ f3 ggxr_eval(const Bsdf& b, uint32_t k, f3 wo, f3 wi) {
+    if (!same_hemi(wo, wi)) return mk(0.0f, 0.0f, 0.0f);
+    const float cosO = fabsf(wo.z), cosI = fabsf(wi.z);
+    if (cosO == 0.0f || cosI == 0.0f) return mk(0.0f, 0.0f, 0.0f);
+    f3 wh = xadd(wo, wi);
+    if (wh.x == 0.0f && wh.y == 0.0f && wh.z == 0.0f) return mk(0.0f, 0.0f, 0.0f);
+    wh = xnorm(wh);
+    if (wh.z < 0.0f) wh = xneg(wh);
+    const f3 F = lobe_fresnel(b, k, xdot(wo, wh));
+    return xmuls(xmul(mk(1.0f, 1.0f, 1.0f), F),
+                 fd(fm(ggx_D(b.alpha, wh), ggx_G(b.alpha, wo, wi)), fm(fm(4.0f, cosO), cosI)));
+}
+__device__ __forceinline__ float ggxr_pdf(const Bsdf& b, f3 wo, f3 wi) {
+    if (!same_hemi(wo, wi)) return 0.0f;
+    f3 wh = xadd(wo, wi);
+    if (wh.x == 0.0f && wh.y == 0.0f && wh.z == 0.0f) return 0.0f;
+    wh = xnorm(wh);
+    if (wh.z < 0.0f) wh = xneg(wh);
+    const float dotOH = xdot(wo, wh);
+    if (dotOH == 0.0f) return 0.0f;
+    return fd(ggx_pdf(b.alpha, wo, wh), fm(4.0f, fabsf(dotOH)));
+}
+__device__ __forceinline__ BSample ggxr_sample(const Bsdf& b, uint32_t k, f3 wo, float u1, float u2) {
+    BSample r = none();
+    if (wo.z == 0.0f) return r;
+    const f3 wh = ggx_sample_wh(b.alpha, wo, u1, u2);
+    const f3 wi = xsub(xmuls(wh, fm(2.0f, xdot(wo, wh))), wo);
+    if (!same_hemi(wo, wi)) return r;
+    const float p = ggxr_pdf(b, wo, wi);
+    if (p <= 0.0f) return r;
+    r.wi = wi;
+    r.pdf = p;
+    r.f = ggxr_eval(b, k, wo, wi);
+    return r;
+}
+
+// MicrofacetTransmissionBSDF (etaOutside = 1, etaInside = ior)
+__device__ __forceinline__ bool ggxt_half(const Bsdf& b, f3 wo, f3 wi, f3& wh, float& eta) {
+    if (same_hemi(wo, wi)) return false;
+    if (wo.z == 0.0f || wi.z == 0.0f) return false;
+    eta = wo.z > 0.0f ? fd(b.ior, 1.0f) : fd(1.0f, b.ior);
+    f3 h = xadd(wo, xmuls(wi, eta));
+    if (h.x == 0.0f && h.y == 0.0f && h.z == 0.0f) return false;
+    h = xnorm(h);
+    if (xdot(wo, h) < 0.0f) h = xneg(h);
+    wh = h;
+    return fm(h.z, wo.z) > 0.0f && xdot(wi, h) <= 0.0f;
+}
+__device__ __forceinline__ f3 ggxt_eval(const Bsdf& b, f3 wo, f3 wi) {
+    f3 wh;
+    float eta;
+    if (!ggxt_half(b, wo, wi, wh, eta)) return mk(0.0f, 0.0f, 0.0f);
+    const float cosO = wo.z, cosI = wi.z;
+    const float dotOH = xdot(wo, wh), dotIH = xdot(wi, wh);
+    const float F = fresnel_dielectric(wo.z > 0.0f ? dotOH : -dotOH, 1.0f, b.ior);
+    const float denom = fa(dotOH, fm(eta, dotIH));
+    if (denom == 0.0f) return mk(0.0f, 0.0f, 0.0f);
+    const float value = fd(fm(fm(ggx_D(b.alpha, wh), ggx_G(b.alpha, wo, wi)), fabsf(fm(dotIH, dotOH))),
+                           fabsf(fm(fm(fm(cosI, cosO), denom), denom)));
+    return xmuls(b.base, fm(fs(1.0f, F), value));
+}
+__device__ __forceinline__ float ggxt_pdf(const Bsdf& b, f3 wo, f3 wi) {
+    f3 wh;
+    float eta;
+    if (!ggxt_half(b, wo, wi, wh, eta)) return 0.0f;
+    const float dotOH = xdot(wo, wh), dotIH = xdot(wi, wh);
+    const float denom = fa(dotOH, fm(eta, dotIH));
+    if (denom == 0.0f) return 0.0f;
+    const float dwh = fd(fabsf(fm(fm(eta, eta), dotIH)), fm(denom, denom));
+    return fm(ggx_pdf(b.alpha, wo, wh), dwh);
+}
+__device__ __forceinline__ BSample ggxt_sample(const Bsdf& b, f3 wo, float u1, float u2) {
+    BSample r = none();
+    if (wo.z == 0.0f) return r;
+    const f3 wh = ggx_sample_wh(b.alpha, wo, u1, u2);
+    const float dotOH = xdot(wo, wh);
+    if (dotOH <= 0.0f) return r;
+    const bool entering = wo.z > 0.0f;
+    const float etaRatio = entering ? fd(1.0f, b.ior) : fd(b.ior, 1.0f);
+    const float sin2T = fm(fm(etaRatio, etaRatio), omax(0.0f, fs(1.0f, fm(dotOH, dotOH))));
+    if (sin2T >= 1.0f) return r;
+    const float cosT = fq(fs(1.0f, sin2T));
+    const f3 wi = xsub(xmuls(wh, fs(fm(etaRatio, dotOH), cosT)), xmuls(wo, etaRatio));
+    if (same_hemi(wo, wi) || wi.z == 0.0f) return r;
+    const float p = ggxt_pdf(b, wo, wi);
+    if (p <= 0.0f) return r;
+    r.wi = wi;
+    r.pdf = p;
+    r.f = ggxt_eval(b, wo, wi);
+    return r;
+}
+
+// Lambertian
+__device__ __forceinline__ f3 cosine_hemisphere(float u1, float u2) {
+    const float r = fq(u1);
+    const float theta = fm(kTwoPi, u2);
+    return mk(fm(r, cosf(theta)), fm(r, sinf(theta)), fq(omax(0.0f, fs(1.0f, u1))));
+}
+
+// Specular lobes
+__device__ __forceinline__ BSample sr_sample(const Bsdf& b, uint32_t k, f3 wo) {
+    BSample r = none();
+    const float cosO = fabsf(wo.z);
+    if (cosO == 0.0f) return r;
+    r.wi = mk(-wo.x, -wo.y, wo.z);
+    r.f = xdivs(xmul(mk(1.0f, 1.0f, 1.0f), lobe_fresnel(b, k, wo.z)), cosO);
+    r.pdf = 1.0f;
+    r.delta = true;
+    return r;
+}
+__device__ __forceinline__ BSample st_sample(const Bsdf& b, uint32_t k, f3 wo) {
+    BSample r = none();
+    if (wo.z == 0.0f) return r;
+    const float etaIn = trans_eta_inside(b, k);
+    const bool entering = wo.z > 0.0f;
+    const float etaI = entering ? 1.0f : etaIn;
+    const float etaT = entering ? etaIn : 1.0f;
+    const float eta = fd(etaI, etaT);
+    const float cosI = fabsf(wo.z);
+    const float sin2T = fm(fm(eta, eta), omax(0.0f, fs(1.0f, fm(cosI, cosI))));
+    if (sin2T >= 1.0f) return r;
+    const float cosT = fq(fs(1.0f, sin2T));
+    r.wi = mk(fm(-eta, wo.x), fm(-eta, wo.y), entering ? -cosT : cosT);
+    const float fr = fresnel_dielectric(wo.z, 1.0f, etaIn);
+    r.f = xmuls(b.base, fd(fm(fm(fs(1.0f, fr), eta), eta), cosT));
+    r.pdf = 1.0f;
+    r.delta = true;
+    return r;
+}
+
+__device__ __forceinline__ f3 lobe_eval(const Bsdf& b, uint32_t k, f3 wo, f3 wi) {
+    switch (k) {
+        case kLambert: return same_hemi(wo, wi) ? xmuls(b.base, kInvPi) : mk(0.0f, 0.0f, 0.0f);
+        case kCondGGX:
+        case kDielGGX: return ggxr_eval(b, k, wo, wi);
+        case kTransGGX: return ggxt_eval(b, wo, wi);
+        default: return mk(0.0f, 0.0f, 0.0f);
+    }
+}
+__device__ __forceinline__ float lobe_pdf(const Bsdf& b, uint32_t k, f3 wo, f3 wi) {
+    switch (k) {
+        case kLambert: return same_hemi(wo, wi) ? fm(fabsf(wi.z), kInvPi) : 0.0f;
+        case kCondGGX:
+        case kDielGGX: return ggxr_pdf(b, wo, wi);
+        case kTransGGX: return ggxt_pdf(b, wo, wi);
+        default: return 0.0f;
+    }
+}
+__device__ __forceinline__ BSample lobe_sample(const Bsdf& b, uint32_t k, f3 wo, float u1, float u2) {
+    switch (k) {
+        case kLambert: {
+            BSample r = none();
+            r.wi = cosine_hemisphere(u1, u2);
+            if (wo.z < 0.0f) r.wi.z = -r.wi.z;
+            r.f = xmuls(b.base, kInvPi);
+            r.pdf = fm(fabsf(r.wi.z), kInvPi);
+            return r;
+        }
+        case kCondSpec:
+        case kDielSpec: return sr_sample(b, k, wo);
+        case kTransSpec:
+        case kPassSpec: return st_sample(b, k, wo);
+        case kCondGGX:
+        case kDielGGX: return ggxr_sample(b, k, wo, u1, u2);
+        default: return ggxt_sample(b, wo, u1, u2);
+    }
+}
+
+// MixtureBSDF
+__device__ __forceinline__ float eff_weight(const Bsdf& b, int i, f3 wo) {
+    if (!b.substrate[i]) return b.weight[i];
+    return fm(b.weight[i], omax(0.0f, fs(1.0f, fresnel_dielectric(wo.z, 1.0f, b.ior))));
+}
+__device__ __forceinline__ float selection(const Bsdf& b, f3 wo, float* w, float* sc) {
+    float total = 0.0f;
+    for (int i = 0; i < b.n; ++i) {
+        w[i] = eff_weight(b, i, wo);
+        sc[i] = fm(w[i], maxc(lobe_rho(b, b.kind[i], wo)));
+        total = fa(total, sc[i]);
+    }
+    return total;
+}
+__device__ __forceinline__ f3 bsdf_eval(const Bsdf& b, f3 wo, f3 wi) {
+    f3 f = mk(0.0f, 0.0f, 0.0f);
+    for (int i = 0; i < b.n; ++i) {
+        if (lobe_delta(b.kind[i])) continue;
+        f = xadd(f, xmuls(lobe_eval(b, b.kind[i], wo, wi), eff_weight(b, i, wo)));
+    }
+    return f;
+}
+__device__ __forceinline__ float bsdf_pdf(const Bsdf& b, f3 wo, f3 wi) {
+    float w[4], sc[4];
+    const float total = selection(b, wo, w, sc);
+    if (total <= 0.0f) return 0.0f;
+    float p = 0.0f;
+    for (int i = 0; i < b.n; ++i) {
+        if (lobe_delta(b.kind[i])) continue;
+        p = fa(p, fm(sc[i], lobe_pdf(b, b.kind[i], wo, wi)));
+    }
+    return fd(p, total);
+}
+__device__ __forceinline__ BSample bsdf_sample(const Bsdf& b, f3 wo, float u1, float u2) {
+    float w[4], sc[4];
+    const float total = selection(b, wo, w, sc);
+    if (total <= 0.0f) return none();
+    float u = fm(u1, total);
+    int chosen = b.n - 1;
+    for (int i = 0; i < b.n; ++i) {
+        if (sc[i] <= 0.0f) continue;
+        if (u < sc[i] || i + 1 == b.n) {
+            chosen = i;
+            break;
+        }
+        u = fs(u, sc[i]);
+    }
+    if (sc[chosen] <= 0.0f) return none();
+    const float v1 = omin(fd(u, sc[chosen]), 0.99999994f);
+    const uint32_t k = b.kind[chosen];
+    BSample s = lobe_sample(b, k, wo, v1, u2);
+    if (s.pdf <= 0.0f || black(s.f)) return none();
+    const float pChosen = fd(sc[chosen], total);
+    if (lobe_delta(k)) {
+        s.f = xmuls(s.f, w[chosen]);
+        s.pdf = fm(s.pdf, pChosen);
+        return s;
+    }
+    s.f = bsdf_eval(b, wo, s.wi);
+    s.pdf = bsdf_pdf(b, wo, s.wi);
+    if (s.pdf <= 0.0f) return none();
+    return s;
+}
+__device__ __forceinline__ uint32_t bsdf_type(const Bsdf& b) {
+    uint32_t t = 0;
+    for (int i = 0; i < b.n; ++i) t |= lobe_type(b.kind[i]);
+    return t;
+}
+
+// sampling::powerHeuristic (sampler.h:137-149)
+__device__ __forceinline__ float power_heuristic(float fPdf, float gPdf) {
+    float f = fPdf, g = gPdf;  // nf = ng = 1
+    if (isinf(f)) return 1.0f;
+    if (isinf(g)) return 0.0f;
+    const float m = omax(f, g);
+    if (m <= 0.0f) return 0.0f;
+    f = fd(f, m);
+    g = fd(g, m);
+    return fd(fm(f, f), fa(fm(f, f), fm(g, g)));
+}
+
+// ----------------------------------------------------------------------------------------
+// Lights
+// ----------------------------------------------------------------------------------------
+struct LSample {
+    f3 wi, Li;
+    float pdf, dist;
+    bool delta;
+};
+__device__ __forceinline__ LSample light_sample(const LightDev& l, f3 p, float u1, float u2) {
+    LSample s;
+    s.delta = false;
+    if (l.type == RBR_LIGHT_AREA) {
+        const f3 lp = xadd(xadd(ld3(l.position), xmuls(ld3(l.u), fs(u1, 0.5f))), xmuls(ld3(l.v), fs(u2, 0.5f)));
+        const f3 toL = xsub(lp, p);
+        const float d2 = xdot(toL, toL);
+        s.dist = fq(d2);
+        s.wi = xdivs(toL, s.dist);
+        const float c = -xdot(ld3(l.normal), s.wi);
+        if (c <= 0.0f) {
+            s.Li = mk(0.0f, 0.0f, 0.0f);
+            s.pdf = 0.0f;
+            return s;
+        }
+        s.pdf = fd(d2, fm(c, l.area));
+        s.Li = xmuls(ld3(l.color), l.intensity);
+    } else {
+        const f3 toL = xsub(ld3(l.position), p);
+        const float d2 = xdot(toL, toL);
+        s.dist = fq(d2);
+        s.wi = xdivs(toL, s.dist);
+        s.Li = xdivs(xmuls(ld3(l.color), l.intensity), d2);
+        s.pdf = 1.0f;
+        s.delta = true;
+    }
+    return s;
+}
+
+// ----------------------------------------------------------------------------------------
+// Camera rays
+// ----------------------------------------------------------------------------------------
+struct CameraDev {
+    int32_t width, height;
+    uint32_t model;
+    float position[3], forward[3], right[3], up[3];
+    float fx, fy, cx, cy;
+    float lens_radius, focal_distance;
+};
+
+__device__ __forceinline__ void concentric_disk(float u1, float u2, float& ox, float& oy) {
+    const float sx = fs(fm(2.0f, u1), 1.0f);
+    const float sy = fs(fm(2.0f, u2), 1.0f);
+    if (sx == 0.0f && sy == 0.0f) {
+        ox = oy = 0.0f;
+        return;
+    }
+    float r, theta;
+    if (fabsf(sx) > fabsf(sy)) {
+        r = sx;
+        theta = fm(kPi / 4.0f, fd(sy, sx));
+    } else {
+        r = sy;
+        theta = fs(kPi / 2.0f, fm(kPi / 4.0f, fd(sx, sy)));
+    }
+    ox = fm(r, cosf(theta));
+    oy = fm(r, sinf(theta));
+}
+
+__device__ __forceinline__ f3 cam_to_world(const CameraDev& c, f3 d) {
+    return xadd(xadd(xmuls(ld3(c.right), d.x), xmuls(ld3(c.up), d.y)), xmuls(ld3(c.forward), d.z));
+}
+
+// PinholeCamera / ThinLensCamera::generateRay
+__device__ __forceinline__ void camera_ray(const CameraDev& c, float px, float py, float lu, float lv, f3& o, f3& d) {
+    const f3 local = mk(fd(fs(px, c.cx), c.fx), fd(fs(c.cy, py), c.fy), 1.0f);
+    const f3 pos = ld3(c.position);
+    const f3 dir = xnorm(xnorm(cam_to_world(c, local)));
+    if (c.model != RBR_CAMERA_THIN_LENS) {
+        o = xadd(pos, cam_to_world(c, mk(0.0f, 0.0f, 0.0f)));
+        d = dir;
+        return;
+    }
+    if (c.lens_radius > 0.0f) {
+        float lx, ly;
+        concentric_disk(lu, lv, lx, ly);
+        const f3 lens = xadd(pos, xmuls(xadd(xmuls(ld3(c.right), lx), xmuls(ld3(c.up), ly)), c.lens_radius));
+        const float ft = fd(c.focal_distance, fabsf(xdot(dir, ld3(c.forward))));
+        const f3 focus = xadd(pos, xmuls(dir, ft));
+        o = lens;
+        d = xnorm(xnorm(xsub(focus, lens)));
+        return;
+    }
+    o = pos;
+    d = xnorm(dir);
+}
+
+}  // namespace rbr

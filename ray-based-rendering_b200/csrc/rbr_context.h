@@ -79,5 +79,6 @@ cudaError_t launch_trace_counts(const DeviceScene& s, const rbr_ray* rays, uint3
 rbr_status render(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_params* p, float* film_mean, float* film_m2,
                   cudaStream_t stream);
 void free_path_buffers(rbr_ctx* ctx);
+rbr_status read_render_counters(rbr_ctx* ctx);
 
 }  // namespace rbr

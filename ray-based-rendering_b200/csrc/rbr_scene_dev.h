@@ -6,10 +6,17 @@
 
 namespace rbr {
 
+// Shading classes: paths are bucketed by the class of the material they hit so that one
+// warp shades one kind of BSDF.
+enum : uint32_t { kClassDiffuse = 0, kClassGlossy = 1, kClassSpecular = 2, kClassNone = 3, kNumClasses = 4 };
+
 struct MaterialDev {
     float base[3];
     float metallic, roughness, ior, transmission;
     float emission[3];
+    uint32_t cls;     // kClass*: any GGX lobe -> glossy; else Lambertian -> diffuse; else delta-only
+                      // -> specular; no lobe at all (lights, black) -> none
+    uint32_t emissive;
 };
 
 struct LightDev {

@@ -47,6 +47,34 @@ inline void box_point(Box& b, V3 p) {
 }
 inline Box empty_box() { return Box{{FLT_MAX, FLT_MAX, FLT_MAX}, {-FLT_MAX, -FLT_MAX, -FLT_MAX}}; }
 
+// The lobes Material::createBSDF (src/materials/material.cpp:69-108) adds for `m`, reduced to
+// the shading class of the material.
+uint32_t material_class(const rbr_material& m) {
+    const float met = std::max(0.0f, std::min(1.0f, m.metallic));
+    const float t = std::max(0.0f, std::min(1.0f, m.transmission));
+    const float diel = 1.0f - met;
+    const bool smooth = m.roughness < 0.03f;
+    const bool iface = std::fabs(m.ior - 1.0f) > 1e-3f;
+    const bool tinted = !(m.base_color[0] <= 0.0f && m.base_color[1] <= 0.0f && m.base_color[2] <= 0.0f);
+    bool ggx = false, lambert = false, delta = false;
+    auto lobe = [&](bool is_delta) { (is_delta ? delta : ggx) = true; };
+    if (met > 0.0f && tinted) lobe(smooth);
+    if (diel > 0.0f) {
+        if (iface) {
+            lobe(smooth);
+            if (t > 0.0f && tinted) lobe(smooth);
+            if (t < 1.0f && tinted) lambert = true;
+        } else {
+            if (t > 0.0f && tinted) delta = true;
+            if (t < 1.0f && tinted) lambert = true;
+        }
+    }
+    if (ggx) return kClassGlossy;
+    if (lambert) return kClassDiffuse;
+    if (delta) return kClassSpecular;
+    return kClassNone;
+}
+
 template <class T>
 rbr_status upload(rbr_ctx* ctx, const std::vector<T>& host, const char* what, void** out) {
     *out = nullptr;
@@ -244,6 +272,8 @@ rbr_status upload_scene(rbr_ctx* ctx, const rbr_scene_desc* d) {
         o.ior = m.ior;
         o.transmission = m.transmission;
         std::memcpy(o.emission, m.emission, 12);
+        o.cls = material_class(m);
+        o.emissive = (m.emission[0] > 0.0f || m.emission[1] > 0.0f || m.emission[2] > 0.0f) ? 1u : 0u;
     }
     std::vector<LightDev> lights(d->num_lights);
     for (uint32_t i = 0; i < d->num_lights; ++i) {
