@@ -1,0 +1,125 @@
+// GpuPathIntegrator through the reference's own Integrator interface on the reference's own
+// Cornell box (cornell_box::createScene: coloured walls, glass and mirror spheres, an area
+// light and a point light): the GPU image must converge to what the reference's
+// PathTracingIntegrator renders, and unsupported input must be reported, not emulated.
+// Exit code 0 = all checks passed. Needs a CUDA device.
+
+#include <chrono>
+#include <cmath>
+#include <iostream>
+#include <memory>
+#include <string>
+
+#include "cornell_box/cornell_box.h"
+#include "gpu_integrator.h"
+#include "render/geometry/sphere.h"
+#include "render/materials/lambertian_bsdf.h"
+#include "render/renderers/path_tracing_integrator.h"
+#include "render/scene/scene_builder.h"
+
+using namespace render;
+
+namespace {
+
+int failures = 0;
+
+void check(bool ok, const std::string& what) {
+    if (!ok) {
+        std::cerr << "FAIL: " << what << "\n";
+        ++failures;
+    }
+}
+
+double seconds(std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// A material with its own createBSDF (as in the reference's tests/test_materials.cpp:263-270).
+class ScaledDiffuse : public Material {
+public:
+    std::unique_ptr<BSDF> createBSDF() const override { return std::make_unique<LambertianBSDF>(baseColor * 0.5f); }
+};
+
+}  // namespace
+
+int main() {
+    const int W = 64, H = 64;
+    Scene scene = cornell_box::createScene(false);
+    auto camera = cornell_box::createCamera(W, H);
+
+    IntegratorConfig cfg;
+    cfg.maxDepth = 8;
+    cfg.samplesPerPixel = 256;
+    PathTracingIntegrator cpu(cfg);
+    Film cpuFilm(W, H);
+    auto t0 = std::chrono::steady_clock::now();
+    cpu.render(scene, *camera, cpuFilm);
+    const double cpuSec = seconds(t0);
+
+    IntegratorConfig gcfg = cfg;
+    gcfg.samplesPerPixel = 4096;
+    GpuPathIntegrator gpu(gcfg, 0, 42);
+    if (gpu.status() != RBR_OK) {
+        std::cerr << "no CUDA device: " << gpu.error() << "\n";
+        return 2;
+    }
+    Film gpuFilm(W, H);
+    t0 = std::chrono::steady_clock::now();
+    gpu.render(scene, *camera, gpuFilm);
+    const double gpuSec = seconds(t0);
+    check(gpu.status() == RBR_OK, "GPU render status: " + gpu.error());
+
+    double sc = 0.0, sg = 0.0, num = 0.0, dc = 0.0, dg = 0.0;
+    for (int y = 0; y < H; ++y)
+        for (int x = 0; x < W; ++x) {
+            const Color c = cpuFilm.getPixel(x, y), g = gpuFilm.getPixel(x, y);
+            sc += c.x + c.y + c.z;
+            sg += g.x + g.y + g.z;
+        }
+    const double mc = sc / (3.0 * W * H), mg = sg / (3.0 * W * H);
+    for (int y = 0; y < H; ++y)
+        for (int x = 0; x < W; ++x) {
+            const Color c = cpuFilm.getPixel(x, y), g = gpuFilm.getPixel(x, y);
+            for (int k = 0; k < 3; ++k) {
+                num += (c[k] - mc) * (g[k] - mg);
+                dc += (c[k] - mc) * (c[k] - mc);
+                dg += (g[k] - mg) * (g[k] - mg);
+            }
+        }
+    const double corr = num / std::sqrt(dc * dg);
+    std::cout << "reference CPU  " << cfg.samplesPerPixel << " spp: mean " << mc << "  " << cpuSec << " s\n";
+    std::cout << "GPU           " << gcfg.samplesPerPixel << " spp: mean " << mg << "  " << gpuSec << " s (device "
+              << gpu.lastMilliseconds() << " ms)\n";
+    std::cout << "image correlation " << corr << "\n";
+    check(std::fabs(mg - mc) < 0.03 * mc, "image means agree within 3%");
+    check(corr > 0.9, "images correlate");
+
+    // Unsupported input is reported and leaves the film untouched.
+    {
+        SceneBuilder b;
+        Material* odd = b.material(std::make_unique<ScaledDiffuse>());
+        b.sphere(Vec3(0, 0, 0), 1.0f, odd);
+        b.areaLight(Vec3(0, 3, 0), Vec3(1, 0, 0), Vec3(0, 0, 1), Color(1.0f), 5.0f);
+        auto s = b.build();
+        GpuPathIntegrator g(gcfg, 0);
+        Film f(8, 8);
+        auto cam = cornell_box::createCamera(8, 8);
+        g.render(*s, *cam, f);
+        check(g.status() == RBR_ERR_UNSUPPORTED && f.getPixel(3, 3).isBlack(), "derived Material is reported");
+    }
+    {
+        Scene fog = cornell_box::createScene(true);
+        GpuPathIntegrator g(gcfg, 0);
+        Film f(8, 8);
+        auto cam = cornell_box::createCamera(8, 8);
+        g.render(fog, *cam, f);
+        check(g.status() == RBR_ERR_UNSUPPORTED, "participating medium is reported");
+    }
+    {
+        UniformSampler sampler(1);
+        const Color c = gpu.Li(Ray(Vec3(0, 1, 5), Vec3(0, 0, -1)), scene, sampler);
+        check(c.isBlack() && gpu.status() == RBR_ERR_UNSUPPORTED, "single-ray Li is reported unsupported");
+    }
+    if (failures == 0) std::cout << "All GPU integrator tests passed\n";
+    return failures == 0 ? 0 : 1;
+}
