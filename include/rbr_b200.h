@@ -244,6 +244,35 @@ rbr_status rbr_render_host(rbr_ctx* ctx, const rbr_camera* camera, const rbr_ren
 /* Counters and device time of the last render (waits for it). */
 rbr_status rbr_render_stats_get(rbr_ctx* ctx, rbr_render_stats* out);
 
+/* Size of the fixed scratch array used by rbr_render_noalloc (16 MiB). */
+#define RBR_NOALLOC_SCRATCH_BYTES (16u << 20)
+
+/* rbr_render without any device allocation (no counterpart in the reference).
+ *
+ * rbr_render allocates its per-path working memory on first use and whenever a larger image
+ * needs more. Some callers can't let it: an application that reserves the GPU's memory for
+ * its own pool up front and allows no other allocation, or a frame loop that must never
+ * stall on cudaMalloc/cudaFree (they can synchronise the whole device). This entry point
+ * keeps the path state in a fixed RBR_NOALLOC_SCRATCH_BYTES array compiled into the library
+ * (every GPU that loads the library holds it until the process exits) and renders in as many
+ * waves as that array requires, so it calls no cudaMalloc, cudaFree or allocating routine.
+ *
+ * Arguments as rbr_render; film_mean is a device pointer (width*height*3 floats, the
+ * per-pixel mean) and params->flags must be 0 (no second moment, no corrected MIS). The
+ * result equals rbr_render's for the same parameters. A sample count per pixel whose wave
+ * state does not fit the array (about 116,000 samples per pixel with one light, fewer with
+ * more lights) is rejected with RBR_ERR_INVALID_ARGUMENT and a message giving the limit.
+ * The scene must have been uploaded with rbr_scene_upload beforehand; render statistics
+ * (rbr_render_stats_get) are not updated.
+ *
+ * The first call on a device looks up the array's device address (which loads the
+ * library's device code on that device if nothing has yet); make that first call before any
+ * stream capture. All calls in the process share the one array per device and it keeps the
+ * previous call's contents, so calls whose work overlaps on the GPU (different streams or
+ * contexts on the same device) race and corrupt each other: serialise them. */
+rbr_status rbr_render_noalloc(rbr_ctx* ctx, const rbr_camera* camera, const rbr_render_params* params,
+                              float* film_mean, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -219,6 +219,13 @@ rbr_status rbr_render(rbr_ctx* ctx, const rbr_camera* camera, const rbr_render_p
     return render(ctx, camera, params, film_mean, film_m2, static_cast<cudaStream_t>(stream));
 }
 
+rbr_status rbr_render_noalloc(rbr_ctx* ctx, const rbr_camera* camera, const rbr_render_params* params,
+                              float* film_mean, void* stream) {
+    if (!ctx) return RBR_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(ctx->device);
+    return render_noalloc(ctx, camera, params, film_mean, static_cast<cudaStream_t>(stream));
+}
+
 rbr_status rbr_render_host(rbr_ctx* ctx, const rbr_camera* camera, const rbr_render_params* params, float* film_mean,
                            float* film_m2) {
     if (!ctx) return RBR_ERR_INVALID_ARGUMENT;

@@ -21,6 +21,7 @@
 // BSDF-sampled "MIS" trace whose result is discarded (path_tracing_integrator.cpp:118-134)
 // changes nothing and is not traced.
 #include <algorithm>
+#include <mutex>
 
 #include "rbr_bsdf.cuh"
 #include "rbr_context.h"
@@ -500,6 +501,137 @@ rbr_status render(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_params* 
     ctx->last_render.waves = waves;
     ctx->last_render.launches = launches;
     ctx->render_pending = true;
+    return RBR_OK;
+}
+
+// ------------------------------------------------------------------------------------------
+// Rendering without allocating: the wave state lives in a fixed array compiled into the
+// library instead of buffers the context allocates on demand.
+// ------------------------------------------------------------------------------------------
+namespace {
+
+// Every GPU that loads this library holds this array until the process exits.
+__device__ __align__(256) unsigned char g_render_scratch[RBR_NOALLOC_SCRATCH_BYTES];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mutex;
+void* g_scratch_ptr[kMaxDevices] = {};
+
+// Device address of g_render_scratch on the current device (looked up once per device).
+// In host code the array's name only stands in for the symbol; kernels must be given this
+// address, never the host-side name.
+cudaError_t scratch_address(int device, unsigned char** out) {
+    if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (!g_scratch_ptr[device]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_render_scratch);
+        if (e != cudaSuccess) return e;
+        g_scratch_ptr[device] = p;
+    }
+    *out = static_cast<unsigned char*>(g_scratch_ptr[device]);
+    return cudaSuccess;
+}
+
+constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+}  // namespace
+
+rbr_status render_noalloc(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_params* p, float* film_mean,
+                          cudaStream_t stream) {
+    if (!cam || !p || !film_mean) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "camera, params or film_mean is NULL");
+    if (!ctx->has_scene) return fail(ctx, RBR_ERR_NO_SCENE, "rbr_render_noalloc before rbr_scene_upload");
+    if (cam->width <= 0 || cam->height <= 0 || p->samples_per_pixel <= 0 || p->max_depth < 0)
+        return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "image size, samples per pixel or max depth out of range");
+    if (cam->model != RBR_CAMERA_PINHOLE && cam->model != RBR_CAMERA_THIN_LENS)
+        return fail(ctx, RBR_ERR_UNSUPPORTED, "camera model " + std::to_string(cam->model));
+    if (p->flags != 0)
+        return fail(ctx, RBR_ERR_UNSUPPORTED, "rbr_render_noalloc takes no flags (it writes the mean film only)");
+    const uint64_t npix = uint64_t(cam->width) * cam->height;
+    const uint32_t spp = static_cast<uint32_t>(p->samples_per_pixel);
+    if (npix * spp > 0xFFFFFFFFull)
+        return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "more than 2^32 camera samples in one render call");
+    // wave capacity that fits the fixed array: 96 B of path state + 48 B per light and path
+    const uint32_t nl = std::max(1u, ctx->scene.num_lights);
+    const size_t per_path = 96 + 48 * size_t(nl);
+    const size_t fixed = 9 * 256;  // counters + alignment of the eight arrays
+    uint64_t cap = (RBR_NOALLOC_SCRATCH_BYTES - fixed) / per_path;
+    cap = std::min<uint64_t>(cap, npix * spp);
+    cap = cap / spp * spp;
+    if (cap < spp)
+        return fail(ctx, RBR_ERR_INVALID_ARGUMENT,
+                    "rbr_render_noalloc: " + std::to_string(spp) + " samples per pixel with " + std::to_string(nl) +
+                        " lights do not fit its " + std::to_string(RBR_NOALLOC_SCRATCH_BYTES) +
+                        "-byte scratch array (at most " +
+                        std::to_string((RBR_NOALLOC_SCRATCH_BYTES - fixed) / per_path) + " samples per pixel)");
+    unsigned char* base = nullptr;
+    cudaError_t e = scratch_address(ctx->device, &base);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "looking up the render scratch array");
+
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        unsigned char* q = base + off;
+        off += align256(bytes);
+        return q;
+    };
+    Paths P;
+    P.counters = reinterpret_cast<uint32_t*>(take(kCWords * 4));
+    P.ray = reinterpret_cast<float4*>(take(cap * 32));
+    P.thr = reinterpret_cast<float4*>(take(cap * 16));
+    P.rad = reinterpret_cast<float4*>(take(cap * 16));
+    P.hit = reinterpret_cast<uint2*>(take(cap * 8));
+    P.q0 = reinterpret_cast<uint32_t*>(take(cap * 4));
+    P.q1 = reinterpret_cast<uint32_t*>(take(cap * 4));
+    P.classq = reinterpret_cast<uint32_t*>(take(cap * 4 * kNumClasses));
+    P.shadow = reinterpret_cast<float4*>(take(cap * nl * 48));
+    if (off > RBR_NOALLOC_SCRATCH_BYTES) return fail(ctx, RBR_ERR_INTERNAL, "scratch layout exceeds the array");
+    P.cap = static_cast<uint32_t>(cap);
+    P.shadow_cap = static_cast<uint32_t>(cap * nl);
+
+    CameraDev cd;
+    cd.width = cam->width;
+    cd.height = cam->height;
+    cd.model = cam->model;
+    for (int a = 0; a < 3; ++a) {
+        cd.position[a] = cam->position[a];
+        cd.forward[a] = cam->forward[a];
+        cd.right[a] = cam->right[a];
+        cd.up[a] = cam->up[a];
+    }
+    cd.fx = cam->fx;
+    cd.fy = cam->fy;
+    cd.cx = cam->cx;
+    cd.cy = cam->cy;
+    cd.lens_radius = cam->lens_radius;
+    cd.focal_distance = cam->focal_distance;
+
+    // The array keeps the previous call's contents: only the counters must start at zero,
+    // every other array is written before it is read within a wave.
+    e = cudaMemsetAsync(P.counters, 0, kCWords * 4, stream);
+    const int grid = ctx->num_sms * 8;
+    const uint32_t pix_per_wave = static_cast<uint32_t>(cap / spp);
+    for (uint64_t p0 = 0; p0 < npix && e == cudaSuccess; p0 += pix_per_wave) {
+        Wave w;
+        w.p0 = static_cast<uint32_t>(p0);
+        w.npaths = static_cast<uint32_t>(std::min<uint64_t>(pix_per_wave, npix - p0)) * spp;
+        w.spp = spp;
+        w.sample_offset = p->sample_offset;
+        w.width = static_cast<uint32_t>(cam->width);
+        w.max_depth = static_cast<uint32_t>(p->max_depth);
+        w.use_nee = p->use_nee != 0;
+        w.use_mis = p->use_mis != 0;
+        w.seed = p->seed;
+        k_raygen<<<grid, kBlock, 0, stream>>>(cd, w, P);
+        for (uint32_t d = 0; d < w.max_depth; ++d) {
+            k_begin<<<1, 1, 0, stream>>>(P, d);
+            k_extend<<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d, ctx->d_error);
+            k_shade<<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d);
+            k_shadow<<<grid, kBlock, 0, stream>>>(ctx->scene, P, ctx->d_error);
+        }
+        k_film<<<grid, kBlock, 0, stream>>>(w, P, film_mean, nullptr);
+        e = cudaGetLastError();
+    }
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "path tracer launch (no-alloc)");
     return RBR_OK;
 }
 

@@ -80,5 +80,7 @@ rbr_status render(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_params* 
                   cudaStream_t stream);
 void free_path_buffers(rbr_ctx* ctx);
 rbr_status read_render_counters(rbr_ctx* ctx);
+rbr_status render_noalloc(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_params* p, float* film_mean,
+                          cudaStream_t stream);
 
 }  // namespace rbr

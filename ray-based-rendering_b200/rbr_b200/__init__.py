@@ -59,6 +59,7 @@ def load_library() -> C.CDLL:
         "rbr_render": (C.c_int, [P, C.POINTER(abi.rbr_camera), C.POINTER(abi.rbr_render_params), P, P, P]),
         "rbr_render_host": (C.c_int, [P, C.POINTER(abi.rbr_camera), C.POINTER(abi.rbr_render_params), P, P]),
         "rbr_render_stats_get": (C.c_int, [P, C.POINTER(abi.rbr_render_stats)]),
+        "rbr_render_noalloc": (C.c_int, [P, C.POINTER(abi.rbr_camera), C.POINTER(abi.rbr_render_params), P, P]),
     }
     for name, (res, args) in sig.items():
         if hasattr(lib, name):
