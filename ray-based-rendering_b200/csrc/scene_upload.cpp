@@ -75,6 +75,62 @@ uint32_t material_class(const rbr_material& m) {
     return kClassNone;
 }
 
+// A box containing every point at which a primitive's reference test can report a hit, for a
+// leaf record `w` whose getBounds() box is `gb`. Two effects make it larger than `gb`:
+//  1. Quad::intersect accepts plane points with 0 <= (p-O).u <= |u|^2 and 0 <= (p-O).v <= |v|^2
+//     (src/geometry/quad.cpp:30-37). For non-orthogonal u, v that is the parallelogram with
+//     corners O + x u + y v, (x, y) = A^-1 (a, b), A = [[u.u, u.v], [u.v, v.v]],
+//     (a, b) in {0, |u|^2} x {0, |v|^2} -- not the parallelogram (O, u, v) that
+//     Quad::getBounds (quad.cpp:44-51) boxes. (The reference's own BVH misses hits there.)
+//  2. Near grazing incidence a test's distance t carries a large rounding error: the tests
+//     reject only |e1.(d x e2)| < 1e-4 or |n.d| < 1e-4 (an absolute EPSILON), so t may be off
+//     by about 2^-24 * L / 1e-4 times the primitive's size factor, L bounding the distances
+//     involved (4x the largest coordinate). Boxes grow by 4x that bound; a sphere's tangent
+//     point moves along the tangent by ~2^-12 L, leaving its box by at most (2^-12 L)^2 / 2r.
+Box hit_region_box(const uint32_t* w, const Box& gb, float maxabs) {
+    float f[12];
+    std::memcpy(f, w, sizeof(f));
+    const uint32_t type = w[9] >> kTypeShift;
+    const double eps = 1.0 / 16777216.0, L = 4.0 * maxabs, K = 4.0;
+    double lo[3] = {gb.lo[0], gb.lo[1], gb.lo[2]}, hi[3] = {gb.hi[0], gb.hi[1], gb.hi[2]};
+    double pad = 0.0;
+    if (type == kPrimTriangle) {
+        const double l1 = std::sqrt(double(f[3]) * f[3] + double(f[4]) * f[4] + double(f[5]) * f[5]);
+        const double l2 = std::sqrt(double(f[6]) * f[6] + double(f[7]) * f[7] + double(f[8]) * f[8]);
+        pad = K * eps * L * std::max(1.0, l1 * l2 / 1e-4);
+    } else if (type == kPrimSphere) {
+        const double r = f[3], s = L / 4096.0;
+        pad = K * std::max(r > 0.0 ? s * s / (2.0 * r) : 0.0, 4.0 * eps * L);
+    } else {  // quad
+        const double O[3] = {f[0], f[1], f[2]}, u[3] = {f[3], f[4], f[5]}, v[3] = {f[6], f[7], f[8]};
+        const double uu = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+        const double vv = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+        const double uv = u[0] * v[0] + u[1] * v[1] + u[2] * v[2];
+        const double det = uu * vv - uv * uv;
+        if (det > 1e-12 * uu * vv) {
+            const double ab[4][2] = {{0, 0}, {uu, 0}, {0, vv}, {uu, vv}};
+            for (const auto& c : ab) {
+                const double x = (c[0] * vv - c[1] * uv) / det, y = (c[1] * uu - c[0] * uv) / det;
+                for (int a = 0; a < 3; ++a) {
+                    const double p = O[a] + x * u[a] + y * v[a];
+                    lo[a] = std::min(lo[a], p);
+                    hi[a] = std::max(hi[a], p);
+                }
+            }
+        }
+        pad = K * eps * L * 3.0 / 1e-4;
+    }
+    pad = std::min(pad, L);
+    Box out;
+    for (int a = 0; a < 3; ++a) {
+        out.lo[a] = static_cast<float>(lo[a] - pad);
+        out.hi[a] = static_cast<float>(hi[a] + pad);
+        if (out.lo[a] > lo[a] - pad) out.lo[a] = std::nextafter(out.lo[a], -FLT_MAX);
+        if (out.hi[a] < hi[a] + pad) out.hi[a] = std::nextafter(out.hi[a], FLT_MAX);
+    }
+    return out;
+}
+
 template <class T>
 rbr_status upload(rbr_ctx* ctx, const std::vector<T>& host, const char* what, void** out) {
     *out = nullptr;
@@ -243,8 +299,11 @@ rbr_status upload_scene(rbr_ctx* ctx, const rbr_scene_desc* d) {
         }
     }
 
+    // BVH boxes bound where each primitive's test can report a hit, not just its getBounds()
+    std::vector<Box> hit_boxes(boxes.size());
+    for (size_t b = 0; b < boxes.size(); ++b) hit_boxes[b] = hit_region_box(&words[b * kRecordWords], boxes[b], maxabs);
     const int threads = std::max(1u, std::thread::hardware_concurrency());
-    WideBVH bvh = build_wide_bvh(boxes, maxabs * (1.0f / 131072.0f), threads);
+    WideBVH bvh = build_wide_bvh(hit_boxes, maxabs * (1.0f / 1048576.0f), threads);
 
     std::vector<uint32_t> records(bvh.leaf_order.size() * kRecordWords);
     for (size_t r = 0; r < bvh.leaf_order.size(); ++r) {

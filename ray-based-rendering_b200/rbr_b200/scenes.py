@@ -426,7 +426,7 @@ def uniform_rays(n: int, lo, hi, seed=0, tmax=np.inf) -> np.ndarray:
 # segment with tmax in [0.5, 40].
 # ----------------------------------------------------------------------------------------
 def random_world(n_spheres: int, n_triangles: int, with_plane: bool = False, seed: int = 0,
-                 flat_triangles: int = 20) -> Scene:
+                 flat_triangles: int = 20, n_quads: int = 0) -> Scene:
     rng = np.random.default_rng(seed)
     s = Scene(name=f"world{n_spheres}_{n_triangles}{'_plane' if with_plane else ''}")
     m = s.diffuse((0.5, 0.5, 0.5))
@@ -448,10 +448,21 @@ def random_world(n_spheres: int, n_triangles: int, with_plane: bool = False, see
     n_sph = len(sph)
     s.sphere_ids = np.arange(n_sph, dtype=np.uint32)
     s.triangle_ids = np.arange(n_sph, n_sph + len(tri), dtype=np.uint32)
+    nxt = n_sph + len(tri)
+    if n_quads:  # tilted quads: origin in the box, u = (a, 0, 0.3), v = (0, b, b)
+        o = pos(n_quads, 3)
+        a, b = size(n_quads), size(n_quads)
+        z = np.zeros(n_quads, F32)
+        u = np.stack([a, z, np.full(n_quads, 0.3, F32)], 1)
+        v = np.stack([z, b, b], 1)
+        s.quads = np.ascontiguousarray(np.concatenate([o, u, v], 1).astype(F32))
+        s.quad_materials = np.full(n_quads, m, np.uint32)
+        s.quad_ids = np.arange(nxt, nxt + n_quads, dtype=np.uint32)
+        nxt += n_quads
     if with_plane:
         s.planes = np.array([[0.0, 1.0, 0.0, 12.0]], F32)  # Plane(Vec3(0,1,0), 12): y = -12
         s.plane_materials = np.array([m], np.uint32)
-        s.plane_ids = np.array([n_sph + len(tri)], np.uint32)
+        s.plane_ids = np.array([nxt], np.uint32)
     return s
 
 

@@ -4,6 +4,7 @@
 // Exit code 0 = all checks passed. Needs a CUDA device.
 
 #include <cmath>
+#include <typeinfo>
 #include <cstring>
 #include <iostream>
 #include <memory>
@@ -94,8 +95,16 @@ void compare(GpuBVHAccelerator& accel, const World& w, std::mt19937& rng, int nR
         hits += refHit;
         Ray r = rays[i];
         const bool hit = accel.intersect(r, got);
-        if (hit != refHit || (hit && (got.primitive != ref.primitive || !bits_equal(got.t, ref.t) || !bits_equal(r.tMax, ref.t))))
+        if (hit != refHit || (hit && (got.primitive != ref.primitive || !bits_equal(got.t, ref.t) || !bits_equal(r.tMax, ref.t)))) {
+            if (bad < 5) {
+                const Primitive* p = refHit ? ref.primitive : got.primitive;
+                std::cerr << "  mismatch " << label << " ray " << i << ": ref " << (refHit ? "hit" : "miss") << " t=" << ref.t
+                          << " gpu " << (hit ? "hit" : "miss") << " t=" << got.t << " tMax=" << rays[i].tMax << " prim "
+                          << (p ? typeid(*p).name() : "-") << " |cos|="
+                          << (refHit ? std::fabs(dot(ref.normal, rays[i].direction)) : -1.0f) << "\n";
+            }
             ++bad;
+        }
         else if (hit && (!same(got.point, ref.point) || !same(got.normal, ref.normal) || got.frontFace != ref.frontFace))
             ++badSurface;
         const bool bh = batch[i].prim != RBR_MISS;

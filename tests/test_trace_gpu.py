@@ -58,6 +58,25 @@ def test_matches_reference_bvh_and_bruteforce(ctx, reference, ns, nt, plane, see
     assert np.array_equal(ctx.trace_host(rays, any_hit=True), reference.trace_any(r, rays))
 
 
+@pytest.mark.parametrize("ns,nt,nq,plane,seed", [(30, 30, 10, False, 21), (400, 1500, 100, False, 22),
+                                                  (60, 200, 20, True, 23)])
+def test_tilted_quads_match_bruteforce(ctx, reference, ns, nt, nq, plane, seed):
+    """Quads with non-orthogonal edges: Quad::intersect accepts a parallelogram that
+    Quad::getBounds does not contain, so the reference's own BVH misses some of their hits.
+    The GPU returns exactly what brute force over the primitives returns."""
+    w = scenes.random_world(ns, nt, plane, seed=seed, n_quads=nq)
+    rays = scenes.random_test_rays(6000, seed=seed + 300)
+    ctx.upload(w)
+    r = reference.scene(w)
+    brute = reference.trace_closest(r, rays, brute=True)
+    got = ctx.trace_host(rays)
+    assert_same_closest(got, brute)
+    assert np.array_equal(ctx.trace_host(rays, any_hit=True), reference.trace_any(r, rays, brute=True))
+    bvh = reference.trace_closest(r, rays)
+    ref_bvh_misses = int(np.sum(bvh["prim"] != brute["prim"]))
+    print(f"reference BVH disagrees with brute force on {ref_bvh_misses} of {len(rays)} rays; GPU on 0")
+
+
 def test_empty_scene(ctx):
     ctx.upload(scenes.Scene())
     rays = abi.make_rays(np.array([[0, 0, 5]], np.float32), np.array([[0, 0, -1]], np.float32))
