@@ -244,6 +244,31 @@ rbr_status rbr_render_host(rbr_ctx* ctx, const rbr_camera* camera, const rbr_ren
 /* Counters and device time of the last render (waits for it). */
 rbr_status rbr_render_stats_get(rbr_ctx* ctx, rbr_render_stats* out);
 
+/* ------------------------------------------------------------------------------------------
+ * Unit entry points: the path tracer's own device functions applied to caller-given inputs
+ * (host buffers, each call waits), for one-to-one comparison with the reference's CPU code.
+ * ------------------------------------------------------------------------------------------ */
+
+/* Material::createBSDF + BSDF::evaluate / pdf (src/materials/material.cpp:69-108,
+ * mixture_bsdf.cpp:48-67) for n (wo, wi) pairs in the shading frame (normal = +z).
+ * out: 6 floats per pair: f[3], pdf, isDelta (0/1), BSDFType bits. */
+rbr_status rbr_bsdf_eval_host(rbr_ctx* ctx, const rbr_material* material, uint32_t n, const float* wo,
+                              const float* wi, float* out);
+/* Material::createBSDF + BSDF::sample (mixture_bsdf.cpp:69-105) for n (wo, u1, u2).
+ * out: 8 floats per sample: wi[3], f[3], pdf, isDelta. */
+rbr_status rbr_bsdf_sample_host(rbr_ctx* ctx, const rbr_material* material, uint32_t n, const float* wo,
+                                const float* u, float* out);
+/* Light::sample at n surface points (area_light.cpp:13-39, point_light.cpp:5-19).
+ * out: 9 floats per sample: wi[3], Li[3], pdf, distance, isDelta. */
+rbr_status rbr_light_sample_host(rbr_ctx* ctx, const rbr_light* light, uint32_t n, const float* points,
+                                 const float* u, float* out);
+/* Camera::generateRay for n CameraSamples (filmX, filmY, lensU, lensV)
+ * (camera.cpp:5-9, pinhole_camera.cpp:5-7, thin_lens_camera.cpp:6-23). out: origin[3], dir[3]. */
+rbr_status rbr_camera_rays_host(rbr_ctx* ctx, const rbr_camera* camera, uint32_t n, const float* samples,
+                                float* out);
+/* sampling::powerHeuristic(1, pdf_pairs[2i], 1, pdf_pairs[2i+1]) (sampler.h:137-149). */
+rbr_status rbr_mis_weights_host(rbr_ctx* ctx, uint32_t n, const float* pdf_pairs, float* out);
+
 /* Size of the fixed scratch array used by rbr_render_noalloc (16 MiB). */
 #define RBR_NOALLOC_SCRATCH_BYTES (16u << 20)
 

@@ -223,8 +223,9 @@ class Reference:
 
     def camera(self, width, height, position, look_at, up, fov, lens_radius=0.0, focal_distance=1.0):
         cam = abi.rbr_camera()
-        self.L.ref_camera_setup(width, height, _ptr(_f(position)), _ptr(_f(look_at)), _ptr(_f(up)), fov,
-                                lens_radius, focal_distance, C.byref(cam))
+        p, t, u = _f(position), _f(look_at), _f(up)  # keep the arrays alive during the call
+        self.L.ref_camera_setup(width, height, _ptr(p), _ptr(t), _ptr(u), fov, lens_radius, focal_distance,
+                                C.byref(cam))
         return cam
 
     def camera_rays(self, cam, samples):
@@ -251,11 +252,13 @@ class Reference:
     def frame(self, n):
         t = np.zeros(3, np.float32)
         b = np.zeros(3, np.float32)
-        self.L.ref_frame(_ptr(_f(n)), _ptr(t), _ptr(b))
+        n = _f(n)
+        self.L.ref_frame(_ptr(n), _ptr(t), _ptr(b))
         return t, b
 
     def set_medium(self, h, sigma_a, sigma_s, g):
-        self.L.ref_scene_set_medium(h.h, _ptr(_f(sigma_a)), _ptr(_f(sigma_s)), g)
+        sa, ss = _f(sigma_a), _f(sigma_s)
+        self.L.ref_scene_set_medium(h.h, _ptr(sa), _ptr(ss), g)
 
 
 class _Handle:

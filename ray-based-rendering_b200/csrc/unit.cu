@@ -1,0 +1,227 @@
+// Diagnostic entry points: the path tracer's device functions applied to caller-given inputs,
+// so that each can be compared one to one with the reference's CPU code
+// (Material::createBSDF + BSDF::evaluate/pdf/sample, Light::sample, Camera::generateRay,
+// sampling::powerHeuristic). Host buffers in, host buffers out; each call waits.
+#include <vector>
+
+#include "rbr_bsdf.cuh"
+#include "rbr_context.h"
+
+namespace rbr {
+
+namespace {
+
+constexpr int kUnitBlock = 128;
+
+__global__ void k_bsdf_eval(MaterialDev m, uint32_t n, const float* wo, const float* wi, float* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const Bsdf b = make_bsdf(m);
+    const f3 o = ld3(wo + 3 * i), w = ld3(wi + 3 * i);
+    const f3 f = bsdf_eval(b, o, w);
+    float* r = out + 6 * i;  // f[3], pdf, isDelta, type bits
+    r[0] = f.x;
+    r[1] = f.y;
+    r[2] = f.z;
+    r[3] = bsdf_pdf(b, o, w);
+    r[4] = bsdf_delta(b) ? 1.0f : 0.0f;
+    r[5] = static_cast<float>(bsdf_type(b));
+}
+
+__global__ void k_bsdf_sample(MaterialDev m, uint32_t n, const float* wo, const float* u, float* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const Bsdf b = make_bsdf(m);
+    const BSample s = bsdf_sample(b, ld3(wo + 3 * i), u[2 * i], u[2 * i + 1]);
+    float* r = out + 8 * i;  // wi[3], f[3], pdf, isDelta
+    r[0] = s.wi.x;
+    r[1] = s.wi.y;
+    r[2] = s.wi.z;
+    r[3] = s.f.x;
+    r[4] = s.f.y;
+    r[5] = s.f.z;
+    r[6] = s.pdf;
+    r[7] = s.delta ? 1.0f : 0.0f;
+}
+
+__global__ void k_light_sample(LightDev l, uint32_t n, const float* p, const float* u, float* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const LSample s = light_sample(l, ld3(p + 3 * i), u[2 * i], u[2 * i + 1]);
+    float* r = out + 9 * i;  // wi[3], Li[3], pdf, distance, isDelta
+    r[0] = s.wi.x;
+    r[1] = s.wi.y;
+    r[2] = s.wi.z;
+    r[3] = s.Li.x;
+    r[4] = s.Li.y;
+    r[5] = s.Li.z;
+    r[6] = s.pdf;
+    r[7] = s.dist;
+    r[8] = s.delta ? 1.0f : 0.0f;
+}
+
+__global__ void k_camera_rays(CameraDev c, uint32_t n, const float* smp, float* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    f3 o, d;
+    const float* s = smp + 4 * i;
+    camera_ray(c, s[0], s[1], s[2], s[3], o, d);
+    float* r = out + 6 * i;
+    r[0] = o.x;
+    r[1] = o.y;
+    r[2] = o.z;
+    r[3] = d.x;
+    r[4] = d.y;
+    r[5] = d.z;
+}
+
+__global__ void k_mis(uint32_t n, const float* pdfs, float* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[i] = power_heuristic(pdfs[2 * i], pdfs[2 * i + 1]);
+}
+
+// Runs `launch` with `in` copied to the device and `out_floats` floats copied back.
+template <class F>
+rbr_status run_unit(rbr_ctx* ctx, const std::vector<std::pair<const float*, size_t>>& ins, size_t out_floats,
+                    float* out, F launch) {
+    size_t total = out_floats;
+    for (auto& in : ins) total += in.second;
+    rbr_status st = ensure(ctx, ctx->stage_in, total * sizeof(float), "unit-test staging");
+    if (st != RBR_OK) return st;
+    float* base = static_cast<float*>(ctx->stage_in.ptr);
+    std::vector<const float*> dev;
+    size_t off = 0;
+    cudaError_t e = cudaSuccess;
+    for (auto& in : ins) {
+        dev.push_back(base + off);
+        if (in.second) e = cudaMemcpyAsync(base + off, in.first, in.second * sizeof(float), cudaMemcpyHostToDevice, ctx->stream);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "unit-test upload");
+        off += in.second;
+    }
+    float* dout = base + off;
+    launch(dev, dout);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, dout, out_floats * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    return e == cudaSuccess ? RBR_OK : cuda_fail(ctx, e, "unit-test kernel");
+}
+
+uint32_t blocks(uint32_t n) { return (n + kUnitBlock - 1) / kUnitBlock; }
+
+MaterialDev to_dev(const rbr_material& m) {
+    MaterialDev o{};
+    for (int a = 0; a < 3; ++a) {
+        o.base[a] = m.base_color[a];
+        o.emission[a] = m.emission[a];
+    }
+    o.metallic = m.metallic;
+    o.roughness = m.roughness;
+    o.ior = m.ior;
+    o.transmission = m.transmission;
+    return o;
+}
+
+}  // namespace
+
+}  // namespace rbr
+
+using namespace rbr;
+
+extern "C" {
+
+rbr_status rbr_bsdf_eval_host(rbr_ctx* ctx, const rbr_material* m, uint32_t n, const float* wo, const float* wi,
+                              float* out) {
+    if (!ctx || !m || (n && (!wo || !wi || !out))) return RBR_ERR_INVALID_ARGUMENT;
+    if (n == 0) return RBR_OK;
+    cudaSetDevice(ctx->device);
+    const MaterialDev md = to_dev(*m);
+    return run_unit(ctx, {{wo, 3 * size_t(n)}, {wi, 3 * size_t(n)}}, 6 * size_t(n), out,
+                    [&](const std::vector<const float*>& d, float* o) {
+                        k_bsdf_eval<<<blocks(n), kUnitBlock, 0, ctx->stream>>>(md, n, d[0], d[1], o);
+                    });
+}
+
+rbr_status rbr_bsdf_sample_host(rbr_ctx* ctx, const rbr_material* m, uint32_t n, const float* wo, const float* u,
+                                float* out) {
+    if (!ctx || !m || (n && (!wo || !u || !out))) return RBR_ERR_INVALID_ARGUMENT;
+    if (n == 0) return RBR_OK;
+    cudaSetDevice(ctx->device);
+    const MaterialDev md = to_dev(*m);
+    return run_unit(ctx, {{wo, 3 * size_t(n)}, {u, 2 * size_t(n)}}, 8 * size_t(n), out,
+                    [&](const std::vector<const float*>& d, float* o) {
+                        k_bsdf_sample<<<blocks(n), kUnitBlock, 0, ctx->stream>>>(md, n, d[0], d[1], o);
+                    });
+}
+
+rbr_status rbr_light_sample_host(rbr_ctx* ctx, const rbr_light* l, uint32_t n, const float* points, const float* u,
+                                 float* out) {
+    if (!ctx || !l || (n && (!points || !u || !out))) return RBR_ERR_INVALID_ARGUMENT;
+    if (l->type != RBR_LIGHT_AREA && l->type != RBR_LIGHT_POINT) return RBR_ERR_UNSUPPORTED;
+    if (n == 0) return RBR_OK;
+    cudaSetDevice(ctx->device);
+    LightDev ld{};
+    ld.type = l->type;
+    for (int a = 0; a < 3; ++a) {
+        ld.position[a] = l->position[a];
+        ld.u[a] = l->u[a];
+        ld.v[a] = l->v[a];
+        ld.color[a] = l->color[a];
+    }
+    ld.intensity = l->intensity;
+    // normal and area as AreaLight's constructor computes them (no FMA contraction on the host)
+    const float cx = l->u[1] * l->v[2] - l->u[2] * l->v[1];
+    const float cy = l->u[2] * l->v[0] - l->u[0] * l->v[2];
+    const float cz = l->u[0] * l->v[1] - l->u[1] * l->v[0];
+    const float len = std::sqrt(cx * cx + cy * cy + cz * cz);
+    if (len > 0.0f) {
+        const float inv = 1.0f / len;
+        ld.normal[0] = cx * inv;
+        ld.normal[1] = cy * inv;
+        ld.normal[2] = cz * inv;
+    }
+    ld.area = len;
+    return run_unit(ctx, {{points, 3 * size_t(n)}, {u, 2 * size_t(n)}}, 9 * size_t(n), out,
+                    [&](const std::vector<const float*>& d, float* o) {
+                        k_light_sample<<<blocks(n), kUnitBlock, 0, ctx->stream>>>(ld, n, d[0], d[1], o);
+                    });
+}
+
+rbr_status rbr_camera_rays_host(rbr_ctx* ctx, const rbr_camera* c, uint32_t n, const float* samples, float* out) {
+    if (!ctx || !c || (n && (!samples || !out))) return RBR_ERR_INVALID_ARGUMENT;
+    if (c->model != RBR_CAMERA_PINHOLE && c->model != RBR_CAMERA_THIN_LENS) return RBR_ERR_UNSUPPORTED;
+    if (n == 0) return RBR_OK;
+    cudaSetDevice(ctx->device);
+    CameraDev cd{};
+    cd.width = c->width;
+    cd.height = c->height;
+    cd.model = c->model;
+    for (int a = 0; a < 3; ++a) {
+        cd.position[a] = c->position[a];
+        cd.forward[a] = c->forward[a];
+        cd.right[a] = c->right[a];
+        cd.up[a] = c->up[a];
+    }
+    cd.fx = c->fx;
+    cd.fy = c->fy;
+    cd.cx = c->cx;
+    cd.cy = c->cy;
+    cd.lens_radius = c->lens_radius;
+    cd.focal_distance = c->focal_distance;
+    return run_unit(ctx, {{samples, 4 * size_t(n)}}, 6 * size_t(n), out,
+                    [&](const std::vector<const float*>& d, float* o) {
+                        k_camera_rays<<<blocks(n), kUnitBlock, 0, ctx->stream>>>(cd, n, d[0], o);
+                    });
+}
+
+rbr_status rbr_mis_weights_host(rbr_ctx* ctx, uint32_t n, const float* pdf_pairs, float* out) {
+    if (!ctx || (n && (!pdf_pairs || !out))) return RBR_ERR_INVALID_ARGUMENT;
+    if (n == 0) return RBR_OK;
+    cudaSetDevice(ctx->device);
+    return run_unit(ctx, {{pdf_pairs, 2 * size_t(n)}}, size_t(n), out,
+                    [&](const std::vector<const float*>& d, float* o) {
+                        k_mis<<<blocks(n), kUnitBlock, 0, ctx->stream>>>(n, d[0], o);
+                    });
+}
+
+}  // extern "C"

@@ -60,6 +60,11 @@ def load_library() -> C.CDLL:
         "rbr_render_host": (C.c_int, [P, C.POINTER(abi.rbr_camera), C.POINTER(abi.rbr_render_params), P, P]),
         "rbr_render_stats_get": (C.c_int, [P, C.POINTER(abi.rbr_render_stats)]),
         "rbr_render_noalloc": (C.c_int, [P, C.POINTER(abi.rbr_camera), C.POINTER(abi.rbr_render_params), P, P]),
+        "rbr_bsdf_eval_host": (C.c_int, [P, C.POINTER(abi.rbr_material), C.c_uint32, P, P, P]),
+        "rbr_bsdf_sample_host": (C.c_int, [P, C.POINTER(abi.rbr_material), C.c_uint32, P, P, P]),
+        "rbr_light_sample_host": (C.c_int, [P, C.POINTER(abi.rbr_light), C.c_uint32, P, P, P]),
+        "rbr_camera_rays_host": (C.c_int, [P, C.POINTER(abi.rbr_camera), C.c_uint32, P, P]),
+        "rbr_mis_weights_host": (C.c_int, [P, C.c_uint32, P, P]),
     }
     for name, (res, args) in sig.items():
         if hasattr(lib, name):
@@ -178,6 +183,41 @@ class Context:
                                              C.c_void_p(mean.ctypes.data),
                                              C.c_void_p(m2.ctypes.data) if m2 is not None else None))
         return (mean, m2) if second_moment else mean
+
+    # device functions on caller inputs (unit parity) -----------------------------------------
+    def _unit(self, fn, args, n, width):
+        out = np.zeros((n, width), np.float32)
+        keep = [np.ascontiguousarray(a, np.float32) for a in args]
+        self._check(fn(self.h, *[C.c_void_p(k.ctypes.data) for k in keep], C.c_void_p(out.ctypes.data)))
+        return out
+
+    def bsdf_eval(self, material: abi.rbr_material, wo, wi):
+        """(n, 6): f[3], pdf, isDelta, type bits."""
+        n = len(wo)
+        return self._unit(lambda h, a, b, o: self.lib.rbr_bsdf_eval_host(h, C.byref(material), n, a, b, o),
+                          [wo, wi], n, 6)
+
+    def bsdf_sample(self, material: abi.rbr_material, wo, u):
+        """(n, 8): wi[3], f[3], pdf, isDelta."""
+        n = len(wo)
+        return self._unit(lambda h, a, b, o: self.lib.rbr_bsdf_sample_host(h, C.byref(material), n, a, b, o),
+                          [wo, u], n, 8)
+
+    def light_sample(self, light: abi.rbr_light, points, u):
+        """(n, 9): wi[3], Li[3], pdf, distance, isDelta."""
+        n = len(points)
+        return self._unit(lambda h, a, b, o: self.lib.rbr_light_sample_host(h, C.byref(light), n, a, b, o),
+                          [points, u], n, 9)
+
+    def camera_rays(self, camera: abi.rbr_camera, samples):
+        """(n, 6): origin[3], direction[3]."""
+        n = len(samples)
+        return self._unit(lambda h, a, o: self.lib.rbr_camera_rays_host(h, C.byref(camera), n, a, o),
+                          [samples], n, 6)
+
+    def mis_weights(self, pdf_pairs):
+        n = len(pdf_pairs)
+        return self._unit(lambda h, a, o: self.lib.rbr_mis_weights_host(h, n, a, o), [pdf_pairs], n, 1)[:, 0]
 
     def render_stats(self) -> abi.rbr_render_stats:
         s = abi.rbr_render_stats()
