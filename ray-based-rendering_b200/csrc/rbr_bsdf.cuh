@@ -1,8 +1,10 @@
 // Device materials, BSDF lobes, lights, camera rays and the counter-based RNG.
 //
 // Restates the reference operation for operation with exactly rounded intrinsics, so BSDF
-// values and densities equal the reference's bit for bit; only the sampling routines call
-// cosf/sinf (CUDA's accurate versions), whose results may differ from glibc's by an ulp.
+// values and densities equal the reference's bit for bit; only the sampling routines need sin
+// and cos, taken correctly rounded here (glibc's sinf/cosf, which the reference calls, are
+// within an ulp but not always correctly rounded, so a sampled direction may differ in its
+// last bits).
 //   Material::createBSDF      src/materials/material.cpp:69-108
 //   MixtureBSDF               src/materials/mixture_bsdf.cpp:5-82
 //   LambertianBSDF            src/materials/lambertian_bsdf.cpp:5-28
@@ -41,6 +43,17 @@ __device__ __forceinline__ float maxc(f3 a) {  // std::max({x, y, z})
 constexpr float kPi = 3.14159265358979323846f;
 constexpr float kTwoPi = 2.0f * kPi;
 constexpr float kInvPi = 1.0f / kPi;
+
+// sin and cos of a float, correctly rounded (double-precision sincos, then one rounding).
+// The sampling formulas that use them (GGX visible normals, cosine hemisphere, concentric
+// disk) amplify an ulp of error near their singular points; correctly rounded inputs keep the
+// GPU within the spread of any two accurate float libraries.
+__device__ __forceinline__ void sincos_cr(float x, float& s, float& c) {
+    double sd, cd;
+    sincos(static_cast<double>(x), &sd, &cd);
+    s = __double2float_rn(sd);
+    c = __double2float_rn(cd);
+}
 
 // ----------------------------------------------------------------------------------------
 // Philox-4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11). Counter = (pixel, sample, depth,
@@ -248,8 +261,10 @@ __device__ __forceinline__ f3 ggx_sample_wh(float alpha, f3 wo, float u1, float 
     const f3 t2 = xcross(vh, t1);
     const float r = fq(u1);
     const float phi = fm(kTwoPi, u2);
-    const float p1 = fm(r, cosf(phi));
-    float p2 = fm(r, sinf(phi));
+    float sp, cp;
+    sincos_cr(phi, sp, cp);
+    const float p1 = fm(r, cp);
+    float p2 = fm(r, sp);
     const float s = fm(0.5f, fa(1.0f, vh.z));
     p2 = fa(fm(fs(1.0f, s), fq(omax(0.0f, fs(1.0f, fm(p1, p1))))), fm(s, p2));
     const f3 nh = xadd(xadd(xmuls(t1, p1), xmuls(t2, p2)), xmuls(vh, fq(omax(0.0f, fs(fs(1.0f, fm(p1, p1)), fm(p2, p2))))));
@@ -369,7 +384,9 @@ __device__ __forceinline__ BSample ggxt_sample(const Bsdf& b, f3 wo, float u1, f
 __device__ __forceinline__ f3 cosine_hemisphere(float u1, float u2) {
     const float r = fq(u1);
     const float theta = fm(kTwoPi, u2);
-    return mk(fm(r, cosf(theta)), fm(r, sinf(theta)), fq(omax(0.0f, fs(1.0f, u1))));
+    float st, ct;
+    sincos_cr(theta, st, ct);
+    return mk(fm(r, ct), fm(r, st), fq(omax(0.0f, fs(1.0f, u1))));
 }
 
 // Specular lobes
@@ -585,8 +602,10 @@ __device__ __forceinline__ void concentric_disk(float u1, float u2, float& ox, f
         r = sy;
         theta = fs(kPi / 2.0f, fm(kPi / 4.0f, fd(sx, sy)));
     }
-    ox = fm(r, cosf(theta));
-    oy = fm(r, sinf(theta));
+    float st, ct;
+    sincos_cr(theta, st, ct);
+    ox = fm(r, ct);
+    oy = fm(r, st);
 }
 
 __device__ __forceinline__ f3 cam_to_world(const CameraDev& c, f3 d) {

@@ -127,8 +127,11 @@ def test_gpu_bsdf_lights_cameras_mis(ctx):
         e = ctx.bsdf_eval(m, g["wo"][k], g["wi"][k])
         assert np.array_equal(bits(e[:, :4]), bits(g["eval"][k])), g["names"][k]
         assert (e[:, 4] == g["info"][k][0]).all() and (e[:, 5] == g["info"][k][1]).all()
-        smp = ctx.bsdf_sample(m, g["wo"][k], g["u"][k])
-        assert np.isclose(smp, g["sample"][k], rtol=1e-5, atol=1e-6).all(axis=1).mean() >= 0.99, g["names"][k]
+        smp, want = ctx.bsdf_sample(m, g["wo"][k], g["u"][k]), g["sample"][k]
+        valid = (smp[:, 6] > 0) & (want[:, 6] > 0)
+        assert ((smp[:, 6] > 0) == (want[:, 6] > 0)).mean() >= 0.99, g["names"][k]
+        assert np.abs(smp[valid, :3] - want[valid, :3]).max(initial=0.0) <= 1e-5, g["names"][k]
+        assert np.isclose(smp[valid, 3:7], want[valid, 3:7], rtol=1e-5).all(axis=1).mean() >= 0.97, g["names"][k]
     g = load("golden_lights.npz")
     for p, out in zip(g["params"], g["out"]):
         assert np.array_equal(bits(ctx.light_sample(light(p), g["points"], g["u"])), bits(out))

@@ -30,17 +30,35 @@ def test_bsdf_eval_pdf_bit_exact(ctx, reference, name, mat):
     assert (got[:, 4] == info[0]).all() and (got[:, 5] == info[1]).all(), "isDelta / type bits"
 
 
+def check_samples(ctx_or_none, reference, mat, wo, got, want, min_close=0.99):
+    """Well-posed comparison of BSDF::sample outputs (8 floats each) from two implementations
+    whose sin/cos may differ in the last bit:
+      - the same samples are valid (pdf > 0) on both sides, up to 0.1 %;
+      - sampled directions agree within 1e-5 (unit vectors);
+      - every non-delta GPU sample carries exactly (bit for bit) the reference's
+        evaluate() and pdf() at the GPU's own direction;
+      - f and pdf agree within 1e-5 relative for at least `min_close` of the samples (sharp GGX
+        lobes, alpha down to 1e-3, turn a 1e-7 change of direction into a large change of value:
+        two accurate CPU libraries disagree there too);
+      - delta samples are bit-exact."""
+    vg, vw = got[:, 6] > 0, want[:, 6] > 0
+    assert (vg == vw).mean() >= 0.999
+    both = vg & vw
+    assert np.abs(got[both, :3] - want[both, :3]).max(initial=0.0) <= 1e-5
+    nd = vg & (got[:, 7] == 0)
+    if nd.any():
+        f, pdf, _ = reference.bsdf_eval(mat, wo[nd], got[nd, :3])
+        assert np.array_equal(bits(got[nd, 3:6]), bits(f)) and np.array_equal(bits(got[nd, 6]), bits(pdf))
+    close = np.isclose(got[both, 3:7], want[both, 3:7], rtol=1e-5, atol=0.0).all(axis=1)
+    assert close.mean() >= min_close, f"{(~close).sum()} of {both.sum()} samples beyond 1e-5"
+    delta = both & (got[:, 7] == 1) & (want[:, 7] == 1)
+    assert np.array_equal(bits(got[delta]), bits(want[delta]))
+
+
 @pytest.mark.parametrize("name,mat", GRID, ids=[n for n, _ in GRID])
-def test_bsdf_sample_within_1e5(ctx, reference, name, mat):
+def test_bsdf_sample_matches_reference(ctx, reference, name, mat):
     wo, _, u = helpers.bsdf_inputs(8192, seed=hash(name) % 991)
-    got = ctx.bsdf_sample(mat, wo, u)
-    want = reference.bsdf_sample(mat, wo, u)
-    close = np.isclose(got, want, rtol=1e-5, atol=1e-6).all(axis=1)
-    # an ulp of cosf/sinf can flip a sample across a hemisphere test at grazing angles
-    assert close.mean() >= 0.999, f"{(~close).sum()} of {len(close)} samples differ; first {np.flatnonzero(~close)[:5]}"
-    exact = (bits(got) == bits(want)).all(axis=1)
-    if mat.metallic == 1.0 and mat.roughness == 0.0:  # delta lobes: no transcendental involved
-        assert exact.all()
+    check_samples(ctx, reference, mat, wo, ctx.bsdf_sample(mat, wo, u), reference.bsdf_sample(mat, wo, u))
 
 
 def test_light_samples_bit_exact(ctx, reference):
