@@ -131,7 +131,8 @@ def test_gpu_bsdf_lights_cameras_mis(ctx):
         valid = (smp[:, 6] > 0) & (want[:, 6] > 0)
         assert ((smp[:, 6] > 0) == (want[:, 6] > 0)).mean() >= 0.99, g["names"][k]
         assert np.abs(smp[valid, :3] - want[valid, :3]).max(initial=0.0) <= 1e-5, g["names"][k]
-        assert np.isclose(smp[valid, 3:7], want[valid, 3:7], rtol=1e-5).all(axis=1).mean() >= 0.97, g["names"][k]
+        if valid.any():
+            assert np.isclose(smp[valid, 3:7], want[valid, 3:7], rtol=1e-5).all(axis=1).mean() >= 0.97, g["names"][k]
     g = load("golden_lights.npz")
     for p, out in zip(g["params"], g["out"]):
         assert np.array_equal(bits(ctx.light_sample(light(p), g["points"], g["u"])), bits(out))

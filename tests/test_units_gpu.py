@@ -50,7 +50,8 @@ def check_samples(ctx_or_none, reference, mat, wo, got, want, min_close=0.99):
         f, pdf, _ = reference.bsdf_eval(mat, wo[nd], got[nd, :3])
         assert np.array_equal(bits(got[nd, 3:6]), bits(f)) and np.array_equal(bits(got[nd, 6]), bits(pdf))
     close = np.isclose(got[both, 3:7], want[both, 3:7], rtol=1e-5, atol=0.0).all(axis=1)
-    assert close.mean() >= min_close, f"{(~close).sum()} of {both.sum()} samples beyond 1e-5"
+    if both.any():  # materials without lobes (black, lights) produce no samples at all
+        assert close.mean() >= min_close, f"{(~close).sum()} of {both.sum()} samples beyond 1e-5"
     delta = both & (got[:, 7] == 1) & (want[:, 7] == 1)
     assert np.array_equal(bits(got[delta]), bits(want[delta]))
 
