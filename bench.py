@@ -49,6 +49,7 @@ def parse():
     p.add_argument("--workload", choices=["rays", "cornell", "ggx"], default="rays")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true", help="skip the host-buffer measurement (profiling runs)")
+    p.add_argument("--param", action="append", default=[], help="NAME=VALUE context tunable (rbr_param_set)")
     p.add_argument("--cpu-seconds", type=float, default=8.0, help="target length of the CPU-baseline sample")
     return p.parse_args()
 
@@ -335,11 +336,17 @@ def main():
     scene, rays = workload(rank)
     ctx = Context(local_rank)
     stats = ctx.upload(scene)
+    for kv in args.param:
+        k, v = kv.split("=")
+        ctx.set_param(k, int(v))
     n = len(rays)
     d_rays = torch.from_numpy(rays.view(np.uint8)).to(f"cuda:{local_rank}")
     d_hits = torch.empty(n * 8, dtype=torch.uint8, device=f"cuda:{local_rank}")
     stream = torch.cuda.current_stream()
     sp = stream.cuda_stream
+
+    tuned = ctx.autotune_trace(d_rays.data_ptr(), n) if not args.param else {k: ctx.get_param(k) for k in
+                                                                           ("trace.kernel", "trace.min_blocks")}
 
     def step():
         ctx.trace_closest_dev(d_rays.data_ptr(), n, d_hits.data_ptr(), sp)
@@ -428,6 +435,7 @@ def main():
             "cpu_baseline": base,
             "clocks": clk,
             "gpu_launches": args.steps,
+            "tuning": tuned,
             "bvh": {"wide_nodes": stats.num_wide_nodes, "leaf_records": stats.num_leaf_records,
                     "depth": stats.max_depth, "build_s": stats.build_seconds,
                     "device_mb": stats.device_bytes / 1e6},

@@ -209,6 +209,22 @@ const char* rbr_last_error(const rbr_ctx* ctx);
  * include/render/acceleration/accelerator.h:25). A rebuild drops the previous contents. */
 rbr_status rbr_scene_upload(rbr_ctx* ctx, const rbr_scene_desc* desc);
 rbr_status rbr_scene_stats_get(const rbr_ctx* ctx, rbr_scene_stats* out);
+
+/* Tunables of a context (no reference counterpart). Names:
+ *   "trace.kernel"         0: one thread per ray (default); 1: persistent warps that hand a
+ *                          finished lane the next ray of the warp's chunk; 2: warp-cooperative,
+ *                          8 lanes per ray, one child box per lane
+ *   "trace.blocks_per_sm"  resident blocks per SM of kernels 1 and 2 (0: occupancy limit)
+ *   "trace.min_blocks"     kernel 0's register budget: 8, 10 or 12 resident blocks per SM
+ *   "pt.wave_paths"        camera samples per path-tracer wave (default 2^22)
+ * Results do not depend on them; only speed and memory do. rbr_autotune picks them. */
+rbr_status rbr_param_set(rbr_ctx* ctx, const char* name, int64_t value);
+rbr_status rbr_param_get(const rbr_ctx* ctx, const char* name, int64_t* value);
+/* Autotuner (no reference counterpart): times every traversal variant ("trace.kernel",
+ * "trace.min_blocks") on n rays of the caller's own workload (device pointer) against the
+ * uploaded scene, keeps the fastest in the context and returns its time per launch in
+ * microseconds (out_us may be NULL). Waits for the timings. */
+rbr_status rbr_autotune_trace(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any_hit, int64_t* out_us);
 /* World bounds of the bounded primitives (Accelerator::worldBounds, accelerator.h:33).
  * An empty scene gives min = +FLT_MAX, max = -FLT_MAX (an empty BoundingBox). */
 rbr_status rbr_world_bounds(const rbr_ctx* ctx, float out_min[3], float out_max[3]);

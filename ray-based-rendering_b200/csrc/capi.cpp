@@ -97,6 +97,7 @@ rbr_status rbr_ctx_create(int device, rbr_ctx** out) {
         (e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess ||
         (e = cudaMalloc(reinterpret_cast<void**>(&ctx->d_error), sizeof(int))) != cudaSuccess ||
         (e = cudaMemset(ctx->d_error, 0, sizeof(int))) != cudaSuccess ||
+        (e = cudaMalloc(reinterpret_cast<void**>(&ctx->d_cursors), kCursorRing * sizeof(uint32_t))) != cudaSuccess ||
         (e = cudaEventCreate(&ctx->ev_start)) != cudaSuccess || (e = cudaEventCreate(&ctx->ev_stop)) != cudaSuccess) {
         cudaGetLastError();
         rbr_ctx_destroy(ctx);
@@ -115,6 +116,7 @@ void rbr_ctx_destroy(rbr_ctx* ctx) {
     release(ctx->stage_in);
     release(ctx->stage_out);
     if (ctx->d_error) cudaFree(ctx->d_error);
+    if (ctx->d_cursors) cudaFree(ctx->d_cursors);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
     if (ctx->ev_stop) cudaEventDestroy(ctx->ev_stop);
@@ -128,6 +130,46 @@ rbr_status rbr_scene_upload(rbr_ctx* ctx, const rbr_scene_desc* desc) {
     cudaSetDevice(ctx->device);
     cudaDeviceSynchronize();  // nothing may still read the scene being replaced
     return upload_scene(ctx, desc);
+}
+
+rbr_status rbr_param_set(rbr_ctx* ctx, const char* name, int64_t value) {
+    if (!ctx || !name) return RBR_ERR_INVALID_ARGUMENT;
+    const std::string n(name);
+    if (n == "trace.kernel") {
+        if (value < 0 || value > 2) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "trace.kernel is 0, 1 or 2");
+        ctx->trace_kernel = static_cast<int>(value);
+    } else if (n == "trace.blocks_per_sm") {
+        if (value < 0 || value > 32) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "trace.blocks_per_sm is 0..32");
+        ctx->trace_blocks_per_sm = static_cast<int>(value);
+    } else if (n == "trace.min_blocks") {
+        if (value != 8 && value != 10 && value != 12) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "trace.min_blocks is 8, 10 or 12");
+        ctx->trace_min_blocks = static_cast<int>(value);
+    } else if (n == "pt.wave_paths") {
+        if (value < 1024 || value > (int64_t(1) << 26)) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "pt.wave_paths is 1024..2^26");
+        ctx->pt_wave_paths = static_cast<uint32_t>(value);
+    } else {
+        return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "unknown parameter " + n);
+    }
+    return RBR_OK;
+}
+
+rbr_status rbr_autotune_trace(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any_hit, int64_t* out_us) {
+    if (!ctx) return RBR_ERR_INVALID_ARGUMENT;
+    if (!ctx->has_scene) return fail(ctx, RBR_ERR_NO_SCENE, "rbr_autotune_trace before rbr_scene_upload");
+    if (!rays || n == 0) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "rbr_autotune_trace needs rays");
+    cudaSetDevice(ctx->device);
+    return autotune_trace(ctx, rays, n, any_hit, out_us);
+}
+
+rbr_status rbr_param_get(const rbr_ctx* ctx, const char* name, int64_t* value) {
+    if (!ctx || !name || !value) return RBR_ERR_INVALID_ARGUMENT;
+    const std::string n(name);
+    if (n == "trace.kernel") *value = ctx->trace_kernel;
+    else if (n == "trace.blocks_per_sm") *value = ctx->trace_blocks_per_sm;
+    else if (n == "trace.min_blocks") *value = ctx->trace_min_blocks;
+    else if (n == "pt.wave_paths") *value = ctx->pt_wave_paths;
+    else return RBR_ERR_INVALID_ARGUMENT;
+    return RBR_OK;
 }
 
 rbr_status rbr_scene_stats_get(const rbr_ctx* ctx, rbr_scene_stats* out) {
@@ -152,8 +194,7 @@ rbr_status rbr_trace_closest(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, rbr_
     if (!ctx->has_scene) return fail(ctx, RBR_ERR_NO_SCENE, "rbr_trace_closest before rbr_scene_upload");
     if (n && (!rays || !hits)) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "rays or hits is NULL");
     cudaSetDevice(ctx->device);
-    const cudaError_t e = launch_trace_closest(ctx->scene, rays, n, hits, ctx->d_error, ctx->num_sms,
-                                               static_cast<cudaStream_t>(stream));
+    const cudaError_t e = launch_trace(ctx, rays, n, 0, hits, static_cast<cudaStream_t>(stream));
     return e == cudaSuccess ? RBR_OK : cuda_fail(ctx, e, "closest-hit launch");
 }
 
@@ -162,8 +203,7 @@ rbr_status rbr_trace_any(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, uint8_t*
     if (!ctx->has_scene) return fail(ctx, RBR_ERR_NO_SCENE, "rbr_trace_any before rbr_scene_upload");
     if (n && (!rays || !occluded)) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "rays or occluded is NULL");
     cudaSetDevice(ctx->device);
-    const cudaError_t e = launch_trace_any(ctx->scene, rays, n, occluded, ctx->d_error, ctx->num_sms,
-                                           static_cast<cudaStream_t>(stream));
+    const cudaError_t e = launch_trace(ctx, rays, n, 1, occluded, static_cast<cudaStream_t>(stream));
     return e == cudaSuccess ? RBR_OK : cuda_fail(ctx, e, "any-hit launch");
 }
 
@@ -181,12 +221,7 @@ rbr_status rbr_trace_host(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any
     cudaStream_t s = ctx->stream;
     cudaError_t e = cudaMemcpyAsync(ctx->stage_in.ptr, rays, in_bytes, cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "ray upload");
-    if (any_hit)
-        e = launch_trace_any(ctx->scene, static_cast<const rbr_ray*>(ctx->stage_in.ptr), n,
-                             static_cast<uint8_t*>(ctx->stage_out.ptr), ctx->d_error, ctx->num_sms, s);
-    else
-        e = launch_trace_closest(ctx->scene, static_cast<const rbr_ray*>(ctx->stage_in.ptr), n,
-                                 static_cast<rbr_hit*>(ctx->stage_out.ptr), ctx->d_error, ctx->num_sms, s);
+    e = launch_trace(ctx, static_cast<const rbr_ray*>(ctx->stage_in.ptr), n, any_hit, ctx->stage_out.ptr, s);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "trace launch");
     e = cudaMemcpyAsync(out, ctx->stage_out.ptr, out_bytes, cudaMemcpyDeviceToHost, s);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "hit download");

@@ -426,7 +426,7 @@ rbr_status render(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_params* 
     if (npix * spp > 0xFFFFFFFFull || spp > kDefaultCapacity)
         return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "more than 2^32 camera samples in one render call");
     const uint32_t nl = std::max(1u, ctx->scene.num_lights);
-    uint32_t cap = static_cast<uint32_t>(std::min<uint64_t>(npix * spp, kDefaultCapacity));
+    uint32_t cap = static_cast<uint32_t>(std::min<uint64_t>(npix * spp, std::max(ctx->pt_wave_paths, spp)));
     cap = std::min<uint64_t>(cap, kShadowBytesLimit / (48ull * nl));
     cap = std::max(spp, cap / spp * spp);
     rbr_status st = ensure_paths(ctx, cap, cap * nl);

@@ -49,6 +49,15 @@ struct rbr_ctx {
     rbr::DevBuf stage_in, stage_out;
     // device error word (rbr::kErr*)
     int* d_error = nullptr;
+    // work cursors of the persistent trace kernel: one per launch, taken round-robin so that
+    // launches overlapping on different streams never share one
+    uint32_t* d_cursors = nullptr;
+    uint32_t cursor_next = 0;
+    // tunables (rbr_param_set / rbr_autotune)
+    int trace_kernel = 0;          // 0: one thread per ray, 1: persistent lane refill, 2: warp-cooperative
+    int trace_blocks_per_sm = 0;   // persistent grid per SM (0: occupancy limit)
+    int trace_min_blocks = 10;     // kernel 0: register budget for 8, 10 or 12 resident blocks per SM
+    uint32_t pt_wave_paths = 1u << 22;
     // path tracer
     rbr::PathBuffers pt;
     rbr_render_stats last_render{};
@@ -74,6 +83,17 @@ cudaError_t launch_trace_any(const DeviceScene& s, const rbr_ray* rays, uint32_t
                              int num_sms, cudaStream_t stream);
 cudaError_t launch_trace_counts(const DeviceScene& s, const rbr_ray* rays, uint32_t n, int any_hit,
                                 unsigned long long* totals, int* err, cudaStream_t stream);
+cudaError_t launch_trace_persist(const DeviceScene& s, const rbr_ray* rays, uint32_t n, int any_hit, void* out,
+                                 int* err, uint32_t* cursor, int grid, cudaStream_t stream);
+int trace_persist_blocks_per_sm(int any_hit);
+cudaError_t launch_trace_coop(const DeviceScene& s, const rbr_ray* rays, uint32_t n, int any_hit, void* out, int* err,
+                              uint32_t* cursor, int grid, cudaStream_t stream);
+int trace_coop_blocks_per_sm(int any_hit);
+rbr_status autotune_trace(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any_hit, int64_t* chosen_us);
+constexpr int kCursorRing = 64;
+// Launches a ray query with the context's chosen kernel (closest hit into rbr_hit[n] or any
+// hit into uint8_t[n]).
+cudaError_t launch_trace(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any_hit, void* out, cudaStream_t stream);
 
 // path tracer (pt.cu)
 rbr_status render(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_params* p, float* film_mean, float* film_m2,

@@ -210,11 +210,12 @@ __device__ __forceinline__ void intersect_node(const uint4* __restrict__ nodes, 
         const float tf = fminf(fminf(tfx, tfy), tfz) * kTHi;
         if (tn <= tf && tn <= tbest) {
             if ((imask >> i) & 1u) {
+                // internal child: bit (slot ^ oct), so the highest set bit is nearest-first
                 cbits |= 1u << (24 + (static_cast<uint32_t>(i) ^ r.oct));
             } else {
+                // leaf: count in bits 5-7, first record offset in bits 0-4 (empty slots: 0)
                 const uint32_t meta = ((i < 4 ? meta_lo : meta_hi) >> (8 * (i & 3))) & 0xFFu;
-                const uint32_t cnt = meta >> 5;
-                pbits |= ((1u << cnt) - 1u) << (meta & 31u);
+                pbits |= ((1u << (meta >> 5)) - 1u) << (meta & 31u);
             }
         }
     }
@@ -294,6 +295,91 @@ __device__ __forceinline__ uint32_t traverse(const DeviceScene& s, f3 o, f3 d, f
     if (kAny) return 0u;
     thit = tbest;
     return best < 0 ? 0xFFFFFFFFu : static_cast<uint32_t>(best);
+}
+
+// ----------------------------------------------------------------------------------------
+// The same traversal as resumable steps, for persistent kernels that give a lane a new ray as
+// soon as its current one is done (so a warp does not idle behind its longest ray).
+// A step is one leaf-record test or one node test (after an optional stack pop).
+// ----------------------------------------------------------------------------------------
+struct TraceState {
+    RayCtx r;
+    float tbest;
+    int best;
+    uint2 ng, pg;
+    int sp;
+};
+
+// Starts a ray: planes, then the root node. Returns true if the ray is already complete
+// (any hit on a plane, or no BVH).
+template <bool kAny>
+__device__ __forceinline__ bool trace_begin(const DeviceScene& s, f3 o, f3 d, float tmax, TraceState& st,
+                                            uint32_t& anyhit) {
+    st.tbest = tmax;
+    st.best = -1;
+    anyhit = 0;
+    for (uint32_t i = 0; i < s.num_planes; ++i) {
+        const float4 pl = __ldg(s.planes + i);
+        const float t = hit_plane(o, d, mk(pl.x, pl.y, pl.z), pl.w, st.tbest);
+        if (t >= 0.0f) {
+            const uint32_t id = __ldg(s.plane_tags + i) & kIdMask;
+            if (kAny) {
+                anyhit = 1;
+                return true;
+            }
+            if (accept(t, id, st.tbest, st.best)) {
+                st.tbest = t;
+                st.best = static_cast<int>(id);
+            }
+        }
+    }
+    if (s.num_nodes == 0) return true;
+    st.r = make_ctx(o, d);
+    st.sp = 0;
+    intersect_node(s.nodes, 0, st.r, st.tbest, st.ng, st.pg);
+    return false;
+}
+
+// One step: the pending leaf records, then one node; returns true when the ray is complete.
+template <bool kAny>
+__device__ __forceinline__ bool trace_step(const DeviceScene& s, TraceState& st, uint2* stack, int* err,
+                                           uint32_t& anyhit) {
+    while (st.pg.y != 0) {
+        const int i = __ffs(st.pg.y) - 1;
+        st.pg.y &= st.pg.y - 1;
+        uint32_t tag;
+        const float t = hit_record(s.records, st.pg.x + i, st.r.o, st.r.d, st.tbest, tag);
+        if (t >= 0.0f) {
+            if (kAny) {
+                anyhit = 1;
+                return true;
+            }
+            const uint32_t id = tag & kIdMask;
+            if (accept(t, id, st.tbest, st.best)) {
+                st.tbest = t;
+                st.best = static_cast<int>(id);
+            }
+        }
+    }
+    if ((st.ng.y & 0xFF000000u) == 0) {
+        if (st.sp == 0) return true;
+        st.ng = stack[--st.sp];  // only non-empty groups are pushed
+    }
+    const int b = 31 - __clz(st.ng.y);
+    st.ng.y &= ~(1u << b);
+    const uint32_t slot = static_cast<uint32_t>(b - 24) ^ st.r.oct;
+    const uint32_t imask = (st.ng.y >> 16) & 0xFFu;
+    const uint32_t child = st.ng.x + __popc(imask & ((1u << slot) - 1u));
+    if (st.ng.y & 0xFF000000u) {
+        if (st.sp < kStackSize) {
+            stack[st.sp++] = st.ng;
+        } else {
+            atomicOr(err, kErrStackOverflow);
+            return true;
+        }
+    }
+    intersect_node(s.nodes, child, st.r, st.tbest, st.ng, st.pg);
+    return false;
 }
 
 }  // namespace rbr

@@ -12,8 +12,11 @@ namespace {
 
 constexpr int kTraceBlock = 128;
 
-__global__ void __launch_bounds__(kTraceBlock) k_trace_closest(DeviceScene s, const float4* __restrict__ rays,
-                                                               uint32_t n, uint2* __restrict__ hits, int* err) {
+// kMinBlocks: resident blocks per SM the register allocation must allow (8: up to 64
+// registers a thread, 10: 48, 12: 40) -- occupancy against register spills, picked by tuning.
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kTraceBlock, kMinBlocks) k_trace_closest(DeviceScene s, const float4* __restrict__ rays,
+                                                                           uint32_t n, uint2* __restrict__ hits, int* err) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float4 a = __ldg(rays + 2 * static_cast<size_t>(i));
@@ -56,7 +59,378 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_count(DeviceScene s, cons
     }
 }
 
+__device__ __forceinline__ uint32_t lane_mask_lt() {
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Persistent warps: each warp takes chunks of kChunk consecutive rays from a global cursor
+// (one atomic per chunk) and hands the next ray of its chunk to any lane whose ray is done,
+// so lanes keep working while the warp's other rays are still traversing. Every loop
+// iteration each active lane advances its ray by one step (a leaf-record test or a node test).
+constexpr int kPersistBlock = 128;
+constexpr uint32_t kChunk = 256;
+
+template <bool kAny>
+__global__ void __launch_bounds__(kPersistBlock) k_trace_persist(DeviceScene s, const float4* __restrict__ rays,
+                                                                 uint32_t n, uint2* __restrict__ hits,
+                                                                 uint8_t* __restrict__ occ, int* err,
+                                                                 uint32_t* cursor) {
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t chunk_next = 0, chunk_end = 0;  // warp-uniform
+    bool exhausted = false;                  // warp-uniform
+    uint32_t idx = 0xFFFFFFFFu;              // this lane's ray
+    uint32_t anyhit = 0;
+    TraceState st;
+    uint2 stack[kStackSize];
+    while (true) {
+        uint32_t need = __ballot_sync(0xFFFFFFFFu, idx == 0xFFFFFFFFu);
+        while (need != 0 && !exhausted) {
+            if (chunk_next == chunk_end) {
+                uint32_t b = 0;
+                if (lane == 0) b = atomicAdd(cursor, kChunk);
+                b = __shfl_sync(0xFFFFFFFFu, b, 0);
+                if (b >= n) {
+                    exhausted = true;
+                    break;
+                }
+                chunk_next = b;
+                chunk_end = min(b + kChunk, n);
+            }
+            const uint32_t avail = chunk_end - chunk_next;
+            const uint32_t rank = __popc(need & lane_mask_lt());
+            if (((need >> lane) & 1u) && rank < avail) {
+                idx = chunk_next + rank;
+                const float4 a = __ldg(rays + 2 * static_cast<size_t>(idx));
+                const float4 b = __ldg(rays + 2 * static_cast<size_t>(idx) + 1);
+                if (trace_begin<kAny>(s, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, st, anyhit)) {
+                    if (kAny) occ[idx] = static_cast<uint8_t>(anyhit);
+                    else hits[idx] = make_uint2(st.best < 0 ? 0xFFFFFFFFu : static_cast<uint32_t>(st.best),
+                                                st.best < 0 ? 0u : __float_as_uint(st.tbest));
+                    idx = 0xFFFFFFFFu;  // finished at once: takes another ray in this round
+                }
+            }
+            chunk_next += min(__popc(need), avail);  // each round consumes at least one ray
+            need = __ballot_sync(0xFFFFFFFFu, idx == 0xFFFFFFFFu);
+        }
+        const bool active = idx != 0xFFFFFFFFu;
+        if (__ballot_sync(0xFFFFFFFFu, active) == 0) break;  // only when the rays are exhausted
+        if (active && trace_step<kAny>(s, st, stack, err, anyhit)) {
+            if (kAny) occ[idx] = static_cast<uint8_t>(anyhit);
+            else hits[idx] = make_uint2(st.best < 0 ? 0xFFFFFFFFu : static_cast<uint32_t>(st.best),
+                                        st.best < 0 ? 0u : __float_as_uint(st.tbest));
+            idx = 0xFFFFFFFFu;
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Warp-cooperative traversal: a group of 8 lanes traces one ray (4 rays per warp). In a node
+// step lane j tests child slot j of the node and the group combines the results with a ballot
+// (internal children) and an OR-shuffle (leaf records); in a leaf step the lanes test up to 8
+// of the node's leaf records at once and keep the closest with a shuffle min-reduction
+// (key = t bits, then the highest id). Group state is replicated in the 8 lanes, so the group
+// never diverges internally; the short stack lives in shared memory (all 8 lanes write the
+// same entry and read back their own write, so no cross-lane synchronisation is needed).
+// ------------------------------------------------------------------------------------------
+constexpr int kCoopBlock = 128;
+constexpr int kCoopGroups = kCoopBlock / 8;
+
+__device__ __forceinline__ uint32_t nth_set_bit(uint32_t m, int n) {  // n-th (0-based) set bit, or 32
+    for (int k = 0; k < n && m; ++k) m &= m - 1;
+    return m ? static_cast<uint32_t>(__ffs(m) - 1) : 32u;
+}
+
+template <bool kAny>
+__global__ void __launch_bounds__(kCoopBlock) k_trace_coop(DeviceScene s, const float4* __restrict__ rays, uint32_t n,
+                                                           uint2* __restrict__ hits, uint8_t* __restrict__ occ,
+                                                           int* err, uint32_t* cursor) {
+    __shared__ uint2 sstack[kCoopGroups][kStackSize];
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t j = lane & 7u;             // slot / record lane within the group
+    const uint32_t g = lane >> 3;             // group within the warp
+    const uint32_t gmask = 0xFFu << (8 * g);  // the group's lanes
+    uint2* stack = sstack[threadIdx.x >> 3];
+    uint32_t chunk_next = 0, chunk_end = 0;   // warp-uniform
+    bool exhausted = false;                   // warp-uniform
+    uint32_t idx = 0xFFFFFFFFu;               // group-uniform
+    RayCtx r;
+    float tbest = 0.0f;
+    int best = -1;
+    uint2 ng = make_uint2(0, 0), pg = make_uint2(0, 0);
+    int sp = 0;
+    while (true) {
+        // give idle groups new rays from the warp's chunk
+        uint32_t need = __ballot_sync(0xFFFFFFFFu, j == 0 && idx == 0xFFFFFFFFu);
+        while (need != 0 && !exhausted) {
+            if (chunk_next == chunk_end) {
+                uint32_t b = 0;
+                if (lane == 0) b = atomicAdd(cursor, kChunk);
+                b = __shfl_sync(0xFFFFFFFFu, b, 0);
+                if (b >= n) {
+                    exhausted = true;
+                    break;
+                }
+                chunk_next = b;
+                chunk_end = min(b + kChunk, n);
+            }
+            const uint32_t avail = chunk_end - chunk_next;
+            const uint32_t rank = __popc(need & ((1u << (8 * g)) - 1u));
+            if (((need >> (8 * g)) & 1u) && rank < avail) {
+                idx = chunk_next + rank;
+                const float4 a = __ldg(rays + 2 * static_cast<size_t>(idx));
+                const float4 b = __ldg(rays + 2 * static_cast<size_t>(idx) + 1);
+                const f3 o = mk(a.x, a.y, a.z), d = mk(b.x, b.y, b.z);
+                tbest = a.w;
+                best = -1;
+                bool done = false;
+                for (uint32_t i = 0; i < s.num_planes && !done; ++i) {
+                    const float4 pl = __ldg(s.planes + i);
+                    const float t = hit_plane(o, d, mk(pl.x, pl.y, pl.z), pl.w, tbest);
+                    if (t >= 0.0f) {
+                        const uint32_t id = __ldg(s.plane_tags + i) & kIdMask;
+                        if (kAny) done = true;
+                        else if (accept(t, id, tbest, best)) {
+                            tbest = t;
+                            best = static_cast<int>(id);
+                        }
+                    }
+                }
+                if (kAny && done) {
+                    if (j == 0) occ[idx] = 1;
+                    idx = 0xFFFFFFFFu;
+                } else if (s.num_nodes == 0) {
+                    if (j == 0) {
+                        if (kAny) occ[idx] = 0;
+                        else hits[idx] = make_uint2(best < 0 ? 0xFFFFFFFFu : static_cast<uint32_t>(best),
+                                                    best < 0 ? 0u : __float_as_uint(tbest));
+                    }
+                    idx = 0xFFFFFFFFu;
+                } else {
+                    r = make_ctx(o, d);
+                    sp = 0;
+                    pg = make_uint2(0, 0);
+                    // a pseudo node group whose only child is the root (slot 0, internal)
+                    ng = make_uint2(0u, (1u << (24 + (0u ^ r.oct))) | (1u << 16));
+                }
+            }
+            chunk_next += min(__popc(need), avail);
+            need = __ballot_sync(0xFFFFFFFFu, j == 0 && idx == 0xFFFFFFFFu);
+        }
+        if (__ballot_sync(0xFFFFFFFFu, idx != 0xFFFFFFFFu) == 0) break;  // rays exhausted
+        if (idx == 0xFFFFFFFFu) continue;
+        bool finished = false;
+        uint32_t anyres = 0;
+        if (pg.y != 0) {
+            // leaf step: up to 8 records at once
+            const uint32_t bit = nth_set_bit(pg.y, static_cast<int>(j));
+            unsigned long long key = ~0ull;
+            if (bit < 32) {
+                uint32_t tag;
+                const float t = hit_record(s.records, pg.x + bit, r.o, r.d, tbest, tag);
+                if (t >= 0.0f) key = (static_cast<unsigned long long>(__float_as_uint(t)) << 32) | (~(tag & kIdMask));
+            }
+            if (kAny) {
+                if (__ballot_sync(gmask, key != ~0ull) != 0) {
+                    finished = true;
+                    anyres = 1;
+                }
+            } else {
+                for (int off = 1; off < 8; off <<= 1) {
+                    const unsigned long long o2 = __shfl_xor_sync(gmask, key, off, 8);
+                    key = o2 < key ? o2 : key;
+                }
+                if (key != ~0ull) {
+                    const float t = __uint_as_float(static_cast<uint32_t>(key >> 32));
+                    const uint32_t id = ~static_cast<uint32_t>(key) & kIdMask;
+                    if (accept(t, id, tbest, best)) {
+                        tbest = t;
+                        best = static_cast<int>(id);
+                    }
+                }
+            }
+            // drop the (up to) 8 records just tested (record bits occupy bits 0-23)
+            pg.y = __popc(pg.y) <= 8 ? 0u : pg.y & ~((2u << nth_set_bit(pg.y, 7)) - 1u);
+        } else {
+            // node step (after a pop if the current group is exhausted)
+            if ((ng.y & 0xFF000000u) == 0) {
+                if (sp == 0) {
+                    finished = true;
+                } else {
+                    ng = stack[--sp];
+                }
+            }
+            if (!finished) {
+                const int b = 31 - __clz(ng.y);
+                ng.y &= ~(1u << b);
+                const uint32_t slot = static_cast<uint32_t>(b - 24) ^ r.oct;
+                const uint32_t imask_p = (ng.y >> 16) & 0xFFu;
+                const uint32_t child = ng.x + __popc(imask_p & ((1u << slot) - 1u));
+                if (ng.y & 0xFF000000u) {
+                    if (sp < kStackSize) stack[sp++] = ng;
+                    else atomicOr(err, kErrStackOverflow);
+                }
+                const uint4* np = s.nodes + 5 * static_cast<size_t>(child);
+                const uint4 w0 = __ldg(np), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3),
+                            w4 = __ldg(np + 4);
+                const float sx = __uint_as_float((w0.w & 0xFFu) << 23);
+                const float sy = __uint_as_float(((w0.w >> 8) & 0xFFu) << 23);
+                const float sz = __uint_as_float(((w0.w >> 16) & 0xFFu) << 23);
+                const uint32_t imask = w0.w >> 24;
+                const int jj = static_cast<int>(j);
+                const uint2 qlox = make_uint2(w2.x, w2.y), qloy = make_uint2(w2.z, w2.w), qloz = make_uint2(w3.x, w3.y);
+                const uint2 qhix = make_uint2(w3.z, w3.w), qhiy = make_uint2(w4.x, w4.y), qhiz = make_uint2(w4.z, w4.w);
+                const float lx = qbyte(qlox, jj), hx = qbyte(qhix, jj);
+                const float ly = qbyte(qloy, jj), hy = qbyte(qhiy, jj);
+                const float lz = qbyte(qloz, jj), hz = qbyte(qhiz, jj);
+                const float ax = sx * r.ix, ay = sy * r.iy, az = sz * r.iz;
+                const float bx = (__uint_as_float(w0.x) - r.o.x) * r.ix;
+                const float by = (__uint_as_float(w0.y) - r.o.y) * r.iy;
+                const float bz = (__uint_as_float(w0.z) - r.o.z) * r.iz;
+                const float tnx = fmaf(r.nx ? hx : lx, ax, bx), tfx = fmaf(r.nx ? lx : hx, ax, bx);
+                const float tny = fmaf(r.ny ? hy : ly, ay, by), tfy = fmaf(r.ny ? ly : hy, ay, by);
+                const float tnz = fmaf(r.nz ? hz : lz, az, bz), tfz = fmaf(r.nz ? lz : hz, az, bz);
+                const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f)) * kTLo;
+                const float tf = fminf(fminf(tfx, tfy), tfz) * kTHi;
+                const bool hit = tn <= tf && tn <= tbest;
+                const uint32_t hm = (__ballot_sync(gmask, hit) >> (8 * g)) & 0xFFu;
+                uint32_t ih = hm & imask;
+                if (r.oct & 1u) ih = ((ih & 0x55u) << 1) | ((ih >> 1) & 0x55u);
+                if (r.oct & 2u) ih = ((ih & 0x33u) << 2) | ((ih >> 2) & 0x33u);
+                if (r.oct & 4u) ih = ((ih & 0x0Fu) << 4) | ((ih >> 4) & 0x0Fu);
+                const uint32_t meta = ((j < 4 ? w1.z : w1.w) >> (8 * (j & 3))) & 0xFFu;
+                uint32_t lb = hit ? ((1u << (meta >> 5)) - 1u) << (meta & 31u) : 0u;  // 0 for internal/empty
+                lb |= __shfl_xor_sync(gmask, lb, 1, 8);
+                lb |= __shfl_xor_sync(gmask, lb, 2, 8);
+                lb |= __shfl_xor_sync(gmask, lb, 4, 8);
+                ng = make_uint2(w1.x, (ih << 24) | (imask << 16));
+                pg = make_uint2(w1.y, lb);
+            }
+        }
+        if (finished) {
+            if (j == 0) {
+                if (kAny) occ[idx] = static_cast<uint8_t>(anyres);
+                else hits[idx] = make_uint2(best < 0 ? 0xFFFFFFFFu : static_cast<uint32_t>(best),
+                                            best < 0 ? 0u : __float_as_uint(tbest));
+            }
+            idx = 0xFFFFFFFFu;
+        }
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_trace_coop(const DeviceScene& s, const rbr_ray* rays, uint32_t n, int any_hit, void* out, int* err,
+                              uint32_t* cursor, int grid, cudaStream_t stream) {
+    if (n == 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(cursor, 0, sizeof(uint32_t), stream);
+    if (e != cudaSuccess) return e;
+    const auto* r = reinterpret_cast<const float4*>(rays);
+    if (any_hit)
+        k_trace_coop<true><<<grid, kCoopBlock, 0, stream>>>(s, r, n, nullptr, static_cast<uint8_t*>(out), err, cursor);
+    else
+        k_trace_coop<false><<<grid, kCoopBlock, 0, stream>>>(s, r, n, static_cast<uint2*>(out), nullptr, err, cursor);
+    return cudaGetLastError();
+}
+
+int trace_coop_blocks_per_sm(int any_hit) {
+    int b = 0;
+    if (any_hit) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_trace_coop<true>, kCoopBlock, 0);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_trace_coop<false>, kCoopBlock, 0);
+    return b > 0 ? b : 1;
+}
+
+cudaError_t launch_trace_persist(const DeviceScene& s, const rbr_ray* rays, uint32_t n, int any_hit, void* out,
+                                 int* err, uint32_t* cursor, int grid, cudaStream_t stream) {
+    if (n == 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(cursor, 0, sizeof(uint32_t), stream);
+    if (e != cudaSuccess) return e;
+    const auto* r = reinterpret_cast<const float4*>(rays);
+    if (any_hit)
+        k_trace_persist<true><<<grid, kPersistBlock, 0, stream>>>(s, r, n, nullptr, static_cast<uint8_t*>(out), err,
+                                                                  cursor);
+    else
+        k_trace_persist<false><<<grid, kPersistBlock, 0, stream>>>(s, r, n, static_cast<uint2*>(out), nullptr, err,
+                                                                   cursor);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_trace(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any_hit, void* out, cudaStream_t stream) {
+    if (ctx->trace_kernel == 0) {
+        return any_hit ? launch_trace_any(ctx->scene, rays, n, static_cast<uint8_t*>(out), ctx->d_error, ctx->trace_min_blocks,
+                                          stream)
+                       : launch_trace_closest(ctx->scene, rays, n, static_cast<rbr_hit*>(out), ctx->d_error,
+                                              ctx->trace_min_blocks, stream);
+    }
+    const bool coop = ctx->trace_kernel == 2;
+    const int per_sm = ctx->trace_blocks_per_sm > 0
+                           ? ctx->trace_blocks_per_sm
+                           : (coop ? trace_coop_blocks_per_sm(any_hit) : trace_persist_blocks_per_sm(any_hit));
+    // no more warps than there are chunks of rays
+    const int need = static_cast<int>((n + kChunk - 1) / kChunk + (kPersistBlock / 32) - 1) / (kPersistBlock / 32);
+    const int grid = std::max(1, std::min(ctx->num_sms * per_sm, need));
+    uint32_t* cursor = ctx->d_cursors + (ctx->cursor_next++ % kCursorRing);
+    if (coop) return launch_trace_coop(ctx->scene, rays, n, any_hit, out, ctx->d_error, cursor, grid, stream);
+    return launch_trace_persist(ctx->scene, rays, n, any_hit, out, ctx->d_error, cursor, grid, stream);
+}
+
+// Times every traversal variant on the caller's rays (device pointer) and keeps the fastest.
+rbr_status autotune_trace(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any_hit, int64_t* chosen_ms_x1000) {
+    struct Cand {
+        int kernel, min_blocks, per_sm;
+    };
+    const Cand cands[] = {{0, 8, 0}, {0, 10, 0}, {0, 12, 0}, {1, 10, 0}, {2, 10, 0}};
+    rbr_status st = ensure(ctx, ctx->stage_out, size_t(n) * (any_hit ? 1 : sizeof(rbr_hit)), "autotune output");
+    if (st != RBR_OK) return st;
+    const Cand saved{ctx->trace_kernel, ctx->trace_min_blocks, ctx->trace_blocks_per_sm};
+    float best_ms = 1e30f;
+    Cand best = saved;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    for (const Cand& c : cands) {
+        ctx->trace_kernel = c.kernel;
+        ctx->trace_min_blocks = c.min_blocks;
+        ctx->trace_blocks_per_sm = c.per_sm;
+        cudaError_t e = launch_trace(ctx, rays, n, any_hit, ctx->stage_out.ptr, ctx->stream);  // warm-up
+        float ms = 0.0f, total = 0.0f;
+        for (int k = 0; k < 3 && e == cudaSuccess; ++k) {
+            cudaEventRecord(a, ctx->stream);
+            e = launch_trace(ctx, rays, n, any_hit, ctx->stage_out.ptr, ctx->stream);
+            cudaEventRecord(b, ctx->stream);
+            cudaEventSynchronize(b);
+            cudaEventElapsedTime(&ms, a, b);
+            total += ms;
+        }
+        if (e != cudaSuccess) {
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+            ctx->trace_kernel = saved.kernel;
+            ctx->trace_min_blocks = saved.min_blocks;
+            ctx->trace_blocks_per_sm = saved.per_sm;
+            return cuda_fail(ctx, e, "autotune launch");
+        }
+        if (total < best_ms) {
+            best_ms = total;
+            best = c;
+        }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    ctx->trace_kernel = best.kernel;
+    ctx->trace_min_blocks = best.min_blocks;
+    ctx->trace_blocks_per_sm = best.per_sm;
+    if (chosen_ms_x1000) *chosen_ms_x1000 = static_cast<int64_t>(best_ms / 3.0f * 1000.0f);
+    return check_device_error(ctx, ctx->stream);
+}
+
+int trace_persist_blocks_per_sm(int any_hit) {
+    int b = 0;
+    if (any_hit) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_trace_persist<true>, kPersistBlock, 0);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_trace_persist<false>, kPersistBlock, 0);
+    return b > 0 ? b : 1;
+}
 
 cudaError_t launch_trace_counts(const DeviceScene& s, const rbr_ray* rays, uint32_t n, int any_hit,
                                 unsigned long long* totals, int* err, cudaStream_t stream) {
@@ -70,11 +444,14 @@ cudaError_t launch_trace_counts(const DeviceScene& s, const rbr_ray* rays, uint3
 }
 
 cudaError_t launch_trace_closest(const DeviceScene& s, const rbr_ray* rays, uint32_t n, rbr_hit* hits, int* err,
-                                 int /*num_sms*/, cudaStream_t stream) {
+                                 int min_blocks, cudaStream_t stream) {
     if (n == 0) return cudaSuccess;
     const uint32_t blocks = (n + kTraceBlock - 1) / kTraceBlock;
-    k_trace_closest<<<blocks, kTraceBlock, 0, stream>>>(s, reinterpret_cast<const float4*>(rays), n,
-                                                        reinterpret_cast<uint2*>(hits), err);
+    const auto* r = reinterpret_cast<const float4*>(rays);
+    auto* h = reinterpret_cast<uint2*>(hits);
+    if (min_blocks >= 12) k_trace_closest<12><<<blocks, kTraceBlock, 0, stream>>>(s, r, n, h, err);
+    else if (min_blocks >= 10) k_trace_closest<10><<<blocks, kTraceBlock, 0, stream>>>(s, r, n, h, err);
+    else k_trace_closest<8><<<blocks, kTraceBlock, 0, stream>>>(s, r, n, h, err);
     return cudaGetLastError();
 }
 

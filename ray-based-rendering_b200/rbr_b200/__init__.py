@@ -65,6 +65,9 @@ def load_library() -> C.CDLL:
         "rbr_light_sample_host": (C.c_int, [P, C.POINTER(abi.rbr_light), C.c_uint32, P, P, P]),
         "rbr_camera_rays_host": (C.c_int, [P, C.POINTER(abi.rbr_camera), C.c_uint32, P, P]),
         "rbr_mis_weights_host": (C.c_int, [P, C.c_uint32, P, P]),
+        "rbr_param_set": (C.c_int, [P, C.c_char_p, C.c_int64]),
+        "rbr_param_get": (C.c_int, [P, C.c_char_p, C.POINTER(C.c_int64)]),
+        "rbr_autotune_trace": (C.c_int, [P, P, C.c_uint32, C.c_int, C.POINTER(C.c_int64)]),
     }
     for name, (res, args) in sig.items():
         if hasattr(lib, name):
@@ -129,6 +132,21 @@ class Context:
 
     def upload_raw(self, desc: abi.rbr_scene_desc) -> int:
         return self.lib.rbr_scene_upload(self.h, C.byref(desc))
+
+    def set_param(self, name: str, value: int):
+        self._check(self.lib.rbr_param_set(self.h, name.encode(), int(value)))
+
+    def get_param(self, name: str) -> int:
+        v = C.c_int64()
+        self._check(self.lib.rbr_param_get(self.h, name.encode(), C.byref(v)))
+        return int(v.value)
+
+    def autotune_trace(self, rays_ptr: int, n: int, any_hit: bool = False) -> dict:
+        """Times the traversal variants on these device rays; keeps the fastest. Returns the choice."""
+        us = C.c_int64()
+        self._check(self.lib.rbr_autotune_trace(self.h, C.c_void_p(rays_ptr), n, int(any_hit), C.byref(us)))
+        return {"trace.kernel": self.get_param("trace.kernel"), "trace.min_blocks": self.get_param("trace.min_blocks"),
+                "us_per_launch": us.value}
 
     def last_error(self) -> str:
         return self.lib.rbr_last_error(self.h).decode()
