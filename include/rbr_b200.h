@@ -285,6 +285,96 @@ rbr_status rbr_camera_rays_host(rbr_ctx* ctx, const rbr_camera* camera, uint32_t
 /* sampling::powerHeuristic(1, pdf_pairs[2i], 1, pdf_pairs[2i+1]) (sampler.h:137-149). */
 rbr_status rbr_mis_weights_host(rbr_ctx* ctx, uint32_t n, const float* pdf_pairs, float* out);
 
+/* ------------------------------------------------------------------------------------------
+ * Learned radiance cache (no reference counterpart): a multiresolution hash-grid encoding
+ * (16 levels x 2^log2_table_size entries x 2 FP16 features) of the surface position, plus
+ * the outgoing direction, shading normal, roughness and diffuse/specular albedo, feeding a
+ * 64-wide MLP of five BF16 weight matrices (64x64 x4, then 64->3 padded to 16 outputs, ReLU
+ * between them, no biases; a constant-1 input stands in for the first layer's bias) that
+ * predicts the outgoing radiance at a path vertex. Inference, the backward pass and Adam run
+ * in the library's own kernels, the matrix products on the tensor cores (tcgen05, FP32
+ * accumulation in tensor memory). Trained online, with the relative L2 loss
+ * mean((y - t)^2 / (y^2 + 0.01)) (y held constant in the denominator), on the radiance that
+ * training paths of the path tracer gather past each vertex.
+ * ------------------------------------------------------------------------------------------ */
+#define RBR_CACHE_LEVELS 16
+#define RBR_CACHE_FEATURES 2
+#define RBR_CACHE_INPUTS 64
+#define RBR_CACHE_MLP_WEIGHTS (4 * 64 * 64 + 16 * 64) /* W0..W3 (64x64), W4 (16x64), row = output */
+#define RBR_CACHE_RECORD_FLOATS 16
+
+/* One cache query / training vertex (16 floats): world position[3], direction[3] (towards
+ * the viewer, -ray.direction), ray-facing shading normal[3], roughness, diffuse albedo[3],
+ * specular albedo[3]. */
+typedef struct rbr_cache_record {
+    float position[3];
+    float direction[3];
+    float normal[3];
+    float roughness;
+    float diffuse[3];
+    float specular[3];
+} rbr_cache_record;
+
+typedef struct rbr_cache_config {
+    int32_t log2_table_size;    /* hash-table entries per level = 2^this (default 19) */
+    int32_t min_resolution;     /* grid resolution of level 0 (default 16) */
+    int32_t max_resolution;     /* grid resolution of level 15 (default 2048) */
+    float learning_rate;        /* Adam (default 1e-2) */
+    float beta1, beta2, epsilon;/* Adam (0.9, 0.99, 1e-15) */
+    uint32_t train_batch;       /* samples per optimiser step (default 16384) */
+    uint32_t train_steps;       /* optimiser steps per rendered frame (default 4) */
+    uint32_t train_paths;       /* training paths per rendered frame (default 65536) */
+    uint32_t termination_depth; /* first vertex depth a path may end into the cache (default 1) */
+    uint64_t seed;              /* initial weights */
+    float bounds_min[3];        /* box the hash grid covers; min >= max on any axis: the */
+    float bounds_max[3];        /* scene's bounded geometry, enlarged by 1% */
+} rbr_cache_config;
+
+typedef struct rbr_cache_info {
+    uint32_t levels, table_size;
+    uint32_t resolution[RBR_CACHE_LEVELS];
+    uint32_t dense_levels;       /* bit l: level l is indexed densely ((res+1)^3 <= table_size) */
+    uint32_t optimiser_steps;    /* Adam steps taken */
+    float bounds_min[3], bounds_max[3];
+    float last_loss;             /* training loss of the last optimiser step (rbr_cache_render) */
+    uint32_t last_queries;       /* paths ended into the cache by the last frame */
+    uint32_t last_train_records; /* training vertices gathered by the last frame */
+} rbr_cache_info;
+
+void rbr_cache_config_default(rbr_cache_config* out);
+/* Creates (or re-creates) the context's cache with seeded initial parameters: Xavier-uniform
+ * MLP weights, hash features uniform in [-1e-4, 1e-4]. Needs a scene unless the config gives
+ * bounds. */
+rbr_status rbr_cache_create(rbr_ctx* ctx, const rbr_cache_config* config);
+void rbr_cache_destroy(rbr_ctx* ctx);
+rbr_status rbr_cache_info_get(rbr_ctx* ctx, rbr_cache_info* out);
+/* Parameters as 16-bit words: mlp = RBR_CACHE_MLP_WEIGHTS BF16 values, grid = levels x
+ * table_size x 2 FP16 values (NULL to leave / skip). Setting also resets Adam's state. */
+rbr_status rbr_cache_set_params(rbr_ctx* ctx, const uint16_t* mlp_bf16, const uint16_t* grid_f16);
+rbr_status rbr_cache_get_params(rbr_ctx* ctx, uint16_t* mlp_bf16, uint16_t* grid_f16);
+/* The FP32 gradient accumulators left by the last rbr_cache_train_host(apply = 0) call:
+ * mlp = RBR_CACHE_MLP_WEIGHTS floats, grid = levels x table_size x 2 floats (NULL to skip). */
+rbr_status rbr_cache_grads_get(rbr_ctx* ctx, float* mlp, float* grid);
+/* Unit entry points on host buffers (each waits): the 64 network inputs of n records before
+ * their BF16 rounding; the cache's prediction (RGB) for n records; one optimiser step on n
+ * (record, target RGB) pairs (apply = 0: gradients only, kept for rbr_cache_grads_get).
+ * loss (may be NULL) receives the mean relative L2 loss of the batch. */
+rbr_status rbr_cache_encode_host(rbr_ctx* ctx, uint32_t n, const rbr_cache_record* records, float* inputs);
+rbr_status rbr_cache_infer_host(rbr_ctx* ctx, uint32_t n, const rbr_cache_record* records, float* rgb);
+rbr_status rbr_cache_train_host(rbr_ctx* ctx, uint32_t n, const rbr_cache_record* records, const float* targets,
+                                int apply, float* loss);
+/* Renders `frames` frames of params->samples_per_pixel samples each with the radiance cache:
+ * a path ends into the cache at its first vertex of depth >= termination_depth reached by a
+ * non-delta bounce on a non-delta material (its emission there is still added, then the
+ * throughput times the cache's prediction replaces everything further), except about
+ * train_paths paths per frame, which continue as the plain path tracer does and whose
+ * vertices, with the radiance gathered past each of them, train the cache for train_steps
+ * Adam steps after the frame. Frame f uses samples sample_offset + f*spp ... ; film_mean
+ * (device) receives the mean over all frames, film_m2 (device or NULL, with
+ * RBR_RENDER_SECOND_MOMENT) the sum of squared sample values. Asynchronous on `stream`. */
+rbr_status rbr_cache_render(rbr_ctx* ctx, const rbr_camera* camera, const rbr_render_params* params,
+                            uint32_t frames, int train, float* film_mean, float* film_m2, void* stream);
+
 /* Size of the fixed scratch array used by rbr_render_noalloc (16 MiB). */
 #define RBR_NOALLOC_SCRATCH_BYTES (16u << 20)
 

@@ -53,6 +53,10 @@ rbr_status check_device_error(rbr_ctx* ctx, cudaStream_t stream) {
     std::string what;
     if (h & kErrStackOverflow) what += " traversal-stack overflow;";
     if (h & kErrQueueOverflow) what += " queue overflow;";
+    if (h & kErrDeviceTimeout) {
+        what += " bounded wait for tensor-core completion ran out;";
+        return fail(ctx, RBR_ERR_DEVICE_TIMEOUT, "device check failed:" + what);
+    }
     return fail(ctx, RBR_ERR_INTERNAL, "device check failed:" + what);
 }
 
@@ -76,6 +80,9 @@ size_t rbr_struct_size(const char* name) {
     if (n == "rbr_camera") return sizeof(rbr_camera);
     if (n == "rbr_render_params") return sizeof(rbr_render_params);
     if (n == "rbr_render_stats") return sizeof(rbr_render_stats);
+    if (n == "rbr_cache_record") return sizeof(rbr_cache_record);
+    if (n == "rbr_cache_config") return sizeof(rbr_cache_config);
+    if (n == "rbr_cache_info") return sizeof(rbr_cache_info);
     return 0;
 }
 
@@ -113,6 +120,7 @@ void rbr_ctx_destroy(rbr_ctx* ctx) {
     cudaDeviceSynchronize();
     free_scene(ctx);
     free_path_buffers(ctx);
+    cache_destroy(ctx);
     release(ctx->stage_in);
     release(ctx->stage_out);
     if (ctx->d_error) cudaFree(ctx->d_error);
@@ -294,6 +302,76 @@ rbr_status rbr_render_stats_get(rbr_ctx* ctx, rbr_render_stats* out) {
     }
     *out = ctx->last_render;
     return RBR_OK;
+}
+
+// ---- radiance cache ----------------------------------------------------------------------
+void rbr_cache_config_default(rbr_cache_config* out) {
+    if (out) cache_config_default(out);
+}
+
+rbr_status rbr_cache_create(rbr_ctx* ctx, const rbr_cache_config* config) {
+    if (!ctx) return RBR_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(ctx->device);
+    cudaDeviceSynchronize();  // nothing may still use the cache being replaced
+    return cache_create(ctx, config);
+}
+
+void rbr_cache_destroy(rbr_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    cudaDeviceSynchronize();
+    cache_destroy(ctx);
+}
+
+rbr_status rbr_cache_info_get(rbr_ctx* ctx, rbr_cache_info* out) {
+    if (!ctx || !out) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "NULL argument");
+    cudaSetDevice(ctx->device);
+    return cache_info(ctx, out);
+}
+
+rbr_status rbr_cache_set_params(rbr_ctx* ctx, const uint16_t* mlp_bf16, const uint16_t* grid_f16) {
+    if (!ctx) return RBR_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(ctx->device);
+    cudaDeviceSynchronize();
+    return cache_set_params(ctx, mlp_bf16, grid_f16);
+}
+
+rbr_status rbr_cache_get_params(rbr_ctx* ctx, uint16_t* mlp_bf16, uint16_t* grid_f16) {
+    if (!ctx) return RBR_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(ctx->device);
+    return cache_get_params(ctx, mlp_bf16, grid_f16);
+}
+
+rbr_status rbr_cache_grads_get(rbr_ctx* ctx, float* mlp, float* grid) {
+    if (!ctx) return RBR_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(ctx->device);
+    return cache_grads(ctx, mlp, grid);
+}
+
+rbr_status rbr_cache_encode_host(rbr_ctx* ctx, uint32_t n, const rbr_cache_record* records, float* inputs) {
+    if (!ctx) return RBR_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(ctx->device);
+    return cache_encode_host(ctx, n, records, inputs);
+}
+
+rbr_status rbr_cache_infer_host(rbr_ctx* ctx, uint32_t n, const rbr_cache_record* records, float* rgb) {
+    if (!ctx) return RBR_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(ctx->device);
+    return cache_infer_host(ctx, n, records, rgb);
+}
+
+rbr_status rbr_cache_train_host(rbr_ctx* ctx, uint32_t n, const rbr_cache_record* records, const float* targets,
+                                int apply, float* loss) {
+    if (!ctx) return RBR_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(ctx->device);
+    return cache_train_host(ctx, n, records, targets, apply, loss);
+}
+
+rbr_status rbr_cache_render(rbr_ctx* ctx, const rbr_camera* camera, const rbr_render_params* params, uint32_t frames,
+                            int train, float* film_mean, float* film_m2, void* stream) {
+    if (!ctx) return RBR_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(ctx->device);
+    return render_cached(ctx, camera, params, frames, train, film_mean, film_m2, static_cast<cudaStream_t>(stream));
 }
 
 }  // extern "C"

@@ -41,6 +41,9 @@ enum : int {
     kCShadow = 6,   // shadow queue count
     kCExt = 8,      // 64-bit: extension rays traced
     kCSh = 10,      // 64-bit: shadow rays traced
+    kCQuery = 12,   // radiance cache: paths ended into the cache in this wave
+    kCTrain = 13,   // radiance cache: training vertices gathered in this frame
+    kCTrainBase = 14,  // radiance cache: kCTrain at the start of this wave
     kCWords = 16
 };
 
@@ -53,6 +56,11 @@ struct Wave {
     uint32_t max_depth;
     uint32_t use_nee, use_mis;
     uint64_t seed;
+    // radiance cache (cache_on = 0: the plain path tracer)
+    uint32_t cache_on = 0;
+    uint32_t term_depth = 0;    // first depth at which a path may end into the cache
+    uint32_t train_thresh = 0;  // a path is a training path if its hash is below this
+    float film_weight = 0.0f;   // > 0: film_mean += weight * mean (frames averaged), else film_mean = mean
 };
 
 struct Paths {
@@ -67,6 +75,12 @@ struct Paths {
     uint32_t* counters;
     uint32_t cap;
     uint32_t shadow_cap;
+    // radiance cache
+    float4* q_rec = nullptr;   // 4 per query (rbr_cache_record)
+    float4* q_info = nullptr;  // per query: throughput rgb, path index bits
+    float4* t_rec = nullptr;   // 4 per training vertex
+    float4* t_aux = nullptr;   // 2 per training vertex: (throughput rgb, path index bits), (radiance before, -)
+    uint32_t t_cap = 0;
 };
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
@@ -106,7 +120,13 @@ __global__ void __launch_bounds__(kBlock) k_raygen(CameraDev cam, Wave w, Paths 
         P.rad[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         P.q0[k] = k;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) P.counters[kCQ0] = w.npaths;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        P.counters[kCQ0] = w.npaths;
+        if (w.cache_on) {
+            P.counters[kCQuery] = 0;
+            P.counters[kCTrainBase] = P.counters[kCTrain];
+        }
+    }
 }
 
 // Resets the counters depth `d` appends to.
@@ -202,6 +222,32 @@ __device__ __forceinline__ void spawn(const Hit& h, f3 dir, f3& o, f3& d) {
     d = xnorm(dir);
 }
 
+// Radiance-cache record of a vertex: position, direction towards the viewer, ray-facing
+// normal, roughness, diffuse albedo base (1-metallic)(1-transmission), specular albedo
+// base*metallic + 0.04 (1-metallic).
+__device__ __forceinline__ void cache_record(const Hit& h, f3 rd, const MaterialDev& m, float4* rec) {
+    const float met = oclamp(m.metallic, 0.0f, 1.0f), tr = oclamp(m.transmission, 0.0f, 1.0f);
+    const float kd = fm(fs(1.0f, met), fs(1.0f, tr));
+    const float k4 = fm(0.04f, fs(1.0f, met));
+    rec[0] = make_float4(h.point.x, h.point.y, h.point.z, -rd.x);
+    rec[1] = make_float4(-rd.y, -rd.z, h.normal.x, h.normal.y);
+    rec[2] = make_float4(h.normal.z, m.roughness, fm(m.base[0], kd), fm(m.base[1], kd));
+    rec[3] = make_float4(fm(m.base[2], kd), fa(fm(m.base[0], met), k4), fa(fm(m.base[1], met), k4),
+                         fa(fm(m.base[2], met), k4));
+}
+
+// Training paths of the radiance cache: a hash of (pixel, sample, seed) below the threshold.
+__device__ __forceinline__ bool train_path(const Wave& w, uint32_t pixel, uint32_t sample) {
+    uint32_t x = (pixel * 0x9E3779B1u) ^ ((sample + 0x7F4A7C15u) * 0x85EBCA77u) ^ static_cast<uint32_t>(w.seed);
+    x ^= x >> 16;
+    x *= 0x7FEB352Du;
+    x ^= x >> 15;
+    x *= 0x846CA68Bu;
+    x ^= x >> 16;
+    return x < w.train_thresh;
+}
+
+template <bool kCache>
 __global__ void __launch_bounds__(kBlock) k_shade(DeviceScene s, Wave w, Paths P, uint32_t d) {
     uint32_t cnt[kNumClasses + 1];
     cnt[0] = 0;
@@ -215,7 +261,8 @@ __global__ void __launch_bounds__(kBlock) k_shade(DeviceScene s, Wave w, Paths P
         const uint32_t j = base + threadIdx.x;
         const bool valid = j < n;
         uint32_t k = 0;
-        bool alive = false, nee = false;
+        bool alive = false, nee = false, to_cache = false, to_train = false;
+        float4 rec[4];
         Hit h;
         f3 T = mk(0.0f, 0.0f, 0.0f), wo = mk(0.0f, 0.0f, 0.0f);
         Frame fr;
@@ -247,6 +294,37 @@ __global__ void __launch_bounds__(kBlock) k_shade(DeviceScene s, Wave w, Paths P
             wo = to_local(fr, xneg(rd));  // isect.wo = -ray.direction
             nee = w.use_nee && !bsdf_delta(bs);
             alive = true;
+            if (kCache && bs.n > 0 && !bsdf_delta(bs)) {
+                if (train_path(w, pixel, sample)) {
+                    to_train = true;
+                } else if (d >= w.term_depth && !specular) {
+                    to_cache = true;  // the cache's prediction replaces NEE and everything further
+                    nee = false;
+                    alive = false;
+                }
+                if (to_train || to_cache) cache_record(h, rd, m, rec);
+            }
+        }
+        if (kCache) {
+            const uint32_t qs = warp_append(P.counters + kCQuery, to_cache);
+            if (to_cache) {
+                float4* q = P.q_rec + 4 * static_cast<size_t>(qs);
+                q[0] = rec[0];
+                q[1] = rec[1];
+                q[2] = rec[2];
+                q[3] = rec[3];
+                P.q_info[qs] = make_float4(T.x, T.y, T.z, __uint_as_float(k));
+            }
+            const uint32_t ts = warp_append(P.counters + kCTrain, to_train);
+            if (to_train && ts < P.t_cap) {
+                float4* q = P.t_rec + 4 * static_cast<size_t>(ts);
+                q[0] = rec[0];
+                q[1] = rec[1];
+                q[2] = rec[2];
+                q[3] = rec[3];
+                P.t_aux[2 * static_cast<size_t>(ts)] = make_float4(T.x, T.y, T.z, __uint_as_float(k));
+                P.t_aux[2 * static_cast<size_t>(ts) + 1] = P.rad[k];  // radiance gathered before this vertex's NEE
+            }
         }
         // next-event estimation: one shadow ray per light (estimateDirectLighting)
         for (uint32_t l = 0; l < s.num_lights; ++l) {
@@ -348,14 +426,25 @@ __global__ void __launch_bounds__(kBlock) k_film(Wave w, Paths P, float* film_me
         }
         const f3 mean = xdivs(sum, static_cast<float>(w.spp));  // pixelColor / samplesPerPixel
         float* o = film_mean + 3 * static_cast<size_t>(w.p0 + i);
-        o[0] = mean.x;
-        o[1] = mean.y;
-        o[2] = mean.z;
-        if (film_m2) {
-            float* q = film_m2 + 3 * static_cast<size_t>(w.p0 + i);
-            q[0] = sq.x;
-            q[1] = sq.y;
-            q[2] = sq.z;
+        float* q = film_m2 ? film_m2 + 3 * static_cast<size_t>(w.p0 + i) : nullptr;
+        if (w.film_weight > 0.0f) {  // average over frames
+            o[0] = fa(o[0], fm(mean.x, w.film_weight));
+            o[1] = fa(o[1], fm(mean.y, w.film_weight));
+            o[2] = fa(o[2], fm(mean.z, w.film_weight));
+            if (q) {
+                q[0] = fa(q[0], sq.x);
+                q[1] = fa(q[1], sq.y);
+                q[2] = fa(q[2], sq.z);
+            }
+        } else {
+            o[0] = mean.x;
+            o[1] = mean.y;
+            o[2] = mean.z;
+            if (q) {
+                q[0] = sq.x;
+                q[1] = sq.y;
+                q[2] = sq.z;
+            }
         }
     }
 }
@@ -484,7 +573,7 @@ rbr_status render(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_params* 
         for (uint32_t d = 0; d < w.max_depth; ++d) {
             k_begin<<<1, 1, 0, stream>>>(P, d);
             k_extend<<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d, ctx->d_error);
-            k_shade<<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d);
+            k_shade<false><<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d);
             k_shadow<<<grid, kBlock, 0, stream>>>(ctx->scene, P, ctx->d_error);
             launches += 4;
         }
@@ -497,6 +586,157 @@ rbr_status render(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_params* 
     if (e != cudaSuccess) return cuda_fail(ctx, e, "path tracer launch");
     ctx->last_render.paths = npix * spp;
     ctx->last_render.extension_rays = 0;  // read from the device by rbr_render_stats_get
+    ctx->last_render.shadow_rays = 0;
+    ctx->last_render.waves = waves;
+    ctx->last_render.launches = launches;
+    ctx->render_pending = true;
+    return RBR_OK;
+}
+
+// ------------------------------------------------------------------------------------------
+// Rendering with the radiance cache: frames of the wavefront path tracer in which paths end
+// into the cache (inference after each wave's bounces), training paths gather targets, and
+// the cache trains after each frame.
+// ------------------------------------------------------------------------------------------
+namespace {
+
+__global__ void k_cache_wave_end(const uint32_t* counters, uint32_t* scalars, uint32_t t_cap) {
+    scalars[kRcLastQueries] += counters[kCQuery];
+    scalars[kRcTrain] = min(counters[kCTrain], t_cap);
+}
+
+CameraDev camera_dev(const rbr_camera* cam) {
+    CameraDev cd;
+    cd.width = cam->width;
+    cd.height = cam->height;
+    cd.model = cam->model;
+    for (int a = 0; a < 3; ++a) {
+        cd.position[a] = cam->position[a];
+        cd.forward[a] = cam->forward[a];
+        cd.right[a] = cam->right[a];
+        cd.up[a] = cam->up[a];
+    }
+    cd.fx = cam->fx;
+    cd.fy = cam->fy;
+    cd.cx = cam->cx;
+    cd.cy = cam->cy;
+    cd.lens_radius = cam->lens_radius;
+    cd.focal_distance = cam->focal_distance;
+    return cd;
+}
+
+}  // namespace
+
+rbr_status render_cached(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_params* p, uint32_t frames, int train,
+                         float* film_mean, float* film_m2, cudaStream_t stream) {
+    if (!cam || !p || !film_mean) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "camera, params or film_mean is NULL");
+    if (!ctx->has_scene) return fail(ctx, RBR_ERR_NO_SCENE, "rbr_cache_render before rbr_scene_upload");
+    CacheState& cs = ctx->cache;
+    if (!cs.ready) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "no radiance cache: call rbr_cache_create first");
+    if (cam->width <= 0 || cam->height <= 0 || p->samples_per_pixel <= 0 || p->max_depth < 0 || frames == 0)
+        return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "image size, samples per pixel, max depth or frames out of range");
+    if (cam->model != RBR_CAMERA_PINHOLE && cam->model != RBR_CAMERA_THIN_LENS)
+        return fail(ctx, RBR_ERR_UNSUPPORTED, "camera model " + std::to_string(cam->model));
+    if (p->flags & RBR_RENDER_CORRECTED_MIS)
+        return fail(ctx, RBR_ERR_UNSUPPORTED, "RBR_RENDER_CORRECTED_MIS is not implemented");
+    if ((p->flags & RBR_RENDER_SECOND_MOMENT) == 0) film_m2 = nullptr;
+    const uint64_t npix = uint64_t(cam->width) * cam->height;
+    const uint32_t spp = static_cast<uint32_t>(p->samples_per_pixel);
+    if (npix * spp > 0xFFFFFFFFull || spp > kDefaultCapacity ||
+        uint64_t(p->sample_offset) + uint64_t(frames) * spp > 0xFFFFFFFFull)
+        return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "more than 2^32 camera samples per frame or sample indices");
+    const uint32_t nl = std::max(1u, ctx->scene.num_lights);
+    uint32_t cap = static_cast<uint32_t>(std::min<uint64_t>(npix * spp, std::max(ctx->pt_wave_paths, spp)));
+    cap = std::min<uint64_t>(cap, kShadowBytesLimit / (48ull * nl));
+    cap = std::max(spp, cap / spp * spp);
+    rbr_status st = ensure_paths(ctx, cap, cap * nl);
+    if (st != RBR_OK) return st;
+    const uint32_t depth = std::max(1, p->max_depth);
+    const uint32_t t_cap =
+        train ? static_cast<uint32_t>(std::min<uint64_t>(uint64_t(std::max(1u, cs.cfg.train_paths)) * depth, 1u << 23)) : 1;
+    st = cache_ensure_render(ctx, cap, t_cap);
+    if (st != RBR_OK) return st;
+
+    PathBuffers& pb = ctx->pt;
+    Paths P;
+    P.ray = static_cast<float4*>(pb.ray.ptr);
+    P.thr = static_cast<float4*>(pb.thr.ptr);
+    P.rad = static_cast<float4*>(pb.rad.ptr);
+    P.hit = static_cast<uint2*>(pb.hit.ptr);
+    P.q0 = static_cast<uint32_t*>(pb.queue[0].ptr);
+    P.q1 = static_cast<uint32_t*>(pb.queue[1].ptr);
+    P.classq = static_cast<uint32_t*>(pb.classq.ptr);
+    P.shadow = static_cast<float4*>(pb.shadow.ptr);
+    P.counters = static_cast<uint32_t*>(pb.counters.ptr);
+    P.cap = pb.capacity;
+    P.shadow_cap = pb.shadow_capacity;
+    P.q_rec = static_cast<float4*>(cs.q_rec);
+    P.q_info = static_cast<float4*>(cs.q_info);
+    P.t_rec = static_cast<float4*>(cs.t_rec);
+    P.t_aux = static_cast<float4*>(cs.t_aux);
+    P.t_cap = train ? cs.t_cap : 0;
+    const CameraDev cd = camera_dev(cam);
+
+    const double frac = train ? double(cs.cfg.train_paths) / double(npix * spp) : 0.0;
+    const uint32_t thresh = static_cast<uint32_t>(std::min(4294967295.0, std::floor(frac * 4294967296.0)));
+    const float weight = 1.0f / static_cast<float>(frames);
+    uint32_t* scalars = static_cast<uint32_t*>(cs.scalars);
+
+    const int grid = ctx->num_sms * 8;
+    const uint32_t pix_per_wave = cap / spp;
+    uint32_t launches = 0, waves = 0;
+    cudaError_t e = cudaMemsetAsync(P.counters, 0, kCWords * 4, stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(film_mean, 0, npix * 12, stream);
+    if (e == cudaSuccess && film_m2) e = cudaMemsetAsync(film_m2, 0, npix * 12, stream);
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_start, stream);
+    for (uint32_t f = 0; f < frames && e == cudaSuccess; ++f) {
+        e = cudaMemsetAsync(P.counters + kCTrain, 0, 4, stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(scalars + kRcLastQueries, 0, 4, stream);
+        for (uint64_t p0 = 0; p0 < npix && e == cudaSuccess; p0 += pix_per_wave) {
+            Wave w;
+            w.p0 = static_cast<uint32_t>(p0);
+            w.npaths = static_cast<uint32_t>(std::min<uint64_t>(pix_per_wave, npix - p0)) * spp;
+            w.spp = spp;
+            w.sample_offset = p->sample_offset + f * spp;
+            w.width = static_cast<uint32_t>(cam->width);
+            w.max_depth = static_cast<uint32_t>(p->max_depth);
+            w.use_nee = p->use_nee != 0;
+            w.use_mis = p->use_mis != 0;
+            w.seed = p->seed;
+            w.cache_on = 1;
+            w.term_depth = cs.cfg.termination_depth;
+            w.train_thresh = thresh;
+            w.film_weight = weight;
+            k_raygen<<<grid, kBlock, 0, stream>>>(cd, w, P);
+            ++launches;
+            for (uint32_t d = 0; d < w.max_depth; ++d) {
+                k_begin<<<1, 1, 0, stream>>>(P, d);
+                k_extend<<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d, ctx->d_error);
+                k_shade<true><<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d);
+                k_shadow<<<grid, kBlock, 0, stream>>>(ctx->scene, P, ctx->d_error);
+                launches += 4;
+            }
+            e = cache_launch_infer(ctx, P.q_rec, w.npaths, P.counters + kCQuery, nullptr, P.rad, P.q_info, stream);
+            ++launches;
+            if (e == cudaSuccess && train) {
+                e = cache_launch_finalize(ctx, P.rad, P.counters, kCTrainBase, kCTrain, stream);
+                ++launches;
+            }
+            k_film<<<grid, kBlock, 0, stream>>>(w, P, film_mean, film_m2);
+            k_cache_wave_end<<<1, 1, 0, stream>>>(P.counters, scalars, P.t_cap);
+            launches += 2;
+            ++waves;
+            if (e == cudaSuccess) e = cudaGetLastError();
+        }
+        if (e == cudaSuccess && train) {
+            e = cache_launch_train_frame(ctx, P.counters + kCTrain, f, stream);
+            launches += 4 * cs.cfg.train_steps;
+        }
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_stop, stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cached path tracer launch");
+    ctx->last_render.paths = npix * spp * frames;
+    ctx->last_render.extension_rays = 0;
     ctx->last_render.shadow_rays = 0;
     ctx->last_render.waves = waves;
     ctx->last_render.launches = launches;
@@ -625,7 +865,7 @@ rbr_status render_noalloc(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_
         for (uint32_t d = 0; d < w.max_depth; ++d) {
             k_begin<<<1, 1, 0, stream>>>(P, d);
             k_extend<<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d, ctx->d_error);
-            k_shade<<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d);
+            k_shade<false><<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d);
             k_shadow<<<grid, kBlock, 0, stream>>>(ctx->scene, P, ctx->d_error);
         }
         k_film<<<grid, kBlock, 0, stream>>>(w, P, film_mean, nullptr);

@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "rbr_b200.h"
+#include "rbr_cache.h"
 #include "rbr_scene_dev.h"
 #include "rbr_layout.h"
 
@@ -63,6 +64,8 @@ struct rbr_ctx {
     rbr_render_stats last_render{};
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
     bool render_pending = false;
+    // radiance cache
+    rbr::CacheState cache;
 };
 
 namespace rbr {
@@ -100,6 +103,27 @@ rbr_status render(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_params* 
                   cudaStream_t stream);
 void free_path_buffers(rbr_ctx* ctx);
 rbr_status read_render_counters(rbr_ctx* ctx);
+// radiance cache (cache.cu)
+void cache_config_default(rbr_cache_config* c);
+rbr_status cache_create(rbr_ctx* ctx, const rbr_cache_config* cfg);
+void cache_destroy(rbr_ctx* ctx);
+rbr_status cache_info(rbr_ctx* ctx, rbr_cache_info* out);
+rbr_status cache_set_params(rbr_ctx* ctx, const uint16_t* mlp, const uint16_t* grid);
+rbr_status cache_get_params(rbr_ctx* ctx, uint16_t* mlp, uint16_t* grid);
+rbr_status cache_grads(rbr_ctx* ctx, float* mlp, float* grid);
+rbr_status cache_encode_host(rbr_ctx* ctx, uint32_t n, const rbr_cache_record* records, float* inputs);
+rbr_status cache_infer_host(rbr_ctx* ctx, uint32_t n, const rbr_cache_record* records, float* rgb);
+rbr_status cache_train_host(rbr_ctx* ctx, uint32_t n, const rbr_cache_record* records, const float* targets, int apply,
+                            float* loss);
+rbr_status cache_ensure_render(rbr_ctx* ctx, uint32_t paths, uint32_t train_cap);
+cudaError_t cache_launch_infer(rbr_ctx* ctx, const float4* records, uint32_t n, const uint32_t* n_ptr, float* rgb,
+                               float4* path_rad, const float4* q_info, cudaStream_t stream);
+cudaError_t cache_launch_finalize(rbr_ctx* ctx, const float4* path_rad, const uint32_t* counters, int base_word,
+                                  int count_word, cudaStream_t stream);
+cudaError_t cache_launch_train_frame(rbr_ctx* ctx, const uint32_t* count_ptr, uint32_t frame, cudaStream_t stream);
+rbr_status render_cached(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_params* p, uint32_t frames, int train,
+                         float* film_mean, float* film_m2, cudaStream_t stream);
+
 rbr_status render_noalloc(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_params* p, float* film_mean,
                           cudaStream_t stream);
 

@@ -48,5 +48,6 @@ constexpr float kEpsilon = 1e-4f;
 // Device-side error bits (rbr_ctx::d_error).
 constexpr int kErrStackOverflow = 1;
 constexpr int kErrQueueOverflow = 2;
+constexpr int kErrDeviceTimeout = 4;  // a bounded wait (tensor-core completion) ran out
 
 }  // namespace rbr

@@ -68,6 +68,18 @@ def load_library() -> C.CDLL:
         "rbr_param_set": (C.c_int, [P, C.c_char_p, C.c_int64]),
         "rbr_param_get": (C.c_int, [P, C.c_char_p, C.POINTER(C.c_int64)]),
         "rbr_autotune_trace": (C.c_int, [P, P, C.c_uint32, C.c_int, C.POINTER(C.c_int64)]),
+        "rbr_cache_config_default": (None, [C.POINTER(abi.rbr_cache_config)]),
+        "rbr_cache_create": (C.c_int, [P, C.POINTER(abi.rbr_cache_config)]),
+        "rbr_cache_destroy": (None, [P]),
+        "rbr_cache_info_get": (C.c_int, [P, C.POINTER(abi.rbr_cache_info)]),
+        "rbr_cache_set_params": (C.c_int, [P, P, P]),
+        "rbr_cache_get_params": (C.c_int, [P, P, P]),
+        "rbr_cache_grads_get": (C.c_int, [P, P, P]),
+        "rbr_cache_encode_host": (C.c_int, [P, C.c_uint32, P, P]),
+        "rbr_cache_infer_host": (C.c_int, [P, C.c_uint32, P, P]),
+        "rbr_cache_train_host": (C.c_int, [P, C.c_uint32, P, P, C.c_int, C.POINTER(C.c_float)]),
+        "rbr_cache_render": (C.c_int, [P, C.POINTER(abi.rbr_camera), C.POINTER(abi.rbr_render_params), C.c_uint32,
+                                       C.c_int, P, P, P]),
     }
     for name, (res, args) in sig.items():
         if hasattr(lib, name):
@@ -236,6 +248,75 @@ class Context:
     def mis_weights(self, pdf_pairs):
         n = len(pdf_pairs)
         return self._unit(lambda h, a, o: self.lib.rbr_mis_weights_host(h, n, a, o), [pdf_pairs], n, 1)[:, 0]
+
+    # radiance cache ------------------------------------------------------------------------
+    def cache_config(self, **kw) -> abi.rbr_cache_config:
+        cfg = abi.rbr_cache_config()
+        self.lib.rbr_cache_config_default(C.byref(cfg))
+        for k, v in kw.items():
+            if k in ("bounds_min", "bounds_max"):
+                getattr(cfg, k)[:] = [float(x) for x in v]
+            else:
+                setattr(cfg, k, v)
+        return cfg
+
+    def cache_create(self, cfg: abi.rbr_cache_config | None = None, **kw):
+        cfg = cfg if cfg is not None else self.cache_config(**kw)
+        self._check(self.lib.rbr_cache_create(self.h, C.byref(cfg)))
+        return self.cache_info()
+
+    def cache_info(self) -> abi.rbr_cache_info:
+        info = abi.rbr_cache_info()
+        self._check(self.lib.rbr_cache_info_get(self.h, C.byref(info)))
+        return info
+
+    def cache_set_params(self, mlp_bf16: np.ndarray | None = None, grid_f16: np.ndarray | None = None):
+        m = None if mlp_bf16 is None else np.ascontiguousarray(mlp_bf16, np.uint16)
+        g = None if grid_f16 is None else np.ascontiguousarray(grid_f16, np.uint16)
+        self._check(self.lib.rbr_cache_set_params(self.h, None if m is None else C.c_void_p(m.ctypes.data),
+                                                  None if g is None else C.c_void_p(g.ctypes.data)))
+
+    def cache_get_params(self, grid: bool = False):
+        info = self.cache_info()
+        m = np.zeros(abi.CACHE_MLP_WEIGHTS, np.uint16)
+        g = np.zeros(info.levels * info.table_size * 2, np.uint16) if grid else None
+        self._check(self.lib.rbr_cache_get_params(self.h, C.c_void_p(m.ctypes.data),
+                                                  None if g is None else C.c_void_p(g.ctypes.data)))
+        return (m, g) if grid else m
+
+    def cache_grads(self, grid: bool = True):
+        info = self.cache_info()
+        m = np.zeros(abi.CACHE_MLP_WEIGHTS, np.float32)
+        g = np.zeros(info.levels * info.table_size * 2, np.float32) if grid else None
+        self._check(self.lib.rbr_cache_grads_get(self.h, C.c_void_p(m.ctypes.data),
+                                                 None if g is None else C.c_void_p(g.ctypes.data)))
+        return m, g
+
+    def cache_encode(self, records: np.ndarray) -> np.ndarray:
+        r = np.ascontiguousarray(records, np.float32).reshape(-1, abi.CACHE_RECORD_FLOATS)
+        out = np.zeros((len(r), abi.CACHE_INPUTS), np.float32)
+        self._check(self.lib.rbr_cache_encode_host(self.h, len(r), C.c_void_p(r.ctypes.data), C.c_void_p(out.ctypes.data)))
+        return out
+
+    def cache_infer(self, records: np.ndarray) -> np.ndarray:
+        r = np.ascontiguousarray(records, np.float32).reshape(-1, abi.CACHE_RECORD_FLOATS)
+        out = np.zeros((len(r), 3), np.float32)
+        self._check(self.lib.rbr_cache_infer_host(self.h, len(r), C.c_void_p(r.ctypes.data), C.c_void_p(out.ctypes.data)))
+        return out
+
+    def cache_train(self, records: np.ndarray, targets: np.ndarray, apply: bool = True) -> float:
+        r = np.ascontiguousarray(records, np.float32).reshape(-1, abi.CACHE_RECORD_FLOATS)
+        t = np.ascontiguousarray(targets, np.float32).reshape(-1, 3)
+        loss = C.c_float()
+        self._check(self.lib.rbr_cache_train_host(self.h, len(r), C.c_void_p(r.ctypes.data), C.c_void_p(t.ctypes.data),
+                                                  int(apply), C.byref(loss)))
+        return float(loss.value)
+
+    def cache_render_dev(self, camera, params, frames: int, film_mean_ptr: int, film_m2_ptr: int = 0,
+                         train: bool = True, stream: int = 0):
+        self._check(self.lib.rbr_cache_render(self.h, C.byref(camera), C.byref(params), frames, int(train),
+                                              C.c_void_p(film_mean_ptr), C.c_void_p(film_m2_ptr or None),
+                                              C.c_void_p(stream)))
 
     def render_stats(self) -> abi.rbr_render_stats:
         s = abi.rbr_render_stats()

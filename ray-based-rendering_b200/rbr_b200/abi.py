@@ -146,6 +146,50 @@ class rbr_render_stats(C.Structure):
 
 
 # numpy views of the ray / hit records
+CACHE_LEVELS = 16
+CACHE_INPUTS = 64
+CACHE_MLP_WEIGHTS = 4 * 64 * 64 + 16 * 64
+CACHE_RECORD_FLOATS = 16
+
+
+class rbr_cache_config(C.Structure):
+    _fields_ = [
+        ("log2_table_size", C.c_int32),
+        ("min_resolution", C.c_int32),
+        ("max_resolution", C.c_int32),
+        ("learning_rate", C.c_float),
+        ("beta1", C.c_float),
+        ("beta2", C.c_float),
+        ("epsilon", C.c_float),
+        ("train_batch", C.c_uint32),
+        ("train_steps", C.c_uint32),
+        ("train_paths", C.c_uint32),
+        ("termination_depth", C.c_uint32),
+        ("seed", C.c_uint64),
+        ("bounds_min", _f3),
+        ("bounds_max", _f3),
+    ]
+
+
+class rbr_cache_info(C.Structure):
+    _fields_ = [
+        ("levels", C.c_uint32),
+        ("table_size", C.c_uint32),
+        ("resolution", C.c_uint32 * CACHE_LEVELS),
+        ("dense_levels", C.c_uint32),
+        ("optimiser_steps", C.c_uint32),
+        ("bounds_min", _f3),
+        ("bounds_max", _f3),
+        ("last_loss", C.c_float),
+        ("last_queries", C.c_uint32),
+        ("last_train_records", C.c_uint32),
+    ]
+
+
+# rbr_cache_record as 16 float32 columns: position[3], direction[3], normal[3], roughness,
+# diffuse[3], specular[3]
+CACHE_RECORD_DTYPE = np.dtype((np.float32, (CACHE_RECORD_FLOATS,)))
+
 RAY_DTYPE = np.dtype(
     [("origin", np.float32, 3), ("tmax", np.float32), ("direction", np.float32, 3), ("pad", np.float32)]
 )

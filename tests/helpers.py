@@ -1,11 +1,19 @@
 """Shared inputs for the unit-parity tests and the golden-fixture script."""
 from __future__ import annotations
 
+import zlib
+
 import numpy as np
 
 from rbr_b200 import abi
 
 F32 = np.float32
+
+
+def name_seed(name: str, modulus: int) -> int:
+    """A seed derived from a test-case name that is the same in every process (str hashes are
+    salted per process)."""
+    return zlib.crc32(name.encode()) % modulus
 
 
 def material(base=(0.8, 0.8, 0.8), metallic=0.0, roughness=1.0, ior=1.5, transmission=0.0, emission=(0, 0, 0)):

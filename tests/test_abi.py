@@ -29,6 +29,8 @@ def test_abi_version():
         ("rbr_camera", abi.rbr_camera),
         ("rbr_render_params", abi.rbr_render_params),
         ("rbr_render_stats", abi.rbr_render_stats),
+        ("rbr_cache_config", abi.rbr_cache_config),
+        ("rbr_cache_info", abi.rbr_cache_info),
     ],
 )
 def test_struct_sizes_match(name, cls):
@@ -39,6 +41,7 @@ def test_record_sizes():
     lib = load_library()
     assert lib.rbr_struct_size(b"rbr_ray") == abi.RAY_DTYPE.itemsize == 32
     assert lib.rbr_struct_size(b"rbr_hit") == abi.HIT_DTYPE.itemsize == 8
+    assert lib.rbr_struct_size(b"rbr_cache_record") == abi.CACHE_RECORD_DTYPE.itemsize == 64
     assert lib.rbr_struct_size(b"no_such_struct") == 0
 
 

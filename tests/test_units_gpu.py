@@ -22,7 +22,7 @@ GRID = helpers.material_grid()
 
 @pytest.mark.parametrize("name,mat", GRID, ids=[n for n, _ in GRID])
 def test_bsdf_eval_pdf_bit_exact(ctx, reference, name, mat):
-    wo, wi, _ = helpers.bsdf_inputs(8192, seed=hash(name) % 997)
+    wo, wi, _ = helpers.bsdf_inputs(8192, seed=helpers.name_seed(name, 997))
     got = ctx.bsdf_eval(mat, wo, wi)
     f, pdf, info = reference.bsdf_eval(mat, wo, wi)
     assert np.array_equal(bits(got[:, :3]), bits(f)), "BSDF values"
@@ -34,7 +34,9 @@ def check_samples(ctx_or_none, reference, mat, wo, got, want, min_close=0.99):
     """Well-posed comparison of BSDF::sample outputs (8 floats each) from two implementations
     whose sin/cos may differ in the last bit:
       - the same samples are valid (pdf > 0) on both sides, up to 0.1 %;
-      - sampled directions agree within 1e-5 (unit vectors);
+      - sampled directions agree within 1e-5 (unit vectors) for all but 0.1 % of the samples and
+        within 1e-3 for all (refraction close to total internal reflection magnifies an ulp of
+        sin/cos);
       - every non-delta GPU sample carries exactly (bit for bit) the reference's
         evaluate() and pdf() at the GPU's own direction;
       - f and pdf agree within 1e-5 relative for at least `min_close` of the samples (sharp GGX
@@ -44,7 +46,9 @@ def check_samples(ctx_or_none, reference, mat, wo, got, want, min_close=0.99):
     vg, vw = got[:, 6] > 0, want[:, 6] > 0
     assert (vg == vw).mean() >= 0.999
     both = vg & vw
-    assert np.abs(got[both, :3] - want[both, :3]).max(initial=0.0) <= 1e-5
+    dev = np.abs(got[both, :3] - want[both, :3]).max(axis=1, initial=0.0)
+    assert dev.max(initial=0.0) <= 1e-3
+    assert (dev <= 1e-5).mean() >= 0.999 if both.any() else True
     nd = vg & (got[:, 7] == 0)
     if nd.any():
         f, pdf, _ = reference.bsdf_eval(mat, wo[nd], got[nd, :3])
@@ -58,7 +62,7 @@ def check_samples(ctx_or_none, reference, mat, wo, got, want, min_close=0.99):
 
 @pytest.mark.parametrize("name,mat", GRID, ids=[n for n, _ in GRID])
 def test_bsdf_sample_matches_reference(ctx, reference, name, mat):
-    wo, _, u = helpers.bsdf_inputs(8192, seed=hash(name) % 991)
+    wo, _, u = helpers.bsdf_inputs(8192, seed=helpers.name_seed(name, 991))
     check_samples(ctx, reference, mat, wo, ctx.bsdf_sample(mat, wo, u), reference.bsdf_sample(mat, wo, u))
 
 
