@@ -43,10 +43,11 @@ ICO_LEVEL = 8
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=200)
+    p.add_argument("--steps", type=int, default=None, help="timed steps (default 200; cache workload: 256 frames)")
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["rays", "cornell", "ggx"], default="rays")
+    p.add_argument("--workload", choices=["rays", "cornell", "ggx", "cache"], default="rays")
+    p.add_argument("--ref-spp", type=int, default=1024, help="cache workload: spp of the converged GPU reference")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true", help="skip the host-buffer measurement (profiling runs)")
     p.add_argument("--param", action="append", default=[], help="NAME=VALUE context tunable (rbr_param_set)")
@@ -309,13 +310,113 @@ def run_render(args, rank, world, local_rank):
     ctx.close()
 
 
+def relmse(x, ref):
+    """mean((x - ref)^2 / (ref^2 + 1e-2)) over pixels and channels."""
+    return float(np.mean((x.astype(np.float64) - ref) ** 2 / (ref.astype(np.float64) ** 2 + 1e-2)))
+
+
+def run_cache(args, rank, world, local_rank):
+    """Learned radiance cache vs the plain GPU path tracer at equal time on the GGX scene
+    (1920x1080, 1 spp per frame). A step is one frame: 1 spp with paths ending into the cache,
+    plus the frame's 4 optimiser steps on 2^16 training paths. Converged reference: the plain
+    GPU path tracer at --ref-spp samples per pixel (independent seed)."""
+    import torch
+
+    from rbr_b200 import Context, render_params, scenes
+
+    torch.cuda.set_device(local_rank)
+    frames = args.steps
+    scene = scenes.ggx_scene()
+    cam = scene.camera
+    W, H = cam.width, cam.height
+    ctx = Context(local_rank)
+    ctx.upload(scene)
+    depth = 16
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    film = torch.zeros(W * H * 3, dtype=torch.float32, device=f"cuda:{local_rank}")
+
+    def plain(spp, seed):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record(stream)
+        ctx.render_dev(cam, render_params(spp=spp, max_depth=depth, seed=seed), film.data_ptr(), 0, sp)
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        return film.cpu().numpy().reshape(H, W, 3).copy(), ev[0].elapsed_time(ev[1])
+
+    ref, ref_ms = plain(args.ref_spp, 777)
+    # warm-up of both paths (kernels loaded, buffers allocated)
+    plain(1, 1)
+    ctx.cache_create(seed=3)
+    ctx.cache_render_dev(cam, render_params(spp=1, max_depth=depth, seed=2), max(3, args.warmup), film.data_ptr(), 0,
+                         True, sp)
+    torch.cuda.synchronize()
+    # the timed cached run starts from a fresh cache
+    ctx.cache_create(seed=3)
+    clocks = Clocks() if rank == 0 else None
+    if clocks:
+        clocks.start()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev[0].record(stream)
+    ctx.cache_render_dev(cam, render_params(spp=1, max_depth=depth, seed=11), frames, film.data_ptr(), 0, True, sp)
+    ev[1].record(stream)
+    torch.cuda.synchronize()
+    cache_ms = ev[0].elapsed_time(ev[1])
+    clk = clocks.stop(visible_gpu_indices(local_rank)) if clocks else None
+    launches = ctx.render_stats().launches
+    cached = film.cpu().numpy().reshape(H, W, 3).copy()
+    info = ctx.cache_info()
+    # plain path tracer: equal samples, then equal time
+    plain_same, plain_same_ms = plain(frames, 11)
+    eq_spp = max(1, int(round(frames * cache_ms / plain_same_ms)))
+    plain_eq, plain_eq_ms = plain(eq_spp, 11)
+    r_cache, r_eq, r_same = relmse(cached, ref), relmse(plain_eq, ref), relmse(plain_same, ref)
+    # end to end: a cached render of a few frames with the film read back to the host
+    t0 = time.perf_counter()
+    e2e_frames = 8
+    ctx.cache_render_dev(cam, render_params(spp=1, max_depth=depth, seed=12), e2e_frames, film.data_ptr(), 0, True, sp)
+    host = film.cpu()
+    e2e_s = time.perf_counter() - t0
+    if rank == 0:
+        print(json.dumps({
+            "metric": "Mpaths/s & RelMSE at equal time: MLP cache vs plain GPU PT", "value":
+                W * H * frames / (cache_ms / 1e3) / 1e6, "unit": "Mpaths/s", "n_gpus": world, "steps": frames,
+            "warmup": max(3, args.warmup), "ms_per_step": cache_ms / frames, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "bf16 (MLP) / f32 (path tracer)",
+            "data": "synthetic (seeded)",
+            "config": {"workload": "learned radiance cache on the GGX scene: 1920x1080, 1 spp per frame, "
+                                   f"{frames} frames; hash grid 16 levels x 2^19 x 2 FP16, MLP 5x64 BF16; "
+                                   "2^16 training paths per frame, 4 Adam steps of 16384 samples, lr 1e-2",
+                       "reference": f"plain GPU path tracer, {args.ref_spp} spp, independent seed "
+                                    f"({ref_ms / 1e3:.1f} s)",
+                       "l2": "path state per frame (2M paths x ~100 B) and hash grid (32 MB) + Adam state "
+                             "(224 MB) exceed L2"},
+            "relmse": {"cache": r_cache, "plain_equal_time": r_eq, "plain_equal_samples": r_same,
+                       "gain_equal_time": r_eq / r_cache, "plain_equal_time_spp": eq_spp,
+                       "plain_equal_time_ms": plain_eq_ms, "cache_ms": cache_ms,
+                       "mean_bias": float(cached.mean() / ref.mean() - 1.0)},
+            "cache": {"optimiser_steps": info.optimiser_steps, "last_loss": info.last_loss,
+                      "queries_last_frame": info.last_queries, "train_records_last_frame": info.last_train_records},
+            "e2e": {"value": W * H * e2e_frames / e2e_s / 1e6, "unit": "Mpaths/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": W * H * 12 // e2e_frames,
+                    "path": f"rbr_cache_render of {e2e_frames} frames + film to host"},
+            "clocks": clk, "gpu_launches": launches,
+        }))
+    del host
+    ctx.close()
+
+
 def main():
     args = parse()
+    if args.steps is None:
+        args.steps = 256 if args.workload == "cache" else 200
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.workload == "cache":
+        return run_cache(args, rank, world, local_rank)
     if args.workload != "rays":
         return run_render(args, rank, world, local_rank)
 
