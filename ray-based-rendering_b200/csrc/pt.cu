@@ -104,6 +104,14 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool pred) {
 
 __device__ __forceinline__ f3 ld_f3(float4 v) { return mk(v.x, v.y, v.z); }
 
+// Origin (o.xyz) or direction (d.xyz) not finite, or a zero direction.
+__device__ __forceinline__ bool degenerate(float4 o, float4 d) {
+    const float big = 3.402823466e38f;
+    const bool finite = fabsf(o.x) <= big && fabsf(o.y) <= big && fabsf(o.z) <= big && fabsf(d.x) <= big &&
+                        fabsf(d.y) <= big && fabsf(d.z) <= big;
+    return !finite || (d.x == 0.0f && d.y == 0.0f && d.z == 0.0f);
+}
+
 // ------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(kBlock) k_raygen(CameraDev cam, Wave w, Paths P) {
     const uint32_t stride = gridDim.x * blockDim.x;
@@ -150,7 +158,10 @@ __global__ void __launch_bounds__(kBlock) k_extend(DeviceScene s, Wave w, Paths 
             k = q[j];
             const float4 a = P.ray[2 * k], b = P.ray[2 * k + 1];
             float t = 0.0f;
-            const uint32_t prim = traverse<false>(s, ld_f3(a), ld_f3(b), __int_as_float(0x7f800000), t, err);
+            // A ray with a zero or non-finite direction or origin hits nothing (every primitive
+            // test rejects it) but would pass every box test: skip the traversal.
+            const uint32_t prim = degenerate(a, b) ? 0xFFFFFFFFu
+                                                   : traverse<false>(s, ld_f3(a), ld_f3(b), __int_as_float(0x7f800000), t, err);
             P.hit[k] = make_uint2(prim, __float_as_uint(t));
             if (prim == 0xFFFFFFFFu) {
                 const float4 T = P.thr[k];
@@ -404,7 +415,7 @@ __global__ void __launch_bounds__(kBlock) k_shadow(DeviceScene s, Paths P, int* 
         const float4* e = P.shadow + 3 * static_cast<size_t>(j);
         const float4 a = e[0], b = e[1];
         float t;
-        if (!traverse<true>(s, ld_f3(a), ld_f3(b), a.w, t, err)) {
+        if (!degenerate(a, b) && !traverse<true>(s, ld_f3(a), ld_f3(b), a.w, t, err)) {
             const float4 c = e[2];
             float4* L = P.rad + __float_as_uint(b.w);
             atomicAdd(&L->x, c.x);

@@ -148,13 +148,23 @@ struct RayCtx {
     bool nx, ny, nz;    // sign of 1/d per axis (near/far plane choice)
 };
 
+// 1 / x with |x| raised to at least 2^-100 (sign kept). With an exact zero component the
+// slab distances of that axis would be q*inf + (-inf) = NaN, which fminf/fmaxf ignore: every
+// box the ray crosses in the other two axes would pass, a traversal of much of the tree. With
+// 2^100 the distances stay finite and the axis is tested by containment, as the reference's
+// BoundingBox::intersect does for a zero component (include/render/acceleration/bbox.h:92-120).
+// Boxes stay conservative: a component below 2^-100 moves the ray by less than 2^-100 * t.
+__device__ __forceinline__ float safe_inv(float x) {
+    return __fdiv_rn(1.0f, copysignf(fmaxf(fabsf(x), 7.888609052e-31f), x));
+}
+
 __device__ __forceinline__ RayCtx make_ctx(f3 o, f3 d) {
     RayCtx r;
     r.o = o;
     r.d = d;
-    r.ix = __fdiv_rn(1.0f, d.x);
-    r.iy = __fdiv_rn(1.0f, d.y);
-    r.iz = __fdiv_rn(1.0f, d.z);
+    r.ix = safe_inv(d.x);
+    r.iy = safe_inv(d.y);
+    r.iz = safe_inv(d.z);
     r.nx = signbit(r.ix);
     r.ny = signbit(r.iy);
     r.nz = signbit(r.iz);
