@@ -46,7 +46,7 @@ def parse():
     p.add_argument("--steps", type=int, default=None, help="timed steps (default 200; cache workload: 256 frames)")
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["rays", "cornell", "ggx", "cache"], default="rays")
+    p.add_argument("--workload", choices=["rays", "cornell", "ggx", "fog", "cache"], default="rays")
     p.add_argument("--ref-spp", type=int, default=1024, help="cache workload: spp of the converged GPU reference")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true", help="skip the host-buffer measurement (profiling runs)")
@@ -216,19 +216,25 @@ RENDER_CONFIGS = {
     "ggx": dict(spp=64, max_depth=16, desc="GGX material scene: 256 spheres + 2M-triangle mound on a ground quad, "
                                            "random per-object materials (20% glass), 2 quad area lights + 1 point "
                                            "light, thin-lens camera, 1920x1080, 64 spp, max depth 16"),
+    "fog": dict(spp=16, max_depth=8, volumetric=True,
+                desc="foggy Cornell box: the Cornell box in a homogeneous medium (sigma_t 0.1, albedo 0.8, "
+                     "Henyey-Greenstein g 0.5) plus a point light under the lamp, volumetric path integrator, "
+                     "256x256, 16 spp, max depth 8"),
 }
 
 
 def render_scene(which):
     from rbr_b200 import scenes
 
+    if which == "fog":
+        return scenes.foggy_cornell_box()
     return scenes.cornell_box() if which == "cornell" else scenes.ggx_scene()
 
 
 def run_render(args, rank, world, local_rank):
     import torch
 
-    from rbr_b200 import Context, render_params
+    from rbr_b200 import Context, abi, render_params
 
     which = args.workload
     cfg = RENDER_CONFIGS[which]
@@ -242,8 +248,10 @@ def run_render(args, rank, world, local_rank):
     stream = torch.cuda.current_stream()
     paths = W * H * cfg["spp"]
 
+    flags = abi.RBR_RENDER_VOLUMETRIC if cfg.get("volumetric") else 0
+
     def step(k):
-        p = render_params(spp=cfg["spp"], max_depth=cfg["max_depth"], seed=rank * 1000003 + k)
+        p = render_params(spp=cfg["spp"], max_depth=cfg["max_depth"], seed=rank * 1000003 + k, flags=flags)
         ctx.render_dev(cam, p, film.data_ptr(), 0, stream.cuda_stream)
 
     for k in range(max(3, args.warmup)):
@@ -266,7 +274,7 @@ def run_render(args, rank, world, local_rank):
         t0 = time.perf_counter()
         e2e_steps = max(3, min(args.steps, 5))
         for k in range(e2e_steps):
-            ctx.render_host(cam, render_params(spp=cfg["spp"], max_depth=cfg["max_depth"], seed=k))
+            ctx.render_host(cam, render_params(spp=cfg["spp"], max_depth=cfg["max_depth"], seed=k, flags=flags))
         e2e_s = time.perf_counter() - t0
         e2e = {"value": paths * e2e_steps / e2e_s / 1e6, "unit": "Mpaths/s", "h2d_bytes_per_step": 0,
                "d2h_bytes_per_step": W * H * 12, "path": "rbr_render_host: render + film -> host"}
@@ -286,15 +294,18 @@ def run_render(args, rank, world, local_rank):
             small.height = max(8, H // 8)
             small.cy = small.cy - (H - small.height) / 2.0
             t0 = time.perf_counter()
-            ref.render(h, small, render_params(spp=cfg["spp"], max_depth=cfg["max_depth"]), threads=0)
+            ref.render(h, small, render_params(spp=cfg["spp"], max_depth=cfg["max_depth"]),
+                       volumetric=bool(flags), threads=0)
             dt = time.perf_counter() - t0
             base = {"value": W * small.height * cfg["spp"] / dt / 1e6, "unit": "Mpaths/s",
                     "cores": ref.max_threads(), "kind": "reference",
                     "sample": f"central {W}x{small.height} band of the image, the reference's own "
-                              f"Integrator::render (OpenMP rows), {dt:.1f} s"}
+                              f"Integrator::render with {'VolumetricPathIntegrator' if flags else 'PathTracingIntegrator'}"
+                              f" (OpenMP rows), {dt:.1f} s"}
     if rank == 0:
         print(json.dumps({
-            "metric": "Mpaths/s (camera samples per second), plain GPU path tracer", "value":
+            "metric": "Mpaths/s (camera samples per second), " + (
+                "GPU volumetric path tracer" if flags else "plain GPU path tracer"), "value":
                 paths * world * args.steps / (total_ms / 1e3) / 1e6, "unit": "Mpaths/s", "n_gpus": world,
             "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": total_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",

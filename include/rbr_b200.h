@@ -77,6 +77,15 @@ typedef struct rbr_light {
     float intensity;
 } rbr_light;
 
+/* render::HomogeneousMedium (include/render/materials/medium.h:54-70): absorption and
+ * scattering coefficients and the Henyey-Greenstein asymmetry g of its phase function. The
+ * medium fills all space (Scene::medium(), include/render/scene/scene.h:95). */
+typedef struct rbr_medium {
+    float sigma_a[3];
+    float sigma_s[3];
+    float g;
+} rbr_medium;
+
 typedef struct rbr_scene_desc {
     /* render::Triangle (include/render/geometry/triangle.h:13-52): v0, v1, v2 per triangle. */
     uint32_t num_triangles;
@@ -104,6 +113,7 @@ typedef struct rbr_scene_desc {
     uint32_t num_lights;                /* in Scene::lights() order */
     const rbr_light* lights;
     float background[3];                /* Scene::backgroundColor */
+    const rbr_medium* medium;           /* Scene::medium(), or NULL for none */
 } rbr_scene_desc;
 
 /* Sizes of what rbr_scene_upload built. */
@@ -165,7 +175,13 @@ enum {
      * Off by default so that images converge to what the reference converges to. */
     RBR_RENDER_CORRECTED_MIS = 1u << 0,
     /* Also return per-pixel sums of squared sample values (for Monte-Carlo error bars). */
-    RBR_RENDER_SECOND_MOMENT = 1u << 1
+    RBR_RENDER_SECOND_MOMENT = 1u << 1,
+    /* VolumetricPathIntegrator's estimator (src/renderers/volumetric_path_integrator.cpp:6-143)
+     * instead of PathTracingIntegrator's: distance sampling in the scene's medium, next-event
+     * estimation from scatter points towards point lights with transmittance and the phase
+     * function, emission added at every surface hit, surface next-event estimation without MIS
+     * weights, Russian roulette at surface vertices after depth 3. */
+    RBR_RENDER_VOLUMETRIC = 1u << 2
 };
 
 /* IntegratorConfig (include/render/renderers/integrator.h:22-28). */
@@ -374,6 +390,15 @@ rbr_status rbr_cache_train_host(rbr_ctx* ctx, uint32_t n, const rbr_cache_record
  * RBR_RENDER_SECOND_MOMENT) the sum of squared sample values. Asynchronous on `stream`. */
 rbr_status rbr_cache_render(rbr_ctx* ctx, const rbr_camera* camera, const rbr_render_params* params,
                             uint32_t frames, int train, float* film_mean, float* film_m2, void* stream);
+
+/* HenyeyGreensteinPhase::evaluate (src/materials/phase_function.cpp:17-21) for n (wo, wi). */
+rbr_status rbr_phase_eval_host(rbr_ctx* ctx, float g, uint32_t n, const float* wo, const float* wi, float* out);
+/* HenyeyGreensteinPhase::sample (phase_function.cpp:23-41) for n (wo, u1, u2); out: wi[3]. */
+rbr_status rbr_phase_sample_host(rbr_ctx* ctx, float g, uint32_t n, const float* wo, const float* u, float* out);
+/* HomogeneousMedium::sampleDistance (src/materials/medium.cpp:9-32) for n (maxDist, u);
+ * out: 5 floats each: t (0 without scattering), weight[3], scattered (0/1). */
+rbr_status rbr_medium_sample_host(rbr_ctx* ctx, const rbr_medium* medium, uint32_t n, const float* max_dist,
+                                  const float* u, float* out);
 
 /* Size of the fixed scratch array used by rbr_render_noalloc (16 MiB). */
 #define RBR_NOALLOC_SCRATCH_BYTES (16u << 20)

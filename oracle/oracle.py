@@ -66,6 +66,9 @@ class Restatement:
         L.orc_render.argtypes = [P, C.POINTER(abi.rbr_camera), C.POINTER(abi.rbr_render_params), P, P, P, C.c_int]
         L.orc_path.argtypes = [P, C.POINTER(abi.rbr_camera), C.POINTER(abi.rbr_render_params), C.c_int, C.c_int,
                                C.c_uint32, P]
+        L.orc_hg_eval.restype = C.c_float
+        L.orc_hg_eval.argtypes = [C.c_float, P, P]
+        L.orc_hg_sample.argtypes = [C.c_float, _i64, P, P, P]
         self.L = L
 
     def scene(self, scene):
@@ -112,6 +115,16 @@ class Restatement:
 
     def power_heuristic(self, nf, fp, ng, gp):
         return self.L.orc_power_heuristic(nf, fp, ng, gp)
+
+    def hg_eval(self, g, wo, wi):
+        wo, wi = _f(wo), _f(wi)
+        return np.array([self.L.orc_hg_eval(g, _ptr(wo[i]), _ptr(wi[i])) for i in range(len(wo))], np.float32)
+
+    def hg_sample(self, g, wo, u):
+        wo, u = _f(wo), _f(u)
+        out = np.zeros((len(wo), 3), np.float32)
+        self.L.orc_hg_sample(g, len(wo), _ptr(wo), _ptr(u), _ptr(out))
+        return out
 
     def philox(self, ctr, key):
         c = np.ascontiguousarray(ctr, np.uint32)
@@ -166,6 +179,9 @@ class Reference:
         L.ref_power_heuristic.restype = C.c_float
         L.ref_power_heuristic.argtypes = [C.c_int, C.c_float, C.c_int, C.c_float]
         L.ref_frame.argtypes = [P, P, P]
+        L.ref_hg_eval.argtypes = [C.c_float, _i64, P, P, P]
+        L.ref_hg_sample.argtypes = [C.c_float, _i64, P, P, P]
+        L.ref_medium_sample.argtypes = [C.POINTER(abi.rbr_medium), _i64, P, P, P]
         self.L = L
 
     def max_threads(self):
@@ -255,6 +271,25 @@ class Reference:
         n = _f(n)
         self.L.ref_frame(_ptr(n), _ptr(t), _ptr(b))
         return t, b
+
+    def hg_eval(self, g, wo, wi):
+        wo, wi = _f(wo), _f(wi)
+        out = np.zeros(len(wo), np.float32)
+        self.L.ref_hg_eval(g, len(wo), _ptr(wo), _ptr(wi), _ptr(out))
+        return out
+
+    def hg_sample(self, g, wo, u):
+        wo, u = _f(wo), _f(u)
+        out = np.zeros((len(wo), 3), np.float32)
+        self.L.ref_hg_sample(g, len(wo), _ptr(wo), _ptr(u), _ptr(out))
+        return out
+
+    def medium_sample(self, medium, max_dist, u):
+        """(n, 5): t, weight[3], scattered (HomogeneousMedium::sampleDistance)."""
+        md, u = _f(max_dist), _f(u)
+        out = np.zeros((len(md), 5), np.float32)
+        self.L.ref_medium_sample(C.byref(medium), len(md), _ptr(md), _ptr(u), _ptr(out))
+        return out
 
     def set_medium(self, h, sigma_a, sigma_s, g):
         sa, ss = _f(sigma_a), _f(sigma_s)

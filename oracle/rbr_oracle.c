@@ -97,7 +97,7 @@ void orc_philox(const uint32_t c[4], const uint32_t k[2], uint32_t out[4]) {
 static inline float u01(uint32_t x) { return (float)(x >> 8) * (1.0f / 16777216.0f); }
 
 /* Purposes of the fourth counter word (must match the GPU library). */
-enum { RNG_CAMERA = 0, RNG_BOUNCE = 1, RNG_LIGHTS = 2 };
+enum { RNG_CAMERA = 0, RNG_BOUNCE = 1, RNG_LIGHTS = 2, RNG_MEDIUM = 3 };
 
 static void draw4(uint64_t seed, uint32_t pixel, uint32_t sample, uint32_t depth, uint32_t purpose, float u[4]) {
     const uint32_t c[4] = {pixel, sample, depth, purpose};
@@ -136,6 +136,9 @@ struct orc_scene {
     uint32_t nlights;
     light* lights;
     v3 background;
+    int has_medium;          /* HomogeneousMedium (medium.h:54-70) */
+    v3 sigma_s, sigma_t;
+    float avg_sigma_t, g;
 };
 
 orc_scene* orc_scene_create(const rbr_scene_desc* d) {
@@ -216,6 +219,13 @@ orc_scene* orc_scene_create(const rbr_scene_desc* d) {
         o->normal = vnorm(vcross(o->u, o->v)); /* AreaLight::AreaLight, area_light.cpp:5-11 */
     }
     s->background = vload(d->background);
+    if (d->medium) {
+        s->has_medium = 1;
+        s->sigma_s = vload(d->medium->sigma_s);
+        s->sigma_t = vadd(vload(d->medium->sigma_a), s->sigma_s); /* Medium::getSigmaT */
+        s->avg_sigma_t = (s->sigma_t.x + s->sigma_t.y + s->sigma_t.z) / 3.0f;
+        s->g = d->medium->g;
+    }
     return s;
 }
 
@@ -1106,6 +1116,141 @@ static v3 path_li(const orc_scene* s, const rbr_render_params* p, ray_t ray, uin
     return L;
 }
 
+/* ---------------------------------------------------------------------------------------
+ * Participating medium and the volumetric path integrator (medium.cpp:9-44,
+ * phase_function.cpp:17-47, volumetric_path_integrator.cpp:6-143) with the counter RNG:
+ * per depth, the distance and the phase direction use purpose RNG_MEDIUM (u0; u1, u2), the
+ * surface lights and the BSDF the same streams as the path tracer.
+ * --------------------------------------------------------------------------------------- */
+float orc_hg_eval(float g, const float wo[3], const float wi[3]) {
+    const float c = vdot(vload(wo), vload(wi));
+    const float denom = 1.0f + g * g + 2.0f * g * c;
+    return (1.0f - g * g) / (4.0f * ORC_PI * denom * sqrtf(denom));
+}
+
+static v3 hg_sample(float g, v3 wo, float u1, float u2) {
+    float c;
+    if (fabsf(g) < 1e-3f) {
+        c = 1.0f - 2.0f * u1;
+    } else {
+        const float sq = (1.0f - g * g) / (1.0f + g - 2.0f * g * u1);
+        c = -(1.0f + g * g - sq * sq) / (2.0f * g);
+    }
+    const float st = sqrtf(omax(0.0f, 1.0f - c * c));
+    const float phi = TWO_PI * u2;
+    const frame f = make_frame(wo); /* coordinateSystem(wo, tangent, bitangent) */
+    return vadd(vadd(vmuls(f.t, st * cosf(phi)), vmuls(f.b, st * sinf(phi))), vmuls(wo, c));
+}
+
+static v3 transmittance(const orc_scene* s, float dist) {
+    return V(expf(-s->sigma_t.x * dist), expf(-s->sigma_t.y * dist), expf(-s->sigma_t.z * dist));
+}
+
+static int medium_sample(const orc_scene* s, float max_dist, float u, float* t, v3* weight) {
+    if (s->avg_sigma_t < 1e-6f) {
+        *weight = V(1, 1, 1);
+        return 0;
+    }
+    *t = -logf(1.0f - u) / s->avg_sigma_t;
+    if (*t < max_dist) {
+        const v3 tr = transmittance(s, *t);
+        *weight = vdivs(vmul(s->sigma_s, tr), s->avg_sigma_t * s->avg_sigma_t);
+        return 1;
+    }
+    *weight = transmittance(s, max_dist);
+    return 0;
+}
+
+void orc_hg_sample(float g, int64_t n, const float* wo, const float* u, float* out) {
+    for (int64_t i = 0; i < n; ++i) vstore(out + 3 * i, hg_sample(g, vload(wo + 3 * i), u[2 * i], u[2 * i + 1]));
+}
+
+static v3 vol_li(const orc_scene* s, const rbr_render_params* p, ray_t ray, uint32_t pixel, uint32_t sample) {
+    v3 L = V(0, 0, 0);
+    v3 T = V(1, 1, 1);
+    for (int depth = 0; depth < p->max_depth; ++depth) {
+        isect_t is;
+        const int hit = closest(s, ray, &is);
+        if (s->has_medium) {
+            float u[4];
+            draw4(p->seed, pixel, sample, (uint32_t)depth, RNG_MEDIUM, u);
+            float t = 0.0f;
+            v3 w;
+            const int scattered = medium_sample(s, hit ? is.t : INFINITY, u[0], &t, &w);
+            T = vmul(T, w);
+            if (scattered) {
+                const v3 sp = vadd(ray.o, vmuls(ray.d, t));
+                if (p->use_nee) {
+                    v3 Ld = V(0, 0, 0);
+                    for (uint32_t li = 0; li < s->nlights; ++li) {
+                        const light* l = &s->lights[li];
+                        if (l->type != RBR_LIGHT_POINT) continue;
+                        const v3 toL = vsub(l->position, sp);
+                        const float dist = vlen(toL);
+                        const v3 wi = vdivs(toL, dist);
+                        ray_t sh;
+                        sh.o = sp;
+                        sh.d = vnorm(wi);
+                        sh.tmax = dist;
+                        if (occluded(s, sh)) continue;
+                        const v3 tr = transmittance(s, dist);
+                        const v3 Li = vdivs(vmuls(l->color, l->intensity), dist * dist);
+                        const float wo3[3] = {ray.d.x, ray.d.y, ray.d.z}, wi3[3] = {wi.x, wi.y, wi.z};
+                        Ld = vadd(Ld, vmuls(vmul(Li, tr), orc_hg_eval(s->g, wo3, wi3)));
+                    }
+                    L = vadd(L, vmul(T, Ld));
+                }
+                ray.o = sp;
+                ray.d = vnorm(hg_sample(s->g, ray.d, u[1], u[2]));
+                ray.tmax = INFINITY;
+                continue;
+            }
+        }
+        if (!hit) {
+            L = vadd(L, vmul(T, s->background));
+            break;
+        }
+        const rbr_material* mat = &s->mats[s->prims[is.prim].material];
+        const v3 emission = vload(mat->emission);
+        if (emission.x > 0.0f || emission.y > 0.0f || emission.z > 0.0f) L = vadd(L, vmul(T, emission));
+        mixture bsdf;
+        create_bsdf(mat, &bsdf);
+        const v3 outward = is.front ? is.normal : vneg(is.normal);
+        const frame fr = make_frame(outward);
+        const v3 woL = to_local(&fr, is.wo);
+        if (p->use_nee && !mix_delta(&bsdf)) {
+            v3 Ld = V(0, 0, 0);
+            for (uint32_t li = 0; li < s->nlights; ++li) {
+                float u[4];
+                draw4(p->seed, pixel, sample, (uint32_t)depth, RNG_LIGHTS + ((li / 2) << 8), u);
+                const lsample ls = light_sample(&s->lights[li], is.point, u[(li & 1) * 2], u[(li & 1) * 2 + 1]);
+                if (ls.pdf <= 0.0f || vblack(ls.Li)) continue;
+                ray_t sh = spawn_ray(&is, ls.wi);
+                sh.tmax = ls.dist - ORC_EPS;
+                if (occluded(s, sh)) continue;
+                const v3 f = mix_eval(&bsdf, woL, to_local(&fr, ls.wi));
+                const float c = fabsf(vdot(ls.wi, is.normal));
+                Ld = vadd(Ld, vdivs(vmuls(vmul(f, ls.Li), c), ls.pdf));
+            }
+            L = vadd(L, vmul(T, Ld));
+        }
+        float u[4];
+        draw4(p->seed, pixel, sample, (uint32_t)depth, RNG_BOUNCE, u);
+        const bsample bs = mix_sample(&bsdf, woL, u[0], u[1]);
+        if (bs.pdf <= 0.0f || vblack(bs.f)) break;
+        const v3 wiW = to_world(&fr, bs.wi);
+        const float c = fabsf(vdot(wiW, is.normal));
+        T = vmul(T, vmuls(bs.f, c / bs.pdf));
+        if (depth > 3) {
+            const float q = omax(0.05f, 1.0f - vmaxc(T));
+            if (u[2] < q) break;
+            T = vdivs(T, 1.0f - q);
+        }
+        ray = spawn_ray(&is, wiW);
+    }
+    return L;
+}
+
 static int nthr(int n) {
 #ifdef _OPENMP
     extern int omp_get_max_threads(void);
@@ -1134,7 +1279,8 @@ void orc_render(const orc_scene* s, const rbr_camera* c, const rbr_render_params
                 const float px = (float)x + u[0];
                 const float py = (float)y + u[1];
                 const ray_t r = camera_ray(c, px, py, u[2], u[3]);
-                const v3 L = path_li(s, p, r, pixel, sample);
+                const v3 L = (p->flags & RBR_RENDER_VOLUMETRIC) ? vol_li(s, p, r, pixel, sample)
+                                                                : path_li(s, p, r, pixel, sample);
                 acc = vadd(acc, L);
                 s0 += L.x; s1 += L.y; s2 += L.z;
                 q0 += (double)L.x * L.x; q1 += (double)L.y * L.y; q2 += (double)L.z * L.z;
@@ -1153,5 +1299,5 @@ void orc_path(const orc_scene* s, const rbr_camera* c, const rbr_render_params* 
     float u[4];
     draw4(p->seed, pixel, sample, 0u, RNG_CAMERA, u);
     const ray_t r = camera_ray(c, (float)x + u[0], (float)y + u[1], u[2], u[3]);
-    vstore(Lout, path_li(s, p, r, pixel, sample));
+    vstore(Lout, (p->flags & RBR_RENDER_VOLUMETRIC) ? vol_li(s, p, r, pixel, sample) : path_li(s, p, r, pixel, sample));
 }

@@ -11,6 +11,8 @@
  *   light sampling                 src/lighting/{area_light,point_light}.cpp
  *   camera rays                    src/camera/{camera,thin_lens_camera}.cpp, perspective_intrinsics.h
  *   the path integrator            src/renderers/path_tracing_integrator.cpp, integrator.cpp
+ *   the volumetric path integrator src/renderers/volumetric_path_integrator.cpp,
+ *                                  src/materials/{medium,phase_function}.cpp
  * with one deliberate difference: random numbers come from the counter-based generator that
  * the GPU library uses (Philox-4x32-10 keyed by the seed, counters = pixel, sample, bounce,
  * purpose), so GPU and oracle draw identical numbers for identical (pixel, sample, bounce).
@@ -49,6 +51,10 @@ void orc_light_sample(const rbr_light* l, int64_t n, const float* points, const 
 void orc_camera_rays(const rbr_camera* c, int64_t n, const float* samples, float* out);
 
 float orc_power_heuristic(int nf, float fpdf, int ng, float gpdf);
+
+/* HenyeyGreensteinPhase::evaluate / sample (phase_function.cpp:17-41). */
+float orc_hg_eval(float g, const float wo[3], const float wi[3]);
+void orc_hg_sample(float g, int64_t n, const float* wo, const float* u, float* out);
 
 /* Philox-4x32-10 block: counters c[4], key k[2] -> out[4]. */
 void orc_philox(const uint32_t c[4], const uint32_t k[2], uint32_t out[4]);

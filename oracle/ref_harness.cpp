@@ -149,6 +149,9 @@ void* ref_scene_create(const rbr_scene_desc* d, int accel_type) {
         }
     }
     scene.backgroundColor = v3(d->background);
+    if (d->medium) {
+        scene.setMedium(std::make_unique<HomogeneousMedium>(v3(d->medium->sigma_a), v3(d->medium->sigma_s), d->medium->g));
+    }
     scene.setAcceleratorType(static_cast<AcceleratorType>(accel_type));
     scene.buildAccelerator();
     for (uint32_t i = 0; i < scene.primitives().size(); ++i) {
@@ -164,6 +167,32 @@ void ref_scene_destroy(void* s) { delete static_cast<RefScene*>(s); }
 void ref_scene_set_medium(void* s, const float sigma_a[3], const float sigma_s[3], float g) {
     static_cast<RefScene*>(s)->scene.setMedium(
         std::make_unique<HomogeneousMedium>(v3(sigma_a), v3(sigma_s), g));
+}
+
+// HenyeyGreensteinPhase::evaluate for n (wo, wi) pairs.
+void ref_hg_eval(float g, int64_t n, const float* wo, const float* wi, float* out) {
+    const HenyeyGreensteinPhase ph(g);
+    for (int64_t i = 0; i < n; ++i) out[i] = ph.evaluate(v3(wo + 3 * i), v3(wi + 3 * i));
+}
+
+// HenyeyGreensteinPhase::sample for n (wo, u1, u2).
+void ref_hg_sample(float g, int64_t n, const float* wo, const float* u, float* out) {
+    const HenyeyGreensteinPhase ph(g);
+    for (int64_t i = 0; i < n; ++i) put3(out + 3 * i, ph.sample(v3(wo + 3 * i), u[2 * i], u[2 * i + 1]));
+}
+
+// HomogeneousMedium::sampleDistance for n (maxDist, u): out = t, weight[3], scattered.
+void ref_medium_sample(const rbr_medium* m, int64_t n, const float* max_dist, const float* u, float* out) {
+    const HomogeneousMedium med(v3(m->sigma_a), v3(m->sigma_s), m->g);
+    const Ray ray(Vec3(0.0f), Vec3(0.0f, 0.0f, 1.0f));
+    for (int64_t i = 0; i < n; ++i) {
+        float t = 0.0f;
+        Color w;
+        const bool sc = med.sampleDistance(ray, max_dist[i], u[i], t, w);
+        out[5 * i] = sc ? t : 0.0f;
+        put3(out + 5 * i + 1, w);
+        out[5 * i + 4] = sc ? 1.0f : 0.0f;
+    }
 }
 
 // Closest hit through the scene's accelerator (Scene::intersect).

@@ -8,8 +8,8 @@
 
 namespace render {
 
-GpuPathIntegrator::GpuPathIntegrator(const IntegratorConfig& config, int device, uint64_t seed)
-    : Integrator(config), seed_(seed) {
+GpuPathIntegrator::GpuPathIntegrator(const IntegratorConfig& config, int device, uint64_t seed, bool volumetric)
+    : Integrator(config), seed_(seed), volumetric_(volumetric) {
     status_ = rbr_ctx_create(device, &ctx_);
     if (status_ != RBR_OK) error_ = "rbr_ctx_create failed (no usable CUDA device)";
 }
@@ -25,18 +25,14 @@ Color GpuPathIntegrator::Li(const Ray&, const Scene&, Sampler&) const {
 
 bool GpuPathIntegrator::upload(const Scene& scene) const {
     if (uploaded_ == &scene && uploaded_count_ == scene.primitives().size()) return true;
-    if (scene.hasMedium()) {
-        status_ = RBR_ERR_UNSUPPORTED;
-        error_ = "participating media are not supported by the GPU path tracer";
-        return false;
-    }
     FlatScene flat;
     std::vector<const Primitive*> prims;
     for (const auto& p : scene.primitives()) prims.push_back(p.get());
     std::vector<const Light*> lights;
     for (const auto& l : scene.lights()) lights.push_back(l.get());
     std::string err;
-    if (!flatten_primitives(prims, /*material_check=*/true, flat, err) || !flatten_lights(lights, flat, err)) {
+    if (!flatten_primitives(prims, /*material_check=*/true, flat, err) || !flatten_lights(lights, flat, err) ||
+        (volumetric_ && scene.hasMedium() && !flatten_medium(scene.medium(), flat, err))) {
         status_ = RBR_ERR_UNSUPPORTED;
         error_ = err;
         return false;
@@ -90,6 +86,7 @@ void GpuPathIntegrator::render(const Scene& scene, const Camera& camera, Film& f
     p.use_nee = config.useNEE ? 1 : 0;
     p.use_mis = config.useMIS ? 1 : 0;
     p.seed = seed_;
+    p.flags = volumetric_ ? RBR_RENDER_VOLUMETRIC : 0u;
     std::vector<float> mean(static_cast<size_t>(film.width) * film.height * 3);
     status_ = rbr_render_host(ctx_, &cam, &p, mean.data(), nullptr);
     if (status_ != RBR_OK) {

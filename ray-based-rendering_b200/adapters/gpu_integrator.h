@@ -8,11 +8,16 @@
 // (src/renderers/integrator.cpp:36). The estimator is the reference's
 // PathTracingIntegrator::Li, quirks included (see DESIGN.md of the library).
 //
+// With volumetric = true it is the drop-in for VolumetricPathIntegrator
+// (src/renderers/volumetric_path_integrator.cpp): the scene's HomogeneousMedium is uploaded and
+// the GPU runs that integrator's estimator (RBR_RENDER_VOLUMETRIC). Without it, as
+// PathTracingIntegrator does, the medium is ignored.
+//
 // Unsupported input — a Material subclass with its own createBSDF(), a camera other than
-// PinholeCamera/ThinLensCamera, a light other than AreaLight/PointLight, a participating
-// medium — leaves the film untouched and is reported by status()/error(). There is no CPU
-// fallback; Li() for single rays is not provided on the GPU and returns black with status
-// RBR_ERR_UNSUPPORTED.
+// PinholeCamera/ThinLensCamera, a light other than AreaLight/PointLight, in volumetric mode a
+// medium other than HomogeneousMedium with a Henyey-Greenstein phase function — leaves the
+// film untouched and is reported by status()/error(). There is no CPU fallback; Li() for
+// single rays is not provided on the GPU and returns black with status RBR_ERR_UNSUPPORTED.
 #pragma once
 
 #include <cstdint>
@@ -27,12 +32,12 @@ namespace render {
 class GpuPathIntegrator : public Integrator {
 public:
     explicit GpuPathIntegrator(const IntegratorConfig& config = IntegratorConfig(), int device = 0,
-                               uint64_t seed = 0);
+                               uint64_t seed = 0, bool volumetric = false);
     ~GpuPathIntegrator() override;
     GpuPathIntegrator(const GpuPathIntegrator&) = delete;
     GpuPathIntegrator& operator=(const GpuPathIntegrator&) = delete;
 
-    std::string name() const override { return "GPU Path Tracing"; }
+    std::string name() const override { return volumetric_ ? "GPU Volumetric Path Tracing" : "GPU Path Tracing"; }
     Color Li(const Ray& ray, const Scene& scene, Sampler& sampler) const override;
     void render(const Scene& scene, const Camera& camera, Film& film,
                 std::function<void(float)> progress = nullptr) const override;
@@ -47,6 +52,7 @@ private:
 
     rbr_ctx* ctx_ = nullptr;
     uint64_t seed_;
+    bool volumetric_;
     mutable std::mutex mu_;
     mutable const Scene* uploaded_ = nullptr;
     mutable size_t uploaded_count_ = 0;

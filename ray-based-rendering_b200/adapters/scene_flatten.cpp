@@ -126,6 +126,21 @@ bool flatten_lights(const std::vector<const Light*>& lights, FlatScene& out, std
     return true;
 }
 
+bool flatten_medium(const Medium* medium, FlatScene& out, std::string& error) {
+    const auto* h = dynamic_cast<const HomogeneousMedium*>(medium);
+    const auto* hg = h ? dynamic_cast<const HenyeyGreensteinPhase*>(h->getPhaseFunction()) : nullptr;
+    if (!h || !hg) {
+        error = std::string("unsupported medium ") + (medium ? typeid(*medium).name() : "(null)") +
+                " (the GPU path implements HomogeneousMedium with a Henyey-Greenstein phase function)";
+        return false;
+    }
+    put3(out.medium.sigma_a, h->sigma_a);
+    put3(out.medium.sigma_s, h->sigma_s);
+    out.medium.g = hg->g;
+    out.has_medium = true;
+    return true;
+}
+
 void FlatScene::finalize(const float background[3]) {
     desc = rbr_scene_desc{};
     desc.num_triangles = static_cast<uint32_t>(tri_mat.size());
@@ -150,6 +165,7 @@ void FlatScene::finalize(const float background[3]) {
     desc.num_lights = static_cast<uint32_t>(lights.size());
     desc.lights = lights.data();
     for (int a = 0; a < 3; ++a) desc.background[a] = background[a];
+    desc.medium = has_medium ? &medium : nullptr;
 }
 
 }  // namespace render

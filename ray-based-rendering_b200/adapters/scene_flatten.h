@@ -9,6 +9,7 @@
 #include "render/geometry/primitive.h"
 #include "render/lighting/light.h"
 #include "render/materials/material.h"
+#include "render/materials/medium.h"
 
 namespace render {
 
@@ -18,6 +19,8 @@ struct FlatScene {
     std::vector<uint32_t> tri_mat, tri_id, sph_mat, sph_id, quad_mat, quad_id, plane_mat, plane_id;
     std::vector<rbr_material> materials;
     std::vector<rbr_light> lights;
+    rbr_medium medium{};
+    bool has_medium = false;
     bool any_normals = false;
     rbr_scene_desc desc{};
 
@@ -34,5 +37,9 @@ bool flatten_primitives(const std::vector<const Primitive*>& prims, bool materia
 
 // Adds AreaLight / PointLight lights; false with `error` for any other light type.
 bool flatten_lights(const std::vector<const Light*>& lights, FlatScene& out, std::string& error);
+
+// Sets the scene's HomogeneousMedium with its Henyey-Greenstein phase function; false with
+// `error` for any other medium or phase function.
+bool flatten_medium(const Medium* medium, FlatScene& out, std::string& error);
 
 }  // namespace render

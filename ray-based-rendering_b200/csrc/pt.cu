@@ -145,39 +145,104 @@ __global__ void k_begin(Paths P, uint32_t d) {
     c[kCShadow] = 0;
 }
 
+// Closest hit for the active queue; misses add the background, hits are appended to their
+// material-class queue. kVol (VolumetricPathIntegrator::Li, volumetric_path_integrator.cpp:
+// 11-43): a distance is sampled in the scene's medium up to the hit (or infinity) and the
+// throughput multiplied by the medium weight; a scattering event is handled here: next-event
+// estimation towards point lights (directLightingVolume, :92-118) and a phase-function sample
+// that continues the path from the scatter point.
+template <bool kVol>
 __global__ void __launch_bounds__(kBlock) k_extend(DeviceScene s, Wave w, Paths P, uint32_t d, int* err) {
     const uint32_t n = P.counters[kCQ0 + (d & 1)];
     const uint32_t* q = (d & 1) ? P.q1 : P.q0;
+    uint32_t* nextq = (d & 1) ? P.q0 : P.q1;
+    uint32_t* nextc = P.counters + kCQ0 + ((d + 1) & 1);
+    const bool last = d + 1 >= w.max_depth;
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(reinterpret_cast<unsigned long long*>(P.counters + kCExt), n);
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {
         const uint32_t j = base + threadIdx.x;
         const bool valid = j < n;
         uint32_t k = 0, cls = kNumClasses;
+        bool scatter = false;
+        f3 T = mk(0.0f, 0.0f, 0.0f), sp = T, rd = T;
+        float4 u = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         if (valid) {
             k = q[j];
             const float4 a = P.ray[2 * k], b = P.ray[2 * k + 1];
             float t = 0.0f;
-            // A ray with a zero or non-finite direction or origin hits nothing (every primitive
-            // test rejects it) but would pass every box test: skip the traversal.
+            // A ray with a zero or non-finite direction or origin: no traversal, no hit.
             const uint32_t prim = degenerate(a, b) ? 0xFFFFFFFFu
                                                    : traverse<false>(s, ld_f3(a), ld_f3(b), __int_as_float(0x7f800000), t, err);
             P.hit[k] = make_uint2(prim, __float_as_uint(t));
-            if (prim == 0xFFFFFFFFu) {
-                const float4 T = P.thr[k];
-                float4 L = P.rad[k];
-                L.x = fa(L.x, fm(T.x, s.background[0]));
-                L.y = fa(L.y, fm(T.y, s.background[1]));
-                L.z = fa(L.z, fm(T.z, s.background[2]));
-                P.rad[k] = L;
-            } else {
-                cls = s.materials[s.prim_material[prim]].cls;
+            if (kVol && s.has_medium) {
+                const float4 T4 = P.thr[k];
+                T = ld_f3(T4);
+                const uint32_t pixel = w.p0 + k / w.spp, sample = w.sample_offset + k % w.spp;
+                u = draw4(w.seed, pixel, sample, d, kRngMedium);
+                float ts = 0.0f;
+                f3 wgt;
+                scatter = medium_sample(s, prim == 0xFFFFFFFFu ? __int_as_float(0x7f800000) : t, u.x, ts, wgt);
+                T = xmul(T, wgt);
+                P.thr[k] = make_float4(T.x, T.y, T.z, T4.w);
+                if (scatter) {
+                    rd = ld_f3(b);
+                    sp = xadd(ld_f3(a), xmuls(rd, ts));  // Ray::at
+                }
+            }
+            if (!scatter) {
+                if (prim == 0xFFFFFFFFu) {
+                    if (!(kVol && s.has_medium)) T = ld_f3(P.thr[k]);
+                    float4 L = P.rad[k];
+                    L.x = fa(L.x, fm(T.x, s.background[0]));
+                    L.y = fa(L.y, fm(T.y, s.background[1]));
+                    L.z = fa(L.z, fm(T.z, s.background[2]));
+                    P.rad[k] = L;
+                } else {
+                    cls = s.materials[s.prim_material[prim]].cls;
+                }
             }
         }
 #pragma unroll
         for (uint32_t c = 0; c < kNumClasses; ++c) {
             const uint32_t slot = warp_append(P.counters + kCClass + c, cls == c);
             if (cls == c) P.classq[c * P.cap + slot] = k;
+        }
+        if (kVol) {
+            // next-event estimation from the scatter point: point lights only, unoccluded
+            // segment of length dist, Li * Tr(dist) * phase(wo = ray direction, wi)
+            for (uint32_t l = 0; l < s.num_lights; ++l) {
+                bool emit = false;
+                f3 contrib, sd;
+                float dist = 0.0f;
+                if (scatter && w.use_nee && s.lights[l].type == RBR_LIGHT_POINT) {
+                    const LightDev& L = s.lights[l];
+                    const f3 toL = xsub(ld3(L.position), sp);
+                    dist = xlen(toL);
+                    const f3 wi = xdivs(toL, dist);
+                    sd = xnorm(wi);  // the shadow Ray's constructor normalises
+                    const f3 Li = xdivs(xmuls(ld3(L.color), L.intensity), fm(dist, dist));
+                    const float ph = hg_eval(s.hg_g, rd, wi);
+                    contrib = xmul(T, xmuls(xmul(Li, transmittance(s, dist)), ph));
+                    emit = true;
+                }
+                const uint32_t slot = warp_append(P.counters + kCShadow, emit);
+                if (emit && slot < P.shadow_cap) {
+                    float4* e = P.shadow + 3 * static_cast<size_t>(slot);
+                    e[0] = make_float4(sp.x, sp.y, sp.z, dist);
+                    e[1] = make_float4(sd.x, sd.y, sd.z, __uint_as_float(k));
+                    e[2] = make_float4(contrib.x, contrib.y, contrib.z, 0.0f);
+                }
+            }
+            // the path continues from the scatter point in a phase-function direction
+            const bool cont = scatter && !last;
+            if (cont) {
+                const f3 nd = xnorm(hg_sample(s.hg_g, rd, u.y, u.z));
+                P.ray[2 * k] = make_float4(sp.x, sp.y, sp.z, 0.0f);
+                P.ray[2 * k + 1] = make_float4(nd.x, nd.y, nd.z, 0.0f);
+            }
+            const uint32_t slot = warp_append(nextc, cont);
+            if (cont) nextq[slot] = k;
         }
     }
 }
@@ -258,8 +323,12 @@ __device__ __forceinline__ bool train_path(const Wave& w, uint32_t pixel, uint32
     return x < w.train_thresh;
 }
 
-template <bool kCache>
+// Surface vertices, per material-class queue. kMode 0: PathTracingIntegrator::Li; 1: the same
+// with the radiance cache; 2: the surface part of VolumetricPathIntegrator::Li
+// (volumetric_path_integrator.cpp:45-88: emission at every hit, NEE without MIS weights).
+template <int kMode>
 __global__ void __launch_bounds__(kBlock) k_shade(DeviceScene s, Wave w, Paths P, uint32_t d) {
+    constexpr bool kCache = kMode == 1, kVolSurface = kMode == 2;
     uint32_t cnt[kNumClasses + 1];
     cnt[0] = 0;
     for (int c = 0; c < kNumClasses; ++c) cnt[c + 1] = cnt[c] + P.counters[kCClass + c];
@@ -293,7 +362,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(DeviceScene s, Wave w, Paths P
             const bool specular = t4.w != 0.0f;
             h = surface(s, hv.x, __uint_as_float(hv.y), ro, rd);
             const MaterialDev& m = s.materials[s.prim_material[hv.x]];
-            if (m.emissive && (d == 0 || specular)) {
+            if (m.emissive && (kVolSurface || d == 0 || specular)) {
                 float4 L = P.rad[k];
                 L.x = fa(L.x, fm(T.x, m.emission[0]));
                 L.y = fa(L.y, fm(T.y, m.emission[1]));
@@ -355,7 +424,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(DeviceScene s, Wave w, Paths P
                         stmax = fs(ls.dist, kEpsilon);
                         const float c = fabsf(xdot(ls.wi, h.normal));
                         f3 ld;
-                        if (w.use_mis && !ls.delta) {
+                        if (!kVolSurface && w.use_mis && !ls.delta) {
                             const float wgt = power_heuristic(ls.pdf, bpdf);
                             ld = xdivs(xmuls(xmuls(xmul(f, ls.Li), c), wgt), ls.pdf);
                         } else {
@@ -521,6 +590,7 @@ rbr_status render(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_params* 
     if (p->flags & RBR_RENDER_CORRECTED_MIS)
         return fail(ctx, RBR_ERR_UNSUPPORTED, "RBR_RENDER_CORRECTED_MIS is not implemented");
     if ((p->flags & RBR_RENDER_SECOND_MOMENT) == 0) film_m2 = nullptr;
+    const bool volumetric = (p->flags & RBR_RENDER_VOLUMETRIC) != 0;
     const uint64_t npix = uint64_t(cam->width) * cam->height;
     const uint32_t spp = static_cast<uint32_t>(p->samples_per_pixel);
     if (npix * spp > 0xFFFFFFFFull || spp > kDefaultCapacity)
@@ -583,8 +653,13 @@ rbr_status render(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_params* 
         ++launches;
         for (uint32_t d = 0; d < w.max_depth; ++d) {
             k_begin<<<1, 1, 0, stream>>>(P, d);
-            k_extend<<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d, ctx->d_error);
-            k_shade<false><<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d);
+            if (volumetric) {
+                k_extend<true><<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d, ctx->d_error);
+                k_shade<2><<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d);
+            } else {
+                k_extend<false><<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d, ctx->d_error);
+                k_shade<0><<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d);
+            }
             k_shadow<<<grid, kBlock, 0, stream>>>(ctx->scene, P, ctx->d_error);
             launches += 4;
         }
@@ -650,6 +725,8 @@ rbr_status render_cached(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_p
         return fail(ctx, RBR_ERR_UNSUPPORTED, "camera model " + std::to_string(cam->model));
     if (p->flags & RBR_RENDER_CORRECTED_MIS)
         return fail(ctx, RBR_ERR_UNSUPPORTED, "RBR_RENDER_CORRECTED_MIS is not implemented");
+    if (p->flags & RBR_RENDER_VOLUMETRIC)
+        return fail(ctx, RBR_ERR_UNSUPPORTED, "the radiance cache serves the surface path tracer, not RBR_RENDER_VOLUMETRIC");
     if ((p->flags & RBR_RENDER_SECOND_MOMENT) == 0) film_m2 = nullptr;
     const uint64_t npix = uint64_t(cam->width) * cam->height;
     const uint32_t spp = static_cast<uint32_t>(p->samples_per_pixel);
@@ -722,8 +799,8 @@ rbr_status render_cached(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_p
             ++launches;
             for (uint32_t d = 0; d < w.max_depth; ++d) {
                 k_begin<<<1, 1, 0, stream>>>(P, d);
-                k_extend<<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d, ctx->d_error);
-                k_shade<true><<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d);
+                k_extend<false><<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d, ctx->d_error);
+                k_shade<1><<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d);
                 k_shadow<<<grid, kBlock, 0, stream>>>(ctx->scene, P, ctx->d_error);
                 launches += 4;
             }
@@ -875,8 +952,8 @@ rbr_status render_noalloc(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_
         k_raygen<<<grid, kBlock, 0, stream>>>(cd, w, P);
         for (uint32_t d = 0; d < w.max_depth; ++d) {
             k_begin<<<1, 1, 0, stream>>>(P, d);
-            k_extend<<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d, ctx->d_error);
-            k_shade<false><<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d);
+            k_extend<false><<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d, ctx->d_error);
+            k_shade<0><<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d);
             k_shadow<<<grid, kBlock, 0, stream>>>(ctx->scene, P, ctx->d_error);
         }
         k_film<<<grid, kBlock, 0, stream>>>(w, P, film_mean, nullptr);

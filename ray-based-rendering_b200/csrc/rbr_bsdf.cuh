@@ -59,7 +59,7 @@ __device__ __forceinline__ void sincos_cr(float x, float& s, float& c) {
 // Philox-4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11). Counter = (pixel, sample, depth,
 // purpose), key = seed. The same streams as the CPU restatement in oracle/rbr_oracle.c.
 // ----------------------------------------------------------------------------------------
-enum : uint32_t { kRngCamera = 0, kRngBounce = 1, kRngLights = 2 };
+enum : uint32_t { kRngCamera = 0, kRngBounce = 1, kRngLights = 2, kRngMedium = 3 };
 
 __device__ __forceinline__ uint4 philox(uint4 c, uint2 k) {
 #pragma unroll
@@ -574,6 +574,57 @@ __device__ __forceinline__ LSample light_sample(const LightDev& l, f3 p, float u
         s.delta = true;
     }
     return s;
+}
+
+// ----------------------------------------------------------------------------------------
+// Participating medium (src/materials/medium.cpp:9-44, src/materials/phase_function.cpp:17-47)
+// ----------------------------------------------------------------------------------------
+// HenyeyGreensteinPhase::evaluate: (1 - g^2) / (4 pi denom sqrt(denom)),
+// denom = 1 + g^2 + 2 g cos(wo, wi), with wo the propagation direction (the reference's sign).
+__device__ __forceinline__ float hg_eval(float g, f3 wo, f3 wi) {
+    const float c = xdot(wo, wi);
+    const float denom = fa(fa(1.0f, fm(g, g)), fm(fm(2.0f, g), c));
+    return fd(fs(1.0f, fm(g, g)), fm(fm(fm(4.0f, kPi), denom), fq(denom)));
+}
+
+// HenyeyGreensteinPhase::sample: cos(theta) by inversion, phi = 2 pi u2, around wo.
+__device__ __forceinline__ f3 hg_sample(float g, f3 wo, float u1, float u2) {
+    float c;
+    if (fabsf(g) < 1e-3f) {
+        c = fs(1.0f, fm(2.0f, u1));
+    } else {
+        const float sq = fd(fs(1.0f, fm(g, g)), fs(fa(1.0f, g), fm(fm(2.0f, g), u1)));
+        c = fd(-fs(fa(1.0f, fm(g, g)), fm(sq, sq)), fm(2.0f, g));
+    }
+    const float st = fq(omax(0.0f, fs(1.0f, fm(c, c))));
+    const float phi = fm(kTwoPi, u2);
+    float sp, cp;
+    sincos_cr(phi, sp, cp);
+    const Frame f = make_frame(wo);  // coordinateSystem(wo, tangent, bitangent)
+    return xadd(xadd(xmuls(f.t, fm(st, cp)), xmuls(f.b, fm(st, sp))), xmuls(wo, c));
+}
+
+// HomogeneousMedium::transmittance: exp(-sigma_t * distance) per channel.
+__device__ __forceinline__ f3 transmittance(const DeviceScene& s, float dist) {
+    return mk(expf(fm(-s.sigma_t[0], dist)), expf(fm(-s.sigma_t[1], dist)), expf(fm(-s.sigma_t[2], dist)));
+}
+
+// HomogeneousMedium::sampleDistance: exponential distance with the mean extinction; returns
+// true and the distance t for a scattering event before maxDist (weight sigma_s * Tr / avg^2),
+// else false with weight Tr(maxDist).
+__device__ __forceinline__ bool medium_sample(const DeviceScene& s, float max_dist, float u, float& t, f3& weight) {
+    if (s.avg_sigma_t < 1e-6f) {
+        weight = mk(1.0f, 1.0f, 1.0f);
+        return false;
+    }
+    t = fd(-logf(fs(1.0f, u)), s.avg_sigma_t);
+    if (t < max_dist) {
+        const f3 tr = transmittance(s, t);
+        weight = xdivs(xmul(ld3(s.sigma_s), tr), fm(s.avg_sigma_t, s.avg_sigma_t));
+        return true;
+    }
+    weight = transmittance(s, max_dist);
+    return false;
 }
 
 // ----------------------------------------------------------------------------------------

@@ -44,6 +44,12 @@ struct DeviceScene {
     uint32_t num_materials;
     uint32_t num_lights;
     float background[3];
+    // homogeneous medium (HomogeneousMedium, src/materials/medium.cpp:9-44)
+    uint32_t has_medium;
+    float sigma_s[3];
+    float sigma_t[3];   // sigma_a + sigma_s
+    float avg_sigma_t;  // (sigma_t.x + sigma_t.y + sigma_t.z) / 3
+    float hg_g;         // Henyey-Greenstein asymmetry
 };
 
 }  // namespace rbr

@@ -212,6 +212,9 @@ rbr_status upload_scene(rbr_ctx* ctx, const rbr_scene_desc* d) {
             !std::isfinite(m.roughness) || !std::isfinite(m.ior) || !std::isfinite(m.transmission))
             return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "material " + std::to_string(i) + " has a non-finite parameter");
     }
+    if (d->medium && (!finite3(d->medium->sigma_a, 3) || !finite3(d->medium->sigma_s, 3) ||
+                      !std::isfinite(d->medium->g) || std::fabs(d->medium->g) >= 1.0f))
+        return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "medium has a non-finite coefficient or |g| >= 1");
     for (uint32_t i = 0; i < d->num_lights; ++i) {
         const rbr_light& l = d->lights[i];
         if (l.type != RBR_LIGHT_AREA && l.type != RBR_LIGHT_POINT)
@@ -380,6 +383,16 @@ rbr_status upload_scene(rbr_ctx* ctx, const rbr_scene_desc* d) {
     s.num_materials = d->num_materials;
     s.num_lights = d->num_lights;
     std::memcpy(s.background, d->background, 12);
+    s.has_medium = d->medium ? 1u : 0u;
+    if (d->medium) {
+        // Color sigma_t = sigma_a + sigma_s; avgSigmaT = (x + y + z) / 3 (medium.cpp:13-14)
+        for (int a = 0; a < 3; ++a) {
+            s.sigma_s[a] = d->medium->sigma_s[a];
+            s.sigma_t[a] = d->medium->sigma_a[a] + d->medium->sigma_s[a];
+        }
+        s.avg_sigma_t = (s.sigma_t[0] + s.sigma_t[1] + s.sigma_t[2]) / 3.0f;
+        s.hg_g = d->medium->g;
+    }
     ctx->scene = s;
     ctx->has_scene = true;
     for (int a = 0; a < 3; ++a) {

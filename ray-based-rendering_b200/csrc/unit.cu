@@ -44,6 +44,35 @@ __global__ void k_bsdf_sample(MaterialDev m, uint32_t n, const float* wo, const 
     r[7] = s.delta ? 1.0f : 0.0f;
 }
 
+__global__ void k_hg_eval(float g, uint32_t n, const float* wo, const float* wi, float* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[i] = hg_eval(g, ld3(wo + 3 * i), ld3(wi + 3 * i));
+}
+
+__global__ void k_hg_sample(float g, uint32_t n, const float* wo, const float* u, float* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const f3 w = hg_sample(g, ld3(wo + 3 * i), u[2 * i], u[2 * i + 1]);
+    out[3 * i] = w.x;
+    out[3 * i + 1] = w.y;
+    out[3 * i + 2] = w.z;
+}
+
+__global__ void k_medium_sample(DeviceScene s, uint32_t n, const float* max_dist, const float* u, float* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float t = 0.0f;
+    f3 w;
+    const bool sc = medium_sample(s, max_dist[i], u[i], t, w);
+    float* r = out + 5 * i;  // t, weight[3], scattered
+    r[0] = sc ? t : 0.0f;
+    r[1] = w.x;
+    r[2] = w.y;
+    r[3] = w.z;
+    r[4] = sc ? 1.0f : 0.0f;
+}
+
 __global__ void k_light_sample(LightDev l, uint32_t n, const float* p, const float* u, float* out) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -221,6 +250,45 @@ rbr_status rbr_mis_weights_host(rbr_ctx* ctx, uint32_t n, const float* pdf_pairs
     return run_unit(ctx, {{pdf_pairs, 2 * size_t(n)}}, size_t(n), out,
                     [&](const std::vector<const float*>& d, float* o) {
                         k_mis<<<blocks(n), kUnitBlock, 0, ctx->stream>>>(n, d[0], o);
+                    });
+}
+
+rbr_status rbr_phase_eval_host(rbr_ctx* ctx, float g, uint32_t n, const float* wo, const float* wi, float* out) {
+    if (!ctx || (n && (!wo || !wi || !out))) return RBR_ERR_INVALID_ARGUMENT;
+    if (n == 0) return RBR_OK;
+    cudaSetDevice(ctx->device);
+    return run_unit(ctx, {{wo, 3 * size_t(n)}, {wi, 3 * size_t(n)}}, size_t(n), out,
+                    [&](const std::vector<const float*>& d, float* o) {
+                        k_hg_eval<<<blocks(n), kUnitBlock, 0, ctx->stream>>>(g, n, d[0], d[1], o);
+                    });
+}
+
+rbr_status rbr_phase_sample_host(rbr_ctx* ctx, float g, uint32_t n, const float* wo, const float* u, float* out) {
+    if (!ctx || (n && (!wo || !u || !out))) return RBR_ERR_INVALID_ARGUMENT;
+    if (n == 0) return RBR_OK;
+    cudaSetDevice(ctx->device);
+    return run_unit(ctx, {{wo, 3 * size_t(n)}, {u, 2 * size_t(n)}}, 3 * size_t(n), out,
+                    [&](const std::vector<const float*>& d, float* o) {
+                        k_hg_sample<<<blocks(n), kUnitBlock, 0, ctx->stream>>>(g, n, d[0], d[1], o);
+                    });
+}
+
+rbr_status rbr_medium_sample_host(rbr_ctx* ctx, const rbr_medium* medium, uint32_t n, const float* max_dist,
+                                  const float* u, float* out) {
+    if (!ctx || !medium || (n && (!max_dist || !u || !out))) return RBR_ERR_INVALID_ARGUMENT;
+    if (n == 0) return RBR_OK;
+    cudaSetDevice(ctx->device);
+    DeviceScene s{};
+    s.has_medium = 1;
+    for (int a = 0; a < 3; ++a) {
+        s.sigma_s[a] = medium->sigma_s[a];
+        s.sigma_t[a] = medium->sigma_a[a] + medium->sigma_s[a];
+    }
+    s.avg_sigma_t = (s.sigma_t[0] + s.sigma_t[1] + s.sigma_t[2]) / 3.0f;
+    s.hg_g = medium->g;
+    return run_unit(ctx, {{max_dist, size_t(n)}, {u, size_t(n)}}, 5 * size_t(n), out,
+                    [&](const std::vector<const float*>& d, float* o) {
+                        k_medium_sample<<<blocks(n), kUnitBlock, 0, ctx->stream>>>(s, n, d[0], d[1], o);
                     });
 }
 

@@ -65,6 +65,9 @@ def load_library() -> C.CDLL:
         "rbr_light_sample_host": (C.c_int, [P, C.POINTER(abi.rbr_light), C.c_uint32, P, P, P]),
         "rbr_camera_rays_host": (C.c_int, [P, C.POINTER(abi.rbr_camera), C.c_uint32, P, P]),
         "rbr_mis_weights_host": (C.c_int, [P, C.c_uint32, P, P]),
+        "rbr_phase_eval_host": (C.c_int, [P, C.c_float, C.c_uint32, P, P, P]),
+        "rbr_phase_sample_host": (C.c_int, [P, C.c_float, C.c_uint32, P, P, P]),
+        "rbr_medium_sample_host": (C.c_int, [P, C.POINTER(abi.rbr_medium), C.c_uint32, P, P, P]),
         "rbr_param_set": (C.c_int, [P, C.c_char_p, C.c_int64]),
         "rbr_param_get": (C.c_int, [P, C.c_char_p, C.POINTER(C.c_int64)]),
         "rbr_autotune_trace": (C.c_int, [P, P, C.c_uint32, C.c_int, C.POINTER(C.c_int64)]),
@@ -317,6 +320,20 @@ class Context:
         self._check(self.lib.rbr_cache_render(self.h, C.byref(camera), C.byref(params), frames, int(train),
                                               C.c_void_p(film_mean_ptr), C.c_void_p(film_m2_ptr or None),
                                               C.c_void_p(stream)))
+
+    def phase_eval(self, g, wo, wi):
+        n = len(wo)
+        return self._unit(lambda h, a, b, o: self.lib.rbr_phase_eval_host(h, g, n, a, b, o), [wo, wi], n, 1)[:, 0]
+
+    def phase_sample(self, g, wo, u):
+        n = len(wo)
+        return self._unit(lambda h, a, b, o: self.lib.rbr_phase_sample_host(h, g, n, a, b, o), [wo, u], n, 3)
+
+    def medium_sample(self, medium: abi.rbr_medium, max_dist, u):
+        """(n, 5): t, weight[3], scattered."""
+        n = len(max_dist)
+        return self._unit(lambda h, a, b, o: self.lib.rbr_medium_sample_host(h, C.byref(medium), n, a, b, o),
+                          [max_dist, u], n, 5)
 
     def render_stats(self) -> abi.rbr_render_stats:
         s = abi.rbr_render_stats()

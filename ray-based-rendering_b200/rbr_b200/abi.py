@@ -36,6 +36,7 @@ RBR_CAMERA_PINHOLE = 0
 RBR_CAMERA_THIN_LENS = 1
 RBR_RENDER_CORRECTED_MIS = 1 << 0
 RBR_RENDER_SECOND_MOMENT = 1 << 1
+RBR_RENDER_VOLUMETRIC = 1 << 2
 
 _f3 = C.c_float * 3
 _u32p = C.POINTER(C.c_uint32)
@@ -64,6 +65,10 @@ class rbr_light(C.Structure):
     ]
 
 
+class rbr_medium(C.Structure):
+    _fields_ = [("sigma_a", _f3), ("sigma_s", _f3), ("g", C.c_float)]
+
+
 class rbr_scene_desc(C.Structure):
     _fields_ = [
         ("num_triangles", C.c_uint32),
@@ -88,6 +93,7 @@ class rbr_scene_desc(C.Structure):
         ("num_lights", C.c_uint32),
         ("lights", C.POINTER(rbr_light)),
         ("background", _f3),
+        ("medium", C.POINTER(rbr_medium)),
     ]
 
 

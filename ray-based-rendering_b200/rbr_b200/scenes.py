@@ -94,6 +94,7 @@ class Scene:
     materials: list = field(default_factory=list)  # list of dicts
     lights: list = field(default_factory=list)  # list of dicts
     background: tuple = (0.0, 0.0, 0.0)
+    medium: dict | None = None  # sigma_a, sigma_s, g (a homogeneous medium filling all space)
     camera: object = None  # rbr_camera or None
     name: str = "scene"
 
@@ -121,6 +122,10 @@ class Scene:
     def point_light(self, position, color, intensity=1.0):
         self.lights.append(dict(type=abi.RBR_LIGHT_POINT, position=tuple(position), u=(0, 0, 0), v=(0, 0, 0),
                                 color=tuple(color), intensity=float(intensity)))
+
+    def set_medium(self, sigma_a, sigma_s, g=0.0):
+        """SceneBuilder::medium (src/scene/scene_builder.cpp:102-105): a HomogeneousMedium."""
+        self.medium = dict(sigma_a=tuple(sigma_a), sigma_s=tuple(sigma_s), g=float(g))
 
     def desc(self) -> "SceneDesc":
         return SceneDesc(self)
@@ -189,6 +194,13 @@ class SceneDesc:
         d.num_lights = len(s.lights)
         d.lights = C.cast(lts, C.POINTER(abi.rbr_light))
         d.background = abi.f3(s.background)
+        if s.medium is not None:
+            med = abi.rbr_medium()
+            med.sigma_a = abi.f3(s.medium["sigma_a"])
+            med.sigma_s = abi.f3(s.medium["sigma_s"])
+            med.g = s.medium["g"]
+            keep(med)
+            d.medium = C.pointer(med)
         self.desc = d
 
     @property
@@ -285,6 +297,21 @@ def cornell_box(width=256, height=256) -> Scene:
     # AreaLight is centre-based (area_light.cpp:13-16); u x v = -y faces the room
     s.area_light((0.0, 1.99, 0.0), (0.5, 0, 0), (0, 0, 0.5), (17.0, 12.0, 4.0), 1.0)
     s.camera = look_at_camera(width, height, (0.0, 1.0, 3.5), (0.0, 1.0, 0.0), (0.0, 1.0, 0.0), 40.0)
+    return s
+
+
+def foggy_cornell_box(width=256, height=256, sigma_t=0.1, albedo=0.8, g=0.5, point_light=True) -> Scene:
+    """The Cornell box filled with a homogeneous medium: sigma_t 0.1, single-scattering albedo
+    0.8 (sigma_s 0.08, sigma_a 0.02 per channel), Henyey-Greenstein g = 0.5, rendered with the
+    volumetric path integrator. The volumetric integrator's next-event estimation from scatter
+    points reaches point lights only (volumetric_path_integrator.cpp:97-116), so a point light
+    below the ceiling lamp lights the fog directly."""
+    s = cornell_box(width, height)
+    ss = F32(sigma_t) * F32(albedo)
+    sa = F32(sigma_t) - ss
+    s.set_medium((sa, sa, sa), (ss, ss, ss), g)
+    if point_light:
+        s.point_light((0.0, 1.8, 0.0), (1.0, 0.85, 0.6), 2.0)
     return s
 
 

@@ -119,3 +119,8 @@ def mis_pairs():
     rng = np.random.default_rng(3)
     extra = rng.lognormal(0, 3, (200, 2))
     return np.concatenate([np.array(base), extra]).astype(F32)
+
+
+def unit_vectors(rng, n):
+    v = rng.normal(size=(n, 3))
+    return (v / np.linalg.norm(v, axis=1, keepdims=True)).astype(F32)
