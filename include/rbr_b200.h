@@ -391,6 +391,70 @@ rbr_status rbr_cache_train_host(rbr_ctx* ctx, uint32_t n, const rbr_cache_record
 rbr_status rbr_cache_render(rbr_ctx* ctx, const rbr_camera* camera, const rbr_render_params* params,
                             uint32_t frames, int train, float* film_mean, float* film_m2, void* stream);
 
+/* ------------------------------------------------------------------------------------------
+ * Batched request loop (no reference counterpart). Requests of uneven resolution, samples
+ * per pixel, scene and integrator are packed into waves of the wavefront path tracer: a wave
+ * holds pixel ranges ("segments") of several requests of one scene, each path reading its
+ * request's camera, random-number key and parameters from a segment table in device memory.
+ * The launch sequence of a wave therefore depends only on (scene, integrator, depth, grid)
+ * and is captured once as a CUDA graph and replayed. Scenes, BVHs, films and caches stay
+ * resident; requests are admitted into a wave while its path-state memory budget allows (a
+ * request larger than a wave is split over several). rbr_batch_autotune picks the wave size
+ * and the grid by timing the pending requests.
+ * ------------------------------------------------------------------------------------------ */
+typedef struct rbr_batch rbr_batch;
+
+typedef struct rbr_batch_config {
+    uint64_t path_memory_bytes; /* budget for one wave's path state (default 1 GiB) */
+    uint32_t wave_paths;        /* paths per wave; 0: the budget decides (at most 2^22) */
+    uint32_t blocks_per_sm;     /* grid of the wavefront kernels = this x SMs (default 8) */
+    int32_t use_graphs;         /* replay each wave shape from a captured CUDA graph (default 1) */
+} rbr_batch_config;
+
+typedef struct rbr_request {
+    uint32_t scene;             /* id from rbr_batch_add_scene */
+    rbr_camera camera;
+    rbr_render_params params;   /* spp, max_depth (>= 1), use_nee, use_mis, seed, sample_offset;
+                                   flags: 0 or RBR_RENDER_VOLUMETRIC */
+    int32_t use_cache;          /* end paths into the scene's radiance cache (rbr_batch_cache_create) */
+    int32_t train_cache;        /* with use_cache: also train it on this request's paths */
+    float* film;                /* device pointer, width*height*3 floats: per-pixel mean */
+} rbr_request;
+
+typedef struct rbr_request_stats {
+    float start_ms;             /* from the start of rbr_batch_run to the start of its first wave */
+    float latency_ms;           /* from the start of rbr_batch_run to the end of its last wave */
+    uint32_t waves;             /* waves it was spread over */
+    uint32_t segments;
+    uint64_t paths;
+} rbr_request_stats;
+
+typedef struct rbr_batch_stats {
+    float milliseconds;         /* device time of the last rbr_batch_run */
+    uint32_t requests, waves, segments;
+    uint32_t graphs_captured, graph_launches, kernel_launches;
+    uint32_t wave_paths, blocks_per_sm;
+    uint64_t paths;
+} rbr_batch_stats;
+
+void rbr_batch_config_default(rbr_batch_config* out);
+/* The batch uses `ctx` (device, path-state buffers) and owns its scenes. */
+rbr_status rbr_batch_create(rbr_ctx* ctx, const rbr_batch_config* config, rbr_batch** out);
+void rbr_batch_destroy(rbr_batch* batch);
+const char* rbr_batch_last_error(const rbr_batch* batch);
+rbr_status rbr_batch_add_scene(rbr_batch* batch, const rbr_scene_desc* desc, uint32_t* scene_id);
+rbr_status rbr_batch_cache_create(rbr_batch* batch, uint32_t scene_id, const rbr_cache_config* config);
+/* Queues a request; it is rendered by the next rbr_batch_run. */
+rbr_status rbr_batch_submit(rbr_batch* batch, const rbr_request* request, uint32_t* request_id);
+/* Renders every queued request (asynchronous on `stream`); the queue is then empty. */
+rbr_status rbr_batch_run(rbr_batch* batch, void* stream);
+/* Per-request and whole-run timings of the last run (wait for it). */
+rbr_status rbr_batch_request_stats(rbr_batch* batch, uint32_t request_id, rbr_request_stats* out);
+rbr_status rbr_batch_stats_get(rbr_batch* batch, rbr_batch_stats* out);
+/* Renders the queued requests once per candidate (wave size x blocks per SM), keeps the
+ * fastest in the batch's configuration and leaves the requests queued. Waits. */
+rbr_status rbr_batch_autotune(rbr_batch* batch, void* stream);
+
 /* HenyeyGreensteinPhase::evaluate (src/materials/phase_function.cpp:17-21) for n (wo, wi). */
 rbr_status rbr_phase_eval_host(rbr_ctx* ctx, float g, uint32_t n, const float* wo, const float* wi, float* out);
 /* HenyeyGreensteinPhase::sample (phase_function.cpp:23-41) for n (wo, u1, u2); out: wi[3]. */

@@ -83,6 +83,11 @@ size_t rbr_struct_size(const char* name) {
     if (n == "rbr_cache_record") return sizeof(rbr_cache_record);
     if (n == "rbr_cache_config") return sizeof(rbr_cache_config);
     if (n == "rbr_cache_info") return sizeof(rbr_cache_info);
+    if (n == "rbr_medium") return sizeof(rbr_medium);
+    if (n == "rbr_batch_config") return sizeof(rbr_batch_config);
+    if (n == "rbr_request") return sizeof(rbr_request);
+    if (n == "rbr_request_stats") return sizeof(rbr_request_stats);
+    if (n == "rbr_batch_stats") return sizeof(rbr_batch_stats);
     return 0;
 }
 

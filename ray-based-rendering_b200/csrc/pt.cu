@@ -81,7 +81,41 @@ struct Paths {
     float4* t_rec = nullptr;   // 4 per training vertex
     float4* t_aux = nullptr;   // 2 per training vertex: (throughput rgb, path index bits), (radiance before, -)
     uint32_t t_cap = 0;
+    // packed waves (several requests in one wave; see SegDev)
+    const SegDev* segs = nullptr;
+    uint32_t* seg_of = nullptr;        // segment of each path (written by k_raygen<true>)
+    const uint32_t* wave_hdr = nullptr;  // [0] paths in the wave, [1] segments
 };
+
+// Which request a path belongs to, and its random-number key and integrator parameters.
+struct PathKey {
+    uint32_t pixel, sample, max_depth;
+    uint64_t seed;
+    bool nee, mis;
+};
+
+template <bool kPacked>
+__device__ __forceinline__ PathKey path_key(const Wave& w, const Paths& P, uint32_t k) {
+    PathKey r;
+    if (kPacked) {
+        const SegDev& g = P.segs[P.seg_of[k]];
+        const uint32_t local = k - g.path0;
+        r.pixel = g.p0 + local / g.spp;
+        r.sample = g.sample_offset + local % g.spp;
+        r.seed = g.seed;
+        r.max_depth = g.max_depth;
+        r.nee = g.use_nee != 0;
+        r.mis = g.use_mis != 0;
+    } else {
+        r.pixel = w.p0 + k / w.spp;
+        r.sample = w.sample_offset + k % w.spp;
+        r.seed = w.seed;
+        r.max_depth = w.max_depth;
+        r.nee = w.use_nee != 0;
+        r.mis = w.use_mis != 0;
+    }
+    return r;
+}
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
     uint32_t m;
@@ -113,15 +147,30 @@ __device__ __forceinline__ bool degenerate(float4 o, float4 d) {
 }
 
 // ------------------------------------------------------------------------------------------
+template <bool kPacked>
 __global__ void __launch_bounds__(kBlock) k_raygen(CameraDev cam, Wave w, Paths P) {
+    const uint32_t n = kPacked ? P.wave_hdr[0] : w.npaths;
     const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < w.npaths; k += stride) {
-        const uint32_t pixel = w.p0 + k / w.spp;
-        const uint32_t sample = w.sample_offset + k % w.spp;
-        const uint32_t x = pixel % w.width, y = pixel / w.width;
-        const float4 u = draw4(w.seed, pixel, sample, 0u, kRngCamera);
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
+        uint32_t width = w.width, seg = 0;
+        if (kPacked) {  // the segment holding path k (segments are sorted by first path)
+            uint32_t hi = P.wave_hdr[1] - 1;
+            while (seg < hi) {
+                const uint32_t mid = (seg + hi + 1) >> 1;
+                if (P.segs[mid].path0 <= k) seg = mid;
+                else hi = mid - 1;
+            }
+            P.seg_of[k] = seg;
+            width = P.segs[seg].width;
+        }
+        const PathKey key = path_key<kPacked>(w, P, k);
+        const uint32_t x = key.pixel % width, y = key.pixel / width;
+        const float4 u = draw4(key.seed, key.pixel, key.sample, 0u, kRngCamera);
         f3 o, d;
-        camera_ray(cam, fa(static_cast<float>(x), u.x), fa(static_cast<float>(y), u.y), u.z, u.w, o, d);
+        if (kPacked)
+            camera_ray(P.segs[seg].cam, fa(static_cast<float>(x), u.x), fa(static_cast<float>(y), u.y), u.z, u.w, o, d);
+        else
+            camera_ray(cam, fa(static_cast<float>(x), u.x), fa(static_cast<float>(y), u.y), u.z, u.w, o, d);
         P.ray[2 * k] = make_float4(o.x, o.y, o.z, 0.0f);
         P.ray[2 * k + 1] = make_float4(d.x, d.y, d.z, 0.0f);
         P.thr[k] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);  // specularBounce starts true
@@ -129,7 +178,7 @@ __global__ void __launch_bounds__(kBlock) k_raygen(CameraDev cam, Wave w, Paths 
         P.q0[k] = k;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        P.counters[kCQ0] = w.npaths;
+        P.counters[kCQ0] = n;
         if (w.cache_on) {
             P.counters[kCQuery] = 0;
             P.counters[kCTrainBase] = P.counters[kCTrain];
@@ -151,20 +200,19 @@ __global__ void k_begin(Paths P, uint32_t d) {
 // throughput multiplied by the medium weight; a scattering event is handled here: next-event
 // estimation towards point lights (directLightingVolume, :92-118) and a phase-function sample
 // that continues the path from the scatter point.
-template <bool kVol>
+template <bool kVol, bool kPacked>
 __global__ void __launch_bounds__(kBlock) k_extend(DeviceScene s, Wave w, Paths P, uint32_t d, int* err) {
     const uint32_t n = P.counters[kCQ0 + (d & 1)];
     const uint32_t* q = (d & 1) ? P.q1 : P.q0;
     uint32_t* nextq = (d & 1) ? P.q0 : P.q1;
     uint32_t* nextc = P.counters + kCQ0 + ((d + 1) & 1);
-    const bool last = d + 1 >= w.max_depth;
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(reinterpret_cast<unsigned long long*>(P.counters + kCExt), n);
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {
         const uint32_t j = base + threadIdx.x;
         const bool valid = j < n;
         uint32_t k = 0, cls = kNumClasses;
-        bool scatter = false;
+        bool scatter = false, last = true, nee = false;
         f3 T = mk(0.0f, 0.0f, 0.0f), sp = T, rd = T;
         float4 u = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         if (valid) {
@@ -178,8 +226,10 @@ __global__ void __launch_bounds__(kBlock) k_extend(DeviceScene s, Wave w, Paths 
             if (kVol && s.has_medium) {
                 const float4 T4 = P.thr[k];
                 T = ld_f3(T4);
-                const uint32_t pixel = w.p0 + k / w.spp, sample = w.sample_offset + k % w.spp;
-                u = draw4(w.seed, pixel, sample, d, kRngMedium);
+                const PathKey key = path_key<kPacked>(w, P, k);
+                last = d + 1 >= key.max_depth;
+                nee = key.nee;
+                u = draw4(key.seed, key.pixel, key.sample, d, kRngMedium);
                 float ts = 0.0f;
                 f3 wgt;
                 scatter = medium_sample(s, prim == 0xFFFFFFFFu ? __int_as_float(0x7f800000) : t, u.x, ts, wgt);
@@ -215,7 +265,7 @@ __global__ void __launch_bounds__(kBlock) k_extend(DeviceScene s, Wave w, Paths 
                 bool emit = false;
                 f3 contrib, sd;
                 float dist = 0.0f;
-                if (scatter && w.use_nee && s.lights[l].type == RBR_LIGHT_POINT) {
+                if (scatter && nee && s.lights[l].type == RBR_LIGHT_POINT) {
                     const LightDev& L = s.lights[l];
                     const f3 toL = xsub(ld3(L.position), sp);
                     dist = xlen(toL);
@@ -313,8 +363,8 @@ __device__ __forceinline__ void cache_record(const Hit& h, f3 rd, const Material
 }
 
 // Training paths of the radiance cache: a hash of (pixel, sample, seed) below the threshold.
-__device__ __forceinline__ bool train_path(const Wave& w, uint32_t pixel, uint32_t sample) {
-    uint32_t x = (pixel * 0x9E3779B1u) ^ ((sample + 0x7F4A7C15u) * 0x85EBCA77u) ^ static_cast<uint32_t>(w.seed);
+__device__ __forceinline__ bool train_path(const Wave& w, uint64_t seed, uint32_t pixel, uint32_t sample) {
+    uint32_t x = (pixel * 0x9E3779B1u) ^ ((sample + 0x7F4A7C15u) * 0x85EBCA77u) ^ static_cast<uint32_t>(seed);
     x ^= x >> 16;
     x *= 0x7FEB352Du;
     x ^= x >> 15;
@@ -326,7 +376,7 @@ __device__ __forceinline__ bool train_path(const Wave& w, uint32_t pixel, uint32
 // Surface vertices, per material-class queue. kMode 0: PathTracingIntegrator::Li; 1: the same
 // with the radiance cache; 2: the surface part of VolumetricPathIntegrator::Li
 // (volumetric_path_integrator.cpp:45-88: emission at every hit, NEE without MIS weights).
-template <int kMode>
+template <int kMode, bool kPacked>
 __global__ void __launch_bounds__(kBlock) k_shade(DeviceScene s, Wave w, Paths P, uint32_t d) {
     constexpr bool kCache = kMode == 1, kVolSurface = kMode == 2;
     uint32_t cnt[kNumClasses + 1];
@@ -335,13 +385,13 @@ __global__ void __launch_bounds__(kBlock) k_shade(DeviceScene s, Wave w, Paths P
     const uint32_t n = cnt[kNumClasses];
     uint32_t* nextq = (d & 1) ? P.q0 : P.q1;
     uint32_t* nextc = P.counters + kCQ0 + ((d + 1) & 1);
-    const bool last = d + 1 >= w.max_depth;
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {
         const uint32_t j = base + threadIdx.x;
         const bool valid = j < n;
         uint32_t k = 0;
-        bool alive = false, nee = false, to_cache = false, to_train = false;
+        bool alive = false, nee = false, to_cache = false, to_train = false, last = true, mis = false;
+        uint64_t seed = 0;
         float4 rec[4];
         Hit h;
         f3 T = mk(0.0f, 0.0f, 0.0f), wo = mk(0.0f, 0.0f, 0.0f);
@@ -353,8 +403,12 @@ __global__ void __launch_bounds__(kBlock) k_shade(DeviceScene s, Wave w, Paths P
             int c = 0;
             while (j >= cnt[c + 1]) ++c;
             k = P.classq[c * P.cap + (j - cnt[c])];
-            pixel = w.p0 + k / w.spp;
-            sample = w.sample_offset + k % w.spp;
+            const PathKey key = path_key<kPacked>(w, P, k);
+            pixel = key.pixel;
+            sample = key.sample;
+            seed = key.seed;
+            last = d + 1 >= key.max_depth;
+            mis = key.mis;
             const uint2 hv = P.hit[k];
             const f3 ro = ld_f3(P.ray[2 * k]), rd = ld_f3(P.ray[2 * k + 1]);
             const float4 t4 = P.thr[k];
@@ -372,10 +426,10 @@ __global__ void __launch_bounds__(kBlock) k_shade(DeviceScene s, Wave w, Paths P
             bs = make_bsdf(m);
             fr = make_frame(h.outward);
             wo = to_local(fr, xneg(rd));  // isect.wo = -ray.direction
-            nee = w.use_nee && !bsdf_delta(bs);
+            nee = key.nee && !bsdf_delta(bs);
             alive = true;
             if (kCache && bs.n > 0 && !bsdf_delta(bs)) {
-                if (train_path(w, pixel, sample)) {
+                if (train_path(w, seed, pixel, sample)) {
                     to_train = true;
                 } else if (d >= w.term_depth && !specular) {
                     to_cache = true;  // the cache's prediction replaces NEE and everything further
@@ -412,7 +466,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(DeviceScene s, Wave w, Paths P
             f3 contrib, so, sd;
             float stmax = 0.0f;
             if (valid && nee) {
-                const float4 u = draw4(w.seed, pixel, sample, d, kRngLights + ((l >> 1) << 8));
+                const float4 u = draw4(seed, pixel, sample, d, kRngLights + ((l >> 1) << 8));
                 const LightDev& L = s.lights[l];
                 const LSample ls = light_sample(L, h.point, (l & 1) ? u.z : u.x, (l & 1) ? u.w : u.y);
                 if (ls.pdf > 0.0f && !black(ls.Li)) {
@@ -424,7 +478,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(DeviceScene s, Wave w, Paths P
                         stmax = fs(ls.dist, kEpsilon);
                         const float c = fabsf(xdot(ls.wi, h.normal));
                         f3 ld;
-                        if (!kVolSurface && w.use_mis && !ls.delta) {
+                        if (!kVolSurface && mis && !ls.delta) {
                             const float wgt = power_heuristic(ls.pdf, bpdf);
                             ld = xdivs(xmuls(xmuls(xmul(f, ls.Li), c), wgt), ls.pdf);
                         } else {
@@ -446,7 +500,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(DeviceScene s, Wave w, Paths P
         // BSDF sampling, throughput update, Russian roulette, next ray
         bool cont = false;
         if (valid && alive && !last) {
-            const float4 u = draw4(w.seed, pixel, sample, d, kRngBounce);
+            const float4 u = draw4(seed, pixel, sample, d, kRngBounce);
             const BSample b = bsdf_sample(bs, wo, u.x, u.y);
             if (b.pdf > 0.0f && !black(b.f)) {
                 const f3 wiW = to_world(fr, b.wi);
@@ -529,6 +583,25 @@ __global__ void __launch_bounds__(kBlock) k_film(Wave w, Paths P, float* film_me
     }
 }
 
+// Film of a packed wave: the first path of each pixel sums the pixel's samples into its
+// request's film.
+__global__ void __launch_bounds__(kBlock) k_film_packed(Paths P) {
+    const uint32_t n = P.wave_hdr[0];
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
+        const SegDev& g = P.segs[P.seg_of[k]];
+        const uint32_t local = k - g.path0;
+        if (local % g.spp != 0) continue;
+        f3 sum = mk(0.0f, 0.0f, 0.0f);
+        for (uint32_t s = 0; s < g.spp; ++s) sum = xadd(sum, ld_f3(P.rad[k + s]));
+        const f3 mean = xdivs(sum, static_cast<float>(g.spp));
+        float* o = g.film + 3 * static_cast<size_t>(g.p0 + local / g.spp);
+        o[0] = mean.x;
+        o[1] = mean.y;
+        o[2] = mean.z;
+    }
+}
+
 }  // namespace
 
 rbr_status read_render_counters(rbr_ctx* ctx) {
@@ -553,6 +626,7 @@ void free_path_buffers(rbr_ctx* ctx) {
     release(p.classq);
     release(p.shadow);
     release(p.counters);
+    release(ctx->pt_seg_of);
     p.capacity = 0;
     p.shadow_capacity = 0;
 }
@@ -649,16 +723,16 @@ rbr_status render(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_params* 
         w.use_nee = p->use_nee != 0;
         w.use_mis = p->use_mis != 0;
         w.seed = p->seed;
-        k_raygen<<<grid, kBlock, 0, stream>>>(cd, w, P);
+        k_raygen<false><<<grid, kBlock, 0, stream>>>(cd, w, P);
         ++launches;
         for (uint32_t d = 0; d < w.max_depth; ++d) {
             k_begin<<<1, 1, 0, stream>>>(P, d);
             if (volumetric) {
-                k_extend<true><<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d, ctx->d_error);
-                k_shade<2><<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d);
+                k_extend<true, false><<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d, ctx->d_error);
+                k_shade<2, false><<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d);
             } else {
-                k_extend<false><<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d, ctx->d_error);
-                k_shade<0><<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d);
+                k_extend<false, false><<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d, ctx->d_error);
+                k_shade<0, false><<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d);
             }
             k_shadow<<<grid, kBlock, 0, stream>>>(ctx->scene, P, ctx->d_error);
             launches += 4;
@@ -691,6 +765,9 @@ __global__ void k_cache_wave_end(const uint32_t* counters, uint32_t* scalars, ui
     scalars[kRcTrain] = min(counters[kCTrain], t_cap);
 }
 
+
+}  // namespace
+
 CameraDev camera_dev(const rbr_camera* cam) {
     CameraDev cd;
     cd.width = cam->width;
@@ -710,8 +787,6 @@ CameraDev camera_dev(const rbr_camera* cam) {
     cd.focal_distance = cam->focal_distance;
     return cd;
 }
-
-}  // namespace
 
 rbr_status render_cached(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_params* p, uint32_t frames, int train,
                          float* film_mean, float* film_m2, cudaStream_t stream) {
@@ -795,12 +870,12 @@ rbr_status render_cached(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_p
             w.term_depth = cs.cfg.termination_depth;
             w.train_thresh = thresh;
             w.film_weight = weight;
-            k_raygen<<<grid, kBlock, 0, stream>>>(cd, w, P);
+            k_raygen<false><<<grid, kBlock, 0, stream>>>(cd, w, P);
             ++launches;
             for (uint32_t d = 0; d < w.max_depth; ++d) {
                 k_begin<<<1, 1, 0, stream>>>(P, d);
-                k_extend<false><<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d, ctx->d_error);
-                k_shade<1><<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d);
+                k_extend<false, false><<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d, ctx->d_error);
+                k_shade<1, false><<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d);
                 k_shadow<<<grid, kBlock, 0, stream>>>(ctx->scene, P, ctx->d_error);
                 launches += 4;
             }
@@ -830,6 +905,83 @@ rbr_status render_cached(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_p
     ctx->last_render.launches = launches;
     ctx->render_pending = true;
     return RBR_OK;
+}
+
+// ------------------------------------------------------------------------------------------
+// Packed waves of the batched request loop (batch.cpp): several requests of one scene in one
+// wave; per-path request data come from the segment table in device memory, so the launch
+// sequence of a wave depends only on (scene, mode, depth, grid) and is captured once as a
+// CUDA graph and replayed for every wave of that shape.
+// ------------------------------------------------------------------------------------------
+rbr_status ensure_wave_buffers(rbr_ctx* ctx, uint32_t cap, uint32_t shadow_cap) {
+    rbr_status st = ensure_paths(ctx, cap, shadow_cap);
+    if (st == RBR_OK) st = ensure(ctx, ctx->pt_seg_of, size_t(cap) * 4, "segment index per path");
+    return st;
+}
+
+cudaError_t launch_packed_wave(rbr_ctx* eng, rbr_ctx* scn, const PackedWave& pw, cudaStream_t stream) {
+    PathBuffers& pb = eng->pt;
+    Paths P;
+    P.ray = static_cast<float4*>(pb.ray.ptr);
+    P.thr = static_cast<float4*>(pb.thr.ptr);
+    P.rad = static_cast<float4*>(pb.rad.ptr);
+    P.hit = static_cast<uint2*>(pb.hit.ptr);
+    P.q0 = static_cast<uint32_t*>(pb.queue[0].ptr);
+    P.q1 = static_cast<uint32_t*>(pb.queue[1].ptr);
+    P.classq = static_cast<uint32_t*>(pb.classq.ptr);
+    P.shadow = static_cast<float4*>(pb.shadow.ptr);
+    P.counters = static_cast<uint32_t*>(pb.counters.ptr);
+    P.cap = pb.capacity;
+    P.shadow_cap = pb.shadow_capacity;
+    P.segs = pw.segs;
+    P.seg_of = static_cast<uint32_t*>(eng->pt_seg_of.ptr);
+    P.wave_hdr = pw.hdr;
+    Wave w{};
+    if (pw.mode == 1) {
+        CacheState& cs = scn->cache;
+        P.q_rec = static_cast<float4*>(cs.q_rec);
+        P.q_info = static_cast<float4*>(cs.q_info);
+        P.t_rec = static_cast<float4*>(cs.t_rec);
+        P.t_aux = static_cast<float4*>(cs.t_aux);
+        P.t_cap = pw.train ? cs.t_cap : 0;
+        w.cache_on = 1;
+        w.term_depth = cs.cfg.termination_depth;
+        w.train_thresh = pw.train_thresh;
+    }
+    const CameraDev unused{};
+    const int grid = pw.grid;
+    cudaError_t e = cudaMemsetAsync(P.counters, 0, kCWords * 4, stream);
+    if (e != cudaSuccess) return e;
+    k_raygen<true><<<grid, kBlock, 0, stream>>>(unused, w, P);
+    for (uint32_t d = 0; d < pw.max_depth; ++d) {
+        k_begin<<<1, 1, 0, stream>>>(P, d);
+        if (pw.mode == 2) {
+            k_extend<true, true><<<grid, kBlock, 0, stream>>>(scn->scene, w, P, d, eng->d_error);
+            k_shade<2, true><<<grid, kBlock, 0, stream>>>(scn->scene, w, P, d);
+        } else {
+            k_extend<false, true><<<grid, kBlock, 0, stream>>>(scn->scene, w, P, d, eng->d_error);
+            if (pw.mode == 1) k_shade<1, true><<<grid, kBlock, 0, stream>>>(scn->scene, w, P, d);
+            else k_shade<0, true><<<grid, kBlock, 0, stream>>>(scn->scene, w, P, d);
+        }
+        k_shadow<<<grid, kBlock, 0, stream>>>(scn->scene, P, eng->d_error);
+    }
+    if (pw.mode == 1) {
+        e = cache_launch_infer(scn, P.q_rec, pw.capacity, P.counters + kCQuery, nullptr, P.rad, P.q_info, stream);
+        if (e == cudaSuccess && pw.train) e = cache_launch_finalize(scn, P.rad, P.counters, kCTrainBase, kCTrain, stream);
+        if (e != cudaSuccess) return e;
+    }
+    k_film_packed<<<grid, kBlock, 0, stream>>>(P);
+    if (pw.mode == 1 && pw.train) {
+        e = cache_launch_train_frame(scn, P.counters + kCTrain, 0, stream);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaGetLastError();
+}
+
+uint32_t packed_wave_launches(const PackedWave& pw) {
+    uint32_t n = 2 + 4 * pw.max_depth;  // raygen, film, depth loop
+    if (pw.mode == 1) n += 1 + (pw.train ? 1 + 4 * pw.train_steps : 0);
+    return n;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -949,11 +1101,11 @@ rbr_status render_noalloc(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_
         w.use_nee = p->use_nee != 0;
         w.use_mis = p->use_mis != 0;
         w.seed = p->seed;
-        k_raygen<<<grid, kBlock, 0, stream>>>(cd, w, P);
+        k_raygen<false><<<grid, kBlock, 0, stream>>>(cd, w, P);
         for (uint32_t d = 0; d < w.max_depth; ++d) {
             k_begin<<<1, 1, 0, stream>>>(P, d);
-            k_extend<false><<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d, ctx->d_error);
-            k_shade<0><<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d);
+            k_extend<false, false><<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d, ctx->d_error);
+            k_shade<0, false><<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d);
             k_shadow<<<grid, kBlock, 0, stream>>>(ctx->scene, P, ctx->d_error);
         }
         k_film<<<grid, kBlock, 0, stream>>>(w, P, film_mean, nullptr);

@@ -630,13 +630,6 @@ __device__ __forceinline__ bool medium_sample(const DeviceScene& s, float max_di
 // ----------------------------------------------------------------------------------------
 // Camera rays
 // ----------------------------------------------------------------------------------------
-struct CameraDev {
-    int32_t width, height;
-    uint32_t model;
-    float position[3], forward[3], right[3], up[3];
-    float fx, fy, cx, cy;
-    float lens_radius, focal_distance;
-};
 
 __device__ __forceinline__ void concentric_disk(float u1, float u2, float& ox, float& oy) {
     const float sx = fs(fm(2.0f, u1), 1.0f);

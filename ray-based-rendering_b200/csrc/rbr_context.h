@@ -61,6 +61,7 @@ struct rbr_ctx {
     uint32_t pt_wave_paths = 1u << 22;
     // path tracer
     rbr::PathBuffers pt;
+    rbr::DevBuf pt_seg_of;  // packed waves: segment of each path
     rbr_render_stats last_render{};
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
     bool render_pending = false;
@@ -123,6 +124,23 @@ cudaError_t cache_launch_finalize(rbr_ctx* ctx, const float4* path_rad, const ui
 cudaError_t cache_launch_train_frame(rbr_ctx* ctx, const uint32_t* count_ptr, uint32_t frame, cudaStream_t stream);
 rbr_status render_cached(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_params* p, uint32_t frames, int train,
                          float* film_mean, float* film_m2, cudaStream_t stream);
+
+// batched request loop (pt.cu, batch.cpp)
+CameraDev camera_dev(const rbr_camera* cam);
+struct PackedWave {
+    int mode = 0;                 // 0 path tracer, 1 path tracer + radiance cache, 2 volumetric
+    uint32_t max_depth = 0;       // depth iterations (the largest max depth of its requests)
+    int grid = 0;                 // blocks of the wavefront kernels
+    const SegDev* segs = nullptr; // device segment table
+    const uint32_t* hdr = nullptr;  // device [paths, segments]
+    uint32_t capacity = 0;        // path capacity of the wave buffers
+    bool train = false;           // mode 1: gather training vertices and train after the wave
+    uint32_t train_thresh = 0;
+    uint32_t train_steps = 0;
+};
+rbr_status ensure_wave_buffers(rbr_ctx* ctx, uint32_t cap, uint32_t shadow_cap);
+cudaError_t launch_packed_wave(rbr_ctx* eng, rbr_ctx* scn, const PackedWave& pw, cudaStream_t stream);
+uint32_t packed_wave_launches(const PackedWave& pw);
 
 rbr_status render_noalloc(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_params* p, float* film_mean,
                           cudaStream_t stream);

@@ -52,4 +52,24 @@ struct DeviceScene {
     float hg_g;         // Henyey-Greenstein asymmetry
 };
 
+// A PinholeCamera or ThinLensCamera (rbr_camera) as the kernels read it.
+struct CameraDev {
+    int32_t width, height;
+    uint32_t model;
+    float position[3], forward[3], right[3], up[3];
+    float fx, fy, cx, cy;
+    float lens_radius, focal_distance;
+};
+
+// One request's share of a packed wave of the batched request loop: a range of its pixels
+// with all their samples.
+struct SegDev {
+    CameraDev cam;
+    float* film;             // the request's film (per-pixel mean, width*height*3)
+    uint64_t seed;
+    uint32_t path0, npaths;  // its paths in the wave
+    uint32_t p0;             // its first pixel in the request's image
+    uint32_t spp, sample_offset, width, max_depth, use_nee, use_mis;
+};
+
 }  // namespace rbr

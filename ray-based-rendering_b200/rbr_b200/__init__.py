@@ -83,6 +83,17 @@ def load_library() -> C.CDLL:
         "rbr_cache_train_host": (C.c_int, [P, C.c_uint32, P, P, C.c_int, C.POINTER(C.c_float)]),
         "rbr_cache_render": (C.c_int, [P, C.POINTER(abi.rbr_camera), C.POINTER(abi.rbr_render_params), C.c_uint32,
                                        C.c_int, P, P, P]),
+        "rbr_batch_config_default": (None, [C.POINTER(abi.rbr_batch_config)]),
+        "rbr_batch_create": (C.c_int, [P, C.POINTER(abi.rbr_batch_config), C.POINTER(P)]),
+        "rbr_batch_destroy": (None, [P]),
+        "rbr_batch_last_error": (C.c_char_p, [P]),
+        "rbr_batch_add_scene": (C.c_int, [P, C.POINTER(abi.rbr_scene_desc), C.POINTER(C.c_uint32)]),
+        "rbr_batch_cache_create": (C.c_int, [P, C.c_uint32, C.POINTER(abi.rbr_cache_config)]),
+        "rbr_batch_submit": (C.c_int, [P, C.POINTER(abi.rbr_request), C.POINTER(C.c_uint32)]),
+        "rbr_batch_run": (C.c_int, [P, P]),
+        "rbr_batch_request_stats": (C.c_int, [P, C.c_uint32, C.POINTER(abi.rbr_request_stats)]),
+        "rbr_batch_stats_get": (C.c_int, [P, C.POINTER(abi.rbr_batch_stats)]),
+        "rbr_batch_autotune": (C.c_int, [P, P]),
     }
     for name, (res, args) in sig.items():
         if hasattr(lib, name):
@@ -341,5 +352,77 @@ class Context:
         return s
 
 
-__all__ = ["Context", "RbrError", "load_library", "header_functions", "render_params", "abi", "RAY_DTYPE",
+class Batch:
+    """An rbr_batch: the batched request loop on a Context's device and path buffers."""
+
+    def __init__(self, ctx: Context, **cfg):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        c = abi.rbr_batch_config()
+        self.lib.rbr_batch_config_default(C.byref(c))
+        for k, v in cfg.items():
+            setattr(c, k, v)
+        h = C.c_void_p()
+        st = self.lib.rbr_batch_create(ctx.h, C.byref(c), C.byref(h))
+        if st != abi.RBR_OK:
+            raise RbrError(st, "rbr_batch_create failed")
+        self.h = h
+        self._keep = []
+
+    def _check(self, st):
+        if st != abi.RBR_OK:
+            raise RbrError(st, self.lib.rbr_batch_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.rbr_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_scene(self, scene) -> int:
+        desc = scene.desc() if hasattr(scene, "desc") and callable(scene.desc) else scene
+        sid = C.c_uint32()
+        self._check(self.lib.rbr_batch_add_scene(self.h, C.byref(desc.desc), C.byref(sid)))
+        self._keep.append(desc)
+        return int(sid.value)
+
+    def cache_create(self, scene_id: int, **kw):
+        cfg = self.ctx.cache_config(**kw)
+        self._check(self.lib.rbr_batch_cache_create(self.h, scene_id, C.byref(cfg)))
+
+    def submit(self, scene_id, camera, params, film_ptr, use_cache=False, train_cache=False) -> int:
+        r = abi.rbr_request()
+        r.scene = scene_id
+        r.camera = camera
+        r.params = params
+        r.use_cache = int(use_cache)
+        r.train_cache = int(train_cache)
+        r.film = film_ptr
+        rid = C.c_uint32()
+        self._check(self.lib.rbr_batch_submit(self.h, C.byref(r), C.byref(rid)))
+        return int(rid.value)
+
+    def run(self, stream: int = 0):
+        self._check(self.lib.rbr_batch_run(self.h, C.c_void_p(stream)))
+
+    def autotune(self, stream: int = 0):
+        self._check(self.lib.rbr_batch_autotune(self.h, C.c_void_p(stream)))
+
+    def request_stats(self, rid: int) -> abi.rbr_request_stats:
+        s = abi.rbr_request_stats()
+        self._check(self.lib.rbr_batch_request_stats(self.h, rid, C.byref(s)))
+        return s
+
+    def stats(self) -> abi.rbr_batch_stats:
+        s = abi.rbr_batch_stats()
+        self._check(self.lib.rbr_batch_stats_get(self.h, C.byref(s)))
+        return s
+
+
+__all__ = ["Context", "Batch", "RbrError", "load_library", "header_functions", "render_params", "abi", "RAY_DTYPE",
            "HIT_DTYPE"]

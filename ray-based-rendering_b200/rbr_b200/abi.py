@@ -192,6 +192,51 @@ class rbr_cache_info(C.Structure):
     ]
 
 
+class rbr_batch_config(C.Structure):
+    _fields_ = [
+        ("path_memory_bytes", C.c_uint64),
+        ("wave_paths", C.c_uint32),
+        ("blocks_per_sm", C.c_uint32),
+        ("use_graphs", C.c_int32),
+    ]
+
+
+class rbr_request(C.Structure):
+    _fields_ = [
+        ("scene", C.c_uint32),
+        ("camera", rbr_camera),
+        ("params", rbr_render_params),
+        ("use_cache", C.c_int32),
+        ("train_cache", C.c_int32),
+        ("film", C.c_void_p),
+    ]
+
+
+class rbr_request_stats(C.Structure):
+    _fields_ = [
+        ("start_ms", C.c_float),
+        ("latency_ms", C.c_float),
+        ("waves", C.c_uint32),
+        ("segments", C.c_uint32),
+        ("paths", C.c_uint64),
+    ]
+
+
+class rbr_batch_stats(C.Structure):
+    _fields_ = [
+        ("milliseconds", C.c_float),
+        ("requests", C.c_uint32),
+        ("waves", C.c_uint32),
+        ("segments", C.c_uint32),
+        ("graphs_captured", C.c_uint32),
+        ("graph_launches", C.c_uint32),
+        ("kernel_launches", C.c_uint32),
+        ("wave_paths", C.c_uint32),
+        ("blocks_per_sm", C.c_uint32),
+        ("paths", C.c_uint64),
+    ]
+
+
 # rbr_cache_record as 16 float32 columns: position[3], direction[3], normal[3], roughness,
 # diffuse[3], specular[3]
 CACHE_RECORD_DTYPE = np.dtype((np.float32, (CACHE_RECORD_FLOATS,)))

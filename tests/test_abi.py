@@ -31,6 +31,11 @@ def test_abi_version():
         ("rbr_render_stats", abi.rbr_render_stats),
         ("rbr_cache_config", abi.rbr_cache_config),
         ("rbr_cache_info", abi.rbr_cache_info),
+        ("rbr_medium", abi.rbr_medium),
+        ("rbr_batch_config", abi.rbr_batch_config),
+        ("rbr_request", abi.rbr_request),
+        ("rbr_request_stats", abi.rbr_request_stats),
+        ("rbr_batch_stats", abi.rbr_batch_stats),
     ],
 )
 def test_struct_sizes_match(name, cls):

@@ -1,0 +1,154 @@
+"""Batched request loop (rbr_batch_*): requests of several scenes, resolutions, sample counts,
+depths and integrators packed into shared waves give the same images as rendering each request
+alone with rbr_render (the same random numbers per (pixel, sample, seed)), whether the waves
+are replayed from captured CUDA graphs or launched directly, and however a request is split
+over waves; per-request latency and batch statistics are reported."""
+import numpy as np
+import pytest
+import torch
+
+from rbr_b200 import Batch, Context, abi, render_params, scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def small_ggx(w, h, seed=0):
+    s = scenes.ggx_scene(width=w, height=h, mesh_n=60, seed=seed)
+    return s
+
+
+def cornell(w, h):
+    s = scenes.cornell_box()
+    s.camera = scenes.look_at_camera(w, h, (0.0, 1.0, 3.5), (0.0, 1.0, 0.0), (0.0, 1.0, 0.0), 40.0)
+    return s
+
+
+def foggy(w, h):
+    s = scenes.foggy_cornell_box()
+    s.camera = scenes.look_at_camera(w, h, (0.0, 1.0, 3.5), (0.0, 1.0, 0.0), (0.0, 1.0, 0.0), 40.0)
+    return s
+
+
+@pytest.fixture(scope="module")
+def bctx():
+    c = Context(0)
+    yield c
+    c.close()
+
+
+def requests():
+    """(scene key, width, height, params) of a mixed set of requests."""
+    vol = abi.RBR_RENDER_VOLUMETRIC
+    return [
+        ("cornell", 48, 40, render_params(spp=3, max_depth=8, seed=11)),
+        ("ggx", 64, 36, render_params(spp=5, max_depth=16, seed=12, sample_offset=7)),
+        ("cornell", 32, 32, render_params(spp=1, max_depth=3, seed=13, use_mis=False)),
+        ("fog", 40, 40, render_params(spp=4, max_depth=6, seed=14, flags=vol)),
+        ("ggx", 50, 30, render_params(spp=2, max_depth=5, seed=15, use_nee=False)),
+        ("cornell", 20, 70, render_params(spp=9, max_depth=8, seed=16)),
+        ("fog", 24, 24, render_params(spp=2, max_depth=3, seed=17, flags=vol)),
+    ]
+
+
+def build_scenes():
+    return {"cornell": cornell, "ggx": small_ggx, "fog": foggy}
+
+
+def alone(ctx, key, w, h, p):
+    s = build_scenes()[key](w, h)
+    ctx.upload(s)
+    return ctx.render_host(s.camera, p)
+
+
+def batched(ctx, **cfg):
+    b = Batch(ctx, **cfg)
+    ids = {}
+    for key, fn in build_scenes().items():
+        ids[key] = b.add_scene(fn(16, 16))
+    films, rids = [], []
+    for key, w, h, p in requests():
+        cam = build_scenes()[key](w, h).camera
+        f = torch.zeros(w * h * 3, device="cuda")
+        films.append(f)
+        rids.append(b.submit(ids[key], cam, p, f.data_ptr()))
+    b.run()
+    torch.cuda.synchronize()
+    stats = [b.request_stats(r) for r in rids]
+    return b, [f.cpu().numpy().reshape(h, w, 3) for f, (_, w, h, _) in zip(films, requests())], stats
+
+
+@pytest.mark.parametrize("cfg", [dict(), dict(use_graphs=0), dict(wave_paths=4096), dict(wave_paths=1000, blocks_per_sm=2)],
+                         ids=["graphs", "direct", "small-waves", "split-requests"])
+def test_packed_requests_equal_single_renders(bctx, cfg):
+    b, films, stats = batched(bctx, **cfg)
+    for (key, w, h, p), got in zip(requests(), films):
+        want = alone(bctx, key, w, h, p)
+        assert np.isfinite(got).all()
+        np.testing.assert_allclose(got, want, rtol=2e-5, atol=2e-6, err_msg=key)
+    bs = b.stats()
+    assert bs.requests == len(requests()) and bs.waves >= 3  # three scenes x modes at least
+    assert bs.paths == sum(w * h * p.samples_per_pixel for _, w, h, p in requests())
+    if cfg.get("use_graphs", 1):
+        assert bs.graph_launches == bs.waves and 1 <= bs.graphs_captured <= bs.waves
+    lat = [s.latency_ms for s in stats]
+    assert all(s.latency_ms > 0 and s.start_ms <= s.latency_ms for s in stats)
+    assert max(lat) <= bs.milliseconds * 1.0001
+    if cfg.get("wave_paths") == 1000:
+        assert any(s.waves > 1 for s in stats)  # a request spread over several waves
+    b.close()
+
+
+def test_graph_replay_across_runs_and_autotune(bctx):
+    b = Batch(bctx)
+    sid = b.add_scene(cornell(16, 16))
+    cam = cornell(64, 64).camera
+    f = torch.zeros(64 * 64 * 3, device="cuda")
+    p = render_params(spp=4, max_depth=8, seed=3)
+    for _ in range(3):
+        b.submit(sid, cam, p, f.data_ptr())
+        b.run()
+    st = b.stats()
+    assert st.graphs_captured == 0 and st.graph_launches == st.waves  # replayed from the first run
+    first = f.cpu().numpy().copy()
+    b.submit(sid, cam, p, f.data_ptr())
+    b.autotune()
+    b.run()
+    torch.cuda.synchronize()
+    np.testing.assert_allclose(f.cpu().numpy(), first, rtol=2e-5, atol=2e-6)
+    st = b.stats()
+    assert st.wave_paths in (1 << 19, 1 << 20, 1 << 21, 1 << 22) and st.blocks_per_sm in (4, 8, 16)
+    b.close()
+
+
+def test_cached_requests_in_a_batch(bctx):
+    b = Batch(bctx)
+    sid = b.add_scene(small_ggx(16, 16))
+    b.cache_create(sid, train_paths=4096, seed=1)
+    cam = small_ggx(96, 54).camera
+    films = [torch.zeros(96 * 54 * 3, device="cuda") for _ in range(4)]
+    for i, f in enumerate(films):
+        b.submit(sid, cam, render_params(spp=1, max_depth=16, seed=5, sample_offset=i), f.data_ptr(),
+                 use_cache=True, train_cache=True)
+    b.run()
+    torch.cuda.synchronize()
+    for f in films:
+        img = f.cpu().numpy()
+        assert np.isfinite(img).all() and (img >= 0).all() and img.mean() > 0
+    assert b.stats().waves == 1
+
+
+def test_invalid_requests_are_rejected(bctx):
+    from rbr_b200 import RbrError
+
+    b = Batch(bctx)
+    sid = b.add_scene(cornell(16, 16))
+    cam = cornell(8, 8).camera
+    f = torch.zeros(8 * 8 * 3, device="cuda")
+    with pytest.raises(RbrError):
+        b.submit(sid + 5, cam, render_params(spp=1), f.data_ptr())
+    with pytest.raises(RbrError):
+        b.submit(sid, cam, render_params(spp=1, max_depth=0), f.data_ptr())
+    with pytest.raises(RbrError):
+        b.submit(sid, cam, render_params(spp=1), f.data_ptr(), use_cache=True)  # no cache on the scene
+    with pytest.raises(RbrError):
+        b.submit(sid, cam, render_params(spp=1, flags=abi.RBR_RENDER_SECOND_MOMENT), f.data_ptr())
