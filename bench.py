@@ -46,7 +46,7 @@ def parse():
     p.add_argument("--steps", type=int, default=None, help="timed steps (default 200; cache workload: 256 frames)")
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["rays", "cornell", "ggx", "fog", "cache"], default="rays")
+    p.add_argument("--workload", choices=["rays", "cornell", "ggx", "fog", "cache", "batch"], default="rays")
     p.add_argument("--ref-spp", type=int, default=1024, help="cache workload: spp of the converged GPU reference")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true", help="skip the host-buffer measurement (profiling runs)")
@@ -417,10 +417,114 @@ def run_cache(args, rank, world, local_rank):
     ctx.close()
 
 
+def run_batch(args, rank, world, local_rank):
+    """Batched request loop (config 5): 64 seeded requests, resolution uniform over {128^2,
+    256^2, 512^2, 1024^2}, spp U{1..64}; scenes: 7 seeded material/light variants of the GGX
+    scene sharing its geometry and BVH, and the foggy Cornell box (volumetric path, 1 in 8
+    requests); run once with the radiance cache off and once on (GGX variants end paths into
+    their scene's cache and train it). Latency of a request = device time from the start of the
+    run to the end of its last wave (all requests are submitted together). A step is one run of
+    the 64 requests."""
+    import torch
+
+    from rbr_b200 import Batch, Context, abi, render_params, scenes
+
+    torch.cuda.set_device(local_rank)
+    rng = np.random.default_rng(5 + rank)
+    ctx = Context(local_rank)
+    batch = Batch(ctx)
+    base = scenes.ggx_scene()
+    ids = [batch.add_scene(base)]
+    for v in range(1, 7):
+        ids.append(batch.add_scene_variant(ids[0], scenes.ggx_variant(base, v)))
+    fog = scenes.foggy_cornell_box()
+    fog_id = batch.add_scene(fog)
+    sizes = [128, 256, 512, 1024]
+    reqs = []
+    for i in range(64):
+        size = int(rng.choice(sizes))
+        spp = int(rng.integers(1, 65))
+        if i % 8 == 7:
+            reqs.append((fog_id, scenes.square_camera(fog.camera, size), spp, 8, abi.RBR_RENDER_VOLUMETRIC))
+        else:
+            reqs.append((ids[int(rng.integers(0, len(ids)))], scenes.square_camera(base.camera, size), spp, 16, 0))
+    films = [torch.zeros(c.width * c.height * 3, device=f"cuda:{local_rank}") for _, c, _, _, _ in reqs]
+    stream = torch.cuda.current_stream().cuda_stream
+    for sid in ids:
+        batch.cache_create(sid, seed=1)
+
+    def submit(use_cache, subset=None):
+        rid = []
+        for i, (sid, cam, spp, depth, flags) in enumerate(reqs if subset is None else reqs[:subset]):
+            cache = use_cache and not flags
+            rid.append(batch.submit(sid, cam, render_params(spp=spp, max_depth=depth, seed=1000 + i, flags=flags),
+                                    films[i].data_ptr(), use_cache=cache, train_cache=cache))
+        return rid
+
+    # autotune wave size and grid on a calibration subset, then warm up (graphs captured)
+    submit(False, subset=8)
+    batch.autotune(stream)
+    batch.run(stream)
+    for _ in range(max(1, args.warmup)):
+        submit(False)
+        batch.run(stream)
+    torch.cuda.synchronize()
+    results = {}
+    clocks = Clocks() if rank == 0 else None
+    if clocks:
+        clocks.start()
+    for mode in ("off", "on"):
+        lat, total_ms, paths, st = [], 0.0, 0, None
+        for step in range(args.steps):
+            rid = submit(mode == "on")
+            t0 = time.perf_counter()
+            batch.run(stream)
+            st = batch.stats()
+            wall = time.perf_counter() - t0
+            total_ms += st.milliseconds
+            paths += st.paths
+            lat += [batch.request_stats(r).latency_ms for r in rid]
+        results[mode] = {
+            "mpaths_per_s": paths / (total_ms / 1e3) / 1e6, "ms_per_run": total_ms / args.steps,
+            "latency_ms_p50": float(np.percentile(lat, 50)), "latency_ms_p99": float(np.percentile(lat, 99)),
+            "waves_per_run": st.waves, "segments_per_run": st.segments, "graph_launches_per_run": st.graph_launches,
+            "kernel_launches_per_run": st.kernel_launches, "wave_paths": st.wave_paths,
+            "blocks_per_sm": st.blocks_per_sm, "host_wall_s_last_run": wall}
+    clk = clocks.stop(visible_gpu_indices(local_rank)) if clocks else None
+    # end to end: submit, run and read every film back to the host
+    t0 = time.perf_counter()
+    submit(False)
+    batch.run(stream)
+    host = [f.cpu() for f in films]
+    e2e_s = time.perf_counter() - t0
+    total_paths = sum(c.width * c.height * spp for _, c, spp, _, _ in reqs)
+    if rank == 0:
+        off = results["off"]
+        print(json.dumps({
+            "metric": "Mpaths/s & p50/p99 request latency, batched request loop (64 requests)",
+            "value": off["mpaths_per_s"] * world, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(1, args.warmup), "ms_per_step": off["ms_per_run"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": "64 seeded requests: resolution uniform over {128^2, 256^2, 512^2, 1024^2}, spp "
+                                   "U{1..64}; 7 material/light variants of the GGX scene (shared geometry, depth 16) "
+                                   "and the foggy Cornell box (volumetric, depth 8, every 8th request)",
+                       "paths_per_run": total_paths,
+                       "l2": "path state of a wave (up to 4M paths x ~250 B) larger than L2"},
+            "latency": {"cache_off": off, "cache_on": results["on"]},
+            "e2e": {"value": total_paths / e2e_s / 1e6, "unit": "Mpaths/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": sum(c.width * c.height * 12 for _, c, _, _, _ in reqs),
+                    "path": "rbr_batch_submit x64 + rbr_batch_run + every film to host"},
+            "clocks": clk, "gpu_launches": off["kernel_launches_per_run"] * args.steps,
+        }))
+    del host
+    batch.close()
+    ctx.close()
+
+
 def main():
     args = parse()
     if args.steps is None:
-        args.steps = 256 if args.workload == "cache" else 200
+        args.steps = {"cache": 256, "batch": 3}.get(args.workload, 200)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
@@ -428,6 +532,8 @@ def main():
         return run_reference(args, rank, world)
     if args.workload == "cache":
         return run_cache(args, rank, world, local_rank)
+    if args.workload == "batch":
+        return run_batch(args, rank, world, local_rank)
     if args.workload != "rays":
         return run_render(args, rank, world, local_rank)
 

@@ -443,6 +443,11 @@ rbr_status rbr_batch_create(rbr_ctx* ctx, const rbr_batch_config* config, rbr_ba
 void rbr_batch_destroy(rbr_batch* batch);
 const char* rbr_batch_last_error(const rbr_batch* batch);
 rbr_status rbr_batch_add_scene(rbr_batch* batch, const rbr_scene_desc* desc, uint32_t* scene_id);
+/* A scene sharing `base_scene`'s geometry and BVH on the device (no rebuild, no copy) with its
+ * own materials (as many as the base has), lights and medium (NULL for none). */
+rbr_status rbr_batch_add_scene_variant(rbr_batch* batch, uint32_t base_scene, const rbr_material* materials,
+                                       uint32_t num_materials, const rbr_light* lights, uint32_t num_lights,
+                                       const rbr_medium* medium, uint32_t* scene_id);
 rbr_status rbr_batch_cache_create(rbr_batch* batch, uint32_t scene_id, const rbr_cache_config* config);
 /* Queues a request; it is rendered by the next rbr_batch_run. */
 rbr_status rbr_batch_submit(rbr_batch* batch, const rbr_request* request, uint32_t* request_id);

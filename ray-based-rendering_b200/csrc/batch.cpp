@@ -324,7 +324,7 @@ void rbr_batch_destroy(rbr_batch* b) {
     cudaDeviceSynchronize();
     drop_graphs(b);
     for (cudaEvent_t e : b->events) cudaEventDestroy(e);
-    for (rbr_ctx* s : b->scenes) rbr_ctx_destroy(s);
+    for (size_t i = b->scenes.size(); i-- > 0;) rbr_ctx_destroy(b->scenes[i]);  // variants before their bases
     if (b->d_table) cudaFree(b->d_table);
     if (b->h_stage) cudaFreeHost(b->h_stage);
     delete b;
@@ -338,6 +338,24 @@ rbr_status rbr_batch_add_scene(rbr_batch* b, const rbr_scene_desc* desc, uint32_
     rbr_status st = rbr_ctx_create(b->eng->device, &s);
     if (st != RBR_OK) return bfail(b, st, "creating the scene slot");
     st = rbr_scene_upload(s, desc);
+    if (st != RBR_OK) {
+        b->error = s->error;
+        rbr_ctx_destroy(s);
+        return st;
+    }
+    *scene_id = static_cast<uint32_t>(b->scenes.size());
+    b->scenes.push_back(s);
+    return RBR_OK;
+}
+
+rbr_status rbr_batch_add_scene_variant(rbr_batch* b, uint32_t base_scene, const rbr_material* materials,
+                                       uint32_t num_materials, const rbr_light* lights, uint32_t num_lights,
+                                       const rbr_medium* medium, uint32_t* scene_id) {
+    if (!b || !scene_id || base_scene >= b->scenes.size()) return bfail(b, RBR_ERR_INVALID_ARGUMENT, "unknown base scene");
+    rbr_ctx* s = nullptr;
+    rbr_status st = rbr_ctx_create(b->eng->device, &s);
+    if (st != RBR_OK) return bfail(b, st, "creating the scene slot");
+    st = upload_scene_variant(s, b->scenes[base_scene], materials, num_materials, lights, num_lights, medium);
     if (st != RBR_OK) {
         b->error = s->error;
         rbr_ctx_destroy(s);

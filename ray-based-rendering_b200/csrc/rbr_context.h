@@ -78,6 +78,8 @@ void release(DevBuf& b);
 rbr_status check_device_error(rbr_ctx* ctx, cudaStream_t stream);
 
 rbr_status upload_scene(rbr_ctx* ctx, const rbr_scene_desc* desc);
+rbr_status upload_scene_variant(rbr_ctx* dst, const rbr_ctx* base, const rbr_material* materials, uint32_t num_materials,
+                                const rbr_light* lights, uint32_t num_lights, const rbr_medium* medium);
 void free_scene(rbr_ctx* ctx);
 
 // kernels (trace.cu)

@@ -87,6 +87,56 @@ uint32_t material_class(const rbr_material& m) {
 //     by about 2^-24 * L / 1e-4 times the primitive's size factor, L bounding the distances
 //     involved (4x the largest coordinate). Boxes grow by 4x that bound; a sphere's tangent
 //     point moves along the tangent by ~2^-12 L, leaving its box by at most (2^-12 L)^2 / 2r.
+std::vector<MaterialDev> device_materials(const rbr_material* src, uint32_t n) {
+    std::vector<MaterialDev> mats(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        const rbr_material& m = src[i];
+        MaterialDev& o = mats[i];
+        std::memcpy(o.base, m.base_color, 12);
+        o.metallic = m.metallic;
+        o.roughness = m.roughness;
+        o.ior = m.ior;
+        o.transmission = m.transmission;
+        std::memcpy(o.emission, m.emission, 12);
+        o.cls = material_class(m);
+        o.emissive = (m.emission[0] > 0.0f || m.emission[1] > 0.0f || m.emission[2] > 0.0f) ? 1u : 0u;
+    }
+    return mats;
+}
+
+std::vector<LightDev> device_lights(const rbr_light* src, uint32_t n) {
+    std::vector<LightDev> lights(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        const rbr_light& l = src[i];
+        LightDev& o = lights[i];
+        o.type = l.type;
+        std::memcpy(o.position, l.position, 12);
+        std::memcpy(o.u, l.u, 12);
+        std::memcpy(o.v, l.v, 12);
+        std::memcpy(o.color, l.color, 12);
+        o.intensity = l.intensity;
+        const V3 c = cross(ld(l.u), ld(l.v));
+        const V3 nn = normalized(c);  // AreaLight::AreaLight (area_light.cpp:5-11)
+        o.normal[0] = nn.x;
+        o.normal[1] = nn.y;
+        o.normal[2] = nn.z;
+        o.area = std::sqrt(dot(c, c));  // cross(u, v).length() (area_light.cpp:33)
+    }
+    return lights;
+}
+
+void set_medium(DeviceScene& s, const rbr_medium* m) {
+    s.has_medium = m ? 1u : 0u;
+    if (!m) return;
+    // Color sigma_t = sigma_a + sigma_s; avgSigmaT = (x + y + z) / 3 (medium.cpp:13-14)
+    for (int a = 0; a < 3; ++a) {
+        s.sigma_s[a] = m->sigma_s[a];
+        s.sigma_t[a] = m->sigma_a[a] + m->sigma_s[a];
+    }
+    s.avg_sigma_t = (s.sigma_t[0] + s.sigma_t[1] + s.sigma_t[2]) / 3.0f;
+    s.hg_g = m->g;
+}
+
 Box hit_region_box(const uint32_t* w, const Box& gb, float maxabs) {
     float f[12];
     std::memcpy(f, w, sizeof(f));
@@ -324,36 +374,8 @@ rbr_status upload_scene(rbr_ctx* ctx, const rbr_scene_desc* d) {
             for (int k = 0; k < 3; ++k) tri_normals[3 * r + k] = make_float4(n[3 * k], n[3 * k + 1], n[3 * k + 2], 0.0f);
         }
     }
-    std::vector<MaterialDev> mats(d->num_materials);
-    for (uint32_t i = 0; i < d->num_materials; ++i) {
-        const rbr_material& m = d->materials[i];
-        MaterialDev& o = mats[i];
-        std::memcpy(o.base, m.base_color, 12);
-        o.metallic = m.metallic;
-        o.roughness = m.roughness;
-        o.ior = m.ior;
-        o.transmission = m.transmission;
-        std::memcpy(o.emission, m.emission, 12);
-        o.cls = material_class(m);
-        o.emissive = (m.emission[0] > 0.0f || m.emission[1] > 0.0f || m.emission[2] > 0.0f) ? 1u : 0u;
-    }
-    std::vector<LightDev> lights(d->num_lights);
-    for (uint32_t i = 0; i < d->num_lights; ++i) {
-        const rbr_light& l = d->lights[i];
-        LightDev& o = lights[i];
-        o.type = l.type;
-        std::memcpy(o.position, l.position, 12);
-        std::memcpy(o.u, l.u, 12);
-        std::memcpy(o.v, l.v, 12);
-        std::memcpy(o.color, l.color, 12);
-        o.intensity = l.intensity;
-        const V3 c = cross(ld(l.u), ld(l.v));
-        const V3 n = normalized(c);  // AreaLight::AreaLight (area_light.cpp:5-11)
-        o.normal[0] = n.x;
-        o.normal[1] = n.y;
-        o.normal[2] = n.z;
-        o.area = std::sqrt(dot(c, c));  // cross(u, v).length() (area_light.cpp:33)
-    }
+    std::vector<MaterialDev> mats = device_materials(d->materials, d->num_materials);
+    std::vector<LightDev> lights = device_lights(d->lights, d->num_lights);
 
     free_scene(ctx);
     ctx->stats.device_bytes = 0;
@@ -383,16 +405,7 @@ rbr_status upload_scene(rbr_ctx* ctx, const rbr_scene_desc* d) {
     s.num_materials = d->num_materials;
     s.num_lights = d->num_lights;
     std::memcpy(s.background, d->background, 12);
-    s.has_medium = d->medium ? 1u : 0u;
-    if (d->medium) {
-        // Color sigma_t = sigma_a + sigma_s; avgSigmaT = (x + y + z) / 3 (medium.cpp:13-14)
-        for (int a = 0; a < 3; ++a) {
-            s.sigma_s[a] = d->medium->sigma_s[a];
-            s.sigma_t[a] = d->medium->sigma_a[a] + d->medium->sigma_s[a];
-        }
-        s.avg_sigma_t = (s.sigma_t[0] + s.sigma_t[1] + s.sigma_t[2]) / 3.0f;
-        s.hg_g = d->medium->g;
-    }
+    set_medium(s, d->medium);
     ctx->scene = s;
     ctx->has_scene = true;
     for (int a = 0; a < 3; ++a) {
@@ -408,6 +421,46 @@ rbr_status upload_scene(rbr_ctx* ctx, const rbr_scene_desc* d) {
     ctx->stats.build_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     if (bvh.max_depth >= static_cast<uint32_t>(kStackSize))
         return fail(ctx, RBR_ERR_INTERNAL, "BVH deeper than the traversal stack");
+    return RBR_OK;
+}
+
+// A scene that shares `base`'s geometry and BVH (device buffers owned by `base`) with its
+// own materials, lights and medium. `dst` owns only the new arrays.
+rbr_status upload_scene_variant(rbr_ctx* dst, const rbr_ctx* base, const rbr_material* materials, uint32_t num_materials,
+                                const rbr_light* lights, uint32_t num_lights, const rbr_medium* medium) {
+    if (!base->has_scene) return fail(dst, RBR_ERR_NO_SCENE, "the base scene is empty");
+    if (num_materials != base->scene.num_materials || (num_materials && !materials) || (num_lights && !lights))
+        return fail(dst, RBR_ERR_INVALID_ARGUMENT, "a variant needs as many materials as its base scene (" +
+                                                       std::to_string(base->scene.num_materials) + ")");
+    for (uint32_t i = 0; i < num_materials; ++i) {
+        const rbr_material& m = materials[i];
+        if (!finite3(m.base_color, 3) || !finite3(m.emission, 3) || !std::isfinite(m.metallic) ||
+            !std::isfinite(m.roughness) || !std::isfinite(m.ior) || !std::isfinite(m.transmission))
+            return fail(dst, RBR_ERR_INVALID_ARGUMENT, "material " + std::to_string(i) + " has a non-finite parameter");
+    }
+    for (uint32_t i = 0; i < num_lights; ++i)
+        if (lights[i].type != RBR_LIGHT_AREA && lights[i].type != RBR_LIGHT_POINT)
+            return fail(dst, RBR_ERR_UNSUPPORTED, "light " + std::to_string(i) + " has unknown type");
+    free_scene(dst);
+    dst->stats.device_bytes = 0;
+    DeviceScene s = base->scene;
+    void* p = nullptr;
+    rbr_status st;
+    if ((st = upload(dst, device_materials(materials, num_materials), "materials", &p)) != RBR_OK) return free_scene(dst), st;
+    s.materials = static_cast<const MaterialDev*>(p);
+    if ((st = upload(dst, device_lights(lights, num_lights), "lights", &p)) != RBR_OK) return free_scene(dst), st;
+    s.lights = static_cast<const LightDev*>(p);
+    s.num_lights = num_lights;
+    set_medium(s, medium);
+    dst->scene = s;
+    dst->has_scene = true;
+    for (int a = 0; a < 3; ++a) {
+        dst->bounds_lo[a] = base->bounds_lo[a];
+        dst->bounds_hi[a] = base->bounds_hi[a];
+    }
+    const uint64_t own = dst->stats.device_bytes;
+    dst->stats = base->stats;
+    dst->stats.device_bytes = own;
     return RBR_OK;
 }
 

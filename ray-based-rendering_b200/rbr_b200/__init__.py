@@ -89,6 +89,9 @@ def load_library() -> C.CDLL:
         "rbr_batch_last_error": (C.c_char_p, [P]),
         "rbr_batch_add_scene": (C.c_int, [P, C.POINTER(abi.rbr_scene_desc), C.POINTER(C.c_uint32)]),
         "rbr_batch_cache_create": (C.c_int, [P, C.c_uint32, C.POINTER(abi.rbr_cache_config)]),
+        "rbr_batch_add_scene_variant": (C.c_int, [P, C.c_uint32, C.POINTER(abi.rbr_material), C.c_uint32,
+                                                  C.POINTER(abi.rbr_light), C.c_uint32, C.POINTER(abi.rbr_medium),
+                                                  C.POINTER(C.c_uint32)]),
         "rbr_batch_submit": (C.c_int, [P, C.POINTER(abi.rbr_request), C.POINTER(C.c_uint32)]),
         "rbr_batch_run": (C.c_int, [P, P]),
         "rbr_batch_request_stats": (C.c_int, [P, C.c_uint32, C.POINTER(abi.rbr_request_stats)]),
@@ -388,6 +391,16 @@ class Batch:
         desc = scene.desc() if hasattr(scene, "desc") and callable(scene.desc) else scene
         sid = C.c_uint32()
         self._check(self.lib.rbr_batch_add_scene(self.h, C.byref(desc.desc), C.byref(sid)))
+        self._keep.append(desc)
+        return int(sid.value)
+
+    def add_scene_variant(self, base_id: int, scene) -> int:
+        """A scene sharing base_id's geometry and BVH, with `scene`'s materials, lights, medium."""
+        desc = scene.desc() if hasattr(scene, "desc") and callable(scene.desc) else scene
+        d = desc.desc
+        sid = C.c_uint32()
+        self._check(self.lib.rbr_batch_add_scene_variant(self.h, base_id, d.materials, d.num_materials, d.lights,
+                                                         d.num_lights, d.medium, C.byref(sid)))
         self._keep.append(desc)
         return int(sid.value)
 

@@ -578,3 +578,41 @@ def ggx_scene(width=1920, height=1080, n_spheres=256, mesh_n=1000, seed=0) -> Sc
     dist = float(np.linalg.norm(np.subtract(tgt, pos)))
     s.camera = look_at_camera(width, height, pos, tgt, (0, 1, 0), 40.0, lens_radius=0.05, focal_distance=dist)
     return s
+
+
+def ggx_variant(base: Scene, seed: int) -> Scene:
+    """A seeded material and light perturbation of a GGX scene with the same geometry: base
+    colours scaled by U[0.7, 1.3] per channel (clamped to 1), roughness shifted by U[-0.1, 0.1]
+    (kept in [0.05, 1]), light intensities scaled by U[0.5, 1.5] and area-light colours tinted."""
+    import copy
+
+    rng = np.random.default_rng(1000 + seed)
+    v = copy.copy(base)
+    v.materials = []
+    for m in base.materials:
+        m = dict(m)
+        if max(m["emission"]) <= 0.0:
+            m["base_color"] = tuple(float(min(1.0, c * rng.uniform(0.7, 1.3))) for c in m["base_color"])
+            m["roughness"] = float(np.clip(m["roughness"] + rng.uniform(-0.1, 0.1), 0.05, 1.0))
+        v.materials.append(m)
+    v.lights = []
+    for l in base.lights:
+        l = dict(l)
+        l["intensity"] = float(l["intensity"] * rng.uniform(0.5, 1.5))
+        if l["type"] == abi.RBR_LIGHT_AREA:
+            l["color"] = tuple(float(c * rng.uniform(0.8, 1.2)) for c in l["color"])
+        v.lights.append(l)
+    return v
+
+
+def square_camera(cam: abi.rbr_camera, size: int) -> abi.rbr_camera:
+    """The same camera with a size x size film and the vertical field of view kept."""
+    c = abi.rbr_camera()
+    C.memmove(C.byref(c), C.byref(cam), C.sizeof(cam))
+    scale = size / cam.height
+    c.width = c.height = size
+    c.fx = cam.fx * scale
+    c.fy = cam.fy * scale
+    c.cx = size / 2.0
+    c.cy = size / 2.0
+    return c

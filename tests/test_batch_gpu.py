@@ -152,3 +152,27 @@ def test_invalid_requests_are_rejected(bctx):
         b.submit(sid, cam, render_params(spp=1), f.data_ptr(), use_cache=True)  # no cache on the scene
     with pytest.raises(RbrError):
         b.submit(sid, cam, render_params(spp=1, flags=abi.RBR_RENDER_SECOND_MOMENT), f.data_ptr())
+
+
+def test_scene_variants_share_geometry(bctx):
+    """A variant (other materials and lights on the base scene's resident BVH) renders what a
+    full upload of the variant renders."""
+    base = small_ggx(16, 16)
+    var = scenes.ggx_variant(base, 3)
+    b = Batch(bctx)
+    bid = b.add_scene(base)
+    vid = b.add_scene_variant(bid, var)
+    cam = small_ggx(64, 48).camera
+    f = torch.zeros(64 * 48 * 3, device="cuda")
+    p = render_params(spp=4, max_depth=8, seed=21)
+    b.submit(vid, cam, p, f.data_ptr())
+    b.run()
+    torch.cuda.synchronize()
+    var.camera = cam
+    bctx.upload(var)
+    want = bctx.render_host(cam, p)
+    np.testing.assert_allclose(f.cpu().numpy().reshape(48, 64, 3), want, rtol=2e-5, atol=2e-6)
+    base.camera = cam
+    bctx.upload(base)
+    assert not np.allclose(bctx.render_host(cam, p), want)
+    b.close()
