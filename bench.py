@@ -129,6 +129,24 @@ def visible_gpu_indices(local_rank):
 
 
 # ------------------------------------------------------------------------------------------
+# multi-rank plumbing (one process per GPU, replicas: no data-path collective)
+def max_over_ranks(x: float, dist, device) -> float:
+    """The largest of the ranks' values (a device time or a wall time): the job's time."""
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def weak_scaling_rate(units_per_rank: int, world: int, seconds: float) -> float:
+    """Whole-job throughput in millions of units per second: every rank processed
+    units_per_rank, the job took the slowest rank's time."""
+    return units_per_rank * world / seconds / 1e6
+
+
 def workload(rank):
     from rbr_b200 import scenes
 
@@ -588,10 +606,7 @@ def main():
         dist.barrier()
     launch_ms = [evs[k].elapsed_time(evs[k + 1]) for k in range(args.steps)]
     total_ms = evs[0].elapsed_time(evs[-1])
-    if dist:
-        t = torch.tensor([total_ms], device=f"cuda:{local_rank}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(total_ms, dist, f"cuda:{local_rank}")
     clk = clocks.stop(visible_gpu_indices(local_rank)) if clocks else None
 
     # algorithmic traffic of one launch
@@ -621,13 +636,10 @@ def main():
         for _ in range(e2e_steps):
             ctx.trace_host(hr, out=hh)
         e2e_s = time.perf_counter() - t0
-        if dist:
-            t = torch.tensor([e2e_s], device=f"cuda:{local_rank}")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
+        e2e_s = max_over_ranks(e2e_s, dist, f"cuda:{local_rank}")
         got = d_hits.cpu().numpy().view(abi.HIT_DTYPE)
         assert np.array_equal(got["prim"], hh["prim"]), "device and host entry points disagree"
-        e2e = {"value": n * world * e2e_steps / e2e_s / 1e6, "unit": "Mrays/s",
+        e2e = {"value": weak_scaling_rate(n * e2e_steps, world, e2e_s), "unit": "Mrays/s",
                "h2d_bytes_per_step": n * 32, "d2h_bytes_per_step": n * 8,
                "path": "rbr_trace_host: pinned host rays -> device, closest hit, hits -> pinned host"}
 
@@ -636,7 +648,7 @@ def main():
         base = cpu_baseline(scene, rays, args.cpu_seconds)
 
     if rank == 0:
-        value = n * world * args.steps / (total_ms / 1e3) / 1e6
+        value = weak_scaling_rate(n * args.steps, world, total_ms / 1e3)
         line = {
             "metric": "Mrays/s traversal (closest hit)", "value": value, "unit": "Mrays/s", "n_gpus": world,
             "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": total_ms / args.steps,

@@ -469,6 +469,33 @@ rbr_status rbr_phase_sample_host(rbr_ctx* ctx, float g, uint32_t n, const float*
 rbr_status rbr_medium_sample_host(rbr_ctx* ctx, const rbr_medium* medium, uint32_t n, const float* max_dist,
                                   const float* u, float* out);
 
+/* ------------------------------------------------------------------------------------------
+ * Meshes and film export.
+ * ------------------------------------------------------------------------------------------ */
+typedef struct rbr_mesh rbr_mesh;
+
+/* ObjImporter::load / ::parse (src/io/obj_importer.cpp) followed by TriangleMesh::toPrimitives
+ * (src/geometry/mesh.cpp:14-38): the mesh as rbr_scene_desc triangle arrays. On failure the
+ * message is written to `error` (may be NULL). */
+rbr_status rbr_mesh_load_obj(const char* path, rbr_mesh** out, char* error, size_t error_len);
+rbr_status rbr_mesh_parse_obj(const char* text, size_t length, rbr_mesh** out, char* error, size_t error_len);
+uint32_t rbr_mesh_triangles(const rbr_mesh* mesh);
+/* 9 floats per triangle (v0, v1, v2) */
+const float* rbr_mesh_triangle_vertices(const rbr_mesh* mesh);
+/* 9 floats per triangle of unit vertex normals when the file gives a normal for every corner
+ * (as Triangle's normal constructor normalises them), else NULL */
+const float* rbr_mesh_triangle_normals(const rbr_mesh* mesh);
+void rbr_mesh_destroy(rbr_mesh* mesh);
+
+/* Film::toRGB8 (tonemap = 0) and Film::toRGB8ToneMapped (tonemap != 0; exposure, then Reinhard)
+ * (src/core/film.cpp:34-62) of a film of per-pixel means (width*height*3 floats) into
+ * width*height*3 bytes: device pointers, asynchronous on `stream`. */
+rbr_status rbr_film_to_rgb8(rbr_ctx* ctx, const float* film, int32_t width, int32_t height, float exposure, float gamma,
+                            int tonemap, uint8_t* out, void* stream);
+/* The same on host buffers; waits. */
+rbr_status rbr_film_to_rgb8_host(rbr_ctx* ctx, const float* film, int32_t width, int32_t height, float exposure,
+                                 float gamma, int tonemap, uint8_t* out);
+
 /* Size of the fixed scratch array used by rbr_render_noalloc (16 MiB). */
 #define RBR_NOALLOC_SCRATCH_BYTES (16u << 20)
 

@@ -179,6 +179,7 @@ class Reference:
         L.ref_power_heuristic.restype = C.c_float
         L.ref_power_heuristic.argtypes = [C.c_int, C.c_float, C.c_int, C.c_float]
         L.ref_frame.argtypes = [P, P, P]
+        L.ref_film_rgb8.argtypes = [P, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int, P]
         L.ref_hg_eval.argtypes = [C.c_float, _i64, P, P, P]
         L.ref_hg_sample.argtypes = [C.c_float, _i64, P, P, P]
         L.ref_medium_sample.argtypes = [C.POINTER(abi.rbr_medium), _i64, P, P, P]
@@ -277,6 +278,31 @@ class Reference:
         out = np.zeros(len(wo), np.float32)
         self.L.ref_hg_eval(g, len(wo), _ptr(wo), _ptr(wi), _ptr(out))
         return out
+
+    def film_rgb8(self, film, exposure=1.0, gamma=2.2, tonemap=False):
+        film = _f(film)
+        h, w = film.shape[:2]
+        out = np.zeros((h, w, 3), np.uint8)
+        self.L.ref_film_rgb8(_ptr(film), w, h, exposure, gamma, int(tonemap), _ptr(out))
+        return out
+
+    def obj_triangles(self, text: bytes):
+        """(vertices [n, 9], normals [n, 9] or None) of the reference's ObjImporter::load +
+        toPrimitives on `text` (run by oracle/_ref/ref_obj_dump), None when it fails."""
+        import subprocess
+        import tempfile
+
+        with tempfile.NamedTemporaryFile(suffix=".obj") as f:
+            f.write(text)
+            f.flush()
+            out = subprocess.run([str(HERE / "_ref" / "ref_obj_dump"), f.name], capture_output=True, check=True).stdout
+        n = int(np.frombuffer(out[:8], np.int64)[0])
+        if n < 0:
+            return None
+        has = int(np.frombuffer(out[8:12], np.int32)[0])
+        data = np.frombuffer(out[12:], np.float32)
+        v = data[:9 * n].reshape(n, 9).copy()
+        return v, (data[9 * n:18 * n].reshape(n, 9).copy() if has else None)
 
     def hg_sample(self, g, wo, u):
         wo, u = _f(wo), _f(u)

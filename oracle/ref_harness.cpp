@@ -195,6 +195,15 @@ void ref_medium_sample(const rbr_medium* m, int64_t n, const float* max_dist, co
     }
 }
 
+// Film::toRGB8 / toRGB8ToneMapped of a film whose pixels hold `film` (one sample each).
+void ref_film_rgb8(const float* film, int w, int h, float exposure, float gamma, int tonemap, uint8_t* out) {
+    Film f(w, h);
+    for (int y = 0; y < h; ++y)
+        for (int x = 0; x < w; ++x) f.addSample(x, y, v3(film + 3 * (static_cast<size_t>(y) * w + x)));
+    const std::vector<unsigned char> d = tonemap ? f.toRGB8ToneMapped(exposure, gamma) : f.toRGB8(gamma);
+    std::memcpy(out, d.data(), d.size());
+}
+
 // Closest hit through the scene's accelerator (Scene::intersect).
 void ref_trace_closest(void* s, const rbr_ray* rays, int64_t n, rbr_hit* hits, int nthreads) {
     const RefScene& rs = *static_cast<RefScene*>(s);

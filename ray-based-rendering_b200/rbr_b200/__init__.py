@@ -83,6 +83,14 @@ def load_library() -> C.CDLL:
         "rbr_cache_train_host": (C.c_int, [P, C.c_uint32, P, P, C.c_int, C.POINTER(C.c_float)]),
         "rbr_cache_render": (C.c_int, [P, C.POINTER(abi.rbr_camera), C.POINTER(abi.rbr_render_params), C.c_uint32,
                                        C.c_int, P, P, P]),
+        "rbr_mesh_load_obj": (C.c_int, [C.c_char_p, C.POINTER(P), C.c_char_p, C.c_size_t]),
+        "rbr_mesh_parse_obj": (C.c_int, [C.c_char_p, C.c_size_t, C.POINTER(P), C.c_char_p, C.c_size_t]),
+        "rbr_mesh_triangles": (C.c_uint32, [P]),
+        "rbr_mesh_triangle_vertices": (C.POINTER(C.c_float), [P]),
+        "rbr_mesh_triangle_normals": (C.POINTER(C.c_float), [P]),
+        "rbr_mesh_destroy": (None, [P]),
+        "rbr_film_to_rgb8": (C.c_int, [P, P, C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_int, P, P]),
+        "rbr_film_to_rgb8_host": (C.c_int, [P, P, C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_int, P]),
         "rbr_batch_config_default": (None, [C.POINTER(abi.rbr_batch_config)]),
         "rbr_batch_create": (C.c_int, [P, C.POINTER(abi.rbr_batch_config), C.POINTER(P)]),
         "rbr_batch_destroy": (None, [P]),
@@ -105,6 +113,44 @@ def load_library() -> C.CDLL:
             f.argtypes = args
     _lib = lib
     return lib
+
+
+def _mesh_arrays(lib, h):
+    n = lib.rbr_mesh_triangles(h)
+    v = np.ctypeslib.as_array(lib.rbr_mesh_triangle_vertices(h), shape=(n * 9,)).reshape(n, 9).copy()
+    np_ = lib.rbr_mesh_triangle_normals(h)
+    nn = np.ctypeslib.as_array(np_, shape=(n * 9,)).reshape(n, 9).copy() if np_ else None
+    return v, nn
+
+
+def parse_obj(text):
+    """Triangles of an OBJ text (ObjImporter::parse + toPrimitives): vertices [n, 9] and unit
+    vertex normals [n, 9] or None. Raises ValueError on a malformed file."""
+    lib = load_library()
+    data = text.encode() if isinstance(text, str) else bytes(text)
+    h = C.c_void_p()
+    err = C.create_string_buffer(256)
+    st = lib.rbr_mesh_parse_obj(data, len(data), C.byref(h), err, 256)
+    if st != abi.RBR_OK:
+        raise ValueError(err.value.decode())
+    try:
+        return _mesh_arrays(lib, h)
+    finally:
+        lib.rbr_mesh_destroy(h)
+
+
+def load_obj(path):
+    """parse_obj of a file (ObjImporter::load)."""
+    lib = load_library()
+    h = C.c_void_p()
+    err = C.create_string_buffer(256)
+    st = lib.rbr_mesh_load_obj(str(path).encode(), C.byref(h), err, 256)
+    if st != abi.RBR_OK:
+        raise ValueError(err.value.decode())
+    try:
+        return _mesh_arrays(lib, h)
+    finally:
+        lib.rbr_mesh_destroy(h)
 
 
 def render_params(spp=16, max_depth=8, use_nee=True, use_mis=True, seed=0, sample_offset=0, flags=0):
@@ -335,6 +381,14 @@ class Context:
                                               C.c_void_p(film_mean_ptr), C.c_void_p(film_m2_ptr or None),
                                               C.c_void_p(stream)))
 
+    def film_to_rgb8(self, film: np.ndarray, exposure=1.0, gamma=2.2, tonemap=False) -> np.ndarray:
+        film = np.ascontiguousarray(film, np.float32)
+        h, w = film.shape[:2]
+        out = np.zeros((h, w, 3), np.uint8)
+        self._check(self.lib.rbr_film_to_rgb8_host(self.h, C.c_void_p(film.ctypes.data), w, h, exposure, gamma,
+                                                   int(tonemap), C.c_void_p(out.ctypes.data)))
+        return out
+
     def phase_eval(self, g, wo, wi):
         n = len(wo)
         return self._unit(lambda h, a, b, o: self.lib.rbr_phase_eval_host(h, g, n, a, b, o), [wo, wi], n, 1)[:, 0]
@@ -437,5 +491,5 @@ class Batch:
         return s
 
 
-__all__ = ["Context", "Batch", "RbrError", "load_library", "header_functions", "render_params", "abi", "RAY_DTYPE",
+__all__ = ["Context", "Batch", "load_obj", "parse_obj", "RbrError", "load_library", "header_functions", "render_params", "abi", "RAY_DTYPE",
            "HIT_DTYPE"]

@@ -123,6 +123,21 @@ class Scene:
         self.lights.append(dict(type=abi.RBR_LIGHT_POINT, position=tuple(position), u=(0, 0, 0), v=(0, 0, 0),
                                 color=tuple(color), intensity=float(intensity)))
 
+    def add_mesh(self, vertices, normals, material: int):
+        """Appends triangles ([n, 9] vertices, optional [n, 9] unit normals) with one material,
+        as TriangleMesh::toPrimitives adds a mesh (src/geometry/mesh.cpp:14-38)."""
+        v = np.asarray(vertices, F32).reshape(-1, 9)
+        old = len(self.triangles)
+        if normals is not None and old and self.triangle_normals is None:
+            raise ValueError("mixing triangles with and without normals")
+        self.triangles = np.concatenate([self.triangles.reshape(-1, 9), v]).astype(F32)
+        if normals is not None:
+            nn = np.asarray(normals, F32).reshape(-1, 9)
+            self.triangle_normals = nn if self.triangle_normals is None else np.concatenate([self.triangle_normals, nn])
+        elif self.triangle_normals is not None:
+            raise ValueError("mixing triangles with and without normals")
+        self.triangle_materials = np.concatenate([self.triangle_materials, np.full(len(v), material, np.uint32)])
+
     def set_medium(self, sigma_a, sigma_s, g=0.0):
         """SceneBuilder::medium (src/scene/scene_builder.cpp:102-105): a HomogeneousMedium."""
         self.medium = dict(sigma_a=tuple(sigma_a), sigma_s=tuple(sigma_s), g=float(g))

@@ -11,7 +11,7 @@ pytestmark = pytest.mark.gpu
 BIN = Path(__file__).resolve().parent / "cpp" / "_bin"
 
 
-@pytest.mark.parametrize("name", ["test_gpu_accelerator", "test_gpu_integrator"])
+@pytest.mark.parametrize("name", ["test_gpu_accelerator", "test_gpu_integrator", "test_gpu_accel_integrators"])
 def test_cpp_adapter(name):
     exe = BIN / name
     if not exe.exists():
