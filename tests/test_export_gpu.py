@@ -53,7 +53,7 @@ def test_film_export_matches_reference(ctx, reference, tonemap, exposure, gamma)
     except where pow() lands within an ulp of a quantisation step (at most one level)."""
     rng = np.random.default_rng(9)
     film = (rng.random((96, 128, 3)) ** 3 * 4.0).astype(np.float32)
-    film[0, :8] = [0.0, 1.0, 1.0000001, 0.9999999, 1e-30, 7.0, 0.5, 2.0 ** -20]
+    film[0, :8] = np.array([0.0, 1.0, 1.0000001, 0.9999999, 1e-30, 7.0, 0.5, 2.0 ** -20], np.float32)[:, None]
     film[1, :3] = -0.25  # negative radiance clamps to 0
     got = ctx.film_to_rgb8(film, exposure, gamma, tonemap)
     want = reference.film_rgb8(film, exposure, gamma, tonemap)
