@@ -10,8 +10,9 @@ namespace {
 // encode(): gamma, clamp to [0, 1] as std::max(0, std::min(1, v)), * 255 + 0.5, truncated.
 __device__ __forceinline__ uint8_t encode8(float v, float inv_gamma) {
     const float p = static_cast<float>(pow(static_cast<double>(v), static_cast<double>(inv_gamma)));
-    const float lo = (p < 1.0f) ? p : 1.0f;
-    const float c = (0.0f < lo) ? lo : 0.0f;
+    // std::max(0, std::min(1, p)) sends NaN (a negative value's power) to 1; a saturating
+    // clamp would send it to 0, so NaN is handled before clamping.
+    const float c = (p != p) ? 1.0f : fminf(fmaxf(p, 0.0f), 1.0f);
     return static_cast<uint8_t>(__float2uint_rz(fa(fm(c, 255.0f), 0.5f)));
 }
 
