@@ -14,6 +14,11 @@ oracle/Makefile). Every expected value below is an output of the reference's cod
   golden_mis.npz      sampling::powerHeuristic
   golden_cornell.npz  per-pixel mean and variance of PathTracingIntegrator::Li on the Cornell
                       box at 24x24, 2048 samples per pixel (independent seeds)
+  golden_volume.npz   HenyeyGreensteinPhase::evaluate / sample, HomogeneousMedium::sampleDistance,
+                      and per-pixel mean and variance of VolumetricPathIntegrator::Li on the
+                      foggy Cornell box at 16x16, depth 3, 4096 samples per pixel
+  golden_obj.npz      ObjImporter::parse + TriangleMesh::toPrimitives on small OBJ texts
+  golden_film.npz     Film::toRGB8 / toRGB8ToneMapped of a seeded film
 """
 import sys
 from pathlib import Path
@@ -28,7 +33,7 @@ sys.path.insert(0, str(HERE.parent))
 
 import helpers  # noqa: E402
 from oracle import Reference  # noqa: E402
-from rbr_b200 import render_params, scenes  # noqa: E402
+from rbr_b200 import abi, render_params, scenes  # noqa: E402
 
 
 def mat_params(m):
@@ -97,6 +102,48 @@ def main():
     mean = acc[0] / n
     var = np.maximum(acc[1] / n - mean ** 2, 0) * n / (n - 1)
     np.savez_compressed(HERE / "golden_cornell.npz", mean=mean, var=var, n=np.array(n), camera=camera_params(cam))
+    # participating medium
+    gs = np.array([0.0, 0.0005, 0.5, -0.3, 0.9], np.float32)
+    rng = np.random.default_rng(77)
+    wo = helpers.unit_vectors(rng, 256)
+    wi = helpers.unit_vectors(rng, 256)
+    u2 = rng.random((256, 2), dtype=np.float32)
+    med = abi.rbr_medium()
+    med.sigma_a = abi.f3((0.02, 0.03, 0.01))
+    med.sigma_s = abi.f3((0.08, 0.07, 0.09))
+    med.g = 0.5
+    md = np.where(rng.random(256) < 0.1, np.inf, rng.uniform(0.01, 40.0, 256)).astype(np.float32)
+    um = rng.random(256, dtype=np.float32)
+    fog = scenes.foggy_cornell_box()
+    fcam = scenes.look_at_camera(16, 16, (0.0, 1.0, 3.5), (0.0, 1.0, 0.0), (0.0, 1.0, 0.0), 40.0)
+    fog.camera = fcam
+    nf = 4096
+    facc = ref.render_moments(ref.scene(fog), fcam, render_params(spp=nf, max_depth=3), batch=13, volumetric=True)
+    fmean = facc[0] / nf
+    fvar = np.maximum(facc[1] / nf - fmean ** 2, 0) * nf / (nf - 1)
+    np.savez_compressed(HERE / "golden_volume.npz", g=gs, wo=wo, wi=wi, u=u2,
+                        hg_eval=np.array([ref.hg_eval(g, wo, wi) for g in gs]),
+                        hg_sample=np.array([ref.hg_sample(g, wo, u2) for g in gs]),
+                        medium=np.array(list(med.sigma_a) + list(med.sigma_s) + [med.g], np.float32),
+                        max_dist=md, u_medium=um, medium_sample=ref.medium_sample(med, md, um),
+                        fog_mean=fmean, fog_var=fvar, fog_n=np.array(nf), fog_camera=camera_params(fcam))
+    # OBJ meshes
+    import test_mesh_obj
+
+    texts, verts, norms = [], [], []
+    for name, text in test_mesh_obj.CASES.items():
+        v, nn = ref.obj_triangles(text)
+        texts.append(text)
+        verts.append(v)
+        norms.append(nn if nn is not None else np.zeros((0, 9), np.float32))
+    np.savez_compressed(HERE / "golden_obj.npz", names=np.array(list(test_mesh_obj.CASES)),
+                        texts=np.array(texts), **{f"v{i}": v for i, v in enumerate(verts)},
+                        **{f"n{i}": nn for i, nn in enumerate(norms)})
+    # film export
+    film = (np.random.default_rng(9).random((48, 64, 3)) ** 3 * 4.0).astype(np.float32)
+    modes = [(False, 1.0, 2.2), (True, 1.5, 2.2), (True, 0.25, 1.0)]
+    np.savez_compressed(HERE / "golden_film.npz", film=film, modes=np.array(modes, np.float32),
+                        rgb8=np.array([ref.film_rgb8(film, e, g, t) for t, e, g in modes]))
     for f in sorted(HERE.glob("*.npz")):
         print(f.name, f.stat().st_size)
 

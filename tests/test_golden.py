@@ -109,6 +109,46 @@ def test_restatement_cornell_converges_to_golden(restatement):
     assert z_fraction(S / n, Q, n, g, True) < 0.01
 
 
+def fog_z(mean, var_or_m2, n, g, from_moments):
+    """z scores of a foggy-Cornell estimate against golden_volume.npz, and of the image mean."""
+    if from_moments:
+        var = np.maximum(var_or_m2 / n - mean.astype(np.float64) ** 2, 0) * n / (n - 1)
+    else:
+        var = var_or_m2
+    ng = int(g["fog_n"])
+    se = np.sqrt(var / n + g["fog_var"] / ng)
+    z = np.abs(mean - g["fog_mean"]) / np.maximum(se, 1e-12)
+    z[(se == 0) & (np.abs(mean - g["fog_mean"]) < 1e-6)] = 0
+    z_img = abs(mean.mean() - g["fog_mean"].mean()) / max(np.sqrt((var / n + g["fog_var"] / ng).sum()) / mean.size, 1e-12)
+    return (z > 3).mean(), z_img
+
+
+def test_restatement_volume(restatement):
+    g = load("golden_volume.npz")
+    for k, gv in enumerate(g["g"]):
+        assert np.array_equal(bits(restatement.hg_eval(float(gv), g["wo"], g["wi"])), bits(g["hg_eval"][k]))
+        assert np.array_equal(bits(restatement.hg_sample(float(gv), g["wo"], g["u"])), bits(g["hg_sample"][k]))
+    s = scenes.foggy_cornell_box()
+    n = 4096
+    p = render_params(spp=n, max_depth=3, seed=19, flags=abi.RBR_RENDER_VOLUMETRIC)
+    _, S, Q = restatement.render(restatement.scene(s), camera(g["fog_camera"]), p, moments=True)
+    tail, z_img = fog_z(S / n, Q, n, g, True)
+    assert tail < 0.015 and z_img < 3.0, (tail, z_img)
+
+
+def test_obj_meshes_golden():
+    from rbr_b200 import parse_obj
+
+    g = load("golden_obj.npz")
+    for i, (name, text) in enumerate(zip(g["names"], g["texts"])):
+        v, nn = parse_obj(bytes(text))
+        assert np.array_equal(bits(v), bits(g[f"v{i}"])), name
+        want_n = g[f"n{i}"]
+        assert (nn is None) == (len(want_n) == 0), name
+        if nn is not None:
+            assert np.array_equal(bits(nn), bits(want_n)), name
+
+
 # ------------------------------------------------------------------------------------------ GPU
 @pytest.mark.gpu
 def test_gpu_rays(ctx):
@@ -152,3 +192,34 @@ def test_gpu_cornell_converges_to_golden(ctx):
     n = 8192
     mean, m2 = ctx.render_host(camera(g["camera"]), render_params(spp=n, seed=10), second_moment=True)
     assert z_fraction(mean, m2, n, g, True) < 0.01
+
+
+@pytest.mark.gpu
+def test_gpu_volume(ctx):
+    g = load("golden_volume.npz")
+    for k, gv in enumerate(g["g"]):
+        assert np.array_equal(bits(ctx.phase_eval(float(gv), g["wo"], g["wi"])), bits(g["hg_eval"][k]))
+        d = np.abs(ctx.phase_sample(float(gv), g["wo"], g["u"]) - g["hg_sample"][k]).max(axis=1)
+        assert d.max() <= 1e-4 and (d <= 1e-5).mean() >= 0.99
+    med = abi.rbr_medium()
+    med.sigma_a, med.sigma_s, med.g = abi.f3(g["medium"][0:3]), abi.f3(g["medium"][3:6]), float(g["medium"][6])
+    got, want = ctx.medium_sample(med, g["max_dist"], g["u_medium"]), g["medium_sample"]
+    same = got[:, 4] == want[:, 4]
+    assert same.mean() >= 0.99
+    np.testing.assert_allclose(got[same], want[same], rtol=2e-6, atol=1e-12)
+    s = scenes.foggy_cornell_box()
+    ctx.upload(s)
+    n = 4096
+    p = render_params(spp=n, max_depth=3, seed=23, flags=abi.RBR_RENDER_VOLUMETRIC)
+    mean, m2 = ctx.render_host(camera(g["fog_camera"]), p, second_moment=True)
+    tail, z_img = fog_z(mean, m2, n, g, True)
+    assert tail < 0.015 and z_img < 3.0, (tail, z_img)
+
+
+@pytest.mark.gpu
+def test_gpu_film_export(ctx):
+    g = load("golden_film.npz")
+    for (t, e, gam), want in zip(g["modes"], g["rgb8"]):
+        got = ctx.film_to_rgb8(g["film"], float(e), float(gam), bool(t))
+        d = np.abs(got.astype(int) - want.astype(int))
+        assert d.max() <= 1 and (d == 0).mean() >= 0.999
