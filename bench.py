@@ -47,7 +47,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--workload", choices=["rays", "cornell", "ggx", "fog", "cache", "batch"], default="rays")
-    p.add_argument("--ref-spp", type=int, default=1024, help="cache workload: spp of the converged GPU reference")
+    p.add_argument("--ref-spp", type=int, default=4096, help="cache workload: spp of the converged GPU reference")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true", help="skip the host-buffer measurement (profiling runs)")
     p.add_argument("--param", action="append", default=[], help="NAME=VALUE context tunable (rbr_param_set)")
@@ -348,7 +348,7 @@ def run_cache(args, rank, world, local_rank):
     """Learned radiance cache vs the plain GPU path tracer at equal time on the GGX scene
     (1920x1080, 1 spp per frame). A step is one frame: 1 spp with paths ending into the cache,
     plus the frame's 4 optimiser steps on 2^16 training paths. Converged reference: the plain
-    GPU path tracer at --ref-spp samples per pixel (independent seed)."""
+    GPU path tracer at --ref-spp samples per pixel (independent seed, default 4096)."""
     import torch
 
     from rbr_b200 import Context, render_params, scenes
