@@ -582,7 +582,8 @@ def main():
     sp = stream.cuda_stream
 
     tuned = ctx.autotune_trace(d_rays.data_ptr(), n) if not args.param else {k: ctx.get_param(k) for k in
-                                                                           ("trace.kernel", "trace.min_blocks")}
+                                                                           ("trace.kernel", "trace.min_blocks",
+                                                                            "trace.order")}
 
     def step():
         ctx.trace_closest_dev(d_rays.data_ptr(), n, d_hits.data_ptr(), sp)
@@ -661,7 +662,9 @@ def main():
                          "algorithmic_bytes_per_launch": alg_bytes,
                          "per_ray": {"nodes": nodes / n, "leaf_records": recs / n,
                                      "bytes": alg_bytes / n},
-                         "kernel": "k_trace_closest", "avg_launch_ms": avg_launch_s * 1e3},
+                         "kernel": "k_trace_closest" if not tuned.get("trace.order") else
+                         "k_trace_closest_perm (timed with its k_ray_keys + radix sort: the whole call)",
+                         "avg_launch_ms": avg_launch_s * 1e3},
             "cpu_baseline": base,
             "clocks": clk,
             "gpu_launches": args.steps,

@@ -232,12 +232,15 @@ rbr_status rbr_scene_stats_get(const rbr_ctx* ctx, rbr_scene_stats* out);
  *                          8 lanes per ray, one child box per lane
  *   "trace.blocks_per_sm"  resident blocks per SM of kernels 1 and 2 (0: occupancy limit)
  *   "trace.min_blocks"     kernel 0's register budget: 8, 10 or 12 resident blocks per SM
+ *   "trace.order"          kernel 0: 0 traces the rays in the order given; 1 first sorts them
+ *                          by direction octant and origin cell (a radix sort on the device) so
+ *                          that warps hold rays that walk the same nodes
  *   "pt.wave_paths"        camera samples per path-tracer wave (default 2^22)
  * Results do not depend on them; only speed and memory do. rbr_autotune picks them. */
 rbr_status rbr_param_set(rbr_ctx* ctx, const char* name, int64_t value);
 rbr_status rbr_param_get(const rbr_ctx* ctx, const char* name, int64_t* value);
 /* Autotuner (no reference counterpart): times every traversal variant ("trace.kernel",
- * "trace.min_blocks") on n rays of the caller's own workload (device pointer) against the
+ * "trace.min_blocks", "trace.order") on n rays of the caller's own workload (device pointer) against the
  * uploaded scene, keeps the fastest in the context and returns its time per launch in
  * microseconds (out_us may be NULL). Waits for the timings. */
 rbr_status rbr_autotune_trace(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any_hit, int64_t* out_us);

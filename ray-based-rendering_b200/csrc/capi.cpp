@@ -128,6 +128,7 @@ void rbr_ctx_destroy(rbr_ctx* ctx) {
     cache_destroy(ctx);
     release(ctx->stage_in);
     release(ctx->stage_out);
+    release(ctx->sort_buf);
     if (ctx->d_error) cudaFree(ctx->d_error);
     if (ctx->d_cursors) cudaFree(ctx->d_cursors);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -154,6 +155,9 @@ rbr_status rbr_param_set(rbr_ctx* ctx, const char* name, int64_t value) {
     } else if (n == "trace.blocks_per_sm") {
         if (value < 0 || value > 32) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "trace.blocks_per_sm is 0..32");
         ctx->trace_blocks_per_sm = static_cast<int>(value);
+    } else if (n == "trace.order") {
+        if (value != 0 && value != 1) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "trace.order is 0 or 1");
+        ctx->trace_order = static_cast<int>(value);
     } else if (n == "trace.min_blocks") {
         if (value != 8 && value != 10 && value != 12) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "trace.min_blocks is 8, 10 or 12");
         ctx->trace_min_blocks = static_cast<int>(value);
@@ -180,6 +184,7 @@ rbr_status rbr_param_get(const rbr_ctx* ctx, const char* name, int64_t* value) {
     if (n == "trace.kernel") *value = ctx->trace_kernel;
     else if (n == "trace.blocks_per_sm") *value = ctx->trace_blocks_per_sm;
     else if (n == "trace.min_blocks") *value = ctx->trace_min_blocks;
+    else if (n == "trace.order") *value = ctx->trace_order;
     else if (n == "pt.wave_paths") *value = ctx->pt_wave_paths;
     else return RBR_ERR_INVALID_ARGUMENT;
     return RBR_OK;

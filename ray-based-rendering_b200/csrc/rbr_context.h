@@ -58,6 +58,8 @@ struct rbr_ctx {
     int trace_kernel = 0;          // 0: one thread per ray, 1: persistent lane refill, 2: warp-cooperative
     int trace_blocks_per_sm = 0;   // persistent grid per SM (0: occupancy limit)
     int trace_min_blocks = 10;     // kernel 0: register budget for 8, 10 or 12 resident blocks per SM
+    int trace_order = 0;           // kernel 0: 0 rays in the given order, 1 sorted by direction octant and origin
+    rbr::DevBuf sort_buf;          // keys, permutation and radix-sort scratch of trace_order 1
     uint32_t pt_wave_paths = 1u << 22;
     // path tracer
     rbr::PathBuffers pt;

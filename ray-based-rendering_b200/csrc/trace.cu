@@ -3,6 +3,10 @@
 // One thread per ray. Rays are read as two 16 B words (origin+tmax, direction+pad), answers
 // written as one 8 B word (closest) or one byte (any). The traversal itself is in
 // rbr_device.cuh.
+#include <cmath>
+
+#include <cub/device/device_radix_sort.cuh>
+
 #include "rbr_context.h"
 #include "rbr_device.cuh"
 
@@ -24,6 +28,63 @@ __global__ void __launch_bounds__(kTraceBlock, kMinBlocks) k_trace_closest(Devic
     float t = 0.0f;
     const uint32_t prim = traverse<false>(s, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, t, err);
     hits[i] = make_uint2(prim, prim == 0xFFFFFFFFu ? 0u : __float_as_uint(t));
+}
+
+// The same query on the rays in the order `perm` (a permutation of 0..n-1): rays that start
+// close together with directions of the same octant share warps, so they walk the same nodes.
+// Answers go to the rays' own positions.
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kTraceBlock, kMinBlocks)
+    k_trace_closest_perm(DeviceScene s, const float4* __restrict__ rays, uint32_t n, const uint32_t* __restrict__ perm,
+                         uint2* __restrict__ hits, int* err) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const uint32_t i = __ldg(perm + j);
+    const float4 a = __ldg(rays + 2 * static_cast<size_t>(i));
+    const float4 b = __ldg(rays + 2 * static_cast<size_t>(i) + 1);
+    float t = 0.0f;
+    const uint32_t prim = traverse<false>(s, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, t, err);
+    hits[i] = make_uint2(prim, prim == 0xFFFFFFFFu ? 0u : __float_as_uint(t));
+}
+
+__global__ void __launch_bounds__(kTraceBlock) k_trace_any_perm(DeviceScene s, const float4* __restrict__ rays, uint32_t n,
+                                                                const uint32_t* __restrict__ perm,
+                                                                uint8_t* __restrict__ occ, int* err) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const uint32_t i = __ldg(perm + j);
+    const float4 a = __ldg(rays + 2 * static_cast<size_t>(i));
+    const float4 b = __ldg(rays + 2 * static_cast<size_t>(i) + 1);
+    float t;
+    occ[i] = static_cast<uint8_t>(traverse<true>(s, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, t, err));
+}
+
+// 3-bit direction octant, then a 27-bit Morton code of the origin's cell (512^3 cells over the
+// scene box): the sort key that groups rays by octant and, within it, by origin.
+__device__ __forceinline__ uint32_t spread3(uint32_t x) {  // 9 bits -> every third of 27
+    x &= 0x1FFu;
+    x = (x | (x << 16)) & 0x030000FFu;
+    x = (x | (x << 8)) & 0x0300F00Fu;
+    x = (x | (x << 4)) & 0x030C30C3u;
+    x = (x | (x << 2)) & 0x09249249u;
+    return x;
+}
+
+__global__ void k_ray_keys(const float4* __restrict__ rays, uint32_t n, float3 lo, float3 scale, uint32_t* keys,
+                           uint32_t* idx) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 a = __ldg(rays + 2 * static_cast<size_t>(i));
+        const float4 b = __ldg(rays + 2 * static_cast<size_t>(i) + 1);
+        const uint32_t oct = (signbit(b.x) ? 4u : 0u) | (signbit(b.y) ? 2u : 0u) | (signbit(b.z) ? 1u : 0u);
+        auto cell = [](float v, float l, float sc) {
+            const float c = (v - l) * sc;  // NaN and out-of-box origins clamp to the box
+            return static_cast<uint32_t>(fminf(fmaxf(c, 0.0f), 511.0f));
+        };
+        const uint32_t m = spread3(cell(a.x, lo.x, scale.x)) << 2 | spread3(cell(a.y, lo.y, scale.y)) << 1 |
+                           spread3(cell(a.z, lo.z, scale.z));
+        keys[i] = (oct << 27) | m;
+        idx[i] = i;
+    }
 }
 
 __global__ void __launch_bounds__(kTraceBlock) k_trace_any(DeviceScene s, const float4* __restrict__ rays, uint32_t n,
@@ -356,7 +417,59 @@ cudaError_t launch_trace_persist(const DeviceScene& s, const rbr_ray* rays, uint
     return cudaGetLastError();
 }
 
+// Sorts the rays by (direction octant, origin cell) on `stream` and returns the permutation.
+static cudaError_t sort_rays(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, const uint32_t** perm, cudaStream_t stream) {
+    size_t temp = 0;
+    cudaError_t e = cub::DeviceRadixSort::SortPairs(nullptr, temp, static_cast<const uint32_t*>(nullptr),
+                                                    static_cast<uint32_t*>(nullptr), static_cast<const uint32_t*>(nullptr),
+                                                    static_cast<uint32_t*>(nullptr), static_cast<int>(n), 0, 30, stream);
+    if (e != cudaSuccess) return e;
+    if (ensure(ctx, ctx->sort_buf, size_t(n) * 16 + temp + 256, "ray sort") != RBR_OK) return cudaErrorMemoryAllocation;
+    uint32_t* base = static_cast<uint32_t*>(ctx->sort_buf.ptr);
+    uint32_t *keys = base, *keys2 = base + n, *idx = base + 2 * size_t(n), *idx2 = base + 3 * size_t(n);
+    void* tmp = reinterpret_cast<char*>(base + 4 * size_t(n)) + (256 - (reinterpret_cast<uintptr_t>(base + 4 * size_t(n)) & 255));
+    float3 lo = make_float3(0.0f, 0.0f, 0.0f), sc = make_float3(0.0f, 0.0f, 0.0f);
+    const float* blo = ctx->bounds_lo;
+    const float* bhi = ctx->bounds_hi;
+    float* so[3] = {&sc.x, &sc.y, &sc.z};
+    float* lo3[3] = {&lo.x, &lo.y, &lo.z};
+    for (int a = 0; a < 3; ++a) {
+        const float ext = bhi[a] - blo[a];
+        if (std::isfinite(blo[a]) && std::isfinite(ext) && ext > 0.0f) {
+            *lo3[a] = blo[a];
+            *so[a] = 512.0f / ext;
+        }
+    }
+    const int grid = std::min<int>((n + 255) / 256, ctx->num_sms * 8);
+    k_ray_keys<<<grid, 256, 0, stream>>>(reinterpret_cast<const float4*>(rays), n, lo, sc, keys, idx);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    e = cub::DeviceRadixSort::SortPairs(tmp, temp, keys, keys2, idx, idx2, static_cast<int>(n), 0, 30, stream);
+    *perm = idx2;
+    return e;
+}
+
 cudaError_t launch_trace(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any_hit, void* out, cudaStream_t stream) {
+    if (ctx->trace_kernel == 0 && ctx->trace_order == 1 && n > 0) {
+        const uint32_t* perm = nullptr;
+        cudaError_t e = sort_rays(ctx, rays, n, &perm, stream);
+        if (e != cudaSuccess) return e;
+        const uint32_t blocks = (n + kTraceBlock - 1) / kTraceBlock;
+        const auto* r = reinterpret_cast<const float4*>(rays);
+        if (any_hit) {
+            k_trace_any_perm<<<blocks, kTraceBlock, 0, stream>>>(ctx->scene, r, n, perm, static_cast<uint8_t*>(out),
+                                                                ctx->d_error);
+        } else {
+            auto* h = static_cast<uint2*>(out);
+            if (ctx->trace_min_blocks >= 12)
+                k_trace_closest_perm<12><<<blocks, kTraceBlock, 0, stream>>>(ctx->scene, r, n, perm, h, ctx->d_error);
+            else if (ctx->trace_min_blocks >= 10)
+                k_trace_closest_perm<10><<<blocks, kTraceBlock, 0, stream>>>(ctx->scene, r, n, perm, h, ctx->d_error);
+            else
+                k_trace_closest_perm<8><<<blocks, kTraceBlock, 0, stream>>>(ctx->scene, r, n, perm, h, ctx->d_error);
+        }
+        return cudaGetLastError();
+    }
     if (ctx->trace_kernel == 0) {
         return any_hit ? launch_trace_any(ctx->scene, rays, n, static_cast<uint8_t*>(out), ctx->d_error, ctx->trace_min_blocks,
                                           stream)
@@ -378,12 +491,13 @@ cudaError_t launch_trace(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any_
 // Times every traversal variant on the caller's rays (device pointer) and keeps the fastest.
 rbr_status autotune_trace(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any_hit, int64_t* chosen_ms_x1000) {
     struct Cand {
-        int kernel, min_blocks, per_sm;
+        int kernel, min_blocks, per_sm, order;
     };
-    const Cand cands[] = {{0, 8, 0}, {0, 10, 0}, {0, 12, 0}, {1, 10, 0}, {2, 10, 0}};
+    const Cand cands[] = {{0, 8, 0, 0}, {0, 10, 0, 0}, {0, 12, 0, 0}, {1, 10, 0, 0}, {2, 10, 0, 0},
+                          {0, 8, 0, 1}, {0, 10, 0, 1}, {0, 12, 0, 1}};
     rbr_status st = ensure(ctx, ctx->stage_out, size_t(n) * (any_hit ? 1 : sizeof(rbr_hit)), "autotune output");
     if (st != RBR_OK) return st;
-    const Cand saved{ctx->trace_kernel, ctx->trace_min_blocks, ctx->trace_blocks_per_sm};
+    const Cand saved{ctx->trace_kernel, ctx->trace_min_blocks, ctx->trace_blocks_per_sm, ctx->trace_order};
     float best_ms = 1e30f;
     Cand best = saved;
     cudaEvent_t a, b;
@@ -393,6 +507,7 @@ rbr_status autotune_trace(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any
         ctx->trace_kernel = c.kernel;
         ctx->trace_min_blocks = c.min_blocks;
         ctx->trace_blocks_per_sm = c.per_sm;
+        ctx->trace_order = c.order;
         cudaError_t e = launch_trace(ctx, rays, n, any_hit, ctx->stage_out.ptr, ctx->stream);  // warm-up
         float ms = 0.0f, total = 0.0f;
         for (int k = 0; k < 3 && e == cudaSuccess; ++k) {
@@ -409,6 +524,7 @@ rbr_status autotune_trace(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any
             ctx->trace_kernel = saved.kernel;
             ctx->trace_min_blocks = saved.min_blocks;
             ctx->trace_blocks_per_sm = saved.per_sm;
+            ctx->trace_order = saved.order;
             return cuda_fail(ctx, e, "autotune launch");
         }
         if (total < best_ms) {
@@ -421,6 +537,7 @@ rbr_status autotune_trace(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any
     ctx->trace_kernel = best.kernel;
     ctx->trace_min_blocks = best.min_blocks;
     ctx->trace_blocks_per_sm = best.per_sm;
+    ctx->trace_order = best.order;
     if (chosen_ms_x1000) *chosen_ms_x1000 = static_cast<int64_t>(best_ms / 3.0f * 1000.0f);
     return check_device_error(ctx, ctx->stream);
 }

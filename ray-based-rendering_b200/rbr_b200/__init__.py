@@ -221,7 +221,7 @@ class Context:
         us = C.c_int64()
         self._check(self.lib.rbr_autotune_trace(self.h, C.c_void_p(rays_ptr), n, int(any_hit), C.byref(us)))
         return {"trace.kernel": self.get_param("trace.kernel"), "trace.min_blocks": self.get_param("trace.min_blocks"),
-                "us_per_launch": us.value}
+                "trace.order": self.get_param("trace.order"), "us_per_launch": us.value}
 
     def last_error(self) -> str:
         return self.lib.rbr_last_error(self.h).decode()

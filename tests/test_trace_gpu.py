@@ -28,15 +28,19 @@ def assert_same_closest(got, want):
 
 
 WORLDS = [(30, 30, False, 1), (400, 1500, False, 2), (60, 200, True, 3)]
-KERNELS = [0, 1, 2]  # trace.kernel: one thread per ray, persistent lane refill, warp-cooperative
+# (trace.kernel, trace.order): one thread per ray, persistent lane refill, warp-cooperative,
+# and one thread per ray on rays sorted by direction octant and origin cell
+KERNELS = [(0, 0), (1, 0), (2, 0), (0, 1)]
 
 
-@pytest.fixture(params=KERNELS, ids=[f"kernel{k}" for k in KERNELS])
+@pytest.fixture(params=KERNELS, ids=["kernel0", "kernel1", "kernel2", "kernel0-sorted"])
 def kctx(ctx, request):
-    """The shared context with trace.kernel set to each variant in turn."""
-    ctx.set_param("trace.kernel", request.param)
+    """The shared context with each traversal variant in turn."""
+    ctx.set_param("trace.kernel", request.param[0])
+    ctx.set_param("trace.order", request.param[1])
     yield ctx
     ctx.set_param("trace.kernel", 0)
+    ctx.set_param("trace.order", 0)
 
 
 @pytest.mark.parametrize("ns,nt,plane,seed", WORLDS)
