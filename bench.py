@@ -667,7 +667,7 @@ def main():
                          "avg_launch_ms": avg_launch_s * 1e3},
             "cpu_baseline": base,
             "clocks": clk,
-            "gpu_launches": args.steps,
+            "gpu_launches": args.steps * (2 if tuned.get("trace.order") else 1),
             "tuning": tuned,
             "bvh": {"wide_nodes": stats.num_wide_nodes, "leaf_records": stats.num_leaf_records,
                     "depth": stats.max_depth, "build_s": stats.build_seconds,
