@@ -471,6 +471,10 @@ rbr_status rbr_phase_sample_host(rbr_ctx* ctx, float g, uint32_t n, const float*
  * out: 5 floats each: t (0 without scattering), weight[3], scattered (0/1). */
 rbr_status rbr_medium_sample_host(rbr_ctx* ctx, const rbr_medium* medium, uint32_t n, const float* max_dist,
                                   const float* u, float* out);
+/* Measurement (no reference counterpart): read bandwidth of an L2-resident buffer of `bytes`
+ * (4 KiB..1 GiB), read `passes` times per launch (1..1000) with L2-only loads; the best of 5
+ * launches in GB/s. The denominator of the traversal kernels' L2 roofline. */
+rbr_status rbr_l2_read_bandwidth(rbr_ctx* ctx, uint64_t bytes, uint32_t passes, double* gb_per_s);
 
 /* ------------------------------------------------------------------------------------------
  * Meshes and film export.

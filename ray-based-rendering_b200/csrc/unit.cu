@@ -110,6 +110,22 @@ __global__ void k_mis(uint32_t n, const float* pdfs, float* out) {
     out[i] = power_heuristic(pdfs[2 * i], pdfs[2 * i + 1]);
 }
 
+// Reads `n4` 16-byte words `passes` times through L2 (ld.global.cg: no L1 allocation). The
+// XOR of everything read is stored only if it equals a constant, which keeps the loads alive.
+__global__ void __launch_bounds__(256) k_l2_read(const uint4* __restrict__ buf, size_t n4, uint32_t passes,
+                                                 uint32_t* sink) {
+    uint32_t acc = 0;
+    const size_t stride = size_t(gridDim.x) * blockDim.x;
+    for (uint32_t p = 0; p < passes; ++p) {
+#pragma unroll 4
+        for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n4; i += stride) {
+            const uint4 v = __ldcg(buf + i);
+            acc ^= v.x ^ v.y ^ v.z ^ v.w;
+        }
+    }
+    if (acc == 0x9E3779B9u) sink[0] = acc;
+}
+
 // Runs `launch` with `in` copied to the device and `out_floats` floats copied back.
 template <class F>
 rbr_status run_unit(rbr_ctx* ctx, const std::vector<std::pair<const float*, size_t>>& ins, size_t out_floats,
@@ -290,6 +306,41 @@ rbr_status rbr_medium_sample_host(rbr_ctx* ctx, const rbr_medium* medium, uint32
                     [&](const std::vector<const float*>& d, float* o) {
                         k_medium_sample<<<blocks(n), kUnitBlock, 0, ctx->stream>>>(s, n, d[0], d[1], o);
                     });
+}
+
+rbr_status rbr_l2_read_bandwidth(rbr_ctx* ctx, uint64_t bytes, uint32_t passes, double* gb_per_s) {
+    if (!ctx || !gb_per_s || bytes < 4096 || bytes > (uint64_t(1) << 30) || passes == 0 || passes > 1000)
+        return RBR_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(ctx->device);
+    const size_t n4 = bytes / 16;
+    rbr_status st = ensure(ctx, ctx->stage_in, n4 * 16 + 16, "L2 bandwidth buffer");
+    if (st != RBR_OK) return st;
+    auto* buf = static_cast<uint4*>(ctx->stage_in.ptr);
+    auto* sink = reinterpret_cast<uint32_t*>(buf + n4);
+    cudaError_t e = cudaMemsetAsync(buf, 0x5A, n4 * 16 + 16, ctx->stream);
+    const int grid = ctx->num_sms * 8;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    float best = 1e30f;
+    if (e == cudaSuccess) {
+        k_l2_read<<<grid, 256, 0, ctx->stream>>>(buf, n4, 2, sink);  // brings the buffer into L2
+        e = cudaGetLastError();
+    }
+    for (int k = 0; k < 5 && e == cudaSuccess; ++k) {
+        cudaEventRecord(a, ctx->stream);
+        k_l2_read<<<grid, 256, 0, ctx->stream>>>(buf, n4, passes, sink);
+        cudaEventRecord(b, ctx->stream);
+        e = cudaEventSynchronize(b);
+        float ms = 0.0f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+        if (e == cudaSuccess && ms > 0.0f && ms < best) best = ms;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "L2 bandwidth kernel");
+    *gb_per_s = double(n4) * 16.0 * passes / (double(best) * 1e-3) / 1e9;
+    return RBR_OK;
 }
 
 }  // extern "C"

@@ -68,6 +68,7 @@ def load_library() -> C.CDLL:
         "rbr_phase_eval_host": (C.c_int, [P, C.c_float, C.c_uint32, P, P, P]),
         "rbr_phase_sample_host": (C.c_int, [P, C.c_float, C.c_uint32, P, P, P]),
         "rbr_medium_sample_host": (C.c_int, [P, C.POINTER(abi.rbr_medium), C.c_uint32, P, P, P]),
+        "rbr_l2_read_bandwidth": (C.c_int, [P, C.c_uint64, C.c_uint32, C.POINTER(C.c_double)]),
         "rbr_param_set": (C.c_int, [P, C.c_char_p, C.c_int64]),
         "rbr_param_get": (C.c_int, [P, C.c_char_p, C.POINTER(C.c_int64)]),
         "rbr_autotune_trace": (C.c_int, [P, P, C.c_uint32, C.c_int, C.POINTER(C.c_int64)]),
@@ -222,6 +223,12 @@ class Context:
         self._check(self.lib.rbr_autotune_trace(self.h, C.c_void_p(rays_ptr), n, int(any_hit), C.byref(us)))
         return {"trace.kernel": self.get_param("trace.kernel"), "trace.min_blocks": self.get_param("trace.min_blocks"),
                 "trace.order": self.get_param("trace.order"), "us_per_launch": us.value}
+
+    def l2_read_bandwidth(self, nbytes: int = 32 << 20, passes: int = 50) -> float:
+        """Read bandwidth (GB/s) of an L2-resident buffer: the traversal roofline's denominator."""
+        v = C.c_double()
+        self._check(self.lib.rbr_l2_read_bandwidth(self.h, nbytes, passes, C.byref(v)))
+        return v.value
 
     def last_error(self) -> str:
         return self.lib.rbr_last_error(self.h).decode()

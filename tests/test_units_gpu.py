@@ -87,3 +87,14 @@ def test_mis_weights_bit_exact(ctx, reference):
     got = ctx.mis_weights(pairs)
     want = np.array([reference.power_heuristic(1, float(a), 1, float(b)) for a, b in pairs], np.float32)
     assert np.array_equal(bits(got), bits(want))
+
+
+def test_l2_read_bandwidth(ctx):
+    """The L2 roofline's denominator: a 32 MiB buffer read from L2 is faster than any HBM copy
+    (B200: about 6.5 TB/s), and sizes outside 4 KiB..1 GiB are refused."""
+    from rbr_b200 import RbrError
+
+    bw = ctx.l2_read_bandwidth(32 << 20, 20)
+    assert 7000.0 < bw < 100000.0, bw
+    with pytest.raises(RbrError):
+        ctx.l2_read_bandwidth(1024, 20)
