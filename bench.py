@@ -262,6 +262,9 @@ def run_render(args, rank, world, local_rank):
     W, H = cam.width, cam.height
     ctx = Context(local_rank)
     ctx.upload(scene)
+    for kv in args.param:
+        k, v = kv.split("=")
+        ctx.set_param(k, int(v))
     film = torch.empty(W * H * 3, dtype=torch.float32, device=f"cuda:{local_rank}")
     stream = torch.cuda.current_stream()
     paths = W * H * cfg["spp"]

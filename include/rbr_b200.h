@@ -235,7 +235,10 @@ rbr_status rbr_scene_stats_get(const rbr_ctx* ctx, rbr_scene_stats* out);
  *   "trace.order"          kernel 0: 0 traces the rays in the order given; 1 first sorts them
  *                          by direction octant and origin cell (a radix sort on the device) so
  *                          that warps hold rays that walk the same nodes
- *   "pt.wave_paths"        camera samples per path-tracer wave (default 2^22)
+ *   "pt.wave_paths"        camera samples per path-tracer wave (default 2^23)
+ *   "pt.streams"           rbr_render: waves in flight, 1 or 2 (default 2: waves alternate
+ *                          between two sets of path buffers on two streams; an image that
+ *                          fits one wave is rendered as two half-image waves)
  * Results do not depend on them; only speed and memory do. rbr_autotune picks them. */
 rbr_status rbr_param_set(rbr_ctx* ctx, const char* name, int64_t value);
 rbr_status rbr_param_get(const rbr_ctx* ctx, const char* name, int64_t* value);

@@ -134,6 +134,9 @@ void rbr_ctx_destroy(rbr_ctx* ctx) {
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
     if (ctx->ev_stop) cudaEventDestroy(ctx->ev_stop);
+    if (ctx->side_stream) cudaStreamDestroy(ctx->side_stream);
+    if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+    if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
     delete ctx;
 }
 
@@ -161,6 +164,9 @@ rbr_status rbr_param_set(rbr_ctx* ctx, const char* name, int64_t value) {
     } else if (n == "trace.min_blocks") {
         if (value != 8 && value != 10 && value != 12) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "trace.min_blocks is 8, 10 or 12");
         ctx->trace_min_blocks = static_cast<int>(value);
+    } else if (n == "pt.streams") {
+        if (value != 1 && value != 2) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "pt.streams is 1 or 2");
+        ctx->pt_streams = static_cast<int>(value);
     } else if (n == "pt.wave_paths") {
         if (value < 1024 || value > (int64_t(1) << 26)) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "pt.wave_paths is 1024..2^26");
         ctx->pt_wave_paths = static_cast<uint32_t>(value);
@@ -186,6 +192,7 @@ rbr_status rbr_param_get(const rbr_ctx* ctx, const char* name, int64_t* value) {
     else if (n == "trace.min_blocks") *value = ctx->trace_min_blocks;
     else if (n == "trace.order") *value = ctx->trace_order;
     else if (n == "pt.wave_paths") *value = ctx->pt_wave_paths;
+    else if (n == "pt.streams") *value = ctx->pt_streams;
     else return RBR_ERR_INVALID_ARGUMENT;
     return RBR_OK;
 }

@@ -376,8 +376,12 @@ __device__ __forceinline__ bool train_path(const Wave& w, uint64_t seed, uint32_
 // Surface vertices, per material-class queue. kMode 0: PathTracingIntegrator::Li; 1: the same
 // with the radiance cache; 2: the surface part of VolumetricPathIntegrator::Li
 // (volumetric_path_integrator.cpp:45-88: emission at every hit, NEE without MIS weights).
+// Register budget for 8 resident blocks per SM (64 registers, a few spills): the kernel is
+// latency-bound on its division and square-root chains, and twice the warps of its natural
+// 124-register allocation hide more of it (GGX scene +5 %, Cornell box +3 %; 5, 6, 10 and 12
+// blocks were measured slower).
 template <int kMode, bool kPacked>
-__global__ void __launch_bounds__(kBlock) k_shade(DeviceScene s, Wave w, Paths P, uint32_t d) {
+__global__ void __launch_bounds__(kBlock, 8) k_shade(DeviceScene s, Wave w, Paths P, uint32_t d) {
     constexpr bool kCache = kMode == 1, kVolSurface = kMode == 2;
     uint32_t cnt[kNumClasses + 1];
     cnt[0] = 0;
@@ -606,17 +610,20 @@ __global__ void __launch_bounds__(kBlock) k_film_packed(Paths P) {
 
 rbr_status read_render_counters(rbr_ctx* ctx) {
     if (!ctx->pt.counters.ptr) return RBR_OK;
-    unsigned long long h[2] = {0, 0};
-    const cudaError_t e = cudaMemcpy(h, static_cast<uint32_t*>(ctx->pt.counters.ptr) + kCExt, 16,
-                                     cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "reading the render counters");
-    ctx->last_render.extension_rays = h[0];
-    ctx->last_render.shadow_rays = h[1];
+    ctx->last_render.extension_rays = 0;
+    ctx->last_render.shadow_rays = 0;
+    for (int b = 0; b < (ctx->pt_last_two ? 2 : 1); ++b) {
+        const PathBuffers& pb = b ? ctx->pt2 : ctx->pt;
+        unsigned long long h[2] = {0, 0};
+        const cudaError_t e = cudaMemcpy(h, static_cast<uint32_t*>(pb.counters.ptr) + kCExt, 16, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "reading the render counters");
+        ctx->last_render.extension_rays += h[0];
+        ctx->last_render.shadow_rays += h[1];
+    }
     return RBR_OK;
 }
 
-void free_path_buffers(rbr_ctx* ctx) {
-    PathBuffers& p = ctx->pt;
+static void free_paths(PathBuffers& p) {
     release(p.ray);
     release(p.thr);
     release(p.rad);
@@ -626,15 +633,22 @@ void free_path_buffers(rbr_ctx* ctx) {
     release(p.classq);
     release(p.shadow);
     release(p.counters);
-    release(ctx->pt_seg_of);
     p.capacity = 0;
     p.shadow_capacity = 0;
 }
 
-static rbr_status ensure_paths(rbr_ctx* ctx, uint32_t cap, uint32_t shadow_cap) {
-    PathBuffers& p = ctx->pt;
+void free_path_buffers(rbr_ctx* ctx) {
+    free_paths(ctx->pt);
+    free_paths(ctx->pt2);
+    release(ctx->pt_seg_of);
+    ctx->pt_last_two = false;
+}
+
+static rbr_status ensure_paths(rbr_ctx* ctx, uint32_t cap, uint32_t shadow_cap, PathBuffers* which = nullptr) {
+    PathBuffers& p = which ? *which : ctx->pt;
     if (p.capacity >= cap && p.shadow_capacity >= shadow_cap && p.counters.ptr) return RBR_OK;
-    free_path_buffers(ctx);
+    free_paths(p);
+    if (&p == &ctx->pt) release(ctx->pt_seg_of);
     rbr_status st;
     if ((st = ensure(ctx, p.ray, size_t(cap) * 32, "path rays")) != RBR_OK ||
         (st = ensure(ctx, p.thr, size_t(cap) * 16, "path throughput")) != RBR_OK ||
@@ -645,7 +659,7 @@ static rbr_status ensure_paths(rbr_ctx* ctx, uint32_t cap, uint32_t shadow_cap) 
         (st = ensure(ctx, p.classq, size_t(cap) * 4 * kNumClasses, "class queues")) != RBR_OK ||
         (st = ensure(ctx, p.shadow, size_t(std::max(1u, shadow_cap)) * 48, "shadow queue")) != RBR_OK ||
         (st = ensure(ctx, p.counters, kCWords * 4, "queue counters")) != RBR_OK) {
-        free_path_buffers(ctx);
+        free_paths(p);
         return st;
     }
     p.capacity = cap;
@@ -673,22 +687,40 @@ rbr_status render(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_params* 
     uint32_t cap = static_cast<uint32_t>(std::min<uint64_t>(npix * spp, std::max(ctx->pt_wave_paths, spp)));
     cap = std::min<uint64_t>(cap, kShadowBytesLimit / (48ull * nl));
     cap = std::max(spp, cap / spp * spp);
+    // Two waves in flight (a second path-buffer set on a second stream): the latency-bound
+    // launches at the end of one wave's bounces, which occupy few SMs, run beside the full
+    // launches of the next wave. An image that fits one wave is split into two halves.
+    const bool two = ctx->pt_streams == 2 && npix >= 2;
+    if (two && npix * spp <= cap) cap = static_cast<uint32_t>((npix + 1) / 2) * spp;
     rbr_status st = ensure_paths(ctx, cap, cap * nl);
     if (st != RBR_OK) return st;
-
-    PathBuffers& pb = ctx->pt;
-    Paths P;
-    P.ray = static_cast<float4*>(pb.ray.ptr);
-    P.thr = static_cast<float4*>(pb.thr.ptr);
-    P.rad = static_cast<float4*>(pb.rad.ptr);
-    P.hit = static_cast<uint2*>(pb.hit.ptr);
-    P.q0 = static_cast<uint32_t*>(pb.queue[0].ptr);
-    P.q1 = static_cast<uint32_t*>(pb.queue[1].ptr);
-    P.classq = static_cast<uint32_t*>(pb.classq.ptr);
-    P.shadow = static_cast<float4*>(pb.shadow.ptr);
-    P.counters = static_cast<uint32_t*>(pb.counters.ptr);
-    P.cap = pb.capacity;
-    P.shadow_cap = pb.shadow_capacity;
+    if (two) {
+        st = ensure_paths(ctx, cap, cap * nl, &ctx->pt2);
+        if (st != RBR_OK) return st;
+        cudaError_t ce = cudaSuccess;
+        if (!ctx->side_stream) ce = cudaStreamCreateWithFlags(&ctx->side_stream, cudaStreamNonBlocking);
+        if (ce == cudaSuccess && !ctx->ev_fork) ce = cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming);
+        if (ce == cudaSuccess && !ctx->ev_join) ce = cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming);
+        if (ce != cudaSuccess) return cuda_fail(ctx, ce, "second path-tracer stream");
+    }
+    ctx->pt_last_two = two;
+    Paths PP[2];
+    for (int b = 0; b < (two ? 2 : 1); ++b) {
+        PathBuffers& pb = b ? ctx->pt2 : ctx->pt;
+        Paths& P = PP[b];
+        P.ray = static_cast<float4*>(pb.ray.ptr);
+        P.thr = static_cast<float4*>(pb.thr.ptr);
+        P.rad = static_cast<float4*>(pb.rad.ptr);
+        P.hit = static_cast<uint2*>(pb.hit.ptr);
+        P.q0 = static_cast<uint32_t*>(pb.queue[0].ptr);
+        P.q1 = static_cast<uint32_t*>(pb.queue[1].ptr);
+        P.classq = static_cast<uint32_t*>(pb.classq.ptr);
+        P.shadow = static_cast<float4*>(pb.shadow.ptr);
+        P.counters = static_cast<uint32_t*>(pb.counters.ptr);
+        P.cap = pb.capacity;
+        P.shadow_cap = pb.shadow_capacity;
+    }
+    const cudaStream_t streams[2] = {stream, two ? ctx->side_stream : stream};
 
     CameraDev cd;
     cd.width = cam->width;
@@ -710,9 +742,14 @@ rbr_status render(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_params* 
     const int grid = ctx->num_sms * 8;
     const uint32_t pix_per_wave = cap / spp;
     uint32_t launches = 0, waves = 0;
-    cudaError_t e = cudaMemsetAsync(P.counters, 0, kCWords * 4, stream);
+    cudaError_t e = cudaMemsetAsync(PP[0].counters, 0, kCWords * 4, stream);
+    if (e == cudaSuccess && two) e = cudaMemsetAsync(PP[1].counters, 0, kCWords * 4, stream);
     if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_start, stream);
+    if (e == cudaSuccess && two) e = cudaEventRecord(ctx->ev_fork, stream);
+    if (e == cudaSuccess && two) e = cudaStreamWaitEvent(ctx->side_stream, ctx->ev_fork, 0);
     for (uint64_t p0 = 0; p0 < npix && e == cudaSuccess; p0 += pix_per_wave) {
+        const Paths& P = PP[waves & (two ? 1u : 0u)];
+        const cudaStream_t ws = streams[waves & 1u];
         Wave w;
         w.p0 = static_cast<uint32_t>(p0);
         w.npaths = static_cast<uint32_t>(std::min<uint64_t>(pix_per_wave, npix - p0)) * spp;
@@ -723,25 +760,27 @@ rbr_status render(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_params* 
         w.use_nee = p->use_nee != 0;
         w.use_mis = p->use_mis != 0;
         w.seed = p->seed;
-        k_raygen<false><<<grid, kBlock, 0, stream>>>(cd, w, P);
+        k_raygen<false><<<grid, kBlock, 0, ws>>>(cd, w, P);
         ++launches;
         for (uint32_t d = 0; d < w.max_depth; ++d) {
-            k_begin<<<1, 1, 0, stream>>>(P, d);
+            k_begin<<<1, 1, 0, ws>>>(P, d);
             if (volumetric) {
-                k_extend<true, false><<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d, ctx->d_error);
-                k_shade<2, false><<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d);
+                k_extend<true, false><<<grid, kBlock, 0, ws>>>(ctx->scene, w, P, d, ctx->d_error);
+                k_shade<2, false><<<grid, kBlock, 0, ws>>>(ctx->scene, w, P, d);
             } else {
-                k_extend<false, false><<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d, ctx->d_error);
-                k_shade<0, false><<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d);
+                k_extend<false, false><<<grid, kBlock, 0, ws>>>(ctx->scene, w, P, d, ctx->d_error);
+                k_shade<0, false><<<grid, kBlock, 0, ws>>>(ctx->scene, w, P, d);
             }
-            k_shadow<<<grid, kBlock, 0, stream>>>(ctx->scene, P, ctx->d_error);
+            k_shadow<<<grid, kBlock, 0, ws>>>(ctx->scene, P, ctx->d_error);
             launches += 4;
         }
-        k_film<<<grid, kBlock, 0, stream>>>(w, P, film_mean, film_m2);
+        k_film<<<grid, kBlock, 0, ws>>>(w, P, film_mean, film_m2);  // the wave's own pixels
         ++launches;
         ++waves;
         e = cudaGetLastError();
     }
+    if (e == cudaSuccess && two) e = cudaEventRecord(ctx->ev_join, ctx->side_stream);
+    if (e == cudaSuccess && two) e = cudaStreamWaitEvent(stream, ctx->ev_join, 0);
     if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_stop, stream);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "path tracer launch");
     ctx->last_render.paths = npix * spp;
@@ -903,6 +942,7 @@ rbr_status render_cached(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_p
     ctx->last_render.shadow_rays = 0;
     ctx->last_render.waves = waves;
     ctx->last_render.launches = launches;
+    ctx->pt_last_two = false;
     ctx->render_pending = true;
     return RBR_OK;
 }

@@ -60,9 +60,14 @@ struct rbr_ctx {
     int trace_min_blocks = 10;     // kernel 0: register budget for 8, 10 or 12 resident blocks per SM
     int trace_order = 0;           // kernel 0: 0 rays in the given order, 1 sorted by direction octant and origin
     rbr::DevBuf sort_buf;          // keys, permutation and radix-sort scratch of trace_order 1
-    uint32_t pt_wave_paths = 1u << 22;
+    uint32_t pt_wave_paths = 1u << 23;
     // path tracer
     rbr::PathBuffers pt;
+    rbr::PathBuffers pt2;                  // second wave in flight (rbr_render, pt_streams 2)
+    int pt_streams = 2;                    // waves in flight in rbr_render: 1 or 2
+    bool pt_last_two = false;              // the last rbr_render used pt2
+    cudaStream_t side_stream = nullptr;    // stream of the second wave
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     rbr::DevBuf pt_seg_of;  // packed waves: segment of each path
     rbr_render_stats last_render{};
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;

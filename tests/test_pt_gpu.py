@@ -63,7 +63,7 @@ def test_second_moment_and_stats(ctx, restatement):
     close = np.isclose(m2, sq, rtol=2e-3, atol=1e-3).all(-1).mean()
     assert close > 0.97
     st = ctx.render_stats()
-    assert st.paths == 32 * 32 * 8 and st.waves == 1
+    assert st.paths == 32 * 32 * 8 and st.waves == 2  # a one-wave image runs as two halves in flight
     assert st.extension_rays >= st.paths and st.shadow_rays > 0 and st.milliseconds > 0
 
 
@@ -77,6 +77,32 @@ def test_waves_do_not_change_results(ctx):
     a = ctx.render_host(s.camera, render_params(spp=2, seed=11, sample_offset=0))
     b = ctx.render_host(s.camera, render_params(spp=2, seed=11, sample_offset=2))
     assert np.allclose(full, 0.5 * (a + b), rtol=1e-5, atol=1e-5)
+
+
+def test_two_waves_in_flight_match_one(ctx):
+    """pt.streams 2 (waves alternate between two path-buffer sets and two streams) renders the
+    same film and counts the same rays as one wave at a time, up to summation order; a small
+    wave size makes four waves, so both buffer sets are reused."""
+    s = scenes.cornell_box(256, 256)
+    ctx.upload(s)
+    wave_paths = ctx.get_param("pt.wave_paths")
+    ctx.set_param("pt.wave_paths", 65536)
+    try:
+        p = render_params(spp=4, seed=21)
+        ctx.set_param("pt.streams", 1)
+        one = ctx.render_host(s.camera, p)
+        st1 = ctx.render_stats()
+        ctx.set_param("pt.streams", 2)
+        two = ctx.render_host(s.camera, p)
+        st2 = ctx.render_stats()
+    finally:
+        ctx.set_param("pt.streams", 2)
+        ctx.set_param("pt.wave_paths", wave_paths)
+    assert st1.waves == st2.waves == 4
+    assert st1.extension_rays == st2.extension_rays and st1.shadow_rays == st2.shadow_rays
+    assert np.allclose(one, two, rtol=1e-5, atol=1e-5)
+    with pytest.raises(RbrError):
+        ctx.set_param("pt.streams", 3)
 
 
 def test_edge_parameters(ctx, restatement):
