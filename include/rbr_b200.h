@@ -415,6 +415,8 @@ typedef struct rbr_batch_config {
     uint32_t wave_paths;        /* paths per wave; 0: the budget decides (at most 2^22) */
     uint32_t blocks_per_sm;     /* grid of the wavefront kernels = this x SMs (default 8) */
     int32_t use_graphs;         /* replay each wave shape from a captured CUDA graph (default 1) */
+    uint32_t waves_in_flight;   /* 1, or 2 (default; 0 means 2): waves alternate between two
+                                   path-buffer sets and streams, each set within the budget */
 } rbr_batch_config;
 
 typedef struct rbr_request {

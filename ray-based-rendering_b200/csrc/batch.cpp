@@ -42,7 +42,7 @@ struct WavePlan {
     std::vector<SegDev> segs;
 };
 
-using GraphKey = std::tuple<uint32_t, int, uint32_t, int, bool, uint32_t>;  // scene, mode, depth, grid, train, capacity
+using GraphKey = std::tuple<uint32_t, int, uint32_t, int, bool, uint32_t, int>;  // scene, mode, depth, grid, train, capacity, slot
 
 }  // namespace
 
@@ -58,10 +58,13 @@ struct rbr_batch {
     void* d_table = nullptr;
     void* h_stage = nullptr;
     size_t h_stage_bytes = 0;
-    std::vector<cudaEvent_t> events;            // [0] run start, [w + 1] end of wave w
+    std::vector<cudaEvent_t> events;            // [0] run start, [w + 1] end of wave w, [waves + 1] run end
     uint32_t run_waves = 0;
+    int run_slots = 1;                           // waves in flight in the last run
+    cudaStream_t side = nullptr;                 // stream of the odd waves (two in flight)
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_cache = nullptr;
     std::map<GraphKey, cudaGraphExec_t> graphs;
-    const void* graph_buffers = nullptr;         // path buffers the graphs were captured with
+    uint32_t graph_generation = 0;               // path-buffer generation the graphs were captured with
     std::map<uint32_t, const void*> cache_buffers;  // per cached scene: its query buffer at capture
     rbr_batch_stats stats{};
     bool ran = false;
@@ -182,9 +185,17 @@ rbr_status ensure_events(rbr_batch* b, size_t n) {
 // Renders `reqs` (the queue is not modified). Fills the requests' wave bookkeeping.
 rbr_status run(rbr_batch* b, std::vector<Req>& reqs, cudaStream_t stream) {
     rbr_ctx* eng = b->eng;
-    if (b->ran && b->run_waves) {  // the staging buffer and events of the previous run are reused
-        const cudaError_t e = cudaEventSynchronize(b->events[b->run_waves]);
+    if (b->ran) {  // the staging buffer and events of the previous run are reused
+        const cudaError_t e = cudaEventSynchronize(b->events[b->run_waves + 1]);
         if (e != cudaSuccess) return bcuda(b, e, "waiting for the previous run");
+    }
+    const int slots = b->cfg.waves_in_flight == 1 ? 1 : 2;
+    if (slots == 2 && !b->side) {
+        cudaError_t e = cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_cache, cudaEventDisableTiming);
+        if (e != cudaSuccess) return bcuda(b, e, "second wave stream");
     }
     bool any_cache = false;
     for (const Req& q : reqs) any_cache = any_cache || q.r.use_cache;
@@ -194,7 +205,7 @@ rbr_status run(rbr_batch* b, std::vector<Req>& reqs, cudaStream_t stream) {
             return bfail(b, RBR_ERR_INVALID_ARGUMENT, "request " + std::to_string(q.id) + ": samples per pixel exceed the wave");
     std::vector<WavePlan> waves = plan(b, reqs, cap);
     const uint32_t nl = max_lights(b);
-    rbr_status st = ensure_wave_buffers(eng, cap, cap * nl);
+    rbr_status st = ensure_wave_buffers(eng, cap, cap * nl, slots);
     if (st != RBR_OK) return bfail(b, st, eng->error);
     for (const WavePlan& w : waves) {
         if (w.mode != 1) continue;
@@ -208,9 +219,9 @@ rbr_status run(rbr_batch* b, std::vector<Req>& reqs, cudaStream_t stream) {
         if (it != b->cache_buffers.end() && (it->second != qb)) drop_graphs(b);
         b->cache_buffers[w.scene] = qb;
     }
-    if (b->graph_buffers != eng->pt.ray.ptr || (!b->graphs.empty() && std::get<5>(b->graphs.begin()->first) != eng->pt.capacity)) {
+    if (b->graph_generation != eng->pt_generation) {  // path buffers reallocated since the capture
         drop_graphs(b);
-        b->graph_buffers = eng->pt.ray.ptr;
+        b->graph_generation = eng->pt_generation;
     }
     const size_t need = std::max<size_t>(1, waves.size()) * kTableBytes;
     if (b->h_stage_bytes < need) {
@@ -221,31 +232,46 @@ rbr_status run(rbr_batch* b, std::vector<Req>& reqs, cudaStream_t stream) {
         if (e != cudaSuccess) return bcuda(b, e, "pinned segment tables");
         b->h_stage_bytes = need;
     }
-    st = ensure_events(b, waves.size() + 1);
+    st = ensure_events(b, waves.size() + 2);
     if (st != RBR_OK) return st;
     const int grid = eng->num_sms * static_cast<int>(b->cfg.blocks_per_sm ? b->cfg.blocks_per_sm : 8);
     rbr_batch_stats s{};
     s.requests = static_cast<uint32_t>(reqs.size());
     s.wave_paths = cap;
     s.blocks_per_sm = b->cfg.blocks_per_sm ? b->cfg.blocks_per_sm : 8;
+    // Waves alternate between two path-buffer sets, segment tables and streams (slot = wave
+    // index & 1), so one wave's latency-bound last bounces run beside the next wave. Waves
+    // with the radiance cache share the scene's cache buffers and weights: each waits for the
+    // previous one.
     cudaError_t e = cudaEventRecord(b->events[0], stream);
+    if (e == cudaSuccess && slots == 2) e = cudaEventRecord(b->ev_fork, stream);
+    if (e == cudaSuccess && slots == 2) e = cudaStreamWaitEvent(b->side, b->ev_fork, 0);
+    bool cache_wave = false;
     for (size_t wi = 0; wi < waves.size() && e == cudaSuccess; ++wi) {
         const WavePlan& w = waves[wi];
         rbr_ctx* scn = b->scenes[w.scene];
+        const int slot = slots == 2 ? static_cast<int>(wi & 1) : 0;
+        const cudaStream_t ws = slot ? b->side : stream;
+        if (w.mode == 1 && cache_wave && slots == 2) {
+            e = cudaStreamWaitEvent(ws, b->ev_cache, 0);
+            if (e != cudaSuccess) break;
+        }
+        char* dtab = static_cast<char*>(b->d_table) + slot * kTableBytes;
         char* tab = static_cast<char*>(b->h_stage) + wi * kTableBytes;
         uint32_t hdr[2] = {w.paths, static_cast<uint32_t>(w.segs.size())};
         std::memcpy(tab, hdr, sizeof(hdr));
         std::memcpy(tab + kHdrBytes, w.segs.data(), w.segs.size() * sizeof(SegDev));
-        e = cudaMemcpyAsync(b->d_table, tab, kHdrBytes + w.segs.size() * sizeof(SegDev), cudaMemcpyHostToDevice, stream);
+        e = cudaMemcpyAsync(dtab, tab, kHdrBytes + w.segs.size() * sizeof(SegDev), cudaMemcpyHostToDevice, ws);
         if (e != cudaSuccess) break;
         PackedWave pw;
         pw.mode = w.mode;
         pw.max_depth = w.max_depth;
         pw.grid = grid;
-        pw.hdr = static_cast<const uint32_t*>(b->d_table);
-        pw.segs = reinterpret_cast<const SegDev*>(static_cast<char*>(b->d_table) + kHdrBytes);
+        pw.hdr = reinterpret_cast<const uint32_t*>(dtab);
+        pw.segs = reinterpret_cast<const SegDev*>(dtab + kHdrBytes);
         pw.capacity = eng->pt.capacity;
         pw.train = w.train;
+        pw.slot = slot;
         if (w.mode == 1) {
             const double frac = double(scn->cache.cfg.train_paths) / double(cap);
             pw.train_thresh = static_cast<uint32_t>(std::min(4294967295.0, frac * 4294967296.0));
@@ -255,7 +281,7 @@ rbr_status run(rbr_batch* b, std::vector<Req>& reqs, cudaStream_t stream) {
         s.segments += static_cast<uint32_t>(w.segs.size());
         s.paths += w.paths;
         if (b->cfg.use_graphs) {
-            const GraphKey key{w.scene, w.mode, w.max_depth, grid, w.train, eng->pt.capacity};
+            const GraphKey key{w.scene, w.mode, w.max_depth, grid, w.train, eng->pt.capacity, slot};
             auto it = b->graphs.find(key);
             if (it == b->graphs.end()) {
                 cudaGraph_t g = nullptr;
@@ -271,17 +297,25 @@ rbr_status run(rbr_batch* b, std::vector<Req>& reqs, cudaStream_t stream) {
                 it = b->graphs.emplace(key, exec).first;
                 ++s.graphs_captured;
             }
-            e = cudaGraphLaunch(it->second, stream);
+            e = cudaGraphLaunch(it->second, ws);
             ++s.graph_launches;
         } else {
-            e = launch_packed_wave(eng, scn, pw, stream);
+            e = launch_packed_wave(eng, scn, pw, ws);
         }
-        if (e == cudaSuccess) e = cudaEventRecord(b->events[wi + 1], stream);
+        if (e == cudaSuccess) e = cudaEventRecord(b->events[wi + 1], ws);
+        if (e == cudaSuccess && w.mode == 1 && slots == 2) {
+            e = cudaEventRecord(b->ev_cache, ws);
+            cache_wave = true;
+        }
     }
+    if (e == cudaSuccess && slots == 2) e = cudaEventRecord(b->ev_join, b->side);
+    if (e == cudaSuccess && slots == 2) e = cudaStreamWaitEvent(stream, b->ev_join, 0);
+    if (e == cudaSuccess) e = cudaEventRecord(b->events[waves.size() + 1], stream);
     if (e != cudaSuccess) return bcuda(b, e, "batched wave launch");
     s.waves = static_cast<uint32_t>(waves.size());
     b->stats = s;
     b->run_waves = s.waves;
+    b->run_slots = slots;
     b->ran = true;
     return RBR_OK;
 }
@@ -297,6 +331,7 @@ void rbr_batch_config_default(rbr_batch_config* out) {
     out->wave_paths = 0;
     out->blocks_per_sm = 8;
     out->use_graphs = 1;
+    out->waves_in_flight = 2;
 }
 
 rbr_status rbr_batch_create(rbr_ctx* ctx, const rbr_batch_config* config, rbr_batch** out) {
@@ -309,7 +344,7 @@ rbr_status rbr_batch_create(rbr_ctx* ctx, const rbr_batch_config* config, rbr_ba
     else rbr_batch_config_default(&b->cfg);
     if (b->cfg.path_memory_bytes == 0) b->cfg.path_memory_bytes = 1ull << 30;
     cudaSetDevice(ctx->device);
-    const cudaError_t e = cudaMalloc(&b->d_table, kTableBytes);
+    const cudaError_t e = cudaMalloc(&b->d_table, 2 * kTableBytes);  // a segment table per wave in flight
     if (e != cudaSuccess) {
         delete b;
         return RBR_ERR_OUT_OF_MEMORY;
@@ -324,6 +359,10 @@ void rbr_batch_destroy(rbr_batch* b) {
     cudaDeviceSynchronize();
     drop_graphs(b);
     for (cudaEvent_t e : b->events) cudaEventDestroy(e);
+    if (b->side) cudaStreamDestroy(b->side);
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+    if (b->ev_join) cudaEventDestroy(b->ev_join);
+    if (b->ev_cache) cudaEventDestroy(b->ev_cache);
     for (size_t i = b->scenes.size(); i-- > 0;) rbr_ctx_destroy(b->scenes[i]);  // variants before their bases
     if (b->d_table) cudaFree(b->d_table);
     if (b->h_stage) cudaFreeHost(b->h_stage);
@@ -417,12 +456,14 @@ rbr_status rbr_batch_request_stats(rbr_batch* b, uint32_t id, rbr_request_stats*
     if (it == b->done_index.end()) return bfail(b, RBR_ERR_INVALID_ARGUMENT, "request not in the last run");
     const Req& q = b->done[it->second];
     cudaSetDevice(b->eng->device);
-    cudaError_t e = cudaEventSynchronize(b->events[q.last_wave + 1]);
+    cudaError_t e = cudaEventSynchronize(b->events[b->run_waves + 1]);
+    // a wave starts when the previous wave of its stream has ended
+    const uint32_t prev = b->run_slots == 2 ? (q.first_wave >= 2 ? q.first_wave - 1 : 0) : q.first_wave;
     float t0 = 0.0f, t1 = 0.0f;
-    if (e == cudaSuccess) e = cudaEventElapsedTime(&t0, b->events[0], b->events[q.first_wave]);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&t0, b->events[0], b->events[prev]);
     if (e == cudaSuccess) e = cudaEventElapsedTime(&t1, b->events[0], b->events[q.last_wave + 1]);
     if (e != cudaSuccess) return bcuda(b, e, "request timing");
-    out->start_ms = q.first_wave == 0 ? 0.0f : t0;
+    out->start_ms = prev == 0 ? 0.0f : t0;
     out->latency_ms = t1;
     out->waves = q.waves;
     out->segments = q.segments;
@@ -434,9 +475,9 @@ rbr_status rbr_batch_stats_get(rbr_batch* b, rbr_batch_stats* out) {
     if (!b || !out) return RBR_ERR_INVALID_ARGUMENT;
     if (!b->ran) return bfail(b, RBR_ERR_INVALID_ARGUMENT, "no run yet");
     cudaSetDevice(b->eng->device);
-    cudaError_t e = cudaEventSynchronize(b->events[b->run_waves]);
+    cudaError_t e = cudaEventSynchronize(b->events[b->run_waves + 1]);
     float ms = 0.0f;
-    if (e == cudaSuccess && b->run_waves) e = cudaEventElapsedTime(&ms, b->events[0], b->events[b->run_waves]);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, b->events[0], b->events[b->run_waves + 1]);
     if (e != cudaSuccess) return bcuda(b, e, "batch timing");
     *out = b->stats;
     out->milliseconds = ms;
@@ -472,8 +513,8 @@ rbr_status rbr_batch_autotune(rbr_batch* b, void* stream) {
                     b->cfg = saved;
                     return st;
                 }
-                const cudaError_t e = cudaEventSynchronize(b->events[b->run_waves]);
-                if (e == cudaSuccess) cudaEventElapsedTime(&ms, b->events[0], b->events[b->run_waves]);
+                const cudaError_t e = cudaEventSynchronize(b->events[b->run_waves + 1]);
+                if (e == cudaSuccess) cudaEventElapsedTime(&ms, b->events[0], b->events[b->run_waves + 1]);
             }
             if (best < 0.0f || ms < best) {
                 best = ms;

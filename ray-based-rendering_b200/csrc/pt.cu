@@ -641,14 +641,16 @@ void free_path_buffers(rbr_ctx* ctx) {
     free_paths(ctx->pt);
     free_paths(ctx->pt2);
     release(ctx->pt_seg_of);
+    release(ctx->pt_seg_of2);
     ctx->pt_last_two = false;
+    ++ctx->pt_generation;
 }
 
 static rbr_status ensure_paths(rbr_ctx* ctx, uint32_t cap, uint32_t shadow_cap, PathBuffers* which = nullptr) {
     PathBuffers& p = which ? *which : ctx->pt;
     if (p.capacity >= cap && p.shadow_capacity >= shadow_cap && p.counters.ptr) return RBR_OK;
     free_paths(p);
-    if (&p == &ctx->pt) release(ctx->pt_seg_of);
+    ++ctx->pt_generation;
     rbr_status st;
     if ((st = ensure(ctx, p.ray, size_t(cap) * 32, "path rays")) != RBR_OK ||
         (st = ensure(ctx, p.thr, size_t(cap) * 16, "path throughput")) != RBR_OK ||
@@ -953,14 +955,22 @@ rbr_status render_cached(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_p
 // sequence of a wave depends only on (scene, mode, depth, grid) and is captured once as a
 // CUDA graph and replayed for every wave of that shape.
 // ------------------------------------------------------------------------------------------
-rbr_status ensure_wave_buffers(rbr_ctx* ctx, uint32_t cap, uint32_t shadow_cap) {
-    rbr_status st = ensure_paths(ctx, cap, shadow_cap);
-    if (st == RBR_OK) st = ensure(ctx, ctx->pt_seg_of, size_t(cap) * 4, "segment index per path");
-    return st;
+rbr_status ensure_wave_buffers(rbr_ctx* ctx, uint32_t cap, uint32_t shadow_cap, int slots) {
+    for (int k = 0; k < slots; ++k) {
+        DevBuf& seg = k ? ctx->pt_seg_of2 : ctx->pt_seg_of;
+        rbr_status st = ensure_paths(ctx, cap, shadow_cap, k ? &ctx->pt2 : &ctx->pt);
+        if (st != RBR_OK) return st;
+        if (seg.bytes < size_t(cap) * 4) {
+            ++ctx->pt_generation;
+            st = ensure(ctx, seg, size_t(cap) * 4, "segment index per path");
+            if (st != RBR_OK) return st;
+        }
+    }
+    return RBR_OK;
 }
 
 cudaError_t launch_packed_wave(rbr_ctx* eng, rbr_ctx* scn, const PackedWave& pw, cudaStream_t stream) {
-    PathBuffers& pb = eng->pt;
+    PathBuffers& pb = pw.slot ? eng->pt2 : eng->pt;
     Paths P;
     P.ray = static_cast<float4*>(pb.ray.ptr);
     P.thr = static_cast<float4*>(pb.thr.ptr);
@@ -974,7 +984,7 @@ cudaError_t launch_packed_wave(rbr_ctx* eng, rbr_ctx* scn, const PackedWave& pw,
     P.cap = pb.capacity;
     P.shadow_cap = pb.shadow_capacity;
     P.segs = pw.segs;
-    P.seg_of = static_cast<uint32_t*>(eng->pt_seg_of.ptr);
+    P.seg_of = static_cast<uint32_t*>((pw.slot ? eng->pt_seg_of2 : eng->pt_seg_of).ptr);
     P.wave_hdr = pw.hdr;
     Wave w{};
     if (pw.mode == 1) {

@@ -69,6 +69,8 @@ struct rbr_ctx {
     cudaStream_t side_stream = nullptr;    // stream of the second wave
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     rbr::DevBuf pt_seg_of;  // packed waves: segment of each path
+    rbr::DevBuf pt_seg_of2;  // the same for the second wave in flight (pt2)
+    uint32_t pt_generation = 0;  // incremented whenever a path buffer set or segment index is reallocated
     rbr_render_stats last_render{};
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
     bool render_pending = false;
@@ -146,8 +148,10 @@ struct PackedWave {
     bool train = false;           // mode 1: gather training vertices and train after the wave
     uint32_t train_thresh = 0;
     uint32_t train_steps = 0;
+    int slot = 0;                 // path buffers: 0 pt / pt_seg_of, 1 pt2 / pt_seg_of2
 };
-rbr_status ensure_wave_buffers(rbr_ctx* ctx, uint32_t cap, uint32_t shadow_cap);
+// Path buffers for packed waves: `slots` (1 or 2) sets of `cap` paths with their segment index.
+rbr_status ensure_wave_buffers(rbr_ctx* ctx, uint32_t cap, uint32_t shadow_cap, int slots = 1);
 cudaError_t launch_packed_wave(rbr_ctx* eng, rbr_ctx* scn, const PackedWave& pw, cudaStream_t stream);
 uint32_t packed_wave_launches(const PackedWave& pw);
 

@@ -198,6 +198,7 @@ class rbr_batch_config(C.Structure):
         ("wave_paths", C.c_uint32),
         ("blocks_per_sm", C.c_uint32),
         ("use_graphs", C.c_int32),
+        ("waves_in_flight", C.c_uint32),
     ]
 
 

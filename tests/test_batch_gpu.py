@@ -77,8 +77,9 @@ def batched(ctx, **cfg):
     return b, [f.cpu().numpy().reshape(h, w, 3) for f, (_, w, h, _) in zip(films, requests())], stats
 
 
-@pytest.mark.parametrize("cfg", [dict(), dict(use_graphs=0), dict(wave_paths=4096), dict(wave_paths=1000, blocks_per_sm=2)],
-                         ids=["graphs", "direct", "small-waves", "split-requests"])
+@pytest.mark.parametrize("cfg", [dict(), dict(use_graphs=0), dict(wave_paths=4096), dict(wave_paths=1000, blocks_per_sm=2),
+                                 dict(wave_paths=4096, waves_in_flight=1)],
+                         ids=["graphs", "direct", "small-waves", "split-requests", "one-wave-in-flight"])
 def test_packed_requests_equal_single_renders(bctx, cfg):
     b, films, stats = batched(bctx, **cfg)
     for (key, w, h, p), got in zip(requests(), films):
