@@ -537,7 +537,7 @@ def run_batch(args, rank, world, local_rank):
                                    "U{1..64}; 7 material/light variants of the GGX scene (shared geometry, depth 16) "
                                    "and the foggy Cornell box (volumetric, depth 8, every 8th request)",
                        "paths_per_run": total_paths,
-                       "l2": "path state of a wave (up to 4M paths x ~250 B) larger than L2"},
+                       "l2": "path state of a wave (up to 8M paths x ~250 B, two waves in flight) larger than L2"},
             "latency": {"cache_off": off, "cache_on": results["on"]},
             "e2e": {"value": total_paths / e2e_s / 1e6, "unit": "Mpaths/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": sum(c.width * c.height * 12 for _, c, _, _, _ in reqs),

@@ -411,8 +411,8 @@ rbr_status rbr_cache_render(rbr_ctx* ctx, const rbr_camera* camera, const rbr_re
 typedef struct rbr_batch rbr_batch;
 
 typedef struct rbr_batch_config {
-    uint64_t path_memory_bytes; /* budget for one wave's path state (default 1 GiB) */
-    uint32_t wave_paths;        /* paths per wave; 0: the budget decides (at most 2^22) */
+    uint64_t path_memory_bytes; /* budget for one wave's path state (default 2 GiB) */
+    uint32_t wave_paths;        /* paths per wave; 0: the budget decides (at most 2^23) */
     uint32_t blocks_per_sm;     /* grid of the wavefront kernels = this x SMs (default 8) */
     int32_t use_graphs;         /* replay each wave shape from a captured CUDA graph (default 1) */
     uint32_t waves_in_flight;   /* 1, or 2 (default; 0 means 2): waves alternate between two

@@ -100,12 +100,12 @@ uint32_t max_lights(const rbr_batch* b) {
 }
 
 // Paths per wave: the configured count, else what the memory budget allows (path state,
-// segment index, shadow queue of every light, cache query records), at most 2^22.
+// segment index, shadow queue of every light, cache query records), at most 2^23.
 uint32_t wave_capacity(const rbr_batch* b, bool any_cache) {
     if (b->cfg.wave_paths) return b->cfg.wave_paths;
     const uint64_t per_path = 96 + 4 + 48ull * max_lights(b) + (any_cache ? 80 : 0);
     const uint64_t cap = b->cfg.path_memory_bytes / per_path;
-    return static_cast<uint32_t>(std::max<uint64_t>(1u << 16, std::min<uint64_t>(cap, 1u << 22)));
+    return static_cast<uint32_t>(std::max<uint64_t>(1u << 16, std::min<uint64_t>(cap, 1u << 23)));
 }
 
 // Groups the pending requests by (scene, mode, train) in order of first appearance and packs
@@ -327,7 +327,7 @@ extern "C" {
 void rbr_batch_config_default(rbr_batch_config* out) {
     if (!out) return;
     std::memset(out, 0, sizeof(*out));
-    out->path_memory_bytes = 1ull << 30;
+    out->path_memory_bytes = 2ull << 30;
     out->wave_paths = 0;
     out->blocks_per_sm = 8;
     out->use_graphs = 1;
@@ -342,7 +342,7 @@ rbr_status rbr_batch_create(rbr_ctx* ctx, const rbr_batch_config* config, rbr_ba
     b->eng = ctx;
     if (config) b->cfg = *config;
     else rbr_batch_config_default(&b->cfg);
-    if (b->cfg.path_memory_bytes == 0) b->cfg.path_memory_bytes = 1ull << 30;
+    if (b->cfg.path_memory_bytes == 0) b->cfg.path_memory_bytes = 2ull << 30;
     cudaSetDevice(ctx->device);
     const cudaError_t e = cudaMalloc(&b->d_table, 2 * kTableBytes);  // a segment table per wave in flight
     if (e != cudaSuccess) {
@@ -499,7 +499,7 @@ rbr_status rbr_batch_autotune(rbr_batch* b, void* stream) {
     const uint32_t budget_cap = wave_capacity(b, any_cache);
     float best = -1.0f;
     rbr_batch_config best_cfg = saved;
-    for (uint32_t wp : {1u << 19, 1u << 20, 1u << 21, 1u << 22}) {
+    for (uint32_t wp : {1u << 20, 1u << 21, 1u << 22, 1u << 23}) {
         if (wp > budget_cap) continue;
         for (uint32_t bps : {4u, 8u, 16u}) {
             b->cfg = saved;
