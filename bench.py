@@ -332,7 +332,8 @@ def run_render(args, rank, world, local_rank):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded)",
             "config": {"workload": cfg["desc"], "paths_per_step": paths,
-                       "l2": "working set per wave (4M paths x ~100 B of state) larger than L2"},
+                       "l2": f"working set of the two waves in flight ({2 * paths // max(1, st.waves)} paths x ~100 B "
+                             "of path state + 48 B per shadow record) larger than L2; the film is written once"},
             "e2e": e2e, "cpu_baseline": base, "clocks": clk,
             "gpu_launches": st.launches * args.steps,
             "render": {"extension_rays_per_path": st.extension_rays / st.paths,

@@ -235,6 +235,8 @@ rbr_status rbr_scene_stats_get(const rbr_ctx* ctx, rbr_scene_stats* out);
  *   "trace.order"          kernel 0: 0 traces the rays in the order given; 1 first sorts them
  *                          by direction octant and origin cell (a radix sort on the device) so
  *                          that warps hold rays that walk the same nodes
+ *   "trace.host_chunk"     rbr_trace_host: rays per chunk of its upload / trace / download
+ *                          pipeline over two streams (default 2^20; 0: one piece)
  *   "pt.wave_paths"        camera samples per path-tracer wave (default 2^23)
  *   "pt.streams"           rbr_render: waves in flight, 1 or 2 (default 2: waves alternate
  *                          between two sets of path buffers on two streams; an image that

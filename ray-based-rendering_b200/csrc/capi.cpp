@@ -1,4 +1,5 @@
 // The C ABI of include/rbr_b200.h.
+#include <algorithm>
 #include <cstring>
 #include <new>
 #include <string>
@@ -39,6 +40,14 @@ rbr_status ensure(rbr_ctx* ctx, DevBuf& b, size_t bytes, const char* what) {
     }
     b.bytes = bytes;
     return RBR_OK;
+}
+
+rbr_status ensure_side_stream(rbr_ctx* ctx) {
+    cudaError_t e = cudaSuccess;
+    if (!ctx->side_stream) e = cudaStreamCreateWithFlags(&ctx->side_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess && !ctx->ev_fork) e = cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess && !ctx->ev_join) e = cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming);
+    return e == cudaSuccess ? RBR_OK : cuda_fail(ctx, e, "second stream");
 }
 
 // Reads (and clears) the device error word after the work on `stream` has finished.
@@ -129,6 +138,7 @@ void rbr_ctx_destroy(rbr_ctx* ctx) {
     release(ctx->stage_in);
     release(ctx->stage_out);
     release(ctx->sort_buf);
+    release(ctx->sort_buf2);
     if (ctx->d_error) cudaFree(ctx->d_error);
     if (ctx->d_cursors) cudaFree(ctx->d_cursors);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -164,6 +174,9 @@ rbr_status rbr_param_set(rbr_ctx* ctx, const char* name, int64_t value) {
     } else if (n == "trace.min_blocks") {
         if (value != 8 && value != 10 && value != 12) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "trace.min_blocks is 8, 10 or 12");
         ctx->trace_min_blocks = static_cast<int>(value);
+    } else if (n == "trace.host_chunk") {
+        if (value < 0 || value > 0xFFFFFFFFll) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "trace.host_chunk is 0..2^32-1");
+        ctx->trace_host_chunk = static_cast<uint32_t>(value);
     } else if (n == "pt.streams") {
         if (value != 1 && value != 2) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "pt.streams is 1 or 2");
         ctx->pt_streams = static_cast<int>(value);
@@ -193,6 +206,7 @@ rbr_status rbr_param_get(const rbr_ctx* ctx, const char* name, int64_t* value) {
     else if (n == "trace.order") *value = ctx->trace_order;
     else if (n == "pt.wave_paths") *value = ctx->pt_wave_paths;
     else if (n == "pt.streams") *value = ctx->pt_streams;
+    else if (n == "trace.host_chunk") *value = ctx->trace_host_chunk;
     else return RBR_ERR_INVALID_ARGUMENT;
     return RBR_OK;
 }
@@ -244,12 +258,36 @@ rbr_status rbr_trace_host(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any
     if ((st = ensure(ctx, ctx->stage_in, in_bytes, "ray staging")) != RBR_OK) return st;
     if ((st = ensure(ctx, ctx->stage_out, out_bytes, "hit staging")) != RBR_OK) return st;
     cudaStream_t s = ctx->stream;
-    cudaError_t e = cudaMemcpyAsync(ctx->stage_in.ptr, rays, in_bytes, cudaMemcpyHostToDevice, s);
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "ray upload");
-    e = launch_trace(ctx, static_cast<const rbr_ray*>(ctx->stage_in.ptr), n, any_hit, ctx->stage_out.ptr, s);
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "trace launch");
-    e = cudaMemcpyAsync(out, ctx->stage_out.ptr, out_bytes, cudaMemcpyDeviceToHost, s);
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "hit download");
+    // Chunks alternate between two streams, so that the upload of one chunk, the traversal
+    // of another and the download of a third overlap (copies in each direction and kernels
+    // run on separate engines).
+    const uint32_t chunk = ctx->trace_host_chunk && n > ctx->trace_host_chunk ? ctx->trace_host_chunk : n;
+    const bool two = chunk < n;
+    if (two && (st = ensure_side_stream(ctx)) != RBR_OK) return st;
+    const size_t osz = any_hit ? 1 : sizeof(rbr_hit);
+    cudaError_t e = cudaSuccess;
+    if (two) {
+        e = cudaEventRecord(ctx->ev_fork, s);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->side_stream, ctx->ev_fork, 0);
+    }
+    uint32_t k = 0;
+    for (uint32_t off = 0; off < n && e == cudaSuccess; off += chunk, ++k) {
+        const uint32_t m = std::min(chunk, n - off);
+        const cudaStream_t cs = (k & 1) ? ctx->side_stream : s;
+        rbr_ray* din = static_cast<rbr_ray*>(ctx->stage_in.ptr) + off;
+        char* dout = static_cast<char*>(ctx->stage_out.ptr) + size_t(off) * osz;
+        e = cudaMemcpyAsync(din, rays + off, size_t(m) * sizeof(rbr_ray), cudaMemcpyHostToDevice, cs);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "ray upload");
+        e = launch_trace(ctx, din, m, any_hit, dout, cs, static_cast<int>(k & 1));
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "trace launch");
+        e = cudaMemcpyAsync(static_cast<char*>(out) + size_t(off) * osz, dout, size_t(m) * osz, cudaMemcpyDeviceToHost, cs);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "hit download");
+    }
+    if (e == cudaSuccess && two) {
+        e = cudaEventRecord(ctx->ev_join, ctx->side_stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(s, ctx->ev_join, 0);
+    }
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "trace pipeline");
     return check_device_error(ctx, s);
 }
 

@@ -698,12 +698,8 @@ rbr_status render(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_params* 
     if (st != RBR_OK) return st;
     if (two) {
         st = ensure_paths(ctx, cap, cap * nl, &ctx->pt2);
+        if (st == RBR_OK) st = ensure_side_stream(ctx);
         if (st != RBR_OK) return st;
-        cudaError_t ce = cudaSuccess;
-        if (!ctx->side_stream) ce = cudaStreamCreateWithFlags(&ctx->side_stream, cudaStreamNonBlocking);
-        if (ce == cudaSuccess && !ctx->ev_fork) ce = cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming);
-        if (ce == cudaSuccess && !ctx->ev_join) ce = cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming);
-        if (ce != cudaSuccess) return cuda_fail(ctx, ce, "second path-tracer stream");
     }
     ctx->pt_last_two = two;
     Paths PP[2];

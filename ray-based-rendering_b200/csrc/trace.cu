@@ -418,14 +418,15 @@ cudaError_t launch_trace_persist(const DeviceScene& s, const rbr_ray* rays, uint
 }
 
 // Sorts the rays by (direction octant, origin cell) on `stream` and returns the permutation.
-static cudaError_t sort_rays(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, const uint32_t** perm, cudaStream_t stream) {
+static cudaError_t sort_rays(rbr_ctx* ctx, DevBuf& sort_buf, const rbr_ray* rays, uint32_t n, const uint32_t** perm,
+                             cudaStream_t stream) {
     size_t temp = 0;
     cudaError_t e = cub::DeviceRadixSort::SortPairs(nullptr, temp, static_cast<const uint32_t*>(nullptr),
                                                     static_cast<uint32_t*>(nullptr), static_cast<const uint32_t*>(nullptr),
                                                     static_cast<uint32_t*>(nullptr), static_cast<int>(n), 0, 30, stream);
     if (e != cudaSuccess) return e;
-    if (ensure(ctx, ctx->sort_buf, size_t(n) * 16 + temp + 256, "ray sort") != RBR_OK) return cudaErrorMemoryAllocation;
-    uint32_t* base = static_cast<uint32_t*>(ctx->sort_buf.ptr);
+    if (ensure(ctx, sort_buf, size_t(n) * 16 + temp + 256, "ray sort") != RBR_OK) return cudaErrorMemoryAllocation;
+    uint32_t* base = static_cast<uint32_t*>(sort_buf.ptr);
     uint32_t *keys = base, *keys2 = base + n, *idx = base + 2 * size_t(n), *idx2 = base + 3 * size_t(n);
     void* tmp = reinterpret_cast<char*>(base + 4 * size_t(n)) + (256 - (reinterpret_cast<uintptr_t>(base + 4 * size_t(n)) & 255));
     float3 lo = make_float3(0.0f, 0.0f, 0.0f), sc = make_float3(0.0f, 0.0f, 0.0f);
@@ -449,10 +450,11 @@ static cudaError_t sort_rays(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, cons
     return e;
 }
 
-cudaError_t launch_trace(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any_hit, void* out, cudaStream_t stream) {
+cudaError_t launch_trace(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any_hit, void* out, cudaStream_t stream,
+                         int slot) {
     if (ctx->trace_kernel == 0 && ctx->trace_order == 1 && n > 0) {
         const uint32_t* perm = nullptr;
-        cudaError_t e = sort_rays(ctx, rays, n, &perm, stream);
+        cudaError_t e = sort_rays(ctx, slot ? ctx->sort_buf2 : ctx->sort_buf, rays, n, &perm, stream);
         if (e != cudaSuccess) return e;
         const uint32_t blocks = (n + kTraceBlock - 1) / kTraceBlock;
         const auto* r = reinterpret_cast<const float4*>(rays);

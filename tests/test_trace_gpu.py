@@ -56,6 +56,25 @@ def test_closest_and_any_match_bruteforce(kctx, restatement, ns, nt, plane, seed
     assert np.array_equal(ctx.trace_host(rays, any_hit=True), restatement.trace_any(h, rays))
 
 
+def test_chunked_host_pipeline_matches(kctx, restatement):
+    """rbr_trace_host in chunks of 1,000 rays over two streams (trace.host_chunk) gives the
+    answers of one piece, with a last chunk shorter than the others."""
+    ctx = kctx
+    w = scenes.random_world(400, 1500, False, seed=9)
+    rays = scenes.random_test_rays(6500, seed=109)
+    ctx.upload(w)
+    h = restatement.scene(w)
+    want = restatement.trace_closest(h, rays)
+    chunk = ctx.get_param("trace.host_chunk")
+    try:
+        for c in (1000, 0):
+            ctx.set_param("trace.host_chunk", c)
+            assert_same_closest(ctx.trace_host(rays), want)
+            assert np.array_equal(ctx.trace_host(rays, any_hit=True), restatement.trace_any(h, rays))
+    finally:
+        ctx.set_param("trace.host_chunk", chunk)
+
+
 @pytest.mark.parametrize("ns,nt,plane,seed", WORLDS)
 def test_matches_reference_bvh_and_bruteforce(ctx, reference, ns, nt, plane, seed):
     """The same worlds through the reference library itself: its brute-force loop and its BVH."""
