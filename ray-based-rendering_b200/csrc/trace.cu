@@ -59,8 +59,10 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_any_perm(DeviceScene s, c
     occ[i] = static_cast<uint8_t>(traverse<true>(s, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, t, err));
 }
 
-// 3-bit direction octant, then a 27-bit Morton code of the origin's cell (512^3 cells over the
-// scene box): the sort key that groups rays by octant and, within it, by origin.
+// Sort keys from the direction octant (3 bits) and a Morton code of the origin's cell over the
+// scene box. order 1: octant, then 27-bit Morton code of 512^3 cells (30 key bits); order 2:
+// octant, then 18-bit code of 64^3 cells (21 bits, one radix pass fewer); order 3: the 64^3
+// cell first, octant last (21 bits), so consecutive warps stay in one region of the scene.
 __device__ __forceinline__ uint32_t spread3(uint32_t x) {  // 9 bits -> every third of 27
     x &= 0x1FFu;
     x = (x | (x << 16)) & 0x030000FFu;
@@ -70,8 +72,8 @@ __device__ __forceinline__ uint32_t spread3(uint32_t x) {  // 9 bits -> every th
     return x;
 }
 
-__global__ void k_ray_keys(const float4* __restrict__ rays, uint32_t n, float3 lo, float3 scale, uint32_t* keys,
-                           uint32_t* idx) {
+__global__ void k_ray_keys(const float4* __restrict__ rays, uint32_t n, float3 lo, float3 scale, int order,
+                           uint32_t* keys, uint32_t* idx) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float4 a = __ldg(rays + 2 * static_cast<size_t>(i));
         const float4 b = __ldg(rays + 2 * static_cast<size_t>(i) + 1);
@@ -82,7 +84,7 @@ __global__ void k_ray_keys(const float4* __restrict__ rays, uint32_t n, float3 l
         };
         const uint32_t m = spread3(cell(a.x, lo.x, scale.x)) << 2 | spread3(cell(a.y, lo.y, scale.y)) << 1 |
                            spread3(cell(a.z, lo.z, scale.z));
-        keys[i] = (oct << 27) | m;
+        keys[i] = order == 1 ? (oct << 27) | m : order == 2 ? (oct << 18) | (m >> 9) : ((m >> 9) << 3) | oct;
         idx[i] = i;
     }
 }
@@ -420,10 +422,12 @@ cudaError_t launch_trace_persist(const DeviceScene& s, const rbr_ray* rays, uint
 // Sorts the rays by (direction octant, origin cell) on `stream` and returns the permutation.
 static cudaError_t sort_rays(rbr_ctx* ctx, DevBuf& sort_buf, const rbr_ray* rays, uint32_t n, const uint32_t** perm,
                              cudaStream_t stream) {
+    const int order = ctx->trace_order;
+    const int key_bits = order == 1 ? 30 : 21;
     size_t temp = 0;
     cudaError_t e = cub::DeviceRadixSort::SortPairs(nullptr, temp, static_cast<const uint32_t*>(nullptr),
                                                     static_cast<uint32_t*>(nullptr), static_cast<const uint32_t*>(nullptr),
-                                                    static_cast<uint32_t*>(nullptr), static_cast<int>(n), 0, 30, stream);
+                                                    static_cast<uint32_t*>(nullptr), static_cast<int>(n), 0, key_bits, stream);
     if (e != cudaSuccess) return e;
     if (ensure(ctx, sort_buf, size_t(n) * 16 + temp + 256, "ray sort") != RBR_OK) return cudaErrorMemoryAllocation;
     uint32_t* base = static_cast<uint32_t*>(sort_buf.ptr);
@@ -442,17 +446,17 @@ static cudaError_t sort_rays(rbr_ctx* ctx, DevBuf& sort_buf, const rbr_ray* rays
         }
     }
     const int grid = std::min<int>((n + 255) / 256, ctx->num_sms * 8);
-    k_ray_keys<<<grid, 256, 0, stream>>>(reinterpret_cast<const float4*>(rays), n, lo, sc, keys, idx);
+    k_ray_keys<<<grid, 256, 0, stream>>>(reinterpret_cast<const float4*>(rays), n, lo, sc, order, keys, idx);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    e = cub::DeviceRadixSort::SortPairs(tmp, temp, keys, keys2, idx, idx2, static_cast<int>(n), 0, 30, stream);
+    e = cub::DeviceRadixSort::SortPairs(tmp, temp, keys, keys2, idx, idx2, static_cast<int>(n), 0, key_bits, stream);
     *perm = idx2;
     return e;
 }
 
 cudaError_t launch_trace(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any_hit, void* out, cudaStream_t stream,
                          int slot) {
-    if (ctx->trace_kernel == 0 && ctx->trace_order == 1 && n > 0) {
+    if (ctx->trace_kernel == 0 && ctx->trace_order != 0 && n > 0) {
         const uint32_t* perm = nullptr;
         cudaError_t e = sort_rays(ctx, slot ? ctx->sort_buf2 : ctx->sort_buf, rays, n, &perm, stream);
         if (e != cudaSuccess) return e;
@@ -496,7 +500,7 @@ rbr_status autotune_trace(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any
         int kernel, min_blocks, per_sm, order;
     };
     const Cand cands[] = {{0, 8, 0, 0}, {0, 10, 0, 0}, {0, 12, 0, 0}, {1, 10, 0, 0}, {2, 10, 0, 0},
-                          {0, 8, 0, 1}, {0, 10, 0, 1}, {0, 12, 0, 1}};
+                          {0, 8, 0, 1}, {0, 10, 0, 1}, {0, 12, 0, 1}, {0, 10, 0, 2}, {0, 10, 0, 3}};
     rbr_status st = ensure(ctx, ctx->stage_out, size_t(n) * (any_hit ? 1 : sizeof(rbr_hit)), "autotune output");
     if (st != RBR_OK) return st;
     const Cand saved{ctx->trace_kernel, ctx->trace_min_blocks, ctx->trace_blocks_per_sm, ctx->trace_order};

@@ -29,11 +29,13 @@ def assert_same_closest(got, want):
 
 WORLDS = [(30, 30, False, 1), (400, 1500, False, 2), (60, 200, True, 3)]
 # (trace.kernel, trace.order): one thread per ray, persistent lane refill, warp-cooperative,
-# and one thread per ray on rays sorted by direction octant and origin cell
-KERNELS = [(0, 0), (1, 0), (2, 0), (0, 1)]
+# and one thread per ray on rays sorted by the three key layouts (direction octant and origin
+# cell of 512^3 or 64^3, or cell first)
+KERNELS = [(0, 0), (1, 0), (2, 0), (0, 1), (0, 2), (0, 3)]
 
 
-@pytest.fixture(params=KERNELS, ids=["kernel0", "kernel1", "kernel2", "kernel0-sorted"])
+@pytest.fixture(params=KERNELS, ids=["kernel0", "kernel1", "kernel2", "kernel0-sorted", "kernel0-sorted64",
+                                     "kernel0-cellfirst"])
 def kctx(ctx, request):
     """The shared context with each traversal variant in turn."""
     ctx.set_param("trace.kernel", request.param[0])
