@@ -241,6 +241,20 @@ __device__ __forceinline__ void ld64(uint32_t taddr, float* v) {
     for (int q = 0; q < 4; ++q) tc::tmem_ld16(taddr + 16 * q, v + 16 * q);
 }
 
+// Records available to a training batch: the first list [0, n0) and, with count2_ptr, a
+// second list that starts at `split`; i-th available record -> its index.
+__device__ __forceinline__ uint32_t batch_avail(const TrainBatchDev& b, uint32_t& n0) {
+    if (!b.count_ptr) {
+        n0 = b.count;
+        return b.count;
+    }
+    n0 = min(*b.count_ptr, b.cap);
+    return n0 + (b.count2_ptr ? min(*b.count2_ptr, b.cap) : 0u);
+}
+__device__ __forceinline__ uint32_t batch_record(const TrainBatchDev& b, uint32_t i, uint32_t n0) {
+    return i < n0 ? i : b.split + (i - n0);
+}
+
 __device__ __forceinline__ uint32_t shuffle_index(uint32_t x, uint32_t n) {
     return static_cast<uint32_t>((static_cast<uint64_t>(x) * 2654435761ull + 0x9E3779B9ull) % n);
 }
@@ -352,7 +366,8 @@ __global__ void __launch_bounds__(128, 1) k_rc_train(CacheDev c, TrainBatchDev b
     uint8_t* del = smem + kWBytes + kActBytesTrain;
     uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + kWBytes + kActBytesTrain + kDelBytes);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + kWBytes + kActBytesTrain + kDelBytes + 8);
-    const uint32_t avail = b.count_ptr ? min(*b.count_ptr, b.cap) : b.count;
+    uint32_t n0 = 0;
+    const uint32_t avail = batch_avail(b, n0);
     const uint32_t nsamp = min(b.batch, avail);
     const uint32_t tiles = (nsamp + kRcTile - 1) / kRcTile;
     if (blockIdx.x >= tiles) return;
@@ -381,7 +396,7 @@ __global__ void __launch_bounds__(128, 1) k_rc_train(CacheDev c, TrainBatchDev b
         const uint32_t j = tile * kRcTile + tid;
         const bool valid = j < nsamp;
         uint32_t ridx = 0;
-        if (valid) ridx = b.shuffle ? shuffle_index(b.step_index * b.batch + j, avail) : j;
+        if (valid) ridx = batch_record(b, b.shuffle ? shuffle_index(b.step_index * b.batch + j, avail) : j, n0);
         const float4* rec = b.records + 4 * static_cast<size_t>(ridx);
         float4 tgt = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         {
@@ -534,7 +549,8 @@ __global__ void __launch_bounds__(128, 1) k_rc_train(CacheDev c, TrainBatchDev b
 // --------------------------------------------------------------------------------------------
 // Starts an optimiser step if the batch had samples: t += 1, bias corrections 1 - beta^t.
 __global__ void k_rc_adam_prep(AdamDev a, TrainBatchDev b, float* scalars) {
-    const uint32_t avail = b.count_ptr ? min(*b.count_ptr, b.cap) : b.count;
+    uint32_t n0 = 0;
+    const uint32_t avail = batch_avail(b, n0);
     uint32_t* step = reinterpret_cast<uint32_t*>(scalars + kRcStep);
     if (avail == 0 || b.batch == 0) {
         scalars[kRcBias] = 0.0f;  // no step: the update kernels do nothing
@@ -1090,23 +1106,28 @@ rbr_status cache_ensure_render(rbr_ctx* ctx, uint32_t paths, uint32_t train_cap)
     return RBR_OK;
 }
 
-cudaError_t cache_launch_finalize(rbr_ctx* ctx, const float4* path_rad, const uint32_t* counters, int base_word,
-                                  int count_word, cudaStream_t stream) {
+cudaError_t cache_launch_finalize(rbr_ctx* ctx, const float4* path_rad, const float4* t_aux, const uint32_t* counters,
+                                  int base_word, int count_word, uint32_t cap, cudaStream_t stream) {
     CacheState& cs = ctx->cache;
-    k_rc_finalize<<<ctx->num_sms * 4, 128, 0, stream>>>(as<float4>(cs.t_aux), as<float4>(cs.t_target), path_rad, counters,
-                                                       base_word, count_word, cs.t_cap);
+    // the targets of a list that starts at t_aux (a wave slot's half) start at the same index
+    const size_t first = static_cast<size_t>(t_aux - as<float4>(cs.t_aux)) / 2;
+    k_rc_finalize<<<ctx->num_sms * 4, 128, 0, stream>>>(t_aux, as<float4>(cs.t_target) + first, path_rad, counters,
+                                                       base_word, count_word, cap);
     return cudaGetLastError();
 }
 
 // The frame's optimiser steps on the training vertices gathered (count on the device).
-cudaError_t cache_launch_train_frame(rbr_ctx* ctx, const uint32_t* count_ptr, uint32_t frame, cudaStream_t stream) {
+cudaError_t cache_launch_train_frame(rbr_ctx* ctx, const uint32_t* count_ptr, const uint32_t* count2_ptr, uint32_t cap,
+                                     uint32_t frame, cudaStream_t stream) {
     CacheState& cs = ctx->cache;
     TrainBatchDev b;
     b.records = as<float4>(cs.t_rec);
     b.targets = as<float4>(cs.t_target);
     b.count_ptr = count_ptr;
+    b.count2_ptr = count2_ptr;
+    b.split = cap;
     b.count = 0;
-    b.cap = cs.t_cap;
+    b.cap = cap;
     b.batch = cs.cfg.train_batch;
     b.shuffle = 1;
     cudaError_t e = cudaSuccess;

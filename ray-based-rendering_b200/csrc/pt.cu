@@ -402,6 +402,8 @@ __global__ void __launch_bounds__(kBlock, 8) k_shade(DeviceScene s, Wave w, Path
         Frame fr;
         Bsdf bs;
         bs.n = 0;
+        Mix mx;
+        mx.total = 0.0f;
         uint32_t pixel = 0, sample = 0;
         if (valid) {
             int c = 0;
@@ -430,6 +432,7 @@ __global__ void __launch_bounds__(kBlock, 8) k_shade(DeviceScene s, Wave w, Path
             bs = make_bsdf(m);
             fr = make_frame(h.outward);
             wo = to_local(fr, xneg(rd));  // isect.wo = -ray.direction
+            mx = mixture(bs, wo);
             nee = key.nee && !bsdf_delta(bs);
             alive = true;
             if (kCache && bs.n > 0 && !bsdf_delta(bs)) {
@@ -475,8 +478,8 @@ __global__ void __launch_bounds__(kBlock, 8) k_shade(DeviceScene s, Wave w, Path
                 const LSample ls = light_sample(L, h.point, (l & 1) ? u.z : u.x, (l & 1) ? u.w : u.y);
                 if (ls.pdf > 0.0f && !black(ls.Li)) {
                     const f3 wiL = to_local(fr, ls.wi);
-                    const f3 f = bsdf_eval(bs, wo, wiL);
-                    const float bpdf = bsdf_pdf(bs, wo, wiL);
+                    const f3 f = bsdf_eval(bs, mx, wo, wiL);
+                    const float bpdf = bsdf_pdf(bs, mx, wo, wiL);
                     if (!black(f)) {
                         spawn(h, ls.wi, so, sd);
                         stmax = fs(ls.dist, kEpsilon);
@@ -505,7 +508,7 @@ __global__ void __launch_bounds__(kBlock, 8) k_shade(DeviceScene s, Wave w, Path
         bool cont = false;
         if (valid && alive && !last) {
             const float4 u = draw4(seed, pixel, sample, d, kRngBounce);
-            const BSample b = bsdf_sample(bs, wo, u.x, u.y);
+            const BSample b = bsdf_sample(bs, mx, wo, u.x, u.y);
             if (b.pdf > 0.0f && !black(b.f)) {
                 const f3 wiW = to_world(fr, b.wi);
                 const float c = fabsf(xdot(wiW, h.normal));
@@ -797,9 +800,13 @@ rbr_status render(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_params* 
 // ------------------------------------------------------------------------------------------
 namespace {
 
-__global__ void k_cache_wave_end(const uint32_t* counters, uint32_t* scalars, uint32_t t_cap) {
-    scalars[kRcLastQueries] += counters[kCQuery];
-    scalars[kRcTrain] = min(counters[kCTrain], t_cap);
+__global__ void k_cache_wave_end(const uint32_t* counters, uint32_t* scalars) {
+    atomicAdd(scalars + kRcLastQueries, counters[kCQuery]);
+}
+
+// Training vertices of the frame: the sum over the waves in flight of their own lists.
+__global__ void k_cache_frame_end(const uint32_t* c0, const uint32_t* c1, uint32_t* scalars, uint32_t cap) {
+    scalars[kRcTrain] = min(*c0, cap) + (c1 ? min(*c1, cap) : 0u);
 }
 
 
@@ -849,32 +856,44 @@ rbr_status render_cached(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_p
     uint32_t cap = static_cast<uint32_t>(std::min<uint64_t>(npix * spp, std::max(ctx->pt_wave_paths, spp)));
     cap = std::min<uint64_t>(cap, kShadowBytesLimit / (48ull * nl));
     cap = std::max(spp, cap / spp * spp);
+    // Two waves in flight as in render(): each has its own path buffers, query records and
+    // half of the training-vertex list with its own counter; the frame's optimiser steps
+    // draw from both halves once both waves have ended.
+    const bool two = ctx->pt_streams == 2 && npix >= 2;
+    if (two && npix * spp <= cap) cap = static_cast<uint32_t>((npix + 1) / 2) * spp;
     rbr_status st = ensure_paths(ctx, cap, cap * nl);
+    if (st == RBR_OK && two) st = ensure_paths(ctx, cap, cap * nl, &ctx->pt2);
+    if (st == RBR_OK && two) st = ensure_side_stream(ctx);
     if (st != RBR_OK) return st;
     const uint32_t depth = std::max(1, p->max_depth);
     const uint32_t t_cap =
         train ? static_cast<uint32_t>(std::min<uint64_t>(uint64_t(std::max(1u, cs.cfg.train_paths)) * depth, 1u << 23)) : 1;
-    st = cache_ensure_render(ctx, cap, t_cap);
+    st = cache_ensure_render(ctx, two ? 2 * cap : cap, two ? 2 * t_cap : t_cap);
     if (st != RBR_OK) return st;
+    const uint32_t t_half = two ? cs.t_cap / 2 : cs.t_cap;  // training vertices per wave slot
 
-    PathBuffers& pb = ctx->pt;
-    Paths P;
-    P.ray = static_cast<float4*>(pb.ray.ptr);
-    P.thr = static_cast<float4*>(pb.thr.ptr);
-    P.rad = static_cast<float4*>(pb.rad.ptr);
-    P.hit = static_cast<uint2*>(pb.hit.ptr);
-    P.q0 = static_cast<uint32_t*>(pb.queue[0].ptr);
-    P.q1 = static_cast<uint32_t*>(pb.queue[1].ptr);
-    P.classq = static_cast<uint32_t*>(pb.classq.ptr);
-    P.shadow = static_cast<float4*>(pb.shadow.ptr);
-    P.counters = static_cast<uint32_t*>(pb.counters.ptr);
-    P.cap = pb.capacity;
-    P.shadow_cap = pb.shadow_capacity;
-    P.q_rec = static_cast<float4*>(cs.q_rec);
-    P.q_info = static_cast<float4*>(cs.q_info);
-    P.t_rec = static_cast<float4*>(cs.t_rec);
-    P.t_aux = static_cast<float4*>(cs.t_aux);
-    P.t_cap = train ? cs.t_cap : 0;
+    Paths PP[2];
+    for (int b = 0; b < (two ? 2 : 1); ++b) {
+        PathBuffers& pb = b ? ctx->pt2 : ctx->pt;
+        Paths& P = PP[b];
+        P.ray = static_cast<float4*>(pb.ray.ptr);
+        P.thr = static_cast<float4*>(pb.thr.ptr);
+        P.rad = static_cast<float4*>(pb.rad.ptr);
+        P.hit = static_cast<uint2*>(pb.hit.ptr);
+        P.q0 = static_cast<uint32_t*>(pb.queue[0].ptr);
+        P.q1 = static_cast<uint32_t*>(pb.queue[1].ptr);
+        P.classq = static_cast<uint32_t*>(pb.classq.ptr);
+        P.shadow = static_cast<float4*>(pb.shadow.ptr);
+        P.counters = static_cast<uint32_t*>(pb.counters.ptr);
+        P.cap = pb.capacity;
+        P.shadow_cap = pb.shadow_capacity;
+        P.q_rec = static_cast<float4*>(cs.q_rec) + 4 * size_t(b) * cap;
+        P.q_info = static_cast<float4*>(cs.q_info) + size_t(b) * cap;
+        P.t_rec = static_cast<float4*>(cs.t_rec) + 4 * size_t(b) * t_half;
+        P.t_aux = static_cast<float4*>(cs.t_aux) + 2 * size_t(b) * t_half;
+        P.t_cap = train ? t_half : 0;
+    }
+    const cudaStream_t streams[2] = {stream, two ? ctx->side_stream : stream};
     const CameraDev cd = camera_dev(cam);
 
     const double frac = train ? double(cs.cfg.train_paths) / double(npix * spp) : 0.0;
@@ -885,14 +904,21 @@ rbr_status render_cached(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_p
     const int grid = ctx->num_sms * 8;
     const uint32_t pix_per_wave = cap / spp;
     uint32_t launches = 0, waves = 0;
-    cudaError_t e = cudaMemsetAsync(P.counters, 0, kCWords * 4, stream);
+    cudaError_t e = cudaMemsetAsync(PP[0].counters, 0, kCWords * 4, stream);
+    if (e == cudaSuccess && two) e = cudaMemsetAsync(PP[1].counters, 0, kCWords * 4, stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(film_mean, 0, npix * 12, stream);
     if (e == cudaSuccess && film_m2) e = cudaMemsetAsync(film_m2, 0, npix * 12, stream);
     if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_start, stream);
     for (uint32_t f = 0; f < frames && e == cudaSuccess; ++f) {
-        e = cudaMemsetAsync(P.counters + kCTrain, 0, 4, stream);
+        e = cudaMemsetAsync(PP[0].counters + kCTrain, 0, 4, stream);
+        if (e == cudaSuccess && two) e = cudaMemsetAsync(PP[1].counters + kCTrain, 0, 4, stream);
         if (e == cudaSuccess) e = cudaMemsetAsync(scalars + kRcLastQueries, 0, 4, stream);
-        for (uint64_t p0 = 0; p0 < npix && e == cudaSuccess; p0 += pix_per_wave) {
+        if (e == cudaSuccess && two) e = cudaEventRecord(ctx->ev_fork, stream);
+        if (e == cudaSuccess && two) e = cudaStreamWaitEvent(ctx->side_stream, ctx->ev_fork, 0);
+        uint32_t wave_in_frame = 0;
+        for (uint64_t p0 = 0; p0 < npix && e == cudaSuccess; p0 += pix_per_wave, ++wave_in_frame) {
+            const Paths& P = PP[two ? (wave_in_frame & 1u) : 0u];
+            const cudaStream_t ws = streams[wave_in_frame & 1u];
             Wave w;
             w.p0 = static_cast<uint32_t>(p0);
             w.npaths = static_cast<uint32_t>(std::min<uint64_t>(pix_per_wave, npix - p0)) * spp;
@@ -907,29 +933,37 @@ rbr_status render_cached(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_p
             w.term_depth = cs.cfg.termination_depth;
             w.train_thresh = thresh;
             w.film_weight = weight;
-            k_raygen<false><<<grid, kBlock, 0, stream>>>(cd, w, P);
+            k_raygen<false><<<grid, kBlock, 0, ws>>>(cd, w, P);
             ++launches;
             for (uint32_t d = 0; d < w.max_depth; ++d) {
-                k_begin<<<1, 1, 0, stream>>>(P, d);
-                k_extend<false, false><<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d, ctx->d_error);
-                k_shade<1, false><<<grid, kBlock, 0, stream>>>(ctx->scene, w, P, d);
-                k_shadow<<<grid, kBlock, 0, stream>>>(ctx->scene, P, ctx->d_error);
+                k_begin<<<1, 1, 0, ws>>>(P, d);
+                k_extend<false, false><<<grid, kBlock, 0, ws>>>(ctx->scene, w, P, d, ctx->d_error);
+                k_shade<1, false><<<grid, kBlock, 0, ws>>>(ctx->scene, w, P, d);
+                k_shadow<<<grid, kBlock, 0, ws>>>(ctx->scene, P, ctx->d_error);
                 launches += 4;
             }
-            e = cache_launch_infer(ctx, P.q_rec, w.npaths, P.counters + kCQuery, nullptr, P.rad, P.q_info, stream);
+            e = cache_launch_infer(ctx, P.q_rec, w.npaths, P.counters + kCQuery, nullptr, P.rad, P.q_info, ws);
             ++launches;
             if (e == cudaSuccess && train) {
-                e = cache_launch_finalize(ctx, P.rad, P.counters, kCTrainBase, kCTrain, stream);
+                e = cache_launch_finalize(ctx, P.rad, P.t_aux, P.counters, kCTrainBase, kCTrain, t_half, ws);
                 ++launches;
             }
-            k_film<<<grid, kBlock, 0, stream>>>(w, P, film_mean, film_m2);
-            k_cache_wave_end<<<1, 1, 0, stream>>>(P.counters, scalars, P.t_cap);
+            k_film<<<grid, kBlock, 0, ws>>>(w, P, film_mean, film_m2);
+            k_cache_wave_end<<<1, 1, 0, ws>>>(P.counters, scalars);
             launches += 2;
             ++waves;
             if (e == cudaSuccess) e = cudaGetLastError();
         }
+        if (e == cudaSuccess && two) e = cudaEventRecord(ctx->ev_join, ctx->side_stream);
+        if (e == cudaSuccess && two) e = cudaStreamWaitEvent(stream, ctx->ev_join, 0);
+        const uint32_t* c1 = two ? PP[1].counters + kCTrain : nullptr;
+        if (e == cudaSuccess) {
+            k_cache_frame_end<<<1, 1, 0, stream>>>(PP[0].counters + kCTrain, c1, scalars, PP[0].t_cap);
+            ++launches;
+            e = cudaGetLastError();
+        }
         if (e == cudaSuccess && train) {
-            e = cache_launch_train_frame(ctx, P.counters + kCTrain, f, stream);
+            e = cache_launch_train_frame(ctx, PP[0].counters + kCTrain, c1, t_half, f, stream);
             launches += 4 * cs.cfg.train_steps;
         }
     }
@@ -1013,12 +1047,13 @@ cudaError_t launch_packed_wave(rbr_ctx* eng, rbr_ctx* scn, const PackedWave& pw,
     }
     if (pw.mode == 1) {
         e = cache_launch_infer(scn, P.q_rec, pw.capacity, P.counters + kCQuery, nullptr, P.rad, P.q_info, stream);
-        if (e == cudaSuccess && pw.train) e = cache_launch_finalize(scn, P.rad, P.counters, kCTrainBase, kCTrain, stream);
+        if (e == cudaSuccess && pw.train)
+            e = cache_launch_finalize(scn, P.rad, P.t_aux, P.counters, kCTrainBase, kCTrain, scn->cache.t_cap, stream);
         if (e != cudaSuccess) return e;
     }
     k_film_packed<<<grid, kBlock, 0, stream>>>(P);
     if (pw.mode == 1 && pw.train) {
-        e = cache_launch_train_frame(scn, P.counters + kCTrain, 0, stream);
+        e = cache_launch_train_frame(scn, P.counters + kCTrain, nullptr, scn->cache.t_cap, 0, stream);
         if (e != cudaSuccess) return e;
     }
     return cudaGetLastError();

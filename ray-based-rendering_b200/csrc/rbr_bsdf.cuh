@@ -463,61 +463,65 @@ __device__ __forceinline__ float eff_weight(const Bsdf& b, int i, f3 wo) {
     if (!b.substrate[i]) return b.weight[i];
     return fm(b.weight[i], omax(0.0f, fs(1.0f, fresnel_dielectric(wo.z, 1.0f, b.ior))));
 }
-__device__ __forceinline__ float selection(const Bsdf& b, f3 wo, float* w, float* sc) {
-    float total = 0.0f;
+// MixtureBSDF::selection: per-lobe effective weights and sampling scores. They depend on wo
+// only, so a vertex computes them once (mixture) and every evaluation, pdf and sample of that
+// vertex reuses them; the values are the ones each reference call recomputes.
+struct Mix {
+    float w[4], sc[4];
+    float total;
+};
+__device__ __forceinline__ Mix mixture(const Bsdf& b, f3 wo) {
+    Mix m;
+    m.total = 0.0f;
     for (int i = 0; i < b.n; ++i) {
-        w[i] = eff_weight(b, i, wo);
-        sc[i] = fm(w[i], maxc(lobe_rho(b, b.kind[i], wo)));
-        total = fa(total, sc[i]);
+        m.w[i] = eff_weight(b, i, wo);
+        m.sc[i] = fm(m.w[i], maxc(lobe_rho(b, b.kind[i], wo)));
+        m.total = fa(m.total, m.sc[i]);
     }
-    return total;
+    return m;
 }
-__device__ __forceinline__ f3 bsdf_eval(const Bsdf& b, f3 wo, f3 wi) {
+__device__ __forceinline__ f3 bsdf_eval(const Bsdf& b, const Mix& m, f3 wo, f3 wi) {
     f3 f = mk(0.0f, 0.0f, 0.0f);
     for (int i = 0; i < b.n; ++i) {
         if (lobe_delta(b.kind[i])) continue;
-        f = xadd(f, xmuls(lobe_eval(b, b.kind[i], wo, wi), eff_weight(b, i, wo)));
+        f = xadd(f, xmuls(lobe_eval(b, b.kind[i], wo, wi), m.w[i]));
     }
     return f;
 }
-__device__ __forceinline__ float bsdf_pdf(const Bsdf& b, f3 wo, f3 wi) {
-    float w[4], sc[4];
-    const float total = selection(b, wo, w, sc);
-    if (total <= 0.0f) return 0.0f;
+__device__ __forceinline__ float bsdf_pdf(const Bsdf& b, const Mix& m, f3 wo, f3 wi) {
+    if (m.total <= 0.0f) return 0.0f;
     float p = 0.0f;
     for (int i = 0; i < b.n; ++i) {
         if (lobe_delta(b.kind[i])) continue;
-        p = fa(p, fm(sc[i], lobe_pdf(b, b.kind[i], wo, wi)));
+        p = fa(p, fm(m.sc[i], lobe_pdf(b, b.kind[i], wo, wi)));
     }
-    return fd(p, total);
+    return fd(p, m.total);
 }
-__device__ __forceinline__ BSample bsdf_sample(const Bsdf& b, f3 wo, float u1, float u2) {
-    float w[4], sc[4];
-    const float total = selection(b, wo, w, sc);
-    if (total <= 0.0f) return none();
-    float u = fm(u1, total);
+__device__ __forceinline__ BSample bsdf_sample(const Bsdf& b, const Mix& m, f3 wo, float u1, float u2) {
+    if (m.total <= 0.0f) return none();
+    float u = fm(u1, m.total);
     int chosen = b.n - 1;
     for (int i = 0; i < b.n; ++i) {
-        if (sc[i] <= 0.0f) continue;
-        if (u < sc[i] || i + 1 == b.n) {
+        if (m.sc[i] <= 0.0f) continue;
+        if (u < m.sc[i] || i + 1 == b.n) {
             chosen = i;
             break;
         }
-        u = fs(u, sc[i]);
+        u = fs(u, m.sc[i]);
     }
-    if (sc[chosen] <= 0.0f) return none();
-    const float v1 = omin(fd(u, sc[chosen]), 0.99999994f);
+    if (m.sc[chosen] <= 0.0f) return none();
+    const float v1 = omin(fd(u, m.sc[chosen]), 0.99999994f);
     const uint32_t k = b.kind[chosen];
     BSample s = lobe_sample(b, k, wo, v1, u2);
     if (s.pdf <= 0.0f || black(s.f)) return none();
-    const float pChosen = fd(sc[chosen], total);
+    const float pChosen = fd(m.sc[chosen], m.total);
     if (lobe_delta(k)) {
-        s.f = xmuls(s.f, w[chosen]);
+        s.f = xmuls(s.f, m.w[chosen]);
         s.pdf = fm(s.pdf, pChosen);
         return s;
     }
-    s.f = bsdf_eval(b, wo, s.wi);
-    s.pdf = bsdf_pdf(b, wo, s.wi);
+    s.f = bsdf_eval(b, m, wo, s.wi);
+    s.pdf = bsdf_pdf(b, m, wo, s.wi);
     if (s.pdf <= 0.0f) return none();
     return s;
 }

@@ -39,7 +39,9 @@ struct TrainBatchDev {
     const float4* records;        // 4 float4 per record (rbr_cache_record)
     const float4* targets;        // rgb + channel mask bits (w, as uint32)
     const uint32_t* count_ptr;
-    uint32_t count, cap;
+    const uint32_t* count2_ptr = nullptr;  // optional second list of *count2_ptr records starting at `split`
+    uint32_t split = 0;
+    uint32_t count, cap;                   // cap: records per list
     uint32_t batch;               // samples per step; sample j of step s reads pair perm(s*batch + j) % avail
     uint32_t step_index;
     uint32_t shuffle;             // 0: sample j reads pair j

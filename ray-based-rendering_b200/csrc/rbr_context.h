@@ -136,9 +136,10 @@ rbr_status cache_train_host(rbr_ctx* ctx, uint32_t n, const rbr_cache_record* re
 rbr_status cache_ensure_render(rbr_ctx* ctx, uint32_t paths, uint32_t train_cap);
 cudaError_t cache_launch_infer(rbr_ctx* ctx, const float4* records, uint32_t n, const uint32_t* n_ptr, float* rgb,
                                float4* path_rad, const float4* q_info, cudaStream_t stream);
-cudaError_t cache_launch_finalize(rbr_ctx* ctx, const float4* path_rad, const uint32_t* counters, int base_word,
-                                  int count_word, cudaStream_t stream);
-cudaError_t cache_launch_train_frame(rbr_ctx* ctx, const uint32_t* count_ptr, uint32_t frame, cudaStream_t stream);
+cudaError_t cache_launch_finalize(rbr_ctx* ctx, const float4* path_rad, const float4* t_aux, const uint32_t* counters,
+                                  int base_word, int count_word, uint32_t cap, cudaStream_t stream);
+cudaError_t cache_launch_train_frame(rbr_ctx* ctx, const uint32_t* count_ptr, const uint32_t* count2_ptr, uint32_t cap,
+                                     uint32_t frame, cudaStream_t stream);
 rbr_status render_cached(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_params* p, uint32_t frames, int train,
                          float* film_mean, float* film_m2, cudaStream_t stream);
 

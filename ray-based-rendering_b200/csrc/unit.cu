@@ -18,12 +18,13 @@ __global__ void k_bsdf_eval(MaterialDev m, uint32_t n, const float* wo, const fl
     if (i >= n) return;
     const Bsdf b = make_bsdf(m);
     const f3 o = ld3(wo + 3 * i), w = ld3(wi + 3 * i);
-    const f3 f = bsdf_eval(b, o, w);
+    const Mix mx = mixture(b, o);
+    const f3 f = bsdf_eval(b, mx, o, w);
     float* r = out + 6 * i;  // f[3], pdf, isDelta, type bits
     r[0] = f.x;
     r[1] = f.y;
     r[2] = f.z;
-    r[3] = bsdf_pdf(b, o, w);
+    r[3] = bsdf_pdf(b, mx, o, w);
     r[4] = bsdf_delta(b) ? 1.0f : 0.0f;
     r[5] = static_cast<float>(bsdf_type(b));
 }
@@ -32,7 +33,8 @@ __global__ void k_bsdf_sample(MaterialDev m, uint32_t n, const float* wo, const 
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const Bsdf b = make_bsdf(m);
-    const BSample s = bsdf_sample(b, ld3(wo + 3 * i), u[2 * i], u[2 * i + 1]);
+    const f3 o = ld3(wo + 3 * i);
+    const BSample s = bsdf_sample(b, mixture(b, o), o, u[2 * i], u[2 * i + 1]);
     float* r = out + 8 * i;  // wi[3], f[3], pdf, isDelta
     r[0] = s.wi.x;
     r[1] = s.wi.y;

@@ -58,3 +58,26 @@ def test_cache_beats_plain_at_equal_samples_on_ggx(ctx):
     r_plain, r_cache = relmse(plain, ref), relmse(cached, ref)
     assert r_cache < 0.7 * r_plain, (r_cache, r_plain)
     assert abs(cached.mean() / ref.mean() - 1.0) < 0.05
+
+
+def test_two_waves_in_flight_gather_the_same_paths(ctx):
+    """pt.streams 2 renders a cached frame as two half-image waves with their own query records
+    and training lists: every frame ends the same paths into the cache and gathers the same
+    training vertices as one wave at a time (only the order of the training list differs, so
+    the trained cache and the image agree statistically, not bit for bit)."""
+    s = small_ggx(96, 54)
+    ctx.upload(s)
+    out = {}
+    try:
+        for streams in (1, 2):
+            ctx.set_param("pt.streams", streams)
+            ctx.cache_create(train_paths=(96 * 54) // 8, seed=1)
+            img = cached_render(ctx, s.camera, 16, 16, 5)
+            info = ctx.cache_info()
+            out[streams] = (img, info.last_queries, info.last_train_records, info.optimiser_steps)
+    finally:
+        ctx.set_param("pt.streams", 2)
+    (a, qa, ta, sa), (b, qb, tb, sb) = out[1], out[2]
+    assert qa == qb and ta == tb and sa == sb == 16 * 4
+    assert np.isfinite(b).all() and (b >= 0).all()
+    assert abs(b.mean() / a.mean() - 1.0) < 0.05
