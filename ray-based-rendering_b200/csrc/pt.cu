@@ -478,8 +478,9 @@ __global__ void __launch_bounds__(kBlock, 8) k_shade(DeviceScene s, Wave w, Path
                 const LSample ls = light_sample(L, h.point, (l & 1) ? u.z : u.x, (l & 1) ? u.w : u.y);
                 if (ls.pdf > 0.0f && !black(ls.Li)) {
                     const f3 wiL = to_local(fr, ls.wi);
-                    const f3 f = bsdf_eval(bs, mx, wo, wiL);
-                    const float bpdf = bsdf_pdf(bs, mx, wo, wiL);
+                    f3 f;
+                    float bpdf;
+                    bsdf_eval_pdf(bs, mx, wo, wiL, f, bpdf);
                     if (!black(f)) {
                         spawn(h, ls.wi, so, sd);
                         stmax = fs(ls.dist, kEpsilon);

@@ -244,14 +244,15 @@ __device__ __forceinline__ float ggx_lambda(float alpha, f3 w) {
     const float tan2 = fd(omax(0.0f, fs(1.0f, cos2)), cos2);
     return fm(0.5f, fs(fq(fa(1.0f, fm(fm(alpha, alpha), tan2))), 1.0f));
 }
-__device__ __forceinline__ float ggx_G1(float alpha, f3 w) { return fd(1.0f, fa(1.0f, ggx_lambda(alpha, w))); }
-__device__ __forceinline__ float ggx_G(float alpha, f3 wo, f3 wi) {
-    return fd(1.0f, fa(fa(1.0f, ggx_lambda(alpha, wo)), ggx_lambda(alpha, wi)));
-}
-__device__ __forceinline__ float ggx_pdf(float alpha, f3 wo, f3 wh) {
+// GGXDistribution::pdf(wo, wh) = D(wh) G1(wo) |wo.wh| / |cos wo|, given D(wh), lambda(wo) and
+// wo.wh; G(wo, wi) = 1 / (1 + lambda(wo) + lambda(wi)).
+__device__ __forceinline__ float ggx_pdf(float D, float lambda_o, float dotOH, f3 wo) {
     const float cosO = fabsf(wo.z);
     if (cosO == 0.0f) return 0.0f;
-    return fd(fm(fm(ggx_D(alpha, wh), ggx_G1(alpha, wo)), fabsf(xdot(wo, wh))), cosO);
+    return fd(fm(fm(D, fd(1.0f, fa(1.0f, lambda_o))), fabsf(dotOH)), cosO);
+}
+__device__ __forceinline__ float ggx_G(float lambda_o, float lambda_i) {
+    return fd(1.0f, fa(fa(1.0f, lambda_o), lambda_i));
 }
 __device__ __forceinline__ f3 ggx_sample_wh(float alpha, f3 wo, float u1, float u2) {
     const bool flip = wo.z < 0.0f;
@@ -287,28 +288,26 @@ __device__ __forceinline__ BSample none() {
 }
 __device__ __forceinline__ bool same_hemi(f3 a, f3 b) { return fm(a.z, b.z) > 0.0f; }
 
-// MicrofacetReflectionBSDF
-__device__ __forceinline__ f3 ggxr_eval(const Bsdf& b, uint32_t k, f3 wo, f3 wi) {
-    if (!same_hemi(wo, wi)) return mk(0.0f, 0.0f, 0.0f);
+// MicrofacetReflectionBSDF: evaluate() and pdf() for one (wo, wi) together. Both take the same
+// half vector; D(wh) and lambda(wo) are computed once for both, with the operations and the
+// zero checks of each of the two (microfacet_bsdf.cpp), so the results are the same as two
+// separate calls.
+__device__ __forceinline__ void ggxr_eval_pdf(const Bsdf& b, uint32_t k, f3 wo, f3 wi, f3& f, float& pdf) {
+    f = mk(0.0f, 0.0f, 0.0f);
+    pdf = 0.0f;
+    if (!same_hemi(wo, wi)) return;
+    f3 wh = xadd(wo, wi);
+    if (wh.x == 0.0f && wh.y == 0.0f && wh.z == 0.0f) return;
+    wh = xnorm(wh);
+    if (wh.z < 0.0f) wh = xneg(wh);
     const float cosO = fabsf(wo.z), cosI = fabsf(wi.z);
-    if (cosO == 0.0f || cosI == 0.0f) return mk(0.0f, 0.0f, 0.0f);
-    f3 wh = xadd(wo, wi);
-    if (wh.x == 0.0f && wh.y == 0.0f && wh.z == 0.0f) return mk(0.0f, 0.0f, 0.0f);
-    wh = xnorm(wh);
-    if (wh.z < 0.0f) wh = xneg(wh);
-    const f3 F = lobe_fresnel(b, k, xdot(wo, wh));
-    return xmuls(xmul(mk(1.0f, 1.0f, 1.0f), F),
-                 fd(fm(ggx_D(b.alpha, wh), ggx_G(b.alpha, wo, wi)), fm(fm(4.0f, cosO), cosI)));
-}
-__device__ __forceinline__ float ggxr_pdf(const Bsdf& b, f3 wo, f3 wi) {
-    if (!same_hemi(wo, wi)) return 0.0f;
-    f3 wh = xadd(wo, wi);
-    if (wh.x == 0.0f && wh.y == 0.0f && wh.z == 0.0f) return 0.0f;
-    wh = xnorm(wh);
-    if (wh.z < 0.0f) wh = xneg(wh);
+    const float D = ggx_D(b.alpha, wh);
+    const float lo = ggx_lambda(b.alpha, wo);
     const float dotOH = xdot(wo, wh);
-    if (dotOH == 0.0f) return 0.0f;
-    return fd(ggx_pdf(b.alpha, wo, wh), fm(4.0f, fabsf(dotOH)));
+    if (dotOH != 0.0f) pdf = fd(ggx_pdf(D, lo, dotOH, wo), fm(4.0f, fabsf(dotOH)));
+    if (cosO == 0.0f || cosI == 0.0f) return;
+    const f3 F = lobe_fresnel(b, k, dotOH);
+    f = xmuls(xmul(mk(1.0f, 1.0f, 1.0f), F), fd(fm(D, ggx_G(lo, ggx_lambda(b.alpha, wi))), fm(fm(4.0f, cosO), cosI)));
 }
 __device__ __forceinline__ BSample ggxr_sample(const Bsdf& b, uint32_t k, f3 wo, float u1, float u2) {
     BSample r = none();
@@ -316,11 +315,13 @@ __device__ __forceinline__ BSample ggxr_sample(const Bsdf& b, uint32_t k, f3 wo,
     const f3 wh = ggx_sample_wh(b.alpha, wo, u1, u2);
     const f3 wi = xsub(xmuls(wh, fm(2.0f, xdot(wo, wh))), wo);
     if (!same_hemi(wo, wi)) return r;
-    const float p = ggxr_pdf(b, wo, wi);
+    f3 f;
+    float p;
+    ggxr_eval_pdf(b, k, wo, wi, f, p);
     if (p <= 0.0f) return r;
     r.wi = wi;
     r.pdf = p;
-    r.f = ggxr_eval(b, k, wo, wi);
+    r.f = f;
     return r;
 }
 
@@ -336,28 +337,25 @@ __device__ __forceinline__ bool ggxt_half(const Bsdf& b, f3 wo, f3 wi, f3& wh, f
     wh = h;
     return fm(h.z, wo.z) > 0.0f && xdot(wi, h) <= 0.0f;
 }
-__device__ __forceinline__ f3 ggxt_eval(const Bsdf& b, f3 wo, f3 wi) {
+// MicrofacetTransmissionBSDF: evaluate() and pdf() together, as for reflection.
+__device__ __forceinline__ void ggxt_eval_pdf(const Bsdf& b, f3 wo, f3 wi, f3& f, float& pdf) {
+    f = mk(0.0f, 0.0f, 0.0f);
+    pdf = 0.0f;
     f3 wh;
     float eta;
-    if (!ggxt_half(b, wo, wi, wh, eta)) return mk(0.0f, 0.0f, 0.0f);
+    if (!ggxt_half(b, wo, wi, wh, eta)) return;
     const float cosO = wo.z, cosI = wi.z;
     const float dotOH = xdot(wo, wh), dotIH = xdot(wi, wh);
-    const float F = fresnel_dielectric(wo.z > 0.0f ? dotOH : -dotOH, 1.0f, b.ior);
     const float denom = fa(dotOH, fm(eta, dotIH));
-    if (denom == 0.0f) return mk(0.0f, 0.0f, 0.0f);
-    const float value = fd(fm(fm(ggx_D(b.alpha, wh), ggx_G(b.alpha, wo, wi)), fabsf(fm(dotIH, dotOH))),
-                           fabsf(fm(fm(fm(cosI, cosO), denom), denom)));
-    return xmuls(b.base, fm(fs(1.0f, F), value));
-}
-__device__ __forceinline__ float ggxt_pdf(const Bsdf& b, f3 wo, f3 wi) {
-    f3 wh;
-    float eta;
-    if (!ggxt_half(b, wo, wi, wh, eta)) return 0.0f;
-    const float dotOH = xdot(wo, wh), dotIH = xdot(wi, wh);
-    const float denom = fa(dotOH, fm(eta, dotIH));
-    if (denom == 0.0f) return 0.0f;
+    if (denom == 0.0f) return;
+    const float D = ggx_D(b.alpha, wh);
+    const float lo = ggx_lambda(b.alpha, wo);
     const float dwh = fd(fabsf(fm(fm(eta, eta), dotIH)), fm(denom, denom));
-    return fm(ggx_pdf(b.alpha, wo, wh), dwh);
+    pdf = fm(ggx_pdf(D, lo, dotOH, wo), dwh);
+    const float F = fresnel_dielectric(wo.z > 0.0f ? dotOH : -dotOH, 1.0f, b.ior);
+    const float value = fd(fm(fm(D, ggx_G(lo, ggx_lambda(b.alpha, wi))), fabsf(fm(dotIH, dotOH))),
+                           fabsf(fm(fm(fm(cosI, cosO), denom), denom)));
+    f = xmuls(b.base, fm(fs(1.0f, F), value));
 }
 __device__ __forceinline__ BSample ggxt_sample(const Bsdf& b, f3 wo, float u1, float u2) {
     BSample r = none();
@@ -372,11 +370,13 @@ __device__ __forceinline__ BSample ggxt_sample(const Bsdf& b, f3 wo, float u1, f
     const float cosT = fq(fs(1.0f, sin2T));
     const f3 wi = xsub(xmuls(wh, fs(fm(etaRatio, dotOH), cosT)), xmuls(wo, etaRatio));
     if (same_hemi(wo, wi) || wi.z == 0.0f) return r;
-    const float p = ggxt_pdf(b, wo, wi);
+    f3 f;
+    float p;
+    ggxt_eval_pdf(b, wo, wi, f, p);
     if (p <= 0.0f) return r;
     r.wi = wi;
     r.pdf = p;
-    r.f = ggxt_eval(b, wo, wi);
+    r.f = f;
     return r;
 }
 
@@ -420,22 +420,21 @@ __device__ __forceinline__ BSample st_sample(const Bsdf& b, uint32_t k, f3 wo) {
     return r;
 }
 
-__device__ __forceinline__ f3 lobe_eval(const Bsdf& b, uint32_t k, f3 wo, f3 wi) {
+// evaluate() and pdf() of a non-delta lobe (delta lobes give 0 and 0)
+__device__ __forceinline__ void lobe_eval_pdf(const Bsdf& b, uint32_t k, f3 wo, f3 wi, f3& f, float& pdf) {
     switch (k) {
-        case kLambert: return same_hemi(wo, wi) ? xmuls(b.base, kInvPi) : mk(0.0f, 0.0f, 0.0f);
+        case kLambert: {
+            const bool same = same_hemi(wo, wi);
+            f = same ? xmuls(b.base, kInvPi) : mk(0.0f, 0.0f, 0.0f);
+            pdf = same ? fm(fabsf(wi.z), kInvPi) : 0.0f;
+            return;
+        }
         case kCondGGX:
-        case kDielGGX: return ggxr_eval(b, k, wo, wi);
-        case kTransGGX: return ggxt_eval(b, wo, wi);
-        default: return mk(0.0f, 0.0f, 0.0f);
-    }
-}
-__device__ __forceinline__ float lobe_pdf(const Bsdf& b, uint32_t k, f3 wo, f3 wi) {
-    switch (k) {
-        case kLambert: return same_hemi(wo, wi) ? fm(fabsf(wi.z), kInvPi) : 0.0f;
-        case kCondGGX:
-        case kDielGGX: return ggxr_pdf(b, wo, wi);
-        case kTransGGX: return ggxt_pdf(b, wo, wi);
-        default: return 0.0f;
+        case kDielGGX: ggxr_eval_pdf(b, k, wo, wi, f, pdf); return;
+        case kTransGGX: ggxt_eval_pdf(b, wo, wi, f, pdf); return;
+        default:
+            f = mk(0.0f, 0.0f, 0.0f);
+            pdf = 0.0f;
     }
 }
 __device__ __forceinline__ BSample lobe_sample(const Bsdf& b, uint32_t k, f3 wo, float u1, float u2) {
@@ -480,22 +479,20 @@ __device__ __forceinline__ Mix mixture(const Bsdf& b, f3 wo) {
     }
     return m;
 }
-__device__ __forceinline__ f3 bsdf_eval(const Bsdf& b, const Mix& m, f3 wo, f3 wi) {
-    f3 f = mk(0.0f, 0.0f, 0.0f);
-    for (int i = 0; i < b.n; ++i) {
-        if (lobe_delta(b.kind[i])) continue;
-        f = xadd(f, xmuls(lobe_eval(b, b.kind[i], wo, wi), m.w[i]));
-    }
-    return f;
-}
-__device__ __forceinline__ float bsdf_pdf(const Bsdf& b, const Mix& m, f3 wo, f3 wi) {
-    if (m.total <= 0.0f) return 0.0f;
+// MixtureBSDF::evaluate and MixtureBSDF::pdf for one (wo, wi), in one pass over the lobes:
+// f = sum of w_i f_i, pdf = (sum of score_i pdf_i) / total over the non-delta lobes.
+__device__ __forceinline__ void bsdf_eval_pdf(const Bsdf& b, const Mix& m, f3 wo, f3 wi, f3& f, float& pdf) {
+    f = mk(0.0f, 0.0f, 0.0f);
     float p = 0.0f;
     for (int i = 0; i < b.n; ++i) {
         if (lobe_delta(b.kind[i])) continue;
-        p = fa(p, fm(m.sc[i], lobe_pdf(b, b.kind[i], wo, wi)));
+        f3 fl;
+        float pl;
+        lobe_eval_pdf(b, b.kind[i], wo, wi, fl, pl);
+        f = xadd(f, xmuls(fl, m.w[i]));
+        p = fa(p, fm(m.sc[i], pl));
     }
-    return fd(p, m.total);
+    pdf = m.total <= 0.0f ? 0.0f : fd(p, m.total);
 }
 __device__ __forceinline__ BSample bsdf_sample(const Bsdf& b, const Mix& m, f3 wo, float u1, float u2) {
     if (m.total <= 0.0f) return none();
@@ -520,8 +517,7 @@ __device__ __forceinline__ BSample bsdf_sample(const Bsdf& b, const Mix& m, f3 w
         s.pdf = fm(s.pdf, pChosen);
         return s;
     }
-    s.f = bsdf_eval(b, m, wo, s.wi);
-    s.pdf = bsdf_pdf(b, m, wo, s.wi);
+    bsdf_eval_pdf(b, m, wo, s.wi, s.f, s.pdf);
     if (s.pdf <= 0.0f) return none();
     return s;
 }

@@ -18,13 +18,14 @@ __global__ void k_bsdf_eval(MaterialDev m, uint32_t n, const float* wo, const fl
     if (i >= n) return;
     const Bsdf b = make_bsdf(m);
     const f3 o = ld3(wo + 3 * i), w = ld3(wi + 3 * i);
-    const Mix mx = mixture(b, o);
-    const f3 f = bsdf_eval(b, mx, o, w);
+    f3 f;
+    float pdf;
+    bsdf_eval_pdf(b, mixture(b, o), o, w, f, pdf);
     float* r = out + 6 * i;  // f[3], pdf, isDelta, type bits
     r[0] = f.x;
     r[1] = f.y;
     r[2] = f.z;
-    r[3] = bsdf_pdf(b, mx, o, w);
+    r[3] = pdf;
     r[4] = bsdf_delta(b) ? 1.0f : 0.0f;
     r[5] = static_cast<float>(bsdf_type(b));
 }
