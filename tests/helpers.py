@@ -76,6 +76,16 @@ def bsdf_inputs(n, seed):
     return np.ascontiguousarray(wo, F32), np.ascontiguousarray(wi, F32), np.ascontiguousarray(u, F32)
 
 
+def edge_directions():
+    """(wo, wi) pairs on which the checks inside BSDF evaluate() and pdf() decide: wi = -wo,
+    a direction on the horizon, normal incidence into either hemisphere, wi = wo."""
+    wo = [[0.6, 0.0, 0.8], [0.0, 0.0, 1.0], [1.0, 0.0, 0.0], [0.6, 0.0, -0.8], [0.0, 0.6, 0.8], [0.28, 0.96, 0.0],
+          [0.0, 0.0, -1.0], [0.8, 0.0, 0.6]]
+    wi = [[-0.6, 0.0, -0.8], [1.0, 0.0, 0.0], [0.0, 0.0, 1.0], [-0.6, 0.0, 0.8], [0.0, -0.6, -0.8], [0.0, 0.0, -1.0],
+          [0.0, 0.0, -1.0], [0.8, 0.0, 0.6]]
+    return np.ascontiguousarray(wo, F32), np.ascontiguousarray(wi, F32)
+
+
 def lights():
     out = []
     for (t, pos, u, v, col, inten) in [

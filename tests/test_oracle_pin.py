@@ -24,6 +24,15 @@ def test_bsdf_eval_and_sample_bit_exact(restatement, reference, name, mat):
     assert np.array_equal(bits(s1), bits(s2))
 
 
+@pytest.mark.parametrize("name,mat", helpers.material_grid(), ids=[n for n, _ in helpers.material_grid()])
+def test_bsdf_eval_edge_directions(restatement, reference, name, mat):
+    """The restatement's evaluate() and pdf() on the direction pairs where their checks decide."""
+    wo, wi = helpers.edge_directions()
+    f1, p1, _ = restatement.bsdf_eval(mat, wo, wi)
+    f2, p2, _ = reference.bsdf_eval(mat, wo, wi)
+    assert np.array_equal(bits(f1), bits(f2)) and np.array_equal(bits(p1), bits(p2))
+
+
 def test_light_samples_bit_exact(restatement, reference):
     p, u = helpers.light_points(4096, seed=4)
     for l in helpers.lights():

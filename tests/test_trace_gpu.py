@@ -59,8 +59,9 @@ def test_closest_and_any_match_bruteforce(kctx, restatement, ns, nt, plane, seed
 
 
 def test_chunked_host_pipeline_matches(kctx, restatement):
-    """rbr_trace_host in chunks of 1,000 rays over two streams (trace.host_chunk) gives the
-    answers of one piece, with a last chunk shorter than the others."""
+    """rbr_trace_host in chunks of 500 rays (trace.host_chunk: uploads, traversals and
+    downloads on three streams; more chunks than the pipeline's event ring) gives the answers
+    of one piece, with a last chunk shorter than the others."""
     ctx = kctx
     w = scenes.random_world(400, 1500, False, seed=9)
     rays = scenes.random_test_rays(6500, seed=109)
@@ -69,7 +70,7 @@ def test_chunked_host_pipeline_matches(kctx, restatement):
     want = restatement.trace_closest(h, rays)
     chunk = ctx.get_param("trace.host_chunk")
     try:
-        for c in (1000, 0):
+        for c in (500, 0):
             ctx.set_param("trace.host_chunk", c)
             assert_same_closest(ctx.trace_host(rays), want)
             assert np.array_equal(ctx.trace_host(rays, any_hit=True), restatement.trace_any(h, rays))

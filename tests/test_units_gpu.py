@@ -30,6 +30,17 @@ def test_bsdf_eval_pdf_bit_exact(ctx, reference, name, mat):
     assert (got[:, 4] == info[0]).all() and (got[:, 5] == info[1]).all(), "isDelta / type bits"
 
 
+@pytest.mark.parametrize("name,mat", GRID, ids=[n for n, _ in GRID])
+def test_bsdf_eval_pdf_edge_directions(ctx, reference, name, mat):
+    """Direction pairs where the checks inside evaluate() and pdf() decide: wi = -wo (the
+    reflection half vector vanishes), a direction on the horizon (cos = 0), normal incidence
+    into both hemispheres, wi = wo. The one-pass value and pdf equal the reference's two calls."""
+    wo, wi = helpers.edge_directions()
+    got = ctx.bsdf_eval(mat, wo, wi)
+    f, pdf, _ = reference.bsdf_eval(mat, wo, wi)
+    assert np.array_equal(bits(got[:, :3]), bits(f)) and np.array_equal(bits(got[:, 3]), bits(pdf))
+
+
 def check_samples(ctx_or_none, reference, mat, wo, got, want, min_close=0.99):
     """Well-posed comparison of BSDF::sample outputs (8 floats each) from two implementations
     whose sin/cos may differ in the last bit:
