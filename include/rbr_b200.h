@@ -237,7 +237,7 @@ rbr_status rbr_scene_stats_get(const rbr_ctx* ctx, rbr_scene_stats* out);
  *                          1 by direction octant, then origin cell of 512^3; 2 octant, then cell
  *                          of 64^3; 3 cell of 64^3, then octant
  *   "trace.host_chunk"     rbr_trace_host: rays per chunk of its upload / trace / download
- *                          pipeline, one stream per stage (default 2^20; 0: one piece)
+ *                          pipeline over two streams (default 2^20; 0: one piece)
  *   "pt.wave_paths"        camera samples per path-tracer wave (default 2^23)
  *   "pt.streams"           rbr_render: waves in flight, 1 or 2 (default 2: waves alternate
  *                          between two sets of path buffers on two streams; an image that

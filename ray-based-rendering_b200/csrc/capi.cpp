@@ -50,17 +50,6 @@ rbr_status ensure_side_stream(rbr_ctx* ctx) {
     return e == cudaSuccess ? RBR_OK : cuda_fail(ctx, e, "second stream");
 }
 
-rbr_status ensure_copy_pipeline(rbr_ctx* ctx) {
-    rbr_status st = ensure_side_stream(ctx);
-    if (st != RBR_OK) return st;
-    cudaError_t e = cudaSuccess;
-    if (!ctx->d2h_stream) e = cudaStreamCreateWithFlags(&ctx->d2h_stream, cudaStreamNonBlocking);
-    for (int a = 0; a < 2 && e == cudaSuccess; ++a)
-        for (int i = 0; i < kPipeEvents && e == cudaSuccess; ++i)
-            if (!ctx->ev_pipe[a][i]) e = cudaEventCreateWithFlags(&ctx->ev_pipe[a][i], cudaEventDisableTiming);
-    return e == cudaSuccess ? RBR_OK : cuda_fail(ctx, e, "copy pipeline streams");
-}
-
 // Reads (and clears) the device error word after the work on `stream` has finished.
 rbr_status check_device_error(rbr_ctx* ctx, cudaStream_t stream) {
     int h = 0;
@@ -149,16 +138,13 @@ void rbr_ctx_destroy(rbr_ctx* ctx) {
     release(ctx->stage_in);
     release(ctx->stage_out);
     release(ctx->sort_buf);
+    release(ctx->sort_buf2);
     if (ctx->d_error) cudaFree(ctx->d_error);
     if (ctx->d_cursors) cudaFree(ctx->d_cursors);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
     if (ctx->ev_stop) cudaEventDestroy(ctx->ev_stop);
     if (ctx->side_stream) cudaStreamDestroy(ctx->side_stream);
-    if (ctx->d2h_stream) cudaStreamDestroy(ctx->d2h_stream);
-    for (auto& row : ctx->ev_pipe)
-        for (cudaEvent_t ev : row)
-            if (ev) cudaEventDestroy(ev);
     if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
     if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
     delete ctx;
@@ -272,40 +258,33 @@ rbr_status rbr_trace_host(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any
     if ((st = ensure(ctx, ctx->stage_in, in_bytes, "ray staging")) != RBR_OK) return st;
     if ((st = ensure(ctx, ctx->stage_out, out_bytes, "hit staging")) != RBR_OK) return st;
     cudaStream_t s = ctx->stream;
-    // A three-stage pipeline over chunks: the context's stream uploads every chunk back to
-    // back, the side stream traces each chunk once its upload has landed, a third stream
-    // downloads each chunk's answers once traced. The two copy directions and the SMs work on
-    // different chunks at the same time.
+    // Chunks alternate between two streams, so that the upload of one chunk, the traversal
+    // of another and the download of a third overlap (copies in each direction and kernels
+    // run on separate engines).
     const uint32_t chunk = ctx->trace_host_chunk && n > ctx->trace_host_chunk ? ctx->trace_host_chunk : n;
-    const bool piped = chunk < n;
-    if (piped && (st = ensure_copy_pipeline(ctx)) != RBR_OK) return st;
+    const bool two = chunk < n;
+    if (two && (st = ensure_side_stream(ctx)) != RBR_OK) return st;
     const size_t osz = any_hit ? 1 : sizeof(rbr_hit);
-    const cudaStream_t up = s, tr = piped ? ctx->side_stream : s, down = piped ? ctx->d2h_stream : s;
     cudaError_t e = cudaSuccess;
-    if (piped) {
+    if (two) {
         e = cudaEventRecord(ctx->ev_fork, s);
-        if (e == cudaSuccess) e = cudaStreamWaitEvent(tr, ctx->ev_fork, 0);
-        if (e == cudaSuccess) e = cudaStreamWaitEvent(down, ctx->ev_fork, 0);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->side_stream, ctx->ev_fork, 0);
     }
     uint32_t k = 0;
     for (uint32_t off = 0; off < n && e == cudaSuccess; off += chunk, ++k) {
         const uint32_t m = std::min(chunk, n - off);
+        const cudaStream_t cs = (k & 1) ? ctx->side_stream : s;
         rbr_ray* din = static_cast<rbr_ray*>(ctx->stage_in.ptr) + off;
         char* dout = static_cast<char*>(ctx->stage_out.ptr) + size_t(off) * osz;
-        cudaEvent_t ev_up = ctx->ev_pipe[0][k % kPipeEvents], ev_tr = ctx->ev_pipe[1][k % kPipeEvents];
-        e = cudaMemcpyAsync(din, rays + off, size_t(m) * sizeof(rbr_ray), cudaMemcpyHostToDevice, up);
-        if (e == cudaSuccess && piped) e = cudaEventRecord(ev_up, up);
-        if (e == cudaSuccess && piped) e = cudaStreamWaitEvent(tr, ev_up, 0);
+        e = cudaMemcpyAsync(din, rays + off, size_t(m) * sizeof(rbr_ray), cudaMemcpyHostToDevice, cs);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "ray upload");
-        e = launch_trace(ctx, din, m, any_hit, dout, tr);
-        if (e == cudaSuccess && piped) e = cudaEventRecord(ev_tr, tr);
-        if (e == cudaSuccess && piped) e = cudaStreamWaitEvent(down, ev_tr, 0);
+        e = launch_trace(ctx, din, m, any_hit, dout, cs, static_cast<int>(k & 1));
         if (e != cudaSuccess) return cuda_fail(ctx, e, "trace launch");
-        e = cudaMemcpyAsync(static_cast<char*>(out) + size_t(off) * osz, dout, size_t(m) * osz, cudaMemcpyDeviceToHost, down);
+        e = cudaMemcpyAsync(static_cast<char*>(out) + size_t(off) * osz, dout, size_t(m) * osz, cudaMemcpyDeviceToHost, cs);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "hit download");
     }
-    if (e == cudaSuccess && piped) {
-        e = cudaEventRecord(ctx->ev_join, down);
+    if (e == cudaSuccess && two) {
+        e = cudaEventRecord(ctx->ev_join, ctx->side_stream);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(s, ctx->ev_join, 0);
     }
     if (e != cudaSuccess) return cuda_fail(ctx, e, "trace pipeline");

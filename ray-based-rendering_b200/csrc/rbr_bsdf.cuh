@@ -147,10 +147,18 @@ struct Bsdf {
     float alpha;       // GGXDistribution alpha: max(roughness^2, 1e-3)
     bool has_sub;      // substrate Fresnel set (dielectric interface)
     int n;
-    uint32_t kind[4];
-    float weight[4];
-    bool substrate[4];
+    // Lobe i (i < n): kind in bits 4i..4i+3 of `kinds`, substrate flag in bit i of `subs`,
+    // weight wt[i]. Packed in scalars so that no lobe list is indexed in local memory.
+    uint32_t kinds, subs;
+    float wt0, wt1, wt2, wt3;
 };
+
+// element i (0..3) of four scalars, without an indexed array
+__device__ __forceinline__ float pick4(float a0, float a1, float a2, float a3, int i) {
+    return i == 0 ? a0 : i == 1 ? a1 : i == 2 ? a2 : a3;
+}
+__device__ __forceinline__ uint32_t kind_of(const Bsdf& b, int i) { return (b.kinds >> (4 * i)) & 0xFu; }
+__device__ __forceinline__ float weight_of(const Bsdf& b, int i) { return pick4(b.wt0, b.wt1, b.wt2, b.wt3, i); }
 
 __device__ __forceinline__ bool lobe_delta(uint32_t k) { return k == kCondSpec || k == kDielSpec || k == kTransSpec || k == kPassSpec; }
 
@@ -168,9 +176,12 @@ __device__ __forceinline__ uint32_t lobe_type(uint32_t k) {
 
 __device__ __forceinline__ void add_lobe(Bsdf& b, uint32_t kind, float w, bool substrate) {
     if (w <= 0.0f || b.n >= 4) return;
-    b.kind[b.n] = kind;
-    b.weight[b.n] = w;
-    b.substrate[b.n] = substrate;
+    b.kinds |= kind << (4 * b.n);
+    b.subs |= (substrate ? 1u : 0u) << b.n;
+    b.wt0 = b.n == 0 ? w : b.wt0;
+    b.wt1 = b.n == 1 ? w : b.wt1;
+    b.wt2 = b.n == 2 ? w : b.wt2;
+    b.wt3 = b.n == 3 ? w : b.wt3;
     ++b.n;
 }
 
@@ -182,6 +193,8 @@ __device__ __forceinline__ Bsdf make_bsdf(const MaterialDev& m) {
     b.alpha = omax(fm(m.roughness, m.roughness), 1e-3f);
     b.has_sub = false;
     b.n = 0;
+    b.kinds = b.subs = 0;
+    b.wt0 = b.wt1 = b.wt2 = b.wt3 = 0.0f;
     const float met = oclamp(m.metallic, 0.0f, 1.0f);
     const float t = oclamp(m.transmission, 0.0f, 1.0f);
     const float diel = fs(1.0f, met);
@@ -206,7 +219,7 @@ __device__ __forceinline__ Bsdf make_bsdf(const MaterialDev& m) {
 __device__ __forceinline__ bool bsdf_delta(const Bsdf& b) {
     if (b.n == 0) return false;
     for (int i = 0; i < b.n; ++i)
-        if (!lobe_delta(b.kind[i])) return false;
+        if (!lobe_delta(kind_of(b, i))) return false;
     return true;
 }
 
@@ -459,23 +472,34 @@ __device__ __forceinline__ BSample lobe_sample(const Bsdf& b, uint32_t k, f3 wo,
 
 // MixtureBSDF
 __device__ __forceinline__ float eff_weight(const Bsdf& b, int i, f3 wo) {
-    if (!b.substrate[i]) return b.weight[i];
-    return fm(b.weight[i], omax(0.0f, fs(1.0f, fresnel_dielectric(wo.z, 1.0f, b.ior))));
+    if (!((b.subs >> i) & 1u)) return weight_of(b, i);
+    return fm(weight_of(b, i), omax(0.0f, fs(1.0f, fresnel_dielectric(wo.z, 1.0f, b.ior))));
 }
 // MixtureBSDF::selection: per-lobe effective weights and sampling scores. They depend on wo
 // only, so a vertex computes them once (mixture) and every evaluation, pdf and sample of that
 // vertex reuses them; the values are the ones each reference call recomputes.
 struct Mix {
-    float w[4], sc[4];
+    float w0, w1, w2, w3;      // effective weights
+    float sc0, sc1, sc2, sc3;  // sampling scores
     float total;
 };
+__device__ __forceinline__ float mix_w(const Mix& m, int i) { return pick4(m.w0, m.w1, m.w2, m.w3, i); }
+__device__ __forceinline__ float mix_sc(const Mix& m, int i) { return pick4(m.sc0, m.sc1, m.sc2, m.sc3, i); }
 __device__ __forceinline__ Mix mixture(const Bsdf& b, f3 wo) {
     Mix m;
+    m.w0 = m.w1 = m.w2 = m.w3 = 0.0f;
+    m.sc0 = m.sc1 = m.sc2 = m.sc3 = 0.0f;
     m.total = 0.0f;
-    for (int i = 0; i < b.n; ++i) {
-        m.w[i] = eff_weight(b, i, wo);
-        m.sc[i] = fm(m.w[i], maxc(lobe_rho(b, b.kind[i], wo)));
-        m.total = fa(m.total, m.sc[i]);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        if (i >= b.n) break;
+        const float w = eff_weight(b, i, wo);
+        const float sc = fm(w, maxc(lobe_rho(b, kind_of(b, i), wo)));
+        if (i == 0) m.w0 = w, m.sc0 = sc;
+        if (i == 1) m.w1 = w, m.sc1 = sc;
+        if (i == 2) m.w2 = w, m.sc2 = sc;
+        if (i == 3) m.w3 = w, m.sc3 = sc;
+        m.total = fa(m.total, sc);
     }
     return m;
 }
@@ -485,12 +509,13 @@ __device__ __forceinline__ void bsdf_eval_pdf(const Bsdf& b, const Mix& m, f3 wo
     f = mk(0.0f, 0.0f, 0.0f);
     float p = 0.0f;
     for (int i = 0; i < b.n; ++i) {
-        if (lobe_delta(b.kind[i])) continue;
+        const uint32_t k = kind_of(b, i);
+        if (lobe_delta(k)) continue;
         f3 fl;
         float pl;
-        lobe_eval_pdf(b, b.kind[i], wo, wi, fl, pl);
-        f = xadd(f, xmuls(fl, m.w[i]));
-        p = fa(p, fm(m.sc[i], pl));
+        lobe_eval_pdf(b, k, wo, wi, fl, pl);
+        f = xadd(f, xmuls(fl, mix_w(m, i)));
+        p = fa(p, fm(mix_sc(m, i), pl));
     }
     pdf = m.total <= 0.0f ? 0.0f : fd(p, m.total);
 }
@@ -499,21 +524,23 @@ __device__ __forceinline__ BSample bsdf_sample(const Bsdf& b, const Mix& m, f3 w
     float u = fm(u1, m.total);
     int chosen = b.n - 1;
     for (int i = 0; i < b.n; ++i) {
-        if (m.sc[i] <= 0.0f) continue;
-        if (u < m.sc[i] || i + 1 == b.n) {
+        const float sc = mix_sc(m, i);
+        if (sc <= 0.0f) continue;
+        if (u < sc || i + 1 == b.n) {
             chosen = i;
             break;
         }
-        u = fs(u, m.sc[i]);
+        u = fs(u, sc);
     }
-    if (m.sc[chosen] <= 0.0f) return none();
-    const float v1 = omin(fd(u, m.sc[chosen]), 0.99999994f);
-    const uint32_t k = b.kind[chosen];
+    const float sc = mix_sc(m, chosen);
+    if (sc <= 0.0f) return none();
+    const float v1 = omin(fd(u, sc), 0.99999994f);
+    const uint32_t k = kind_of(b, chosen);
     BSample s = lobe_sample(b, k, wo, v1, u2);
     if (s.pdf <= 0.0f || black(s.f)) return none();
-    const float pChosen = fd(m.sc[chosen], m.total);
+    const float pChosen = fd(sc, m.total);
     if (lobe_delta(k)) {
-        s.f = xmuls(s.f, m.w[chosen]);
+        s.f = xmuls(s.f, mix_w(m, chosen));
         s.pdf = fm(s.pdf, pChosen);
         return s;
     }
@@ -523,7 +550,7 @@ __device__ __forceinline__ BSample bsdf_sample(const Bsdf& b, const Mix& m, f3 w
 }
 __device__ __forceinline__ uint32_t bsdf_type(const Bsdf& b) {
     uint32_t t = 0;
-    for (int i = 0; i < b.n; ++i) t |= lobe_type(b.kind[i]);
+    for (int i = 0; i < b.n; ++i) t |= lobe_type(kind_of(b, i));
     return t;
 }
 

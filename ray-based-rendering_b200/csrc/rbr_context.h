@@ -20,8 +20,6 @@ struct DevBuf {
 };
 
 // Path-tracer working set (sized for one wave of paths).
-constexpr int kPipeEvents = 8;  // event ring of the rbr_trace_host pipeline
-
 struct PathBuffers {
     uint32_t capacity = 0;      // paths per wave
     uint32_t shadow_capacity = 0;
@@ -62,6 +60,7 @@ struct rbr_ctx {
     int trace_min_blocks = 10;     // kernel 0: register budget for 8, 10 or 12 resident blocks per SM
     int trace_order = 0;           // kernel 0: 0 rays in the given order, 1 sorted by direction octant and origin
     rbr::DevBuf sort_buf;          // keys, permutation and radix-sort scratch of trace_order 1
+    rbr::DevBuf sort_buf2;         // the same for the second stream of a chunked rbr_trace_host
     uint32_t trace_host_chunk = 1u << 20;  // rbr_trace_host: rays per pipelined chunk (0: one piece)
     uint32_t pt_wave_paths = 1u << 23;
     // path tracer
@@ -71,8 +70,6 @@ struct rbr_ctx {
     bool pt_last_two = false;              // the last rbr_render used pt2
     cudaStream_t side_stream = nullptr;    // stream of the second wave
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-    cudaStream_t d2h_stream = nullptr;     // downloads of the rbr_trace_host pipeline
-    cudaEvent_t ev_pipe[2][rbr::kPipeEvents] = {};  // per chunk (ring): upload done, trace done
     rbr::DevBuf pt_seg_of;  // packed waves: segment of each path
     rbr::DevBuf pt_seg_of2;  // the same for the second wave in flight (pt2)
     uint32_t pt_generation = 0;  // incremented whenever a path buffer set or segment index is reallocated
@@ -113,11 +110,11 @@ rbr_status autotune_trace(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any
 constexpr int kCursorRing = 64;
 // Launches a ray query with the context's chosen kernel (closest hit into rbr_hit[n] or any
 // hit into uint8_t[n]).
-cudaError_t launch_trace(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any_hit, void* out, cudaStream_t stream);
+// slot 0 or 1: which sort scratch a sorted launch uses (launches in flight on two streams).
+cudaError_t launch_trace(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any_hit, void* out, cudaStream_t stream,
+                         int slot = 0);
 // Creates the context's second stream and its fork/join events on first use.
 rbr_status ensure_side_stream(rbr_ctx* ctx);
-// The same plus the download stream and the event ring of the rbr_trace_host pipeline.
-rbr_status ensure_copy_pipeline(rbr_ctx* ctx);
 
 // path tracer (pt.cu)
 rbr_status render(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_params* p, float* film_mean, float* film_m2,

@@ -454,10 +454,11 @@ static cudaError_t sort_rays(rbr_ctx* ctx, DevBuf& sort_buf, const rbr_ray* rays
     return e;
 }
 
-cudaError_t launch_trace(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any_hit, void* out, cudaStream_t stream) {
+cudaError_t launch_trace(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any_hit, void* out, cudaStream_t stream,
+                         int slot) {
     if (ctx->trace_kernel == 0 && ctx->trace_order != 0 && n > 0) {
         const uint32_t* perm = nullptr;
-        cudaError_t e = sort_rays(ctx, ctx->sort_buf, rays, n, &perm, stream);
+        cudaError_t e = sort_rays(ctx, slot ? ctx->sort_buf2 : ctx->sort_buf, rays, n, &perm, stream);
         if (e != cudaSuccess) return e;
         const uint32_t blocks = (n + kTraceBlock - 1) / kTraceBlock;
         const auto* r = reinterpret_cast<const float4*>(rays);

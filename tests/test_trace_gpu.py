@@ -59,9 +59,8 @@ def test_closest_and_any_match_bruteforce(kctx, restatement, ns, nt, plane, seed
 
 
 def test_chunked_host_pipeline_matches(kctx, restatement):
-    """rbr_trace_host in chunks of 500 rays (trace.host_chunk: uploads, traversals and
-    downloads on three streams; more chunks than the pipeline's event ring) gives the answers
-    of one piece, with a last chunk shorter than the others."""
+    """rbr_trace_host in chunks of 500 rays over two streams (trace.host_chunk) gives the
+    answers of one piece, with a last chunk shorter than the others."""
     ctx = kctx
     w = scenes.random_world(400, 1500, False, seed=9)
     rays = scenes.random_test_rays(6500, seed=109)
