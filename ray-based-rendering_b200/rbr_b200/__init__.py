@@ -273,9 +273,13 @@ class Context:
         self._check(self.lib.rbr_render(self.h, C.byref(camera), C.byref(params), C.c_void_p(film_mean_ptr),
                                         C.c_void_p(film_m2_ptr or None), C.c_void_p(stream)))
 
-    def render_host(self, camera, params, second_moment: bool = False):
+    def render_host(self, camera, params, second_moment: bool = False, out: np.ndarray | None = None):
+        """Renders into host memory: `out` (float32, H x W x 3, e.g. a view of pinned memory) or a
+        new array."""
         W, H = camera.width, camera.height
-        mean = np.zeros((H, W, 3), np.float32)
+        if out is not None and (out.dtype != np.float32 or out.size != H * W * 3 or not out.flags.c_contiguous):
+            raise ValueError("out must be a C-contiguous float32 array of H x W x 3")
+        mean = out.reshape(H, W, 3) if out is not None else np.zeros((H, W, 3), np.float32)
         m2 = np.zeros((H, W, 3), np.float32) if second_moment else None
         if second_moment:
             params.flags |= abi.RBR_RENDER_SECOND_MOMENT
