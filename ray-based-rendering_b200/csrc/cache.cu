@@ -594,7 +594,31 @@ __global__ void k_rc_adam_grid(AdamDev a, float2* master, float2* m, float2* v, 
                                const float* scalars) {
     const float c1 = scalars[kRcBias], c2 = scalars[kRcBias + 1];
     if (c1 == 0.0f) return;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    // Four entries per thread and pass, their gradients loaded together (two 16-byte loads), so
+    // that the scan of the (mostly untouched) gradient array keeps several loads in flight.
+    const uint32_t quads = count / 4;
+    const float4* g4 = reinterpret_cast<const float4*>(grad);
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < quads; q += gridDim.x * blockDim.x) {
+        const float4 ga = g4[2 * q], gb = g4[2 * q + 1];
+        const float2 gs[4] = {make_float2(ga.x, ga.y), make_float2(ga.z, ga.w), make_float2(gb.x, gb.y),
+                              make_float2(gb.z, gb.w)};
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const float2 g = gs[e];
+            if (g.x == 0.0f && g.y == 0.0f) continue;
+            const uint32_t i = 4 * q + e;
+            grad[i] = make_float2(0.0f, 0.0f);
+            float2 mi = m[i], vi = v[i], p = master[i];
+            p.x = adam_update(p.x, mi.x, vi.x, g.x, a, c1, c2);
+            p.y = adam_update(p.y, mi.y, vi.y, g.y, a, c1, c2);
+            m[i] = mi;
+            v[i] = vi;
+            master[i] = p;
+            h[i] = __floats2half2_rn(p.x, p.y);
+        }
+    }
+    // entries past the last full group of four
+    for (uint32_t i = 4 * quads + blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
         const float2 g = grad[i];
         if (g.x == 0.0f && g.y == 0.0f) continue;
         grad[i] = make_float2(0.0f, 0.0f);
