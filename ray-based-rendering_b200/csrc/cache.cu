@@ -755,8 +755,8 @@ size_t grid_entries(const CacheState& cs) { return size_t(kRcLevels) * cs.table;
 // --------------------------------------------------------------------------------------------
 // Host side
 // --------------------------------------------------------------------------------------------
-void cache_destroy(rbr_ctx* ctx) {
-    CacheState& cs = ctx->cache;
+// The cache's parameters and optimiser state.
+static void free_cache_params(CacheState& cs) {
     free_dev(cs.grid_h);
     free_dev(cs.grid_master);
     free_dev(cs.grid_m);
@@ -765,13 +765,18 @@ void cache_destroy(rbr_ctx* ctx) {
     free_dev(cs.w_bf16);
     free_dev(cs.w_master);
     free_dev(cs.scalars);
-    free_dev(cs.q_rec);
+    cs.ready = false;
+}
+
+void cache_destroy(rbr_ctx* ctx) {
+    CacheState& cs = ctx->cache;
+    free_cache_params(cs);
+    free_dev(cs.q_rec);  // render buffers (queries, training vertices)
     free_dev(cs.q_info);
     free_dev(cs.t_rec);
     free_dev(cs.t_aux);
     free_dev(cs.t_target);
     cs.q_cap = cs.t_cap = 0;
-    cs.ready = false;
 }
 
 void cache_config_default(rbr_cache_config* c) {
@@ -879,7 +884,8 @@ rbr_status cache_create(rbr_ctx* ctx, const rbr_cache_config* cfg_in) {
     cudaError_t e = cudaSetDevice(ctx->device);
     if (e == cudaSuccess) e = set_kernel_attributes(ctx->device);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "radiance cache: device setup");
-    cache_destroy(ctx);
+    // a new cache replaces the parameters; the render buffers stay (they only grow)
+    free_cache_params(ctx->cache);
     CacheState& cs = ctx->cache;
     cs.cfg = cfg;
     cs.table = 1u << cfg.log2_table_size;
