@@ -1,7 +1,7 @@
 // Host BVH construction for the GPU traversal kernels.
 //
 // 1. Binary tree, binned SAH (32 bins on each of the three axes, centroid binning), leaves of
-//    at most 3 primitives. The reference's own builder (src/acceleration/bvh.cpp:47-209) bins
+//    at most 4 primitives (a wide node's leaf records then fit one 32-bit mask). The reference's own builder (src/acceleration/bvh.cpp:47-209) bins
 //    12 buckets on the single axis of largest centroid extent and stops at 4 primitives; its
 //    tree shape does not enter any result here: closest-hit answers are defined by the
 //    primitives alone (smallest t, ties to the highest primitive id, as a brute-force loop in

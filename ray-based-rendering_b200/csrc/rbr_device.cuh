@@ -184,7 +184,8 @@ constexpr float kTLo = 1.0f - 1.0f / 65536.0f;
 constexpr float kTHi = 1.0f + 1.0f / 65536.0f;
 
 // Tests the 8 children of node `idx`. ngroup = (child_base, hit bits << 24 | imask << 16),
-// pgroup = (prim_base, 24-bit mask of leaf records to test).
+// pgroup = (prim_base, mask of the node's leaf records to test: up to 8 leaves of up to 4
+// records, 32 bits).
 __device__ __forceinline__ void intersect_node(const uint4* __restrict__ nodes, uint32_t idx, const RayCtx& r,
                                                float tbest, uint2& ngroup, uint2& pgroup) {
     const uint4* np = nodes + 5 * static_cast<size_t>(idx);

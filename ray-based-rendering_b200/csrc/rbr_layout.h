@@ -38,7 +38,7 @@ constexpr uint32_t kIdMask = (1u << kTypeShift) - 1;
 
 constexpr int kNodeWords = 20;   // u32 words per wide node
 constexpr int kRecordWords = 12; // u32 words per leaf record
-constexpr int kMaxLeafPrims = 3;
+constexpr int kMaxLeafPrims = 4;
 constexpr int kStackSize = 64;   // traversal stack entries; the builder keeps the tree shallower
 constexpr int kMaxTreeDepth = 62;
 
