@@ -48,6 +48,8 @@ def parse():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--workload", choices=["rays", "cornell", "ggx", "fog", "cache", "batch"], default="rays")
     p.add_argument("--ref-spp", type=int, default=4096, help="cache workload: spp of the converged GPU reference")
+    p.add_argument("--cache-suffix", type=int, default=None,
+                   help="cache workload: rbr_cache_config.train_suffix (default: the library's)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true", help="skip the host-buffer measurement (profiling runs)")
     p.add_argument("--param", action="append", default=[], help="NAME=VALUE context tunable (rbr_param_set)")
@@ -383,6 +385,7 @@ def run_cache(args, rank, world, local_rank):
 
     # converged reference in calls of at most 1024 spp (one call takes at most 2^32 camera
     # samples), each with its own seed; the film is the sample-weighted mean of the calls
+    cache_kw = {} if args.cache_suffix is None else {"train_suffix": args.cache_suffix}
     ref, ref_ms, done = 0.0, 0.0, 0
     while done < args.ref_spp:
         spp = min(1024, args.ref_spp - done)
@@ -391,12 +394,12 @@ def run_cache(args, rank, world, local_rank):
     ref = ref / args.ref_spp
     # warm-up of both paths (kernels loaded, buffers allocated)
     plain(1, 1)
-    ctx.cache_create(seed=3)
+    ctx.cache_create(seed=3, **cache_kw)
     ctx.cache_render_dev(cam, render_params(spp=1, max_depth=depth, seed=2), max(3, args.warmup), film.data_ptr(), 0,
                          True, sp)
     torch.cuda.synchronize()
     # the timed cached run starts from a fresh cache
-    ctx.cache_create(seed=3)
+    ctx.cache_create(seed=3, **cache_kw)
     clocks = Clocks() if rank == 0 else None
     if clocks:
         clocks.start()
@@ -440,7 +443,8 @@ def run_cache(args, rank, world, local_rank):
                        "plain_equal_time_ms": plain_eq_ms, "cache_ms": cache_ms,
                        "mean_bias": float(cached.mean() / ref.mean() - 1.0)},
             "cache": {"optimiser_steps": info.optimiser_steps, "last_loss": info.last_loss,
-                      "queries_last_frame": info.last_queries, "train_records_last_frame": info.last_train_records},
+                      "queries_last_frame": info.last_queries, "train_records_last_frame": info.last_train_records,
+                      "train_suffix": ctx.cache_config(**cache_kw).train_suffix},
             "e2e": {"value": W * H * e2e_frames / e2e_s / 1e6, "unit": "Mpaths/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": W * H * 12 // e2e_frames,
                     "path": f"rbr_cache_render of {e2e_frames} frames + film to host"},

@@ -353,6 +353,9 @@ typedef struct rbr_cache_config {
     uint64_t seed;              /* initial weights */
     float bounds_min[3];        /* box the hash grid covers; min >= max on any axis: the */
     float bounds_max[3];        /* scene's bounded geometry, enlarged by 1% */
+    uint32_t train_suffix;      /* k > 0 (default 2): training paths end into the cache k bounces
+                                   after termination_depth, so their targets include the cache's
+                                   own prediction (self-training); 0: they run to max_depth */
 } rbr_cache_config;
 
 typedef struct rbr_cache_info {

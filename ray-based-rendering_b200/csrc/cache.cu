@@ -792,6 +792,7 @@ void cache_config_default(rbr_cache_config* c) {
     c->train_steps = 4;
     c->train_paths = 65536;
     c->termination_depth = 1;
+    c->train_suffix = 2;
     c->seed = 0;
     for (int a = 0; a < 3; ++a) {
         c->bounds_min[a] = 0.0f;

@@ -59,6 +59,7 @@ struct Wave {
     // radiance cache (cache_on = 0: the plain path tracer)
     uint32_t cache_on = 0;
     uint32_t term_depth = 0;    // first depth at which a path may end into the cache
+    uint32_t train_suffix = 0;  // > 0: training paths end into the cache at term_depth + this
     uint32_t train_thresh = 0;  // a path is a training path if its hash is below this
     float film_weight = 0.0f;   // > 0: film_mean += weight * mean (frames averaged), else film_mean = mean
 };
@@ -437,7 +438,13 @@ __global__ void __launch_bounds__(kBlock, 8) k_shade(DeviceScene s, Wave w, Path
             alive = true;
             if (kCache && bs.n > 0 && !bsdf_delta(bs)) {
                 if (train_path(w, seed, pixel, sample)) {
-                    to_train = true;
+                    if (w.train_suffix != 0 && d >= w.term_depth + w.train_suffix && !specular) {
+                        to_cache = true;  // self-training: the suffix ends in the cache's prediction
+                        nee = false;
+                        alive = false;
+                    } else {
+                        to_train = true;
+                    }
                 } else if (d >= w.term_depth && !specular) {
                     to_cache = true;  // the cache's prediction replaces NEE and everything further
                     nee = false;
@@ -932,6 +939,7 @@ rbr_status render_cached(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_p
             w.seed = p->seed;
             w.cache_on = 1;
             w.term_depth = cs.cfg.termination_depth;
+            w.train_suffix = cs.cfg.train_suffix;
             w.train_thresh = thresh;
             w.film_weight = weight;
             k_raygen<false><<<grid, kBlock, 0, ws>>>(cd, w, P);
@@ -1027,6 +1035,7 @@ cudaError_t launch_packed_wave(rbr_ctx* eng, rbr_ctx* scn, const PackedWave& pw,
         P.t_cap = pw.train ? cs.t_cap : 0;
         w.cache_on = 1;
         w.term_depth = cs.cfg.termination_depth;
+        w.train_suffix = cs.cfg.train_suffix;
         w.train_thresh = pw.train_thresh;
     }
     const CameraDev unused{};

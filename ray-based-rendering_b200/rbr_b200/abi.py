@@ -174,6 +174,7 @@ class rbr_cache_config(C.Structure):
         ("seed", C.c_uint64),
         ("bounds_min", _f3),
         ("bounds_max", _f3),
+        ("train_suffix", C.c_uint32),
     ]
 
 
