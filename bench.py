@@ -376,22 +376,24 @@ def run_cache(args, rank, world, local_rank):
     film = torch.zeros(W * H * 3, dtype=torch.float32, device=f"cuda:{local_rank}")
 
     def plain(spp, seed):
-        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
-        ev[0].record(stream)
-        ctx.render_dev(cam, render_params(spp=spp, max_depth=depth, seed=seed), film.data_ptr(), 0, sp)
-        ev[1].record(stream)
-        torch.cuda.synchronize()
-        return film.cpu().numpy().reshape(H, W, 3).copy(), ev[0].elapsed_time(ev[1])
+        """The plain path tracer at `spp`, in calls of at most 1024 spp (one call takes at most
+        2^32 camera samples) with consecutive sample ranges; film = the sample-weighted mean."""
+        img, total_ms, done = 0.0, 0.0, 0
+        while done < spp:
+            n = min(1024, spp - done)
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+            ev[0].record(stream)
+            ctx.render_dev(cam, render_params(spp=n, max_depth=depth, seed=seed, sample_offset=done), film.data_ptr(),
+                           0, sp)
+            ev[1].record(stream)
+            torch.cuda.synchronize()
+            img = img + film.cpu().numpy().reshape(H, W, 3) * n
+            total_ms += ev[0].elapsed_time(ev[1])
+            done += n
+        return img / spp, total_ms
 
-    # converged reference in calls of at most 1024 spp (one call takes at most 2^32 camera
-    # samples), each with its own seed; the film is the sample-weighted mean of the calls
     cache_kw = {} if args.cache_suffix is None else {"train_suffix": args.cache_suffix}
-    ref, ref_ms, done = 0.0, 0.0, 0
-    while done < args.ref_spp:
-        spp = min(1024, args.ref_spp - done)
-        img, ms = plain(spp, 777 + done)
-        ref, ref_ms, done = ref + img * spp, ref_ms + ms, done + spp
-    ref = ref / args.ref_spp
+    ref, ref_ms = plain(args.ref_spp, 777)  # converged reference, independent seed
     # warm-up of both paths (kernels loaded, buffers allocated)
     plain(1, 1)
     ctx.cache_create(seed=3, **cache_kw)
