@@ -81,3 +81,20 @@ def test_two_waves_in_flight_gather_the_same_paths(ctx):
     assert qa == qb and ta == tb and sa == sb == 16 * 4
     assert np.isfinite(b).all() and (b >= 0).all()
     assert abs(b.mean() / a.mean() - 1.0) < 0.05
+
+
+def test_self_training_suffix(ctx):
+    """train_suffix k > 0 ends training paths into the cache k bounces after the termination
+    depth: fewer training vertices and more queries per frame than full training paths
+    (train_suffix 0), and an image of the same brightness."""
+    s = small_ggx(96, 54)
+    ctx.upload(s)
+    out = {}
+    for k in (0, 2):
+        ctx.cache_create(train_paths=(96 * 54) // 8, seed=1, train_suffix=k)
+        img = cached_render(ctx, s.camera, 16, 16, 5)
+        info = ctx.cache_info()
+        out[k] = (img, info.last_queries, info.last_train_records)
+    (a, q0, t0), (b, q2, t2) = out[0], out[2]
+    assert t2 < t0 and q2 > q0, (t0, t2, q0, q2)
+    assert np.isfinite(b).all() and abs(b.mean() / a.mean() - 1.0) < 0.05
