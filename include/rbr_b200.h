@@ -274,7 +274,10 @@ rbr_status rbr_trace_counts(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int a
  * film_mean: device pointer, width*height*3 floats, receives the per-pixel mean over the
  * samples, as Film::addSample(x, y, sum / spp) stores it (src/renderers/integrator.cpp:36).
  * film_m2: device pointer or NULL; with RBR_RENDER_SECOND_MOMENT it receives per-pixel sums
- * of squared sample values (width*height*3 floats). Asynchronous on `stream`.
+ * of squared sample values (width*height*3 floats). Asynchronous on `stream`: with
+ * "pt.streams" 2 every other wave runs on a second stream of the context that forks from
+ * `stream` at the start and joins it at the end, so work queued on `stream` afterwards sees
+ * the whole film.
  * Replaces: Integrator::render with PathTracingIntegrator::Li (src/renderers/integrator.cpp:7-50,
  * src/renderers/path_tracing_integrator.cpp:5-138). */
 rbr_status rbr_render(rbr_ctx* ctx, const rbr_camera* camera, const rbr_render_params* params,
