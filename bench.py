@@ -50,6 +50,8 @@ def parse():
     p.add_argument("--ref-spp", type=int, default=4096, help="cache workload: spp of the converged GPU reference")
     p.add_argument("--cache-suffix", type=int, default=None,
                    help="cache workload: rbr_cache_config.train_suffix (default: the library's)")
+    p.add_argument("--cache-config", action="append", default=[],
+                   help="cache workload: NAME=INT field of rbr_cache_config (e.g. termination_depth=2)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true", help="skip the host-buffer measurement (profiling runs)")
     p.add_argument("--param", action="append", default=[], help="NAME=VALUE context tunable (rbr_param_set)")
@@ -393,6 +395,9 @@ def run_cache(args, rank, world, local_rank):
         return img / spp, total_ms
 
     cache_kw = {} if args.cache_suffix is None else {"train_suffix": args.cache_suffix}
+    for kv in args.cache_config:
+        k, v = kv.split("=")
+        cache_kw[k] = int(v)
     ref, ref_ms = plain(args.ref_spp, 777)  # converged reference, independent seed
     # warm-up of both paths (kernels loaded, buffers allocated)
     plain(1, 1)
@@ -446,7 +451,8 @@ def run_cache(args, rank, world, local_rank):
                        "mean_bias": float(cached.mean() / ref.mean() - 1.0)},
             "cache": {"optimiser_steps": info.optimiser_steps, "last_loss": info.last_loss,
                       "queries_last_frame": info.last_queries, "train_records_last_frame": info.last_train_records,
-                      "train_suffix": ctx.cache_config(**cache_kw).train_suffix},
+                      "train_suffix": ctx.cache_config(**cache_kw).train_suffix,
+                      "termination_depth": ctx.cache_config(**cache_kw).termination_depth},
             "e2e": {"value": W * H * e2e_frames / e2e_s / 1e6, "unit": "Mpaths/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": W * H * 12 // e2e_frames,
                     "path": f"rbr_cache_render of {e2e_frames} frames + film to host"},
