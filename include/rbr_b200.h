@@ -398,9 +398,12 @@ rbr_status rbr_cache_train_host(rbr_ctx* ctx, uint32_t n, const rbr_cache_record
  * a path ends into the cache at its first vertex of depth >= termination_depth reached by a
  * non-delta bounce on a non-delta material (its emission there is still added, then the
  * throughput times the cache's prediction replaces everything further), except about
- * train_paths paths per frame, which continue as the plain path tracer does and whose
- * vertices, with the radiance gathered past each of them, train the cache for train_steps
- * Adam steps after the frame. Frame f uses samples sample_offset + f*spp ... ; film_mean
+ * train_paths paths per frame, which continue as the plain path tracer does (for train_suffix
+ * more bounces, then they end into the cache as well; train_suffix 0: to the maximum depth) and
+ * whose vertices, with the radiance gathered past each of them, train the cache for
+ * train_steps Adam steps after the frame. A frame runs as two half-image waves in flight
+ * ("pt.streams" 2) on a second stream that forks from and joins `stream`.
+ * Frame f uses samples sample_offset + f*spp ... ; film_mean
  * (device) receives the mean over all frames, film_m2 (device or NULL, with
  * RBR_RENDER_SECOND_MOMENT) the sum of squared sample values. Asynchronous on `stream`. */
 rbr_status rbr_cache_render(rbr_ctx* ctx, const rbr_camera* camera, const rbr_render_params* params,
