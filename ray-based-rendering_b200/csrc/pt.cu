@@ -31,7 +31,7 @@ namespace rbr {
 namespace {
 
 constexpr int kBlock = 128;
-constexpr uint32_t kDefaultCapacity = 1u << 22;  // paths per wave
+constexpr uint32_t kDefaultCapacity = 1u << 22;  // most samples per pixel in one call (a wave holds a pixel's samples)
 constexpr size_t kShadowBytesLimit = size_t(2) << 30;
 
 // counters (uint32 words)
