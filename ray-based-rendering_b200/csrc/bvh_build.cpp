@@ -6,8 +6,11 @@
 //    tree shape does not enter any result here: closest-hit answers are defined by the
 //    primitives alone (smallest t, ties to the highest primitive id, as a brute-force loop in
 //    primitive order gives), so the GPU tree is free to be a better one.
-// 2. Collapse into 8-wide nodes: starting from a node's two children, the child with the
-//    largest surface area is replaced by its two children until 8 slots are full.
+// 2. Collapse into 8-wide nodes by dynamic programming over the binary tree: for every binary
+//    node and every slot budget i = 1..8, the least SAH cost of representing its subtree with
+//    at most i children of the parent wide node, where a child is a leaf (a subtree of at most
+//    kMaxLeafPrims primitives, cost area x primitives) or a wide node of its own (cost area +
+//    the best spread of its subtree over 8 slots); the tree is then read off top-down.
 // 3. Quantise each node's child boxes to 8-bit coordinates on a per-axis power-of-two grid,
 //    rounded outwards, after growing every box by `pad`.
 #include "bvh_build.h"
@@ -211,6 +214,84 @@ struct ChildRef {
     bool leaf;
 };
 
+// The collapse's cost tables. Children have larger indices than their parent, so one pass from
+// the last binary node to the root fills them.
+struct Collapse {
+    static constexpr double kNodeCost = 1.0;  // per unit of half area: a wide-node test
+    static constexpr double kPrimCost = 1.0;  // per unit of half area and primitive: a record test
+    const Builder& B;
+    std::vector<float> cost;     // cost[8 n + i - 1]: subtree n in at most i slots
+    std::vector<float> single;   // subtree n in one slot: a leaf or a wide node
+    std::vector<uint8_t> as_leaf;
+    std::vector<uint32_t> rbeg, rcnt;  // the subtree's primitives: refs[rbeg, rbeg + rcnt)
+
+    Collapse(const Builder& b, uint32_t used) : B(b) {
+        cost.assign(size_t(used) * 8, 0.0f);
+        single.assign(used, 0.0f);
+        as_leaf.assign(used, 0);
+        rbeg.assign(used, 0);
+        rcnt.assign(used, 0);
+        for (uint32_t ni = used; ni-- > 0;) {
+            const BNode& nd = B.nodes[ni];
+            const double area = half_area(nd.box);
+            float* c = &cost[size_t(ni) * 8];
+            if (nd.count > 0) {
+                rbeg[ni] = nd.begin;
+                rcnt[ni] = nd.count;
+                single[ni] = static_cast<float>(area * nd.count * kPrimCost);
+                as_leaf[ni] = 1;
+                for (int i = 0; i < 8; ++i) c[i] = single[ni];
+                continue;
+            }
+            rbeg[ni] = rbeg[nd.left];  // the left subtree's primitives precede the right's
+            rcnt[ni] = rcnt[nd.left] + rcnt[nd.right];
+            const double leafc = rcnt[ni] <= static_cast<uint32_t>(kMaxLeafPrims) ? area * rcnt[ni] * kPrimCost : 1e30;
+            const double nodec = area * kNodeCost + spread(ni, 8);
+            single[ni] = static_cast<float>(std::min(leafc, nodec));
+            as_leaf[ni] = leafc <= nodec;
+            c[0] = single[ni];
+            for (int i = 2; i <= 8; ++i) c[i - 1] = static_cast<float>(std::min<double>(c[i - 2], spread(ni, i)));
+        }
+    }
+    // least cost of spreading internal node ni's two subtrees over j slots, and the left's share
+    double spread(uint32_t ni, int j, int* left_slots = nullptr) const {
+        const BNode& nd = B.nodes[ni];
+        double best = 1e30;
+        for (int k = 1; k < j; ++k) {
+            const double v = double(cost[size_t(nd.left) * 8 + k - 1]) + cost[size_t(nd.right) * 8 + j - k - 1];
+            if (v < best) {
+                best = v;
+                if (left_slots) *left_slots = k;
+            }
+        }
+        return best;
+    }
+    // the children of the wide node made from internal node ni
+    void children(uint32_t ni, int j, std::vector<uint32_t>& out) const {
+        int k = 1;
+        spread(ni, j, &k);
+        place(B.nodes[ni].left, k, out);
+        place(B.nodes[ni].right, j - k, out);
+    }
+    void place(uint32_t m, int i, std::vector<uint32_t>& out) const {
+        if (i == 1 || B.nodes[m].count > 0) {
+            out.push_back(m);
+            return;
+        }
+        double best = single[m];
+        int bj = 1;
+        for (int j = 2; j <= i; ++j) {
+            const double v = spread(m, j);
+            if (v < best) {
+                best = v;
+                bj = j;
+            }
+        }
+        if (bj == 1) out.push_back(m);
+        else children(m, bj, out);
+    }
+};
+
 }  // namespace
 
 WideBVH build_wide_bvh(const std::vector<Box>& boxes, float pad, int threads) {
@@ -229,6 +310,7 @@ WideBVH build_wide_bvh(const std::vector<Box>& boxes, float pad, int threads) {
     B.threads_left = std::max(0, threads - 1);
     B.build(0, 0, n, 1);
     out.binary_nodes = B.next_node.load();
+    const Collapse CP(B, out.binary_nodes);
 
     // Collapse to 8-wide nodes, breadth first.
     struct Item {
@@ -249,24 +331,9 @@ WideBVH build_wide_bvh(const std::vector<Box>& boxes, float pad, int threads) {
         if (root.count > 0) {
             ch[k++] = {item.bnode, true};
         } else {
-            ch[k++] = {root.left, B.nodes[root.left].count > 0};
-            ch[k++] = {root.right, B.nodes[root.right].count > 0};
-            while (k < 8) {
-                int pick = -1;
-                float best = -1.0f;
-                for (int i = 0; i < k; ++i) {
-                    if (ch[i].leaf) continue;
-                    const float a = half_area(B.nodes[ch[i].bnode].box);
-                    if (a > best) {
-                        best = a;
-                        pick = i;
-                    }
-                }
-                if (pick < 0) break;
-                const BNode& bn = B.nodes[ch[pick].bnode];
-                ch[pick] = {bn.left, B.nodes[bn.left].count > 0};
-                ch[k++] = {bn.right, B.nodes[bn.right].count > 0};
-            }
+            std::vector<uint32_t> lst;
+            CP.children(item.bnode, 8, lst);
+            for (uint32_t m : lst) ch[k++] = {m, CP.as_leaf[m] != 0};
         }
         // padded child boxes in double precision
         double clo[8][3], chi[8][3], nlo[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, nhi[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
@@ -352,11 +419,11 @@ WideBVH build_wide_bvh(const std::vector<Box>& boxes, float pad, int threads) {
                 qlo[a][s] = static_cast<uint8_t>(std::max(0.0, std::min(255.0, lo)));
                 qhi[a][s] = static_cast<uint8_t>(std::max(0.0, std::min(255.0, hi)));
             }
-            const BNode& bn = B.nodes[ch[i].bnode];
             if (ch[i].leaf) {
-                meta[s] = static_cast<uint8_t>((bn.count << 5) | prim_offset);
-                for (uint32_t j = 0; j < bn.count; ++j) out.leaf_order.push_back(B.refs[bn.begin + j]);
-                prim_offset += bn.count;
+                const uint32_t cb = CP.rbeg[ch[i].bnode], cc = CP.rcnt[ch[i].bnode];
+                meta[s] = static_cast<uint8_t>((cc << 5) | prim_offset);
+                for (uint32_t j = 0; j < cc; ++j) out.leaf_order.push_back(B.refs[cb + j]);
+                prim_offset += cc;
             } else {
                 imask |= 1u << s;
                 queue.push_back({child_base + internal_rank, ch[i].bnode, item.depth + 1});
