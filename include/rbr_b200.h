@@ -124,6 +124,9 @@ typedef struct rbr_scene_stats {
     uint32_t num_wide_nodes;      /* 8-wide nodes (80 B each) */
     uint32_t num_leaf_records;    /* leaf primitive records (48 B each) */
     uint32_t max_depth;           /* depth of the wide tree */
+    uint32_t wrapped_leaves;      /* leaves given a wide node of their own: a node beside internal
+                                     children holds at most 24 leaf records */
+    uint32_t record_cost_milli;   /* "bvh.record_cost_milli" the tree was built with */
     uint64_t device_bytes;        /* device memory held by the scene */
     double build_seconds;         /* host SAH build + collapse + quantisation */
 } rbr_scene_stats;
@@ -242,6 +245,9 @@ rbr_status rbr_scene_stats_get(const rbr_ctx* ctx, rbr_scene_stats* out);
  *   "pt.streams"           rbr_render: waves in flight, 1 or 2 (default 2: waves alternate
  *                          between two sets of path buffers on two streams; an image that
  *                          fits one wave is rendered as two half-image waves)
+ *   "bvh.record_cost_milli" cost of testing one leaf record relative to one wide-node test,
+ *                          x1000, in the 8-wide collapse's surface-area cost (default 1000);
+ *                          applies to the next rbr_scene_upload
  * Results do not depend on them; only speed and memory do. rbr_autotune picks them. */
 rbr_status rbr_param_set(rbr_ctx* ctx, const char* name, int64_t value);
 rbr_status rbr_param_get(const rbr_ctx* ctx, const char* name, int64_t* value);
@@ -541,9 +547,10 @@ rbr_status rbr_film_to_rgb8_host(rbr_ctx* ctx, const float* film, int32_t width,
  * The scene must have been uploaded with rbr_scene_upload beforehand; render statistics
  * (rbr_render_stats_get) are not updated.
  *
- * The first call on a device looks up the array's device address (which loads the
- * library's device code on that device if nothing has yet); make that first call before any
- * stream capture. All calls in the process share the one array per device and it keeps the
+ * Every call looks up the array's device address on the context's device (the first lookup
+ * on a device loads the library's device code there if nothing has yet, so make the first
+ * call on a device before any stream capture); a device reset between calls is therefore
+ * harmless. All calls in the process share the one array per device and it keeps the
  * previous call's contents, so calls whose work overlaps on the GPU (different streams or
  * contexts on the same device) race and corrupt each other: serialise them. */
 rbr_status rbr_render_noalloc(rbr_ctx* ctx, const rbr_camera* camera, const rbr_render_params* params,

@@ -12,6 +12,7 @@ built file travels with the repository).
 from __future__ import annotations
 
 import ctypes as C
+import os
 import sys
 from pathlib import Path
 
@@ -26,6 +27,12 @@ from rbr_b200.abi import HIT_DTYPE, RAY_DTYPE  # noqa: E402
 
 ORACLE_LIB = HERE / "_build" / "librbr_oracle.so"
 REF_LIB = HERE / "_ref" / "librbr_ref.so"
+
+
+def reference_dir() -> Path:
+    """Where the reference's sources lie (only where they were cloned; never on the GPU box):
+    the RBR_REFERENCE setting, the same one oracle/Makefile and adapters/Makefile read."""
+    return Path(os.environ.get("RBR_REFERENCE", "/root/reference"))
 
 P = C.c_void_p
 _i64 = C.c_int64

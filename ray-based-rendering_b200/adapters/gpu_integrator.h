@@ -6,7 +6,9 @@
 // config.samplesPerPixel samples per pixel with config.maxDepth, useNEE and useMIS, and adds
 // one averaged sample per pixel to the film, as Integrator::render does
 // (src/renderers/integrator.cpp:36). The estimator is the reference's
-// PathTracingIntegrator::Li, quirks included (see DESIGN.md of the library).
+// PathTracingIntegrator::Li, quirks included: emission only at depth 0 or after a delta
+// bounce, MIS weights on light samples without the BSDF-sampled emitter term, next-event
+// estimation over every light, Russian roulette always on after depth 3.
 //
 // With volumetric = true it is the drop-in for VolumetricPathIntegrator
 // (src/renderers/volumetric_path_integrator.cpp): the scene's HomogeneousMedium is uploaded and

@@ -343,7 +343,7 @@ rbr_status rbr_batch_create(rbr_ctx* ctx, const rbr_batch_config* config, rbr_ba
     if (config) b->cfg = *config;
     else rbr_batch_config_default(&b->cfg);
     if (b->cfg.path_memory_bytes == 0) b->cfg.path_memory_bytes = 2ull << 30;
-    cudaSetDevice(ctx->device);
+    const DeviceScope scope(ctx->device);
     const cudaError_t e = cudaMalloc(&b->d_table, 2 * kTableBytes);  // a segment table per wave in flight
     if (e != cudaSuccess) {
         delete b;
@@ -355,7 +355,7 @@ rbr_status rbr_batch_create(rbr_ctx* ctx, const rbr_batch_config* config, rbr_ba
 
 void rbr_batch_destroy(rbr_batch* b) {
     if (!b) return;
-    cudaSetDevice(b->eng->device);
+    const DeviceScope scope(b->eng->device);
     cudaDeviceSynchronize();
     drop_graphs(b);
     for (cudaEvent_t e : b->events) cudaEventDestroy(e);
@@ -439,7 +439,7 @@ rbr_status rbr_batch_submit(rbr_batch* b, const rbr_request* r, uint32_t* reques
 
 rbr_status rbr_batch_run(rbr_batch* b, void* stream) {
     if (!b) return RBR_ERR_INVALID_ARGUMENT;
-    cudaSetDevice(b->eng->device);
+    const DeviceScope scope(b->eng->device);
     std::vector<Req> reqs = b->pending;
     const rbr_status st = run(b, reqs, static_cast<cudaStream_t>(stream));
     if (st != RBR_OK) return st;
@@ -455,7 +455,7 @@ rbr_status rbr_batch_request_stats(rbr_batch* b, uint32_t id, rbr_request_stats*
     auto it = b->done_index.find(id);
     if (it == b->done_index.end()) return bfail(b, RBR_ERR_INVALID_ARGUMENT, "request not in the last run");
     const Req& q = b->done[it->second];
-    cudaSetDevice(b->eng->device);
+    const DeviceScope scope(b->eng->device);
     cudaError_t e = cudaEventSynchronize(b->events[b->run_waves + 1]);
     // a wave starts when the previous wave of its stream has ended
     const uint32_t prev = b->run_slots == 2 ? (q.first_wave >= 2 ? q.first_wave - 1 : 0) : q.first_wave;
@@ -474,7 +474,7 @@ rbr_status rbr_batch_request_stats(rbr_batch* b, uint32_t id, rbr_request_stats*
 rbr_status rbr_batch_stats_get(rbr_batch* b, rbr_batch_stats* out) {
     if (!b || !out) return RBR_ERR_INVALID_ARGUMENT;
     if (!b->ran) return bfail(b, RBR_ERR_INVALID_ARGUMENT, "no run yet");
-    cudaSetDevice(b->eng->device);
+    const DeviceScope scope(b->eng->device);
     cudaError_t e = cudaEventSynchronize(b->events[b->run_waves + 1]);
     float ms = 0.0f;
     if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, b->events[0], b->events[b->run_waves + 1]);
@@ -489,7 +489,7 @@ rbr_status rbr_batch_stats_get(rbr_batch* b, rbr_batch_stats* out) {
 rbr_status rbr_batch_autotune(rbr_batch* b, void* stream) {
     if (!b) return RBR_ERR_INVALID_ARGUMENT;
     if (b->pending.empty()) return bfail(b, RBR_ERR_INVALID_ARGUMENT, "no queued requests to tune on");
-    cudaSetDevice(b->eng->device);
+    const DeviceScope scope(b->eng->device);
     const rbr_batch_config saved = b->cfg;
     bool any_cache = false;
     for (const Req& q : b->pending) any_cache = any_cache || q.r.use_cache;

@@ -12,7 +12,8 @@
 //    kMaxLeafPrims primitives, cost area x primitives) or a wide node of its own (cost area +
 //    the best spread of its subtree over 8 slots); the tree is then read off top-down.
 // 3. Quantise each node's child boxes to 8-bit coordinates on a per-axis power-of-two grid,
-//    rounded outwards, after growing every box by `pad`.
+//    rounded outwards with a margin of kQuantMargin steps, after growing every box by `pad`.
+//    The stored grid origin is biased by kGridBias steps (rbr_layout.h).
 #include "bvh_build.h"
 
 #include <algorithm>
@@ -216,29 +217,31 @@ struct ChildRef {
 
 // The collapse's cost tables. Children have larger indices than their parent, so one pass from
 // the last binary node to the root fills them.
+// Costs are kept in double throughout, so that equal-cost choices resolve the same way in
+// the table fill and in the read-off.
 struct Collapse {
     static constexpr double kNodeCost = 1.0;  // per unit of half area: a wide-node test
-    static constexpr double kPrimCost = 1.0;  // per unit of half area and primitive: a record test
+    const double kPrimCost;                   // per unit of half area and primitive: a record test
     const Builder& B;
-    std::vector<float> cost;     // cost[8 n + i - 1]: subtree n in at most i slots
-    std::vector<float> single;   // subtree n in one slot: a leaf or a wide node
+    std::vector<double> cost;    // cost[8 n + i - 1]: subtree n in at most i slots
+    std::vector<double> single;  // subtree n in one slot: a leaf or a wide node
     std::vector<uint8_t> as_leaf;
     std::vector<uint32_t> rbeg, rcnt;  // the subtree's primitives: refs[rbeg, rbeg + rcnt)
 
-    Collapse(const Builder& b, uint32_t used) : B(b) {
-        cost.assign(size_t(used) * 8, 0.0f);
-        single.assign(used, 0.0f);
+    Collapse(const Builder& b, uint32_t used, double record_cost) : kPrimCost(record_cost), B(b) {
+        cost.assign(size_t(used) * 8, 0.0);
+        single.assign(used, 0.0);
         as_leaf.assign(used, 0);
         rbeg.assign(used, 0);
         rcnt.assign(used, 0);
         for (uint32_t ni = used; ni-- > 0;) {
             const BNode& nd = B.nodes[ni];
             const double area = half_area(nd.box);
-            float* c = &cost[size_t(ni) * 8];
+            double* c = &cost[size_t(ni) * 8];
             if (nd.count > 0) {
                 rbeg[ni] = nd.begin;
                 rcnt[ni] = nd.count;
-                single[ni] = static_cast<float>(area * nd.count * kPrimCost);
+                single[ni] = area * nd.count * kPrimCost;
                 as_leaf[ni] = 1;
                 for (int i = 0; i < 8; ++i) c[i] = single[ni];
                 continue;
@@ -247,10 +250,10 @@ struct Collapse {
             rcnt[ni] = rcnt[nd.left] + rcnt[nd.right];
             const double leafc = rcnt[ni] <= static_cast<uint32_t>(kMaxLeafPrims) ? area * rcnt[ni] * kPrimCost : 1e30;
             const double nodec = area * kNodeCost + spread(ni, 8);
-            single[ni] = static_cast<float>(std::min(leafc, nodec));
+            single[ni] = std::min(leafc, nodec);
             as_leaf[ni] = leafc <= nodec;
             c[0] = single[ni];
-            for (int i = 2; i <= 8; ++i) c[i - 1] = static_cast<float>(std::min<double>(c[i - 2], spread(ni, i)));
+            for (int i = 2; i <= 8; ++i) c[i - 1] = std::min(c[i - 2], spread(ni, i));
         }
     }
     // least cost of spreading internal node ni's two subtrees over j slots, and the left's share
@@ -258,7 +261,7 @@ struct Collapse {
         const BNode& nd = B.nodes[ni];
         double best = 1e30;
         for (int k = 1; k < j; ++k) {
-            const double v = double(cost[size_t(nd.left) * 8 + k - 1]) + cost[size_t(nd.right) * 8 + j - k - 1];
+            const double v = cost[size_t(nd.left) * 8 + k - 1] + cost[size_t(nd.right) * 8 + j - k - 1];
             if (v < best) {
                 best = v;
                 if (left_slots) *left_slots = k;
@@ -294,7 +297,7 @@ struct Collapse {
 
 }  // namespace
 
-WideBVH build_wide_bvh(const std::vector<Box>& boxes, float pad, int threads) {
+WideBVH build_wide_bvh(const std::vector<Box>& boxes, float pad, int threads, double record_cost) {
     WideBVH out;
     const uint32_t n = static_cast<uint32_t>(boxes.size());
     if (n == 0) return out;
@@ -310,7 +313,7 @@ WideBVH build_wide_bvh(const std::vector<Box>& boxes, float pad, int threads) {
     B.threads_left = std::max(0, threads - 1);
     B.build(0, 0, n, 1);
     out.binary_nodes = B.next_node.load();
-    const Collapse CP(B, out.binary_nodes);
+    const Collapse CP(B, out.binary_nodes, record_cost);
 
     // Collapse to 8-wide nodes, breadth first.
     struct Item {
@@ -334,6 +337,25 @@ WideBVH build_wide_bvh(const std::vector<Box>& boxes, float pad, int threads) {
             std::vector<uint32_t> lst;
             CP.children(item.bnode, 8, lst);
             for (uint32_t m : lst) ch[k++] = {m, CP.as_leaf[m] != 0};
+        }
+        // A node with internal children keeps its leaf records below bit kInnerRecordLimit of
+        // the hit mask; over that, its largest leaves become internal children of their own
+        // (a wide node holding just that leaf).
+        {
+            bool has_inner = false;
+            uint32_t records = 0;
+            for (int i = 0; i < k; ++i) {
+                if (ch[i].leaf) records += CP.rcnt[ch[i].bnode];
+                else has_inner = true;
+            }
+            while (has_inner && records > kInnerRecordLimit) {
+                int big = -1;
+                for (int i = 0; i < k; ++i)
+                    if (ch[i].leaf && (big < 0 || CP.rcnt[ch[i].bnode] > CP.rcnt[ch[big].bnode])) big = i;
+                ch[big].leaf = false;
+                records -= CP.rcnt[ch[big].bnode];
+                ++out.wrapped_leaves;
+            }
         }
         // padded child boxes in double precision
         double clo[8][3], chi[8][3], nlo[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, nhi[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
@@ -380,22 +402,29 @@ WideBVH build_wide_bvh(const std::vector<Box>& boxes, float pad, int threads) {
                 slot_child[bs] = bi;
             }
         }
-        // quantisation grid
+        // Quantisation grid per axis: step s = 2^e, stored origin p (a float), grid coordinate 0
+        // at g = p + kGridBias * s (exact in double). Every child plane must land on 0..255
+        // with kQuantMargin steps to spare: g <= lo - margin and hi + margin <= g + 255 s.
         uint32_t* w = &out.nodes[static_cast<size_t>(item.wide) * kNodeWords];
         float p[3];
-        double scale[3];
+        double scale[3], gorg[3];
         uint32_t ebits = 0;
         for (int a = 0; a < 3; ++a) {
-            p[a] = nudge_down(nlo[a]);
-            const double ext = nhi[a] - static_cast<double>(p[a]);
-            int e = -100;
+            const double ext = nhi[a] - nlo[a];
+            int e = -126;
             if (ext > 0.0) {
-                e = static_cast<int>(std::ceil(std::log2(ext / 255.0)));
-                while (std::ldexp(255.0, e) < ext) ++e;
-                while (e > -126 && std::ldexp(255.0, e - 1) >= ext) --e;
+                e = static_cast<int>(std::ceil(std::log2(ext / 254.0)));
+                e = std::max(-126, std::min(127, e));
+                while (e > -126 && std::ldexp(254.0, e - 1) >= ext) --e;
             }
-            e = std::max(-126, std::min(127, e));
-            scale[a] = std::ldexp(1.0, e);
+            for (;; ++e) {
+                scale[a] = std::ldexp(1.0, e);
+                p[a] = nudge_down(nlo[a] - (kGridBias + 2.0 * kQuantMargin) * scale[a]);
+                gorg[a] = static_cast<double>(p[a]) + kGridBias * scale[a];
+                if ((nlo[a] - gorg[a] >= kQuantMargin * scale[a] &&
+                     nhi[a] - gorg[a] <= (255.0 - kQuantMargin) * scale[a]) || e >= 127)
+                    break;
+            }
             ebits |= static_cast<uint32_t>(e + 127) << (8 * a);
             std::memcpy(&w[a], &p[a], 4);
         }
@@ -414,8 +443,8 @@ WideBVH build_wide_bvh(const std::vector<Box>& boxes, float pad, int threads) {
                 continue;
             }
             for (int a = 0; a < 3; ++a) {
-                const double lo = std::floor((clo[i][a] - p[a]) / scale[a]);
-                const double hi = std::ceil((chi[i][a] - p[a]) / scale[a]);
+                const double lo = std::floor((clo[i][a] - gorg[a]) / scale[a] - kQuantMargin);
+                const double hi = std::ceil((chi[i][a] - gorg[a]) / scale[a] + kQuantMargin);
                 qlo[a][s] = static_cast<uint8_t>(std::max(0.0, std::min(255.0, lo)));
                 qhi[a][s] = static_cast<uint8_t>(std::max(0.0, std::min(255.0, hi)));
             }
@@ -425,6 +454,7 @@ WideBVH build_wide_bvh(const std::vector<Box>& boxes, float pad, int threads) {
                 for (uint32_t j = 0; j < cc; ++j) out.leaf_order.push_back(B.refs[cb + j]);
                 prim_offset += cc;
             } else {
+                meta[s] = static_cast<uint8_t>((1u << 5) | (24u + static_cast<uint32_t>(s)));
                 imask |= 1u << s;
                 queue.push_back({child_base + internal_rank, ch[i].bnode, item.depth + 1});
                 ++internal_rank;

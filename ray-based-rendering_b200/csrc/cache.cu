@@ -882,7 +882,8 @@ rbr_status cache_create(rbr_ctx* ctx, const rbr_cache_config* cfg_in) {
             hi[a] = h + pad;
         }
     }
-    cudaError_t e = cudaSetDevice(ctx->device);
+    const DeviceScope scope(ctx->device);
+    cudaError_t e = scope.status();
     if (e == cudaSuccess) e = set_kernel_attributes(ctx->device);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "radiance cache: device setup");
     // a new cache replaces the parameters; the render buffers stay (they only grow)

@@ -113,7 +113,8 @@ rbr_status rbr_ctx_create(int device, rbr_ctx** out) {
     rbr_ctx* ctx = new (std::nothrow) rbr_ctx();
     if (!ctx) return RBR_ERR_OUT_OF_MEMORY;
     ctx->device = device;
-    if ((e = cudaSetDevice(device)) != cudaSuccess ||
+    const DeviceScope scope(device);
+    if ((e = scope.status()) != cudaSuccess ||
         (e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess ||
         (e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess ||
         (e = cudaMalloc(reinterpret_cast<void**>(&ctx->d_error), sizeof(int))) != cudaSuccess ||
@@ -130,7 +131,7 @@ rbr_status rbr_ctx_create(int device, rbr_ctx** out) {
 
 void rbr_ctx_destroy(rbr_ctx* ctx) {
     if (!ctx) return;
-    cudaSetDevice(ctx->device);
+    const DeviceScope scope(ctx->device);
     cudaDeviceSynchronize();
     free_scene(ctx);
     free_path_buffers(ctx);
@@ -154,7 +155,7 @@ const char* rbr_last_error(const rbr_ctx* ctx) { return ctx ? ctx->error.c_str()
 
 rbr_status rbr_scene_upload(rbr_ctx* ctx, const rbr_scene_desc* desc) {
     if (!ctx) return RBR_ERR_INVALID_ARGUMENT;
-    cudaSetDevice(ctx->device);
+    const DeviceScope scope(ctx->device);
     cudaDeviceSynchronize();  // nothing may still read the scene being replaced
     return upload_scene(ctx, desc);
 }
@@ -183,6 +184,9 @@ rbr_status rbr_param_set(rbr_ctx* ctx, const char* name, int64_t value) {
     } else if (n == "pt.wave_paths") {
         if (value < 1024 || value > (int64_t(1) << 26)) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "pt.wave_paths is 1024..2^26");
         ctx->pt_wave_paths = static_cast<uint32_t>(value);
+    } else if (n == "bvh.record_cost_milli") {
+        if (value < 1 || value > 100000) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "bvh.record_cost_milli is 1..100000");
+        ctx->bvh_record_cost_milli = static_cast<int>(value);
     } else {
         return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "unknown parameter " + n);
     }
@@ -193,7 +197,7 @@ rbr_status rbr_autotune_trace(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int
     if (!ctx) return RBR_ERR_INVALID_ARGUMENT;
     if (!ctx->has_scene) return fail(ctx, RBR_ERR_NO_SCENE, "rbr_autotune_trace before rbr_scene_upload");
     if (!rays || n == 0) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "rbr_autotune_trace needs rays");
-    cudaSetDevice(ctx->device);
+    const DeviceScope scope(ctx->device);
     return autotune_trace(ctx, rays, n, any_hit, out_us);
 }
 
@@ -207,6 +211,7 @@ rbr_status rbr_param_get(const rbr_ctx* ctx, const char* name, int64_t* value) {
     else if (n == "pt.wave_paths") *value = ctx->pt_wave_paths;
     else if (n == "pt.streams") *value = ctx->pt_streams;
     else if (n == "trace.host_chunk") *value = ctx->trace_host_chunk;
+    else if (n == "bvh.record_cost_milli") *value = ctx->bvh_record_cost_milli;
     else return RBR_ERR_INVALID_ARGUMENT;
     return RBR_OK;
 }
@@ -232,7 +237,7 @@ rbr_status rbr_trace_closest(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, rbr_
     if (!ctx) return RBR_ERR_INVALID_ARGUMENT;
     if (!ctx->has_scene) return fail(ctx, RBR_ERR_NO_SCENE, "rbr_trace_closest before rbr_scene_upload");
     if (n && (!rays || !hits)) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "rays or hits is NULL");
-    cudaSetDevice(ctx->device);
+    const DeviceScope scope(ctx->device);
     const cudaError_t e = launch_trace(ctx, rays, n, 0, hits, static_cast<cudaStream_t>(stream));
     return e == cudaSuccess ? RBR_OK : cuda_fail(ctx, e, "closest-hit launch");
 }
@@ -241,7 +246,7 @@ rbr_status rbr_trace_any(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, uint8_t*
     if (!ctx) return RBR_ERR_INVALID_ARGUMENT;
     if (!ctx->has_scene) return fail(ctx, RBR_ERR_NO_SCENE, "rbr_trace_any before rbr_scene_upload");
     if (n && (!rays || !occluded)) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "rays or occluded is NULL");
-    cudaSetDevice(ctx->device);
+    const DeviceScope scope(ctx->device);
     const cudaError_t e = launch_trace(ctx, rays, n, 1, occluded, static_cast<cudaStream_t>(stream));
     return e == cudaSuccess ? RBR_OK : cuda_fail(ctx, e, "any-hit launch");
 }
@@ -251,7 +256,7 @@ rbr_status rbr_trace_host(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any
     if (!ctx->has_scene) return fail(ctx, RBR_ERR_NO_SCENE, "rbr_trace_host before rbr_scene_upload");
     if (n == 0) return RBR_OK;
     if (!rays || !out) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "rays or out is NULL");
-    cudaSetDevice(ctx->device);
+    const DeviceScope scope(ctx->device);
     const size_t in_bytes = size_t(n) * sizeof(rbr_ray);
     const size_t out_bytes = size_t(n) * (any_hit ? 1 : sizeof(rbr_hit));
     rbr_status st;
@@ -295,7 +300,7 @@ rbr_status rbr_trace_counts(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int a
     if (!ctx || !out) return RBR_ERR_INVALID_ARGUMENT;
     if (!ctx->has_scene) return fail(ctx, RBR_ERR_NO_SCENE, "rbr_trace_counts before rbr_scene_upload");
     if (n && !rays) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "rays is NULL");
-    cudaSetDevice(ctx->device);
+    const DeviceScope scope(ctx->device);
     rbr_status st = ensure(ctx, ctx->stage_out, 2 * sizeof(unsigned long long), "count totals");
     if (st != RBR_OK) return st;
     auto* d = static_cast<unsigned long long*>(ctx->stage_out.ptr);
@@ -313,14 +318,14 @@ rbr_status rbr_trace_counts(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int a
 rbr_status rbr_render(rbr_ctx* ctx, const rbr_camera* camera, const rbr_render_params* params, float* film_mean,
                       float* film_m2, void* stream) {
     if (!ctx) return RBR_ERR_INVALID_ARGUMENT;
-    cudaSetDevice(ctx->device);
+    const DeviceScope scope(ctx->device);
     return render(ctx, camera, params, film_mean, film_m2, static_cast<cudaStream_t>(stream));
 }
 
 rbr_status rbr_render_noalloc(rbr_ctx* ctx, const rbr_camera* camera, const rbr_render_params* params,
                               float* film_mean, void* stream) {
     if (!ctx) return RBR_ERR_INVALID_ARGUMENT;
-    cudaSetDevice(ctx->device);
+    const DeviceScope scope(ctx->device);
     return render_noalloc(ctx, camera, params, film_mean, static_cast<cudaStream_t>(stream));
 }
 
@@ -329,7 +334,7 @@ rbr_status rbr_render_host(rbr_ctx* ctx, const rbr_camera* camera, const rbr_ren
     if (!ctx) return RBR_ERR_INVALID_ARGUMENT;
     if (!camera || !film_mean) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "camera or film_mean is NULL");
     if (camera->width <= 0 || camera->height <= 0) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "empty image");
-    cudaSetDevice(ctx->device);
+    const DeviceScope scope(ctx->device);
     const size_t bytes = size_t(camera->width) * camera->height * 3 * sizeof(float);
     rbr_status st;
     if ((st = ensure(ctx, ctx->stage_out, 2 * bytes, "film staging")) != RBR_OK) return st;
@@ -345,7 +350,7 @@ rbr_status rbr_render_host(rbr_ctx* ctx, const rbr_camera* camera, const rbr_ren
 rbr_status rbr_render_stats_get(rbr_ctx* ctx, rbr_render_stats* out) {
     if (!ctx || !out) return RBR_ERR_INVALID_ARGUMENT;
     if (ctx->render_pending) {
-        cudaSetDevice(ctx->device);
+        const DeviceScope scope(ctx->device);
         cudaError_t e = cudaEventSynchronize(ctx->ev_stop);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "waiting for the render");
         float ms = 0.0f;
@@ -366,66 +371,66 @@ void rbr_cache_config_default(rbr_cache_config* out) {
 
 rbr_status rbr_cache_create(rbr_ctx* ctx, const rbr_cache_config* config) {
     if (!ctx) return RBR_ERR_INVALID_ARGUMENT;
-    cudaSetDevice(ctx->device);
+    const DeviceScope scope(ctx->device);
     cudaDeviceSynchronize();  // nothing may still use the cache being replaced
     return cache_create(ctx, config);
 }
 
 void rbr_cache_destroy(rbr_ctx* ctx) {
     if (!ctx) return;
-    cudaSetDevice(ctx->device);
+    const DeviceScope scope(ctx->device);
     cudaDeviceSynchronize();
     cache_destroy(ctx);
 }
 
 rbr_status rbr_cache_info_get(rbr_ctx* ctx, rbr_cache_info* out) {
     if (!ctx || !out) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "NULL argument");
-    cudaSetDevice(ctx->device);
+    const DeviceScope scope(ctx->device);
     return cache_info(ctx, out);
 }
 
 rbr_status rbr_cache_set_params(rbr_ctx* ctx, const uint16_t* mlp_bf16, const uint16_t* grid_f16) {
     if (!ctx) return RBR_ERR_INVALID_ARGUMENT;
-    cudaSetDevice(ctx->device);
+    const DeviceScope scope(ctx->device);
     cudaDeviceSynchronize();
     return cache_set_params(ctx, mlp_bf16, grid_f16);
 }
 
 rbr_status rbr_cache_get_params(rbr_ctx* ctx, uint16_t* mlp_bf16, uint16_t* grid_f16) {
     if (!ctx) return RBR_ERR_INVALID_ARGUMENT;
-    cudaSetDevice(ctx->device);
+    const DeviceScope scope(ctx->device);
     return cache_get_params(ctx, mlp_bf16, grid_f16);
 }
 
 rbr_status rbr_cache_grads_get(rbr_ctx* ctx, float* mlp, float* grid) {
     if (!ctx) return RBR_ERR_INVALID_ARGUMENT;
-    cudaSetDevice(ctx->device);
+    const DeviceScope scope(ctx->device);
     return cache_grads(ctx, mlp, grid);
 }
 
 rbr_status rbr_cache_encode_host(rbr_ctx* ctx, uint32_t n, const rbr_cache_record* records, float* inputs) {
     if (!ctx) return RBR_ERR_INVALID_ARGUMENT;
-    cudaSetDevice(ctx->device);
+    const DeviceScope scope(ctx->device);
     return cache_encode_host(ctx, n, records, inputs);
 }
 
 rbr_status rbr_cache_infer_host(rbr_ctx* ctx, uint32_t n, const rbr_cache_record* records, float* rgb) {
     if (!ctx) return RBR_ERR_INVALID_ARGUMENT;
-    cudaSetDevice(ctx->device);
+    const DeviceScope scope(ctx->device);
     return cache_infer_host(ctx, n, records, rgb);
 }
 
 rbr_status rbr_cache_train_host(rbr_ctx* ctx, uint32_t n, const rbr_cache_record* records, const float* targets,
                                 int apply, float* loss) {
     if (!ctx) return RBR_ERR_INVALID_ARGUMENT;
-    cudaSetDevice(ctx->device);
+    const DeviceScope scope(ctx->device);
     return cache_train_host(ctx, n, records, targets, apply, loss);
 }
 
 rbr_status rbr_cache_render(rbr_ctx* ctx, const rbr_camera* camera, const rbr_render_params* params, uint32_t frames,
                             int train, float* film_mean, float* film_m2, void* stream) {
     if (!ctx) return RBR_ERR_INVALID_ARGUMENT;
-    cudaSetDevice(ctx->device);
+    const DeviceScope scope(ctx->device);
     return render_cached(ctx, camera, params, frames, train, film_mean, film_m2, static_cast<cudaStream_t>(stream));
 }
 

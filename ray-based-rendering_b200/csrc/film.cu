@@ -40,7 +40,7 @@ extern "C" {
 rbr_status rbr_film_to_rgb8(rbr_ctx* ctx, const float* film, int32_t width, int32_t height, float exposure, float gamma,
                             int tonemap, uint8_t* out, void* stream) {
     if (!ctx || !film || !out || width <= 0 || height <= 0 || !(gamma > 0.0f)) return RBR_ERR_INVALID_ARGUMENT;
-    cudaSetDevice(ctx->device);
+    const DeviceScope scope(ctx->device);
     const uint32_t npix = static_cast<uint32_t>(width) * static_cast<uint32_t>(height);
     const float inv_gamma = 1.0f / gamma;
     const int grid = std::min<int>((npix + 255) / 256, ctx->num_sms * 16);
@@ -53,7 +53,7 @@ rbr_status rbr_film_to_rgb8(rbr_ctx* ctx, const float* film, int32_t width, int3
 rbr_status rbr_film_to_rgb8_host(rbr_ctx* ctx, const float* film, int32_t width, int32_t height, float exposure,
                                  float gamma, int tonemap, uint8_t* out) {
     if (!ctx || !film || !out || width <= 0 || height <= 0) return RBR_ERR_INVALID_ARGUMENT;
-    cudaSetDevice(ctx->device);
+    const DeviceScope scope(ctx->device);
     const size_t npix = size_t(width) * size_t(height);
     rbr_status st = ensure(ctx, ctx->stage_in, npix * 12, "film staging");
     if (st == RBR_OK) st = ensure(ctx, ctx->stage_out, npix * 3, "film staging");

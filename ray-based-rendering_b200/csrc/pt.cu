@@ -21,7 +21,6 @@
 // BSDF-sampled "MIS" trace whose result is discarded (path_tracing_integrator.cpp:118-134)
 // changes nothing and is not traced.
 #include <algorithm>
-#include <mutex>
 
 #include "rbr_bsdf.cuh"
 #include "rbr_context.h"
@@ -1087,23 +1086,15 @@ namespace {
 // Every GPU that loads this library holds this array until the process exits.
 __device__ __align__(256) unsigned char g_render_scratch[RBR_NOALLOC_SCRATCH_BYTES];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_scratch_mutex;
-void* g_scratch_ptr[kMaxDevices] = {};
-
-// Device address of g_render_scratch on the current device (looked up once per device).
-// In host code the array's name only stands in for the symbol; kernels must be given this
-// address, never the host-side name.
-cudaError_t scratch_address(int device, unsigned char** out) {
-    if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> lock(g_scratch_mutex);
-    if (!g_scratch_ptr[device]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_render_scratch);
-        if (e != cudaSuccess) return e;
-        g_scratch_ptr[device] = p;
-    }
-    *out = static_cast<unsigned char*>(g_scratch_ptr[device]);
+// Device address of g_render_scratch on the current device, looked up on every call: the
+// lookup allocates nothing, and a cached address would go stale if the application reset the
+// device or its primary context between calls. In host code the array's name only stands in
+// for the symbol; kernels must be given this address, never the host-side name.
+cudaError_t scratch_address(unsigned char** out) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_render_scratch);
+    if (e != cudaSuccess) return e;
+    *out = static_cast<unsigned char*>(p);
     return cudaSuccess;
 }
 
@@ -1139,7 +1130,7 @@ rbr_status render_noalloc(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_
                         "-byte scratch array (at most " +
                         std::to_string((RBR_NOALLOC_SCRATCH_BYTES - fixed) / per_path) + " samples per pixel)");
     unsigned char* base = nullptr;
-    cudaError_t e = scratch_address(ctx->device, &base);
+    cudaError_t e = scratch_address(&base);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "looking up the render scratch array");
 
     size_t off = 0;

@@ -63,6 +63,7 @@ struct rbr_ctx {
     rbr::DevBuf sort_buf2;         // the same for the second stream of a chunked rbr_trace_host
     uint32_t trace_host_chunk = 1u << 20;  // rbr_trace_host: rays per pipelined chunk (0: one piece)
     uint32_t pt_wave_paths = 1u << 23;
+    int bvh_record_cost_milli = 1000;      // 8-wide collapse: record test cost / node test cost x1000
     // path tracer
     rbr::PathBuffers pt;
     rbr::PathBuffers pt2;                  // second wave in flight (rbr_render, pt_streams 2)
@@ -81,6 +82,30 @@ struct rbr_ctx {
 };
 
 namespace rbr {
+
+// Makes `device` current for the lifetime of the scope and gives the calling thread its
+// previous current device back at exit: an entry point never changes the caller's device.
+class DeviceScope {
+  public:
+    explicit DeviceScope(int device) : device_(device) {
+        if (cudaGetDevice(&prev_) != cudaSuccess) {
+            cudaGetLastError();
+            prev_ = -1;
+        }
+        if (prev_ != device_) status_ = cudaSetDevice(device_);
+    }
+    ~DeviceScope() {
+        if (prev_ >= 0 && prev_ != device_) cudaSetDevice(prev_);
+    }
+    DeviceScope(const DeviceScope&) = delete;
+    DeviceScope& operator=(const DeviceScope&) = delete;
+    cudaError_t status() const { return status_; }
+
+  private:
+    int device_;
+    int prev_ = -1;
+    cudaError_t status_ = cudaSuccess;
+};
 
 rbr_status fail(rbr_ctx* ctx, rbr_status code, const std::string& msg);
 rbr_status cuda_fail(rbr_ctx* ctx, cudaError_t e, const char* what);

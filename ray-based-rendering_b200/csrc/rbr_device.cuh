@@ -172,10 +172,34 @@ __device__ __forceinline__ RayCtx make_ctx(f3 o, f3 d) {
     return r;
 }
 
-// byte i of a 64-bit pair, as an exact float
-__device__ __forceinline__ float qbyte(uint2 w, int i) {
-    const uint32_t word = (i < 4) ? w.x : w.y;
-    return __uint_as_float(__byte_perm(word, 0x4B000000u, 0x7650 | (i & 3))) - 8388608.0f;
+// kGridBias + (byte k of word), exactly: one byte permute of the byte into bits 8-15 of the
+// mantissa of 32768.0f (bits 0x47000000).
+__device__ __forceinline__ float qplane(uint32_t word, uint32_t k) {
+    return __uint_as_float(__byte_perm(word, kGridBiasBits, 0x7404u | (k << 4)));
+}
+
+// Three-input minimum / maximum (sm_100); a NaN input is ignored unless all three are NaN.
+__device__ __forceinline__ float fmax3(float a, float b, float c) {
+    float d;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+__device__ __forceinline__ float fmin3(float a, float b, float c) {
+    float d;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+
+// Mask of (width & 31) bits starting at bit (pos & 31); bits above 31 are dropped.
+__device__ __forceinline__ uint32_t bitmask_at(uint32_t pos, uint32_t width) {
+    uint32_t d;
+    asm("bmsk.wrap.b32 %0, %1, %2;" : "=r"(d) : "r"(pos), "r"(width));
+    return d;
+}
+
+// Byte j of the result = oct if slot j of the four slots in imask4 is internal, else 0.
+__device__ __forceinline__ uint32_t inner_oct4(uint32_t imask4, uint32_t oct) {
+    return ((imask4 * 0x00204081u) & 0x01010101u) * oct;
 }
 
 // Relative widening of box intervals in t (2^-16): covers the rounding of the slab
@@ -183,55 +207,93 @@ __device__ __forceinline__ float qbyte(uint2 w, int i) {
 constexpr float kTLo = 1.0f - 1.0f / 65536.0f;
 constexpr float kTHi = 1.0f + 1.0f / 65536.0f;
 
-// Tests the 8 children of node `idx`. ngroup = (child_base, hit bits << 24 | imask << 16),
-// pgroup = (prim_base, mask of the node's leaf records to test: up to 8 leaves of up to 4
-// records, 32 bits).
-__device__ __forceinline__ void intersect_node(const uint4* __restrict__ nodes, uint32_t idx, const RayCtx& r,
-                                               float tbest, uint2& ngroup, uint2& pgroup) {
+// Per node and ray: the slab arithmetic of the node's grid and its slot bookkeeping.
+// Plane byte q of axis k is hit at t = (kGridBias + q) a_k + b_k with a_k = s_k / d_k and
+// b_k = (p_k - o_k) / d_k; near planes are scaled by kTLo and far planes by kTHi (the
+// widening), so a (near, far) pair is one packed FMA.
+struct NodeView {
+    float2 ax, bx, ay, by, az, bz;   // (near, far) factors per axis
+    uint2 nx, fx, ny, fy, nz, fz;    // near / far plane bytes per axis (8 slots)
+    uint32_t pos_lo, pos_hi;         // meta bytes with internal positions XOR the ray octant
+    uint32_t wid_lo, wid_hi;         // widths of the slots' bit ranges
+    uint32_t imask, child_base, prim_base;
+};
+
+__device__ __forceinline__ NodeView node_view(const uint4* __restrict__ nodes, uint32_t idx, const RayCtx& r) {
     const uint4* np = nodes + 5 * static_cast<size_t>(idx);
     const uint4 w0 = __ldg(np);
     const uint4 w1 = __ldg(np + 1);
     const uint4 w2 = __ldg(np + 2);
     const uint4 w3 = __ldg(np + 3);
     const uint4 w4 = __ldg(np + 4);
+    NodeView v;
     const float sx = __uint_as_float((w0.w & 0xFFu) << 23);
     const float sy = __uint_as_float(((w0.w >> 8) & 0xFFu) << 23);
     const float sz = __uint_as_float(((w0.w >> 16) & 0xFFu) << 23);
-    const uint32_t imask = w0.w >> 24;
+    const float2 kw = make_float2(kTLo, kTHi);
     const float ax = sx * r.ix, ay = sy * r.iy, az = sz * r.iz;
     const float bx = (__uint_as_float(w0.x) - r.o.x) * r.ix;
     const float by = (__uint_as_float(w0.y) - r.o.y) * r.iy;
     const float bz = (__uint_as_float(w0.z) - r.o.z) * r.iz;
+    v.ax = __fmul2_rn(make_float2(ax, ax), kw);
+    v.bx = __fmul2_rn(make_float2(bx, bx), kw);
+    v.ay = __fmul2_rn(make_float2(ay, ay), kw);
+    v.by = __fmul2_rn(make_float2(by, by), kw);
+    v.az = __fmul2_rn(make_float2(az, az), kw);
+    v.bz = __fmul2_rn(make_float2(bz, bz), kw);
     const uint2 qlox = make_uint2(w2.x, w2.y), qloy = make_uint2(w2.z, w2.w), qloz = make_uint2(w3.x, w3.y);
     const uint2 qhix = make_uint2(w3.z, w3.w), qhiy = make_uint2(w4.x, w4.y), qhiz = make_uint2(w4.z, w4.w);
-    const uint2 nearx = r.nx ? qhix : qlox, farx = r.nx ? qlox : qhix;
-    const uint2 neary = r.ny ? qhiy : qloy, fary = r.ny ? qloy : qhiy;
-    const uint2 nearz = r.nz ? qhiz : qloz, farz = r.nz ? qloz : qhiz;
-    uint32_t cbits = 0, pbits = 0;
-    const uint32_t meta_lo = w1.z, meta_hi = w1.w;
+    v.nx = r.nx ? qhix : qlox;
+    v.fx = r.nx ? qlox : qhix;
+    v.ny = r.ny ? qhiy : qloy;
+    v.fy = r.ny ? qloy : qhiy;
+    v.nz = r.nz ? qhiz : qloz;
+    v.fz = r.nz ? qloz : qhiz;
+    v.imask = w0.w >> 24;
+    v.pos_lo = w1.z ^ inner_oct4(v.imask & 0xFu, r.oct);
+    v.pos_hi = w1.w ^ inner_oct4(v.imask >> 4, r.oct);
+    v.wid_lo = (w1.z >> 5) & 0x07070707u;
+    v.wid_hi = (w1.w >> 5) & 0x07070707u;
+    v.child_base = w1.x;
+    v.prim_base = w1.y;
+    return v;
+}
+
+// Slab test of slot i (0..7) against [0, tbest].
+__device__ __forceinline__ bool slot_hit(const NodeView& v, int i, float tbest) {
+    const uint32_t k = static_cast<uint32_t>(i & 3);
+    const bool h = i >= 4;
+    const float2 tx = __ffma2_rn(make_float2(qplane(h ? v.nx.y : v.nx.x, k), qplane(h ? v.fx.y : v.fx.x, k)), v.ax, v.bx);
+    const float2 ty = __ffma2_rn(make_float2(qplane(h ? v.ny.y : v.ny.x, k), qplane(h ? v.fy.y : v.fy.x, k)), v.ay, v.by);
+    const float2 tz = __ffma2_rn(make_float2(qplane(h ? v.nz.y : v.nz.x, k), qplane(h ? v.fz.y : v.fz.x, k)), v.az, v.bz);
+    const float tn = fmax3(tx.x, ty.x, tz.x);
+    const float tf = fmin3(tx.y, ty.y, tz.y);
+    return fmaxf(tn, 0.0f) <= fminf(tf, tbest);
+}
+
+// Bits of slot i in the node's hit mask: its leaf records, or bit 24 + (slot ^ octant).
+__device__ __forceinline__ uint32_t slot_bits(const NodeView& v, int i) {
+    const uint32_t sh = 8u * static_cast<uint32_t>(i & 3);
+    return bitmask_at((i >= 4 ? v.pos_hi : v.pos_lo) >> sh, (i >= 4 ? v.wid_hi : v.wid_lo) >> sh);
+}
+
+// Splits a node's hit mask into ngroup = (child_base, internal hit bits << 24 | imask << 16)
+// and pgroup = (prim_base, mask of the leaf records to test).
+__device__ __forceinline__ void split_hits(const NodeView& v, uint32_t bits, uint2& ngroup, uint2& pgroup) {
+    const uint32_t inner = v.imask ? 0xFF000000u : 0u;
+    ngroup = make_uint2(v.child_base, (bits & inner) | (v.imask << 16));
+    pgroup = make_uint2(v.prim_base, bits & ~inner);
+}
+
+// Tests the 8 children of node `idx`.
+__device__ __forceinline__ void intersect_node(const uint4* __restrict__ nodes, uint32_t idx, const RayCtx& r,
+                                               float tbest, uint2& ngroup, uint2& pgroup) {
+    const NodeView v = node_view(nodes, idx, r);
+    uint32_t bits = 0;
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        const float tnx = fmaf(qbyte(nearx, i), ax, bx);
-        const float tny = fmaf(qbyte(neary, i), ay, by);
-        const float tnz = fmaf(qbyte(nearz, i), az, bz);
-        const float tfx = fmaf(qbyte(farx, i), ax, bx);
-        const float tfy = fmaf(qbyte(fary, i), ay, by);
-        const float tfz = fmaf(qbyte(farz, i), az, bz);
-        const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f)) * kTLo;
-        const float tf = fminf(fminf(tfx, tfy), tfz) * kTHi;
-        if (tn <= tf && tn <= tbest) {
-            if ((imask >> i) & 1u) {
-                // internal child: bit (slot ^ oct), so the highest set bit is nearest-first
-                cbits |= 1u << (24 + (static_cast<uint32_t>(i) ^ r.oct));
-            } else {
-                // leaf: count in bits 5-7, first record offset in bits 0-4 (empty slots: 0)
-                const uint32_t meta = ((i < 4 ? meta_lo : meta_hi) >> (8 * (i & 3))) & 0xFFu;
-                pbits |= ((1u << (meta >> 5)) - 1u) << (meta & 31u);
-            }
-        }
-    }
-    ngroup = make_uint2(w1.x, cbits | (imask << 16));
-    pgroup = make_uint2(w1.y, pbits);
+    for (int i = 0; i < 8; ++i)
+        if (slot_hit(v, i, tbest)) bits |= slot_bits(v, i);
+    split_hits(v, bits, ngroup, pgroup);
 }
 
 // ----------------------------------------------------------------------------------------

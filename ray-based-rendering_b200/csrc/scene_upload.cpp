@@ -356,7 +356,7 @@ rbr_status upload_scene(rbr_ctx* ctx, const rbr_scene_desc* d) {
     std::vector<Box> hit_boxes(boxes.size());
     for (size_t b = 0; b < boxes.size(); ++b) hit_boxes[b] = hit_region_box(&words[b * kRecordWords], boxes[b], maxabs);
     const int threads = std::max(1u, std::thread::hardware_concurrency());
-    WideBVH bvh = build_wide_bvh(hit_boxes, maxabs * (1.0f / 1048576.0f), threads);
+    WideBVH bvh = build_wide_bvh(hit_boxes, maxabs * (1.0f / 1048576.0f), threads, ctx->bvh_record_cost_milli / 1000.0);
 
     std::vector<uint32_t> records(bvh.leaf_order.size() * kRecordWords);
     for (size_t r = 0; r < bvh.leaf_order.size(); ++r) {
@@ -418,6 +418,8 @@ rbr_status upload_scene(rbr_ctx* ctx, const rbr_scene_desc* d) {
     ctx->stats.num_wide_nodes = s.num_nodes;
     ctx->stats.num_leaf_records = static_cast<uint32_t>(bvh.leaf_order.size());
     ctx->stats.max_depth = bvh.max_depth;
+    ctx->stats.wrapped_leaves = bvh.wrapped_leaves;
+    ctx->stats.record_cost_milli = static_cast<uint32_t>(ctx->bvh_record_cost_milli);
     ctx->stats.build_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     if (bvh.max_depth >= static_cast<uint32_t>(kStackSize))
         return fail(ctx, RBR_ERR_INTERNAL, "BVH deeper than the traversal stack");

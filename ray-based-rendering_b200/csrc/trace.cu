@@ -190,8 +190,8 @@ __global__ void __launch_bounds__(kPersistBlock) k_trace_persist(DeviceScene s, 
 
 // ------------------------------------------------------------------------------------------
 // Warp-cooperative traversal: a group of 8 lanes traces one ray (4 rays per warp). In a node
-// step lane j tests child slot j of the node and the group combines the results with a ballot
-// (internal children) and an OR-shuffle (leaf records); in a leaf step the lanes test up to 8
+// step lane j tests child slot j of the node and the group ORs the slots' bits of the node's
+// hit mask (internal children and leaf records) with shuffles; in a leaf step the lanes test up to 8
 // of the node's leaf records at once and keep the closest with a shuffle min-reduction
 // (key = t bits, then the highest id). Group state is replicated in the 8 lanes, so the group
 // never diverges internally; the short stack lives in shared memory (all 8 lanes write the
@@ -313,7 +313,7 @@ __global__ void __launch_bounds__(kCoopBlock) k_trace_coop(DeviceScene s, const 
                     }
                 }
             }
-            // drop the (up to) 8 records just tested (record bits occupy bits 0-23)
+            // drop the (up to) 8 records just tested
             pg.y = __popc(pg.y) <= 8 ? 0u : pg.y & ~((2u << nth_set_bit(pg.y, 7)) - 1u);
         } else {
             // node step (after a pop if the current group is exhausted)
@@ -334,41 +334,14 @@ __global__ void __launch_bounds__(kCoopBlock) k_trace_coop(DeviceScene s, const 
                     if (sp < kStackSize) stack[sp++] = ng;
                     else atomicOr(err, kErrStackOverflow);
                 }
-                const uint4* np = s.nodes + 5 * static_cast<size_t>(child);
-                const uint4 w0 = __ldg(np), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3),
-                            w4 = __ldg(np + 4);
-                const float sx = __uint_as_float((w0.w & 0xFFu) << 23);
-                const float sy = __uint_as_float(((w0.w >> 8) & 0xFFu) << 23);
-                const float sz = __uint_as_float(((w0.w >> 16) & 0xFFu) << 23);
-                const uint32_t imask = w0.w >> 24;
+                // lane j tests slot j; the group ORs the slots' bits of the node's hit mask
+                const NodeView v = node_view(s.nodes, child, r);
                 const int jj = static_cast<int>(j);
-                const uint2 qlox = make_uint2(w2.x, w2.y), qloy = make_uint2(w2.z, w2.w), qloz = make_uint2(w3.x, w3.y);
-                const uint2 qhix = make_uint2(w3.z, w3.w), qhiy = make_uint2(w4.x, w4.y), qhiz = make_uint2(w4.z, w4.w);
-                const float lx = qbyte(qlox, jj), hx = qbyte(qhix, jj);
-                const float ly = qbyte(qloy, jj), hy = qbyte(qhiy, jj);
-                const float lz = qbyte(qloz, jj), hz = qbyte(qhiz, jj);
-                const float ax = sx * r.ix, ay = sy * r.iy, az = sz * r.iz;
-                const float bx = (__uint_as_float(w0.x) - r.o.x) * r.ix;
-                const float by = (__uint_as_float(w0.y) - r.o.y) * r.iy;
-                const float bz = (__uint_as_float(w0.z) - r.o.z) * r.iz;
-                const float tnx = fmaf(r.nx ? hx : lx, ax, bx), tfx = fmaf(r.nx ? lx : hx, ax, bx);
-                const float tny = fmaf(r.ny ? hy : ly, ay, by), tfy = fmaf(r.ny ? ly : hy, ay, by);
-                const float tnz = fmaf(r.nz ? hz : lz, az, bz), tfz = fmaf(r.nz ? lz : hz, az, bz);
-                const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f)) * kTLo;
-                const float tf = fminf(fminf(tfx, tfy), tfz) * kTHi;
-                const bool hit = tn <= tf && tn <= tbest;
-                const uint32_t hm = (__ballot_sync(gmask, hit) >> (8 * g)) & 0xFFu;
-                uint32_t ih = hm & imask;
-                if (r.oct & 1u) ih = ((ih & 0x55u) << 1) | ((ih >> 1) & 0x55u);
-                if (r.oct & 2u) ih = ((ih & 0x33u) << 2) | ((ih >> 2) & 0x33u);
-                if (r.oct & 4u) ih = ((ih & 0x0Fu) << 4) | ((ih >> 4) & 0x0Fu);
-                const uint32_t meta = ((j < 4 ? w1.z : w1.w) >> (8 * (j & 3))) & 0xFFu;
-                uint32_t lb = hit ? ((1u << (meta >> 5)) - 1u) << (meta & 31u) : 0u;  // 0 for internal/empty
-                lb |= __shfl_xor_sync(gmask, lb, 1, 8);
-                lb |= __shfl_xor_sync(gmask, lb, 2, 8);
-                lb |= __shfl_xor_sync(gmask, lb, 4, 8);
-                ng = make_uint2(w1.x, (ih << 24) | (imask << 16));
-                pg = make_uint2(w1.y, lb);
+                uint32_t bits = slot_hit(v, jj, tbest) ? slot_bits(v, jj) : 0u;
+                bits |= __shfl_xor_sync(gmask, bits, 1, 8);
+                bits |= __shfl_xor_sync(gmask, bits, 2, 8);
+                bits |= __shfl_xor_sync(gmask, bits, 4, 8);
+                split_hits(v, bits, ng, pg);
             }
         }
         if (finished) {

@@ -182,7 +182,7 @@ rbr_status rbr_bsdf_eval_host(rbr_ctx* ctx, const rbr_material* m, uint32_t n, c
                               float* out) {
     if (!ctx || !m || (n && (!wo || !wi || !out))) return RBR_ERR_INVALID_ARGUMENT;
     if (n == 0) return RBR_OK;
-    cudaSetDevice(ctx->device);
+    const DeviceScope scope(ctx->device);
     const MaterialDev md = to_dev(*m);
     return run_unit(ctx, {{wo, 3 * size_t(n)}, {wi, 3 * size_t(n)}}, 6 * size_t(n), out,
                     [&](const std::vector<const float*>& d, float* o) {
@@ -194,7 +194,7 @@ rbr_status rbr_bsdf_sample_host(rbr_ctx* ctx, const rbr_material* m, uint32_t n,
                                 float* out) {
     if (!ctx || !m || (n && (!wo || !u || !out))) return RBR_ERR_INVALID_ARGUMENT;
     if (n == 0) return RBR_OK;
-    cudaSetDevice(ctx->device);
+    const DeviceScope scope(ctx->device);
     const MaterialDev md = to_dev(*m);
     return run_unit(ctx, {{wo, 3 * size_t(n)}, {u, 2 * size_t(n)}}, 8 * size_t(n), out,
                     [&](const std::vector<const float*>& d, float* o) {
@@ -207,7 +207,7 @@ rbr_status rbr_light_sample_host(rbr_ctx* ctx, const rbr_light* l, uint32_t n, c
     if (!ctx || !l || (n && (!points || !u || !out))) return RBR_ERR_INVALID_ARGUMENT;
     if (l->type != RBR_LIGHT_AREA && l->type != RBR_LIGHT_POINT) return RBR_ERR_UNSUPPORTED;
     if (n == 0) return RBR_OK;
-    cudaSetDevice(ctx->device);
+    const DeviceScope scope(ctx->device);
     LightDev ld{};
     ld.type = l->type;
     for (int a = 0; a < 3; ++a) {
@@ -239,7 +239,7 @@ rbr_status rbr_camera_rays_host(rbr_ctx* ctx, const rbr_camera* c, uint32_t n, c
     if (!ctx || !c || (n && (!samples || !out))) return RBR_ERR_INVALID_ARGUMENT;
     if (c->model != RBR_CAMERA_PINHOLE && c->model != RBR_CAMERA_THIN_LENS) return RBR_ERR_UNSUPPORTED;
     if (n == 0) return RBR_OK;
-    cudaSetDevice(ctx->device);
+    const DeviceScope scope(ctx->device);
     CameraDev cd{};
     cd.width = c->width;
     cd.height = c->height;
@@ -265,7 +265,7 @@ rbr_status rbr_camera_rays_host(rbr_ctx* ctx, const rbr_camera* c, uint32_t n, c
 rbr_status rbr_mis_weights_host(rbr_ctx* ctx, uint32_t n, const float* pdf_pairs, float* out) {
     if (!ctx || (n && (!pdf_pairs || !out))) return RBR_ERR_INVALID_ARGUMENT;
     if (n == 0) return RBR_OK;
-    cudaSetDevice(ctx->device);
+    const DeviceScope scope(ctx->device);
     return run_unit(ctx, {{pdf_pairs, 2 * size_t(n)}}, size_t(n), out,
                     [&](const std::vector<const float*>& d, float* o) {
                         k_mis<<<blocks(n), kUnitBlock, 0, ctx->stream>>>(n, d[0], o);
@@ -275,7 +275,7 @@ rbr_status rbr_mis_weights_host(rbr_ctx* ctx, uint32_t n, const float* pdf_pairs
 rbr_status rbr_phase_eval_host(rbr_ctx* ctx, float g, uint32_t n, const float* wo, const float* wi, float* out) {
     if (!ctx || (n && (!wo || !wi || !out))) return RBR_ERR_INVALID_ARGUMENT;
     if (n == 0) return RBR_OK;
-    cudaSetDevice(ctx->device);
+    const DeviceScope scope(ctx->device);
     return run_unit(ctx, {{wo, 3 * size_t(n)}, {wi, 3 * size_t(n)}}, size_t(n), out,
                     [&](const std::vector<const float*>& d, float* o) {
                         k_hg_eval<<<blocks(n), kUnitBlock, 0, ctx->stream>>>(g, n, d[0], d[1], o);
@@ -285,7 +285,7 @@ rbr_status rbr_phase_eval_host(rbr_ctx* ctx, float g, uint32_t n, const float* w
 rbr_status rbr_phase_sample_host(rbr_ctx* ctx, float g, uint32_t n, const float* wo, const float* u, float* out) {
     if (!ctx || (n && (!wo || !u || !out))) return RBR_ERR_INVALID_ARGUMENT;
     if (n == 0) return RBR_OK;
-    cudaSetDevice(ctx->device);
+    const DeviceScope scope(ctx->device);
     return run_unit(ctx, {{wo, 3 * size_t(n)}, {u, 2 * size_t(n)}}, 3 * size_t(n), out,
                     [&](const std::vector<const float*>& d, float* o) {
                         k_hg_sample<<<blocks(n), kUnitBlock, 0, ctx->stream>>>(g, n, d[0], d[1], o);
@@ -296,7 +296,7 @@ rbr_status rbr_medium_sample_host(rbr_ctx* ctx, const rbr_medium* medium, uint32
                                   const float* u, float* out) {
     if (!ctx || !medium || (n && (!max_dist || !u || !out))) return RBR_ERR_INVALID_ARGUMENT;
     if (n == 0) return RBR_OK;
-    cudaSetDevice(ctx->device);
+    const DeviceScope scope(ctx->device);
     DeviceScene s{};
     s.has_medium = 1;
     for (int a = 0; a < 3; ++a) {
@@ -314,7 +314,7 @@ rbr_status rbr_medium_sample_host(rbr_ctx* ctx, const rbr_medium* medium, uint32
 rbr_status rbr_l2_read_bandwidth(rbr_ctx* ctx, uint64_t bytes, uint32_t passes, double* gb_per_s) {
     if (!ctx || !gb_per_s || bytes < 4096 || bytes > (uint64_t(1) << 30) || passes == 0 || passes > 1000)
         return RBR_ERR_INVALID_ARGUMENT;
-    cudaSetDevice(ctx->device);
+    const DeviceScope scope(ctx->device);
     const size_t n4 = bytes / 16;
     rbr_status st = ensure(ctx, ctx->stage_in, n4 * 16 + 16, "L2 bandwidth buffer");
     if (st != RBR_OK) return st;

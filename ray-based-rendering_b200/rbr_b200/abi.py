@@ -105,6 +105,8 @@ class rbr_scene_stats(C.Structure):
         ("num_wide_nodes", C.c_uint32),
         ("num_leaf_records", C.c_uint32),
         ("max_depth", C.c_uint32),
+        ("wrapped_leaves", C.c_uint32),
+        ("record_cost_milli", C.c_uint32),
         ("device_bytes", C.c_uint64),
         ("build_seconds", C.c_double),
     ]

@@ -63,8 +63,8 @@ void slot_box(const uint32_t* w, int s, double lo[3], double hi[3]) {
         uint64_t ql, qh;
         std::memcpy(&ql, &w[8 + 2 * a], 8);
         std::memcpy(&qh, &w[14 + 2 * a], 8);
-        lo[a] = p + std::ldexp(static_cast<double>((ql >> (8 * s)) & 0xFFu), e);
-        hi[a] = p + std::ldexp(static_cast<double>((qh >> (8 * s)) & 0xFFu), e);
+        lo[a] = p + std::ldexp(kGridBias + static_cast<double>((ql >> (8 * s)) & 0xFFu), e);
+        hi[a] = p + std::ldexp(kGridBias + static_cast<double>((qh >> (8 * s)) & 0xFFu), e);
     }
 }
 
@@ -96,6 +96,7 @@ int check_layout(const Tree& t, const std::vector<Box>& boxes) {
         for (int s = 0; s < 8; ++s) {
             const uint32_t m = static_cast<uint32_t>((meta >> (8 * s)) & 0xFFu);
             if ((imask >> s) & 1u) {
+                if (m != ((1u << 5) | (24u + static_cast<uint32_t>(s)))) return fail("internal slot meta", it.node, s);
                 Item c{w[4] + rank++, it.path};
                 c.path.push_back({it.node, s});
                 todo.push_back(c);
@@ -125,6 +126,8 @@ int check_layout(const Tree& t, const std::vector<Box>& boxes) {
             }
         }
         if (records > 32) return fail("more than 32 records in one node", records);
+        if (imask != 0 && records > kInnerRecordLimit)
+            return fail("records beside internal children beyond the limit", it.node, records);
     }
     for (size_t i = 0; i < n; ++i)
         if (seen[i] != 1) return fail("primitive not in exactly one leaf", i, static_cast<size_t>(seen[i]));
@@ -148,14 +151,17 @@ int replay(const Tree& t, const std::vector<float>& tris, V o, V d, float tmax) 
     };
     auto visit = [&](uint32_t idx, G& ng, G& pg) {
         const uint32_t* w = t.node(idx);
-        float p[3], A[3], B[3];
+        float p[3], A[3][2], B[3][2];
         std::memcpy(p, w, 12);
+        const float kw[2] = {1.0f - 1.0f / 65536.0f, 1.0f + 1.0f / 65536.0f};
         for (int a = 0; a < 3; ++a) {
             const uint32_t bits = ((w[3] >> (8 * a)) & 0xFFu) << 23;
             float sc;
             std::memcpy(&sc, &bits, 4);
-            A[a] = sc * inv[a];
-            B[a] = (p[a] - oo[a]) * inv[a];
+            for (int j = 0; j < 2; ++j) {
+                A[a][j] = (sc * inv[a]) * kw[j];
+                B[a][j] = ((p[a] - oo[a]) * inv[a]) * kw[j];
+            }
         }
         const uint32_t imask = w[3] >> 24;
         uint64_t ql[3], qh[3], meta;
@@ -164,26 +170,26 @@ int replay(const Tree& t, const std::vector<float>& tris, V o, V d, float tmax) 
             std::memcpy(&qh[a], &w[14 + 2 * a], 8);
         }
         std::memcpy(&meta, &w[6], 8);
-        uint32_t cbits = 0, pbits = 0;
+        uint32_t bits = 0;
         for (int i = 0; i < 8; ++i) {
             float tn[3], tf[3];
             for (int a = 0; a < 3; ++a) {
-                tn[a] = std::fma(qbyte(neg[a] ? qh[a] : ql[a], i), A[a], B[a]);
-                tf[a] = std::fma(qbyte(neg[a] ? ql[a] : qh[a], i), A[a], B[a]);
+                tn[a] = std::fma(static_cast<float>(kGridBias) + qbyte(neg[a] ? qh[a] : ql[a], i), A[a][0], B[a][0]);
+                tf[a] = std::fma(static_cast<float>(kGridBias) + qbyte(neg[a] ? ql[a] : qh[a], i), A[a][1], B[a][1]);
             }
-            const float n_ = std::max(std::max(tn[0], tn[1]), std::max(tn[2], 0.0f)) * (1.0f - 1.0f / 65536.0f);
-            const float f_ = std::min(std::min(tf[0], tf[1]), tf[2]) * (1.0f + 1.0f / 65536.0f);
-            if (n_ <= f_ && n_ <= tbest) {
-                if ((imask >> i) & 1u) {
-                    cbits |= 1u << (24 + (static_cast<uint32_t>(i) ^ oct));
-                } else {
-                    const uint32_t m = static_cast<uint32_t>((meta >> (8 * i)) & 0xFFu);
-                    pbits |= ((1u << (m >> 5)) - 1u) << (m & 31u);
-                }
+            const float n_ = std::max({tn[0], tn[1], tn[2], 0.0f});
+            const float f_ = std::min({tf[0], tf[1], tf[2], tbest});
+            if (n_ <= f_) {
+                uint32_t m = static_cast<uint32_t>((meta >> (8 * i)) & 0xFFu);
+                if ((imask >> i) & 1u) m ^= oct;  // internal: bit 24 + (slot ^ octant)
+                const uint32_t pos = m & 31u, width = m >> 5;
+                const uint64_t mask = ((uint64_t(1) << width) - 1u) << pos;
+                bits |= static_cast<uint32_t>(mask);
             }
         }
-        ng = {w[4], cbits | (imask << 16)};
-        pg = {w[5], pbits};
+        const uint32_t inner = imask ? 0xFF000000u : 0u;
+        ng = {w[4], (bits & inner) | (imask << 16)};
+        pg = {w[5], bits & ~inner};
     };
     G stack[kStackSize];
     int sp = 0;
@@ -281,17 +287,24 @@ int main() {
         std::normal_distribution<float> N(0.0f, 1.0f);
         int mismatches = 0, hits = 0;
         const int rays = 2000;
+        std::uniform_int_distribution<size_t> T(0, nt - 1);
         for (int r = 0; r < rays; ++r) {
             V o{U(rng), U(rng), U(rng)}, d{N(rng), N(rng), N(rng)};
-            if (r % 5 == 0) d = {0.0f, 0.0f, (r % 10 == 0) ? 1.0f : -1.0f};  // axis-aligned: zero components
+            if (r % 2 == 1) {  // aimed at a random triangle's centroid: hits in every case
+                const float* tr = &tris[9 * T(rng)];
+                const V c{(tr[0] + tr[3] + tr[6]) / 3.0f, (tr[1] + tr[4] + tr[7]) / 3.0f, (tr[2] + tr[5] + tr[8]) / 3.0f};
+                d = sub(c, o);
+            } else if (r % 5 == 0) {
+                d = {0.0f, 0.0f, (r % 10 == 0) ? 1.0f : -1.0f};  // axis-aligned: zero components
+            }
             const float l = std::sqrt(dot(d, d));
             d = {d.x / l, d.y / l, d.z / l};
             const int a = replay(t, tris, o, d, 1e30f), b = brute(tris, o, d, 1e30f);
             hits += b >= 0;
             if (a != b) ++mismatches;
         }
-        std::printf("kind %d, %zu triangles: %zu wide nodes, depth %u, %d of %d rays hit, %d mismatches\n", c.kind, nt,
-                    t.nodes(), bvh.max_depth, hits, rays, mismatches);
+        std::printf("kind %d, %zu triangles: %zu wide nodes, depth %u, %u wrapped leaves, %d of %d rays hit, "
+                    "%d mismatches\n", c.kind, nt, t.nodes(), bvh.max_depth, bvh.wrapped_leaves, hits, rays, mismatches);
         if (mismatches) ++failures;
     }
     return failures ? 1 : 0;

@@ -1,7 +1,7 @@
 // The reference's own non-path-tracing integrators (Whitted, simple, normals, depth, ambient
 // occlusion) rendering the reference's Cornell box with GpuBVHAccelerator as the scene's
-// accelerator, selected through Scene::setAcceleratorType the way the registration shown in
-// INTEGRATION.md selects it: every image equals the one rendered through the reference's BVH
+// accelerator, selected through Scene::setAcceleratorType the way a registration of
+// GpuBVHAccelerator in the reference's accelerator factory selects it: every image equals the one rendered through the reference's BVH
 // (the GPU answers each per-ray query with the same primitive and the same t). This is the
 // per-ray path of the accelerator drop-in. Exit code 0 = all checks passed. Needs a CUDA device.
 

@@ -134,3 +134,54 @@ def mis_pairs():
 def unit_vectors(rng, n):
     v = rng.normal(size=(n, 3))
     return (v / np.linalg.norm(v, axis=1, keepdims=True)).astype(F32)
+
+
+def ggx_small(width=64, height=36, mesh_n=60):
+    """The GGX material scene (rbr_b200.scenes.ggx_scene: 256 spheres of random materials with
+    20 % glass, rough metals and rough dielectrics, a mound mesh on a ground quad, two quad area
+    lights with coincident emissive quads, a point light, a thin-lens camera) on a reduced film
+    and mesh, plus four spheres in front of the mound with the smooth (delta-lobe) materials the
+    random draw never produces (roughness below 0.03): clear glass, a mirror, smooth plastic and a
+    smooth half-transmissive dielectric."""
+    from rbr_b200 import scenes
+
+    s = scenes.ggx_scene(width=width, height=height, mesh_n=mesh_n, seed=0)
+    extra = [((-2.2, 0.6, 6.0, 0.6), dict(base_color=(1, 1, 1), roughness=0.0, ior=1.5, transmission=1.0)),
+             ((-0.7, 0.5, 7.0, 0.5), dict(base_color=(0.9, 0.9, 0.9), metallic=1.0, roughness=0.0)),
+             ((0.8, 0.5, 7.0, 0.5), dict(base_color=(0.2, 0.4, 0.8), roughness=0.0, ior=1.5)),
+             ((2.3, 0.6, 6.0, 0.6), dict(base_color=(0.8, 0.9, 0.7), roughness=0.0, ior=1.5, transmission=0.5))]
+    sph, mats = list(s.spheres), list(s.sphere_materials)
+    for geom, m in extra:
+        sph.append(geom)
+        mats.append(s.add_material(**m))
+    s.spheres = np.asarray(sph, F32)
+    s.sphere_materials = np.asarray(mats, np.uint32)
+    return s
+
+
+def moments_z(S1, Q1, n1, S2, Q2, n2):
+    """Per-pixel-channel z scores of two sets of sample moments (sums and sums of squares of n1
+    and n2 independent samples), and the z score of the difference of their image means."""
+    mu1, mu2 = S1 / n1, S2 / n2
+    var1 = np.maximum(Q1 / n1 - mu1 ** 2, 0) * n1 / (n1 - 1)
+    var2 = np.maximum(Q2 / n2 - mu2 ** 2, 0) * n2 / (n2 - 1)
+    se = np.sqrt(var1 / n1 + var2 / n2)
+    z = np.abs(mu1 - mu2) / np.maximum(se, 1e-12)
+    z[(se == 0) & (np.abs(mu1 - mu2) < 1e-6)] = 0
+    m = mu1.size
+    z_img = abs(mu1.mean() - mu2.mean()) / max(np.sqrt((var1 / n1 + var2 / n2).sum()) / m, 1e-12)
+    return z, z_img
+
+
+def crop_camera(cam, x0, y0, width, height):
+    """The pixels [x0, x0 + width) x [y0, y0 + height) of `cam`'s film as a camera of their own:
+    the same rays per pixel, principal point shifted by the crop origin."""
+    import ctypes as C
+
+    c = abi.rbr_camera()
+    C.memmove(C.byref(c), C.byref(cam), C.sizeof(cam))
+    c.width, c.height = width, height
+    c.cx = cam.cx - x0
+    c.cy = cam.cy - y0
+    return c
+

@@ -31,3 +31,7 @@ def test_wide_bvh_layout_and_traversal_replay(exe):
     assert r.returncode == 0, r.stdout + r.stderr
     lines = r.stdout.strip().splitlines()
     assert len(lines) == 8 and all(l.endswith(" 0 mismatches") for l in lines), r.stdout
+    # every case (the 1- and 7-triangle trees included) is exercised by many hitting rays:
+    # half of the rays aim at a random triangle's centroid
+    hits = [int(l.split(" rays hit")[0].split(", ")[-1].split(" of ")[0]) for l in lines]
+    assert min(hits) >= 600, r.stdout

@@ -1,14 +1,13 @@
 """OBJ meshes (rbr_mesh_*: host code of the library, no GPU needed) against the reference's own
 ObjImporter + TriangleMesh::toPrimitives on identical text: the same triangles, bit for bit,
 with the same (normalised) vertex normals, and the same failures."""
-from pathlib import Path
-
 import numpy as np
 import pytest
 
+from oracle import reference_dir
 from rbr_b200 import load_obj, parse_obj
 
-ASSETS = Path("/root/reference/assets")
+ASSETS = reference_dir() / "assets"
 
 CASES = {
     "triangles": b"v 0 0 0\nv 1 0 0\nv 0 1 0\nv 0 0 1\nf 1 2 3\nf 1 3 4\n",

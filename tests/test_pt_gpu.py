@@ -12,6 +12,7 @@
 import numpy as np
 import pytest
 
+import helpers
 from rbr_b200 import RbrError, abi, render_params, scenes
 
 pytestmark = pytest.mark.gpu
@@ -141,31 +142,42 @@ def test_thin_lens_point_light_glass(ctx, restatement):
     assert path_agreement(gpu, cpu) > 0.98
 
 
-def _z_test(gpu_mean, gpu_m2, n_gpu, ref_sum, ref_sq, n_ref):
-    mu_g = gpu_mean.astype(np.float64)
-    var_g = np.maximum(gpu_m2 / n_gpu - mu_g ** 2, 0.0) * n_gpu / (n_gpu - 1)
-    mu_r = ref_sum / n_ref
-    var_r = np.maximum(ref_sq / n_ref - mu_r ** 2, 0.0) * n_ref / (n_ref - 1)
-    se = np.sqrt(var_g / n_gpu + var_r / n_ref)
-    z = np.abs(mu_g - mu_r) / np.maximum(se, 1e-12)
-    z[(se == 0) & (np.abs(mu_g - mu_r) < 1e-6)] = 0.0
-    return z, mu_g, mu_r
+@pytest.mark.slow
+def test_cornell_converges_to_reference_integrator(ctx, reference):
+    """Cornell box on the configured 256x256 camera (pinhole, fov 40), central 96x96 crop: per-pixel
+    means of the GPU and of the reference's PathTracingIntegrator::Li agree within 3 standard
+    errors (independent random numbers on the two sides), and so do the image means."""
+    s = scenes.cornell_box()
+    assert (s.camera.width, s.camera.height) == (256, 256)
+    cam = helpers.crop_camera(s.camera, 80, 80, 96, 96)
+    ctx.upload(s)
+    n_gpu = 4096
+    mean, m2 = ctx.render_host(cam, render_params(spp=n_gpu, max_depth=8, seed=2024), second_moment=True)
+    n_ref = 512
+    acc = reference.render_moments(reference.scene(s), cam, render_params(spp=n_ref, max_depth=8), batch=0)
+    z, z_img = helpers.moments_z(mean.astype(np.float64) * n_gpu, m2, n_gpu, acc[0], acc[1], n_ref)
+    tail = (z > 3).mean()
+    assert tail < 0.01, f"{tail:.4f} of pixel channels beyond 3 standard errors"
+    assert z_img < 3.0, f"image means differ by {z_img:.2f} standard errors"
 
 
 @pytest.mark.slow
-def test_cornell_converges_to_reference_integrator(ctx, reference):
-    """Cornell box: per-pixel means of the GPU and of the reference's PathTracingIntegrator::Li
-    agree within 3 standard errors (independent random numbers on the two sides)."""
-    w, h = 48, 48
-    s = small_cornell(w, h)
+def test_ggx_scene_converges_to_reference_integrator(ctx, reference):
+    """The GGX material scene at 64x36 (mound of 7,200 triangles, 260 spheres of every material
+    class including smooth glass, a mirror and smooth dielectrics, two area lights with emissive
+    quads, a point light, thin-lens camera, max depth 16): the GPU path tracer and the
+    reference's own PathTracingIntegrator::Li agree per pixel channel within 3 standard errors
+    (independent random numbers) and in the image mean. This pins the GPU estimator on the
+    delta / transmission / MIS paths directly against the reference, not only against the
+    restatement that shares its random numbers."""
+    s = helpers.ggx_small(64, 36, mesh_n=60)
     ctx.upload(s)
-    n_gpu = 4096
-    mean, m2 = ctx.render_host(s.camera, render_params(spp=n_gpu, max_depth=8, seed=2024), second_moment=True)
-    n_ref = 512
-    r = reference.scene(s)
-    acc = reference.render_moments(r, s.camera, render_params(spp=n_ref, max_depth=8), batch=0)
-    z, mu_g, mu_r = _z_test(mean, m2, n_gpu, acc[0], acc[1], n_ref)
+    n_gpu = 16384
+    mean, m2 = ctx.render_host(s.camera, render_params(spp=n_gpu, max_depth=16, seed=2025), second_moment=True)
+    n_ref = 2048
+    acc = reference.render_moments(reference.scene(s), s.camera, render_params(spp=n_ref, max_depth=16), batch=0)
+    z, z_img = helpers.moments_z(mean.astype(np.float64) * n_gpu, m2, n_gpu, acc[0], acc[1], n_ref)
+    assert (acc[0] > 0).mean() > 0.5
     tail = (z > 3).mean()
     assert tail < 0.01, f"{tail:.4f} of pixel channels beyond 3 standard errors"
-    rel = abs(mu_g.mean() - mu_r.mean()) / mu_r.mean()
-    assert rel < 0.01, f"image means differ by {rel:.4f}"
+    assert z_img < 3.0, f"image means differ by {z_img:.2f} standard errors"
