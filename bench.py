@@ -48,6 +48,12 @@ def parse():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--workload", choices=["rays", "cornell", "ggx", "fog", "cache", "batch"], default="rays")
     p.add_argument("--ref-spp", type=int, default=4096, help="cache workload: spp of the converged GPU reference")
+    p.add_argument("--cpu-ref-crop", type=int, default=0,
+                   help="cache workload: also compare against the reference CPU integrator on a central crop of "
+                        "this many pixels square")
+    p.add_argument("--cpu-ref-spp", type=int, default=4096, help="cache workload: spp of the CPU reference crop")
+    p.add_argument("--no-sub", action="store_true",
+                   help="rays workload: skip the path-tracer and cache sub-measurements after the headline")
     p.add_argument("--cache-suffix", type=int, default=None,
                    help="cache workload: rbr_cache_config.train_suffix (default: the library's)")
     p.add_argument("--cache-config", action="append", default=[],
@@ -253,33 +259,81 @@ def render_scene(which):
     return scenes.cornell_box() if which == "cornell" else scenes.ggx_scene()
 
 
-def run_render(args, rank, world, local_rank):
+# Algorithmic bytes of the wavefront path tracer, per event (the fixed record sizes its kernels
+# read and write; traversal bytes come from counted nodes and leaf records, 80 B and 48 B):
+#   camera path (k_raygen: ray 32 + throughput 16 + radiance 16 + queue 4; k_film: radiance 16)
+#   extension ray (k_extend: queue 4 + ray 32 + hit 8 + class queue 4)
+#   shaded vertex (k_shade: class queue 4 + hit 8 + ray 32 + throughput 16 + leaf record 48 +
+#                  material index 4 + material 44)
+#   continuation (k_shade: next ray 32 + throughput 16 + queue 4)
+#   shadow ray (k_shade writes and k_shadow reads its 48 B record)
+#   pixel (k_film: 12 B of RGB film written)
+PT_BYTES = {"path": 68 + 16, "extension_ray": 48, "shaded_vertex": 156, "continuation": 52, "shadow_ray": 96,
+            "pixel": 12, "node": 80, "leaf_record": 48}
+
+
+def path_tracer_bytes(st, pixels):
+    """Algorithmic bytes of one render from its counted events (rbr_render_stats)."""
+    b = PT_BYTES
+    return (st.paths * b["path"] + st.extension_rays * b["extension_ray"] + st.shaded_vertices * b["shaded_vertex"]
+            + (st.extension_rays - st.paths) * b["continuation"] + st.shadow_rays * b["shadow_ray"]
+            + pixels * b["pixel"] + (st.ext_nodes + st.shadow_nodes) * b["node"]
+            + (st.ext_records + st.shadow_records) * b["leaf_record"])
+
+
+def cpu_render_baseline(scene, cam, spp, max_depth, volumetric, row_frac):
+    """The reference's own Integrator::render (oracle/_ref) on a central band of the image."""
+    sys.path.insert(0, str(REPO / "oracle"))
+    from oracle import Reference, have_reference
+
+    from rbr_b200 import render_params
+
+    if not have_reference():
+        return None
+    import ctypes
+
+    ref = Reference()
+    h = ref.scene(scene)
+    small = type(cam)()
+    ctypes.memmove(ctypes.byref(small), ctypes.byref(cam), ctypes.sizeof(cam))
+    small.height = max(8, int(cam.height * row_frac))
+    small.cy = small.cy - (cam.height - small.height) / 2.0
+    t0 = time.perf_counter()
+    ref.render(h, small, render_params(spp=spp, max_depth=max_depth), volumetric=volumetric, threads=0)
+    dt = time.perf_counter() - t0
+    return {"value": cam.width * small.height * spp / dt / 1e6, "unit": "Mpaths/s", "cores": ref.max_threads(),
+            "kind": "reference",
+            "sample": f"central {cam.width}x{small.height} band of the image, the reference's own Integrator::render "
+                      f"with {'VolumetricPathIntegrator' if volumetric else 'PathTracingIntegrator'} (OpenMP rows), "
+                      f"{dt:.1f} s"}
+
+
+def measure_render(which, ctx, local_rank, rank, world, steps, warmup, e2e_steps, cpu_row_frac, params=()):
+    """Mpaths/s of the path tracer on one configuration: device-timed steps (one rbr_render of the
+    whole image each), end to end through rbr_render_host, the reference CPU integrator on a band
+    of the image, and the algorithmic-bytes roofline of one step from a counted render."""
     import torch
 
-    from rbr_b200 import Context, abi, render_params
+    from rbr_b200 import abi, render_params
 
-    which = args.workload
     cfg = RENDER_CONFIGS[which]
-    torch.cuda.set_device(local_rank)
     scene = render_scene(which)
     cam = scene.camera
     W, H = cam.width, cam.height
-    ctx = Context(local_rank)
     ctx.upload(scene)
-    for kv in args.param:
+    for kv in params:
         k, v = kv.split("=")
         ctx.set_param(k, int(v))
     film = torch.empty(W * H * 3, dtype=torch.float32, device=f"cuda:{local_rank}")
     stream = torch.cuda.current_stream()
     paths = W * H * cfg["spp"]
-
     flags = abi.RBR_RENDER_VOLUMETRIC if cfg.get("volumetric") else 0
 
-    def step(k):
-        p = render_params(spp=cfg["spp"], max_depth=cfg["max_depth"], seed=rank * 1000003 + k, flags=flags)
+    def step(k, extra=0):
+        p = render_params(spp=cfg["spp"], max_depth=cfg["max_depth"], seed=rank * 1000003 + k, flags=flags | extra)
         ctx.render_dev(cam, p, film.data_ptr(), 0, stream.cuda_stream)
 
-    for k in range(max(3, args.warmup)):
+    for k in range(max(3, warmup)):
         step(k)
     torch.cuda.synchronize()
     clocks = Clocks() if rank == 0 else None
@@ -287,16 +341,24 @@ def run_render(args, rank, world, local_rank):
         clocks.start()
     evs = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
     evs[0].record(stream)
-    for k in range(args.steps):
+    for k in range(steps):
         step(1000 + k)
     evs[1].record(stream)
     torch.cuda.synchronize()
     total_ms = evs[0].elapsed_time(evs[1])
-    st = ctx.render_stats()
     clk = clocks.stop(visible_gpu_indices(local_rank)) if clocks else None
+    st = ctx.render_stats()
+    launches = st.launches
+    # one counted render of the first timed step's samples: nodes and records per ray
+    step(1000, abi.RBR_RENDER_COUNT_TRAFFIC)
+    torch.cuda.synchronize()
+    cst = ctx.render_stats()
+    alg = path_tracer_bytes(cst, W * H)
+    ms_step = total_ms / steps
+    peak, peak_kind = measured_peaks()
+    achieved = alg / (ms_step / 1e3) / 1e9
     e2e = None
-    if not args.no_e2e:
-        e2e_steps = max(3, min(args.steps, 20))
+    if e2e_steps:
         host_film = torch.empty(W * H * 3, dtype=torch.float32).pin_memory().numpy()
         ctx.render_host(cam, render_params(spp=cfg["spp"], max_depth=cfg["max_depth"], seed=0, flags=flags),
                         out=host_film)  # warm-up: staging buffers
@@ -306,103 +368,116 @@ def run_render(args, rank, world, local_rank):
                             out=host_film)
         e2e_s = time.perf_counter() - t0
         e2e = {"value": paths * e2e_steps / e2e_s / 1e6, "unit": "Mpaths/s", "h2d_bytes_per_step": 0,
-               "d2h_bytes_per_step": W * H * 12, "path": "rbr_render_host: render + film -> pinned host"}
+               "d2h_bytes_per_step": W * H * 12, "steps": e2e_steps,
+               "path": "rbr_render_host: render + film -> pinned host"}
     base = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        sys.path.insert(0, str(REPO / "oracle"))
-        from oracle import Reference, have_reference
+    if rank == 0 and world == 1 and cpu_row_frac:
+        base = cpu_render_baseline(scene, cam, cfg["spp"], cfg["max_depth"], bool(flags), cpu_row_frac)
+    n = cst.extension_rays + cst.shadow_rays
+    return {
+        "metric": "Mpaths/s (camera samples per second), " + (
+            "GPU volumetric path tracer" if flags else "plain GPU path tracer"),
+        "value": paths * world * steps / (total_ms / 1e3) / 1e6, "unit": "Mpaths/s", "steps": steps,
+        "warmup": max(3, warmup), "ms_per_step": ms_step, "workload": cfg["desc"], "paths_per_step": paths,
+        "e2e": e2e, "cpu_baseline": base, "clocks": clk, "gpu_launches": launches * steps,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_source": f"{peak_kind} HBM copy bandwidth",
+                     "algorithmic_bytes_per_step": alg, "bytes_per_path": alg / paths,
+                     "record_bytes": PT_BYTES,
+                     "per_path": {"extension_rays": cst.extension_rays / paths, "shadow_rays": cst.shadow_rays / paths,
+                                  "shaded_vertices": cst.shaded_vertices / paths},
+                     "per_ray": {"nodes": (cst.ext_nodes + cst.shadow_nodes) / max(1, n),
+                                 "leaf_records": (cst.ext_records + cst.shadow_records) / max(1, n)},
+                     "counted": "nodes and records of one render with RBR_RENDER_COUNT_TRAFFIC, same samples as the "
+                                "first timed step"},
+        "render": {"waves": st.waves, "launches_per_step": st.launches},
+    }
 
-        if have_reference():
-            ref = Reference()
-            h = ref.scene(scene)
-            # bounded sample: the same camera, the central band of about 1/8 of the rows
-            import ctypes
 
-            small = type(cam)()
-            ctypes.memmove(ctypes.byref(small), ctypes.byref(cam), ctypes.sizeof(cam))
-            small.height = max(8, H // 8)
-            small.cy = small.cy - (H - small.height) / 2.0
-            t0 = time.perf_counter()
-            ref.render(h, small, render_params(spp=cfg["spp"], max_depth=cfg["max_depth"]),
-                       volumetric=bool(flags), threads=0)
-            dt = time.perf_counter() - t0
-            base = {"value": W * small.height * cfg["spp"] / dt / 1e6, "unit": "Mpaths/s",
-                    "cores": ref.max_threads(), "kind": "reference",
-                    "sample": f"central {W}x{small.height} band of the image, the reference's own "
-                              f"Integrator::render with {'VolumetricPathIntegrator' if flags else 'PathTracingIntegrator'}"
-                              f" (OpenMP rows), {dt:.1f} s"}
-    if rank == 0:
-        print(json.dumps({
-            "metric": "Mpaths/s (camera samples per second), " + (
-                "GPU volumetric path tracer" if flags else "plain GPU path tracer"), "value":
-                paths * world * args.steps / (total_ms / 1e3) / 1e6, "unit": "Mpaths/s", "n_gpus": world,
-            "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": total_ms / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded)",
-            "config": {"workload": cfg["desc"], "paths_per_step": paths,
-                       "l2": f"working set of the two waves in flight ({2 * paths // max(1, st.waves)} paths x ~100 B "
-                             "of path state + 48 B per shadow record) larger than L2; the film is written once"},
-            "e2e": e2e, "cpu_baseline": base, "clocks": clk,
-            "gpu_launches": st.launches * args.steps,
-            "render": {"extension_rays_per_path": st.extension_rays / st.paths,
-                       "shadow_rays_per_path": st.shadow_rays / st.paths, "waves": st.waves,
-                       "launches_per_step": st.launches},
-        }))
+def run_render(args, rank, world, local_rank):
+    import torch
+
+    from rbr_b200 import Context
+
+    torch.cuda.set_device(local_rank)
+    ctx = Context(local_rank)
+    r = measure_render(args.workload, ctx, local_rank, rank, world, args.steps, args.warmup,
+                       0 if args.no_e2e else max(3, min(args.steps, 20)), 0 if args.no_cpu_baseline else 1.0 / 8,
+                       args.param)
     ctx.close()
+    if rank == 0:
+        line = {"metric": r["metric"], "value": r["value"], "unit": r["unit"], "n_gpus": world, "steps": r["steps"],
+                "warmup": r["warmup"], "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+                "config": {"workload": r["workload"], "paths_per_step": r["paths_per_step"],
+                           "l2": "working set of the two waves in flight (path state + 48 B per shadow record) larger "
+                                 "than L2; the film is written once"}}
+        for k in ("e2e", "cpu_baseline", "roofline", "clocks", "gpu_launches", "render"):
+            line[k] = r[k]
+        print(json.dumps(line))
 
 
-def relmse(x, ref):
-    """mean((x - ref)^2 / (ref^2 + 1e-2)) over pixels and channels."""
-    return float(np.mean((x.astype(np.float64) - ref) ** 2 / (ref.astype(np.float64) ** 2 + 1e-2)))
+def relmse(x, ref, ref_var=None):
+    """mean((x - ref)^2 / (ref^2 + 1e-2)) over pixels and channels. With ref_var (the variance of
+    the reference's per-pixel mean) the reference's own Monte-Carlo noise, which inflates the
+    squared difference by ref_var on average, is subtracted: an estimate of the error against
+    the converged image."""
+    d2 = (x.astype(np.float64) - ref) ** 2
+    if ref_var is not None:
+        d2 = d2 - ref_var
+    return float(np.mean(d2 / (ref.astype(np.float64) ** 2 + 1e-2)))
 
 
-def run_cache(args, rank, world, local_rank):
+def measure_cache(ctx, local_rank, rank, frames, warmup, ref_spp, cache_kw, e2e_frames=8, cpu_crop=0, cpu_spp=0):
     """Learned radiance cache vs the plain GPU path tracer at equal time on the GGX scene
     (1920x1080, 1 spp per frame). A step is one frame: 1 spp with paths ending into the cache,
     plus the frame's 4 optimiser steps on 2^16 training paths. Converged reference: the plain
-    GPU path tracer at --ref-spp samples per pixel (independent seed, default 4096)."""
+    GPU path tracer at ref_spp samples per pixel (independent seed) with its per-pixel variance,
+    which the corrected RelMSE subtracts; optionally the reference's own CPU integrator on a
+    central crop of cpu_crop^2 pixels at cpu_spp samples per pixel."""
     import torch
 
-    from rbr_b200 import Context, render_params, scenes
+    from rbr_b200 import abi, render_params, scenes
 
-    torch.cuda.set_device(local_rank)
-    frames = args.steps
     scene = scenes.ggx_scene()
     cam = scene.camera
     W, H = cam.width, cam.height
-    ctx = Context(local_rank)
     ctx.upload(scene)
     depth = 16
     stream = torch.cuda.current_stream()
     sp = stream.cuda_stream
     film = torch.zeros(W * H * 3, dtype=torch.float32, device=f"cuda:{local_rank}")
+    film2 = torch.zeros(W * H * 3, dtype=torch.float32, device=f"cuda:{local_rank}")
 
-    def plain(spp, seed):
+    def plain(spp, seed, var=False):
         """The plain path tracer at `spp`, in calls of at most 1024 spp (one call takes at most
-        2^32 camera samples) with consecutive sample ranges; film = the sample-weighted mean."""
-        img, total_ms, done = 0.0, 0.0, 0
+        2^32 camera samples) with consecutive sample ranges; film = the sample-weighted mean, and
+        with var the variance of that mean from the per-pixel second moments."""
+        img, sq, total_ms, done = 0.0, 0.0, 0.0, 0
         while done < spp:
             n = min(1024, spp - done)
             ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
             ev[0].record(stream)
-            ctx.render_dev(cam, render_params(spp=n, max_depth=depth, seed=seed, sample_offset=done), film.data_ptr(),
-                           0, sp)
+            ctx.render_dev(cam, render_params(spp=n, max_depth=depth, seed=seed, sample_offset=done,
+                                              flags=abi.RBR_RENDER_SECOND_MOMENT if var else 0),
+                           film.data_ptr(), film2.data_ptr() if var else 0, sp)
             ev[1].record(stream)
             torch.cuda.synchronize()
-            img = img + film.cpu().numpy().reshape(H, W, 3) * n
+            img = img + film.cpu().numpy().reshape(H, W, 3).astype(np.float64) * n
+            if var:
+                sq = sq + film2.cpu().numpy().reshape(H, W, 3).astype(np.float64)
             total_ms += ev[0].elapsed_time(ev[1])
             done += n
-        return img / spp, total_ms
+        mean = img / spp
+        if not var:
+            return mean, total_ms
+        return mean, total_ms, np.maximum(sq / spp - mean ** 2, 0.0) / (spp - 1)
 
-    cache_kw = {} if args.cache_suffix is None else {"train_suffix": args.cache_suffix}
-    for kv in args.cache_config:
-        k, v = kv.split("=")
-        cache_kw[k] = int(v)
-    ref, ref_ms = plain(args.ref_spp, 777)  # converged reference, independent seed
+    ref, ref_ms, ref_var = plain(ref_spp, 777, var=True)  # converged reference, independent seed
     # warm-up of both paths (kernels loaded, buffers allocated)
     plain(1, 1)
     ctx.cache_create(seed=3, **cache_kw)
-    ctx.cache_render_dev(cam, render_params(spp=1, max_depth=depth, seed=2), max(3, args.warmup), film.data_ptr(), 0,
+    ctx.cache_render_dev(cam, render_params(spp=1, max_depth=depth, seed=2), max(3, warmup), film.data_ptr(), 0,
                          True, sp)
     torch.cuda.synchronize()
     # the timed cached run starts from a fresh cache
@@ -418,48 +493,105 @@ def run_cache(args, rank, world, local_rank):
     cache_ms = ev[0].elapsed_time(ev[1])
     clk = clocks.stop(visible_gpu_indices(local_rank)) if clocks else None
     launches = ctx.render_stats().launches
-    cached = film.cpu().numpy().reshape(H, W, 3).copy()
+    cached = film.cpu().numpy().reshape(H, W, 3).astype(np.float64)
     info = ctx.cache_info()
     # plain path tracer: equal samples, then equal time
     plain_same, plain_same_ms = plain(frames, 11)
     eq_spp = max(1, int(round(frames * cache_ms / plain_same_ms)))
     plain_eq, plain_eq_ms = plain(eq_spp, 11)
-    r_cache, r_eq, r_same = relmse(cached, ref), relmse(plain_eq, ref), relmse(plain_same, ref)
-    # end to end: a cached render of a few frames with the film read back to the host
-    t0 = time.perf_counter()
-    e2e_frames = 8
-    ctx.cache_render_dev(cam, render_params(spp=1, max_depth=depth, seed=12), e2e_frames, film.data_ptr(), 0, True, sp)
-    host = film.cpu()
-    e2e_s = time.perf_counter() - t0
-    if rank == 0:
-        print(json.dumps({
-            "metric": "Mpaths/s & RelMSE at equal time: MLP cache vs plain GPU PT", "value":
-                W * H * frames / (cache_ms / 1e3) / 1e6, "unit": "Mpaths/s", "n_gpus": world, "steps": frames,
-            "warmup": max(3, args.warmup), "ms_per_step": cache_ms / frames, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "bf16 (MLP) / f32 (path tracer)",
-            "data": "synthetic (seeded)",
-            "config": {"workload": "learned radiance cache on the GGX scene: 1920x1080, 1 spp per frame, "
-                                   f"{frames} frames; hash grid 16 levels x 2^19 x 2 FP16, MLP 5x64 BF16; "
-                                   "2^16 training paths per frame, 4 Adam steps of 16384 samples, lr 1e-2",
-                       "reference": f"plain GPU path tracer, {args.ref_spp} spp, independent seed "
-                                    f"({ref_ms / 1e3:.1f} s)",
-                       "l2": "path state per frame (2M paths x ~100 B) and hash grid (32 MB) + Adam state "
-                             "(224 MB) exceed L2"},
-            "relmse": {"cache": r_cache, "plain_equal_time": r_eq, "plain_equal_samples": r_same,
-                       "gain_equal_time": r_eq / r_cache, "plain_equal_time_spp": eq_spp,
-                       "plain_equal_time_ms": plain_eq_ms, "cache_ms": cache_ms,
-                       "mean_bias": float(cached.mean() / ref.mean() - 1.0)},
-            "cache": {"optimiser_steps": info.optimiser_steps, "last_loss": info.last_loss,
-                      "queries_last_frame": info.last_queries, "train_records_last_frame": info.last_train_records,
-                      "train_suffix": ctx.cache_config(**cache_kw).train_suffix,
-                      "termination_depth": ctx.cache_config(**cache_kw).termination_depth},
-            "e2e": {"value": W * H * e2e_frames / e2e_s / 1e6, "unit": "Mpaths/s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": W * H * 12 // e2e_frames,
-                    "path": f"rbr_cache_render of {e2e_frames} frames + film to host"},
-            "clocks": clk, "gpu_launches": launches,
-        }))
-    del host
+    r = {k: relmse(x, ref) for k, x in (("cache", cached), ("plain_equal_time", plain_eq),
+                                         ("plain_equal_samples", plain_same))}
+    rc = {k: relmse(x, ref, ref_var) for k, x in (("cache", cached), ("plain_equal_time", plain_eq),
+                                                   ("plain_equal_samples", plain_same))}
+    out = {
+        "metric": "Mpaths/s & RelMSE at equal time: MLP cache vs plain GPU PT",
+        "value": W * H * frames / (cache_ms / 1e3) / 1e6, "unit": "Mpaths/s", "steps": frames,
+        "warmup": max(3, warmup), "ms_per_step": cache_ms / frames,
+        "workload": "learned radiance cache on the GGX scene: 1920x1080, 1 spp per frame, "
+                    f"{frames} frames; hash grid 16 levels x 2^19 x 2 FP16, MLP 5x64 BF16; "
+                    "2^16 training paths per frame, 4 Adam steps of 16384 samples, lr 1e-2",
+        "reference": f"plain GPU path tracer, {ref_spp} spp, independent seed ({ref_ms / 1e3:.1f} s)",
+        "relmse": {**r, "gain_equal_time": r["plain_equal_time"] / r["cache"], "plain_equal_time_spp": eq_spp,
+                   "plain_equal_time_ms": plain_eq_ms, "cache_ms": cache_ms,
+                   "mean_bias": float(cached.mean() / ref.mean() - 1.0)},
+        "relmse_noise_corrected": {**rc, "gain_equal_time": rc["plain_equal_time"] / max(rc["cache"], 1e-12),
+                                   "reference_noise": float(np.mean(ref_var / (ref ** 2 + 1e-2))),
+                                   "note": "the reference's per-pixel variance of its mean subtracted from the "
+                                           "squared differences"},
+        "cache": {"optimiser_steps": info.optimiser_steps, "last_loss": info.last_loss,
+                  "queries_last_frame": info.last_queries, "train_records_last_frame": info.last_train_records,
+                  "train_suffix": ctx.cache_config(**cache_kw).train_suffix,
+                  "termination_depth": ctx.cache_config(**cache_kw).termination_depth},
+        "clocks": clk, "gpu_launches": launches,
+    }
+    if cpu_crop and cpu_spp:
+        sys.path.insert(0, str(REPO / "oracle"))
+        from oracle import Reference, have_reference
+
+        if have_reference():
+            import ctypes
+
+            cref = Reference()
+            crop = type(cam)()
+            ctypes.memmove(ctypes.byref(crop), ctypes.byref(cam), ctypes.sizeof(cam))
+            x0, y0 = (W - cpu_crop) // 2, (H - cpu_crop) // 2
+            crop.width = crop.height = cpu_crop
+            crop.cx, crop.cy = cam.cx - x0, cam.cy - y0
+            t0 = time.perf_counter()
+            acc = cref.render_moments(cref.scene(scene), crop, render_params(spp=cpu_spp, max_depth=depth), batch=1)
+            cpu_s = time.perf_counter() - t0
+            cmean = acc[0] / cpu_spp
+            cvar = np.maximum(acc[1] / cpu_spp - cmean ** 2, 0.0) / (cpu_spp - 1)
+            sl = (slice(y0, y0 + cpu_crop), slice(x0, x0 + cpu_crop))
+            out["relmse_cpu_reference"] = {
+                "reference": f"the reference's own PathTracingIntegrator::Li, central {cpu_crop}x{cpu_crop} crop, "
+                             f"{cpu_spp} spp, {cpu_s:.0f} s on {cref.max_threads()} host threads",
+                "cache": relmse(cached[sl], cmean, cvar), "plain_equal_time": relmse(plain_eq[sl], cmean, cvar),
+                "gpu_reference": relmse(ref[sl], cmean, cvar),
+                "mean_bias_cache": float(cached[sl].mean() / cmean.mean() - 1.0),
+                "mean_bias_gpu_reference": float(ref[sl].mean() / cmean.mean() - 1.0),
+                "note": "noise-corrected by the CPU reference's variance of its mean"}
+            out["relmse_cpu_reference"]["gain_equal_time"] = (out["relmse_cpu_reference"]["plain_equal_time"] /
+                                                              max(out["relmse_cpu_reference"]["cache"], 1e-12))
+    if e2e_frames:
+        t0 = time.perf_counter()
+        ctx.cache_render_dev(cam, render_params(spp=1, max_depth=depth, seed=12), e2e_frames, film.data_ptr(), 0,
+                             True, sp)
+        host = film.cpu()
+        e2e_s = time.perf_counter() - t0
+        del host
+        out["e2e"] = {"value": W * H * e2e_frames / e2e_s / 1e6, "unit": "Mpaths/s", "h2d_bytes_per_step": 0,
+                      "d2h_bytes_per_step": W * H * 12 // e2e_frames,
+                      "path": f"rbr_cache_render of {e2e_frames} frames + film to host"}
+    return out
+
+
+def run_cache(args, rank, world, local_rank):
+    import torch
+
+    from rbr_b200 import Context
+
+    torch.cuda.set_device(local_rank)
+    cache_kw = {} if args.cache_suffix is None else {"train_suffix": args.cache_suffix}
+    for kv in args.cache_config:
+        k, v = kv.split("=")
+        cache_kw[k] = int(v)
+    ctx = Context(local_rank)
+    r = measure_cache(ctx, local_rank, rank, args.steps, args.warmup, args.ref_spp, cache_kw,
+                      cpu_crop=args.cpu_ref_crop, cpu_spp=args.cpu_ref_spp)
     ctx.close()
+    if rank == 0:
+        line = {"metric": r["metric"], "value": r["value"], "unit": r["unit"], "n_gpus": world, "steps": r["steps"],
+                "warmup": r["warmup"], "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "bf16 (MLP) / f32 (path tracer)", "data": "synthetic (seeded)",
+                "config": {"workload": r["workload"], "reference": r["reference"],
+                           "l2": "path state per frame (2M paths x ~100 B) and hash grid (32 MB) + Adam state "
+                                 "(224 MB) exceed L2"}}
+        for k in ("relmse", "relmse_noise_corrected", "relmse_cpu_reference", "cache", "e2e", "clocks",
+                  "gpu_launches"):
+            if k in r:
+                line[k] = r[k]
+        print(json.dumps(line))
 
 
 def run_batch(args, rank, world, local_rank):
@@ -702,8 +834,20 @@ def main():
             "tuning": tuned,
             "bvh": {"wide_nodes": stats.num_wide_nodes, "leaf_records": stats.num_leaf_records,
                     "depth": stats.max_depth, "build_s": stats.build_seconds,
-                    "device_mb": stats.device_bytes / 1e6},
+                    "device_mb": stats.device_bytes / 1e6, "wrapped_leaves": stats.wrapped_leaves},
         }
+    if world == 1 and not args.no_sub:
+        # the metric's other parts, after the headline's timed region: the plain path tracer on the
+        # Cornell box and the GGX scene (Mpaths/s), and the radiance cache's RelMSE at equal time
+        e2e_on = not args.no_e2e
+        cpu_on = not args.no_cpu_baseline
+        line["path_tracer"] = {
+            "cornell": measure_render("cornell", ctx, local_rank, rank, world, 20, 3, 10 if e2e_on else 0,
+                                      1.0 / 8 if cpu_on else 0),
+            "ggx": measure_render("ggx", ctx, local_rank, rank, world, 5, 3, 3 if e2e_on else 0,
+                                  1.0 / 32 if cpu_on else 0)}
+        line["radiance_cache"] = measure_cache(ctx, local_rank, rank, 256, 3, 2048, {}, 8 if e2e_on else 0)
+    if rank == 0:
         print(json.dumps(line))
     ctx.close()
     if dist:

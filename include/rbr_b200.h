@@ -184,7 +184,11 @@ enum {
      * estimation from scatter points towards point lights with transmittance and the phase
      * function, emission added at every surface hit, surface next-event estimation without MIS
      * weights, Russian roulette at surface vertices after depth 3. */
-    RBR_RENDER_VOLUMETRIC = 1u << 2
+    RBR_RENDER_VOLUMETRIC = 1u << 2,
+    /* Diagnostic (rbr_render only): also count the 8-wide nodes fetched and leaf records tested
+     * by every extension and shadow ray (rbr_render_stats), for the path tracer's algorithmic
+     * traffic. Same images; the counting kernels run slower. */
+    RBR_RENDER_COUNT_TRAFFIC = 1u << 3
 };
 
 /* IntegratorConfig (include/render/renderers/integrator.h:22-28). */
@@ -206,6 +210,11 @@ typedef struct rbr_render_stats {
     uint32_t waves;           /* path chunks processed */
     uint32_t launches;        /* kernels launched */
     float milliseconds;       /* device time of the whole render (CUDA events) */
+    uint64_t shaded_vertices; /* extension rays that hit a surface and were shaded */
+    uint64_t ext_nodes;       /* with RBR_RENDER_COUNT_TRAFFIC: wide nodes fetched by extension rays */
+    uint64_t ext_records;     /*   leaf records tested by extension rays */
+    uint64_t shadow_nodes;    /*   wide nodes fetched by shadow rays */
+    uint64_t shadow_records;  /*   leaf records tested by shadow rays (0 without the flag) */
 } rbr_render_stats;
 
 /* ------------------------------------------------------------------------------------------
@@ -245,6 +254,15 @@ rbr_status rbr_scene_stats_get(const rbr_ctx* ctx, rbr_scene_stats* out);
  *   "pt.streams"           rbr_render: waves in flight, 1 or 2 (default 2: waves alternate
  *                          between two sets of path buffers on two streams; an image that
  *                          fits one wave is rendered as two half-image waves)
+ *   "pt.shade_split"       rbr_render: 1 shades each material class (glossy, diffuse, delta-only,
+ *                          none) in a launch of its own, compiled for that class's lobes; 0 one
+ *                          launch for all classes (default)
+ *   "cache.wait_limit"     polls of a tensor-core completion wait in the radiance-cache kernels
+ *                          before it gives up with RBR_ERR_DEVICE_TIMEOUT (default 2^22; 0
+ *                          makes every such wait give up at once, which tests the error path:
+ *                          the kernel still drains its work before it frees tensor memory)
+ *   "debug.fail_alloc"     n > 0: the n-th next device allocation of the context fails with
+ *                          RBR_ERR_OUT_OF_MEMORY (fault injection for callers' error paths)
  *   "bvh.record_cost_milli" cost of testing one leaf record relative to one wide-node test,
  *                          x1000, in the 8-wide collapse's surface-area cost (default 1000);
  *                          applies to the next rbr_scene_upload

@@ -219,9 +219,11 @@ __device__ __forceinline__ void scatter_grid_grad(const CacheDev& c, float4 r0, 
     }
 }
 
-// Waits for the pending tensor-core work; all threads agree on the outcome.
-__device__ __forceinline__ bool wait_mma(uint64_t* mbar, uint32_t& phase, int* err) {
-    const bool done = tc::mbar_wait(mbar, phase);
+// Waits for the pending tensor-core work (at most `limit` polls); all threads agree on the
+// outcome. A wait that ran out sets kErrDeviceTimeout; the kernel then stops issuing work and
+// drains the outstanding MMA with the full bound before it frees its tensor memory.
+__device__ __forceinline__ bool wait_mma(uint64_t* mbar, uint32_t& phase, int* err, uint32_t limit) {
+    const bool done = tc::mbar_wait(mbar, phase, limit);
     phase ^= 1u;
     const int bad = __syncthreads_or(done ? 0 : 1);
     if (bad && threadIdx.x == 0) atomicOr(err, kErrDeviceTimeout);
@@ -317,7 +319,7 @@ __global__ void __launch_bounds__(128, 4)
                                  tc::sdesc(w_s + l * 8192 + k * 256, 128, 1024), id, k > 0);
                 tc::mma_commit(mbar);
             }
-            ok = wait_mma(mbar, phase, err);
+            ok = wait_mma(mbar, phase, err, c.wait_limit);
             if (!ok) break;
             tc::fence_after_sync();
             if (l < 4) {
@@ -423,7 +425,7 @@ __global__ void __launch_bounds__(128, 1) k_rc_train(CacheDev c, TrainBatchDev b
                                  tc::sdesc(w_s + l * 8192 + k * 256, 128, 1024), id, k > 0);
                 tc::mma_commit(mbar);
             }
-            ok = wait_mma(mbar, phase, err);
+            ok = wait_mma(mbar, phase, err, c.wait_limit);
             if (!ok) break;
             tc::fence_after_sync();
             if (l < 4) {
@@ -474,7 +476,7 @@ __global__ void __launch_bounds__(128, 1) k_rc_train(CacheDev c, TrainBatchDev b
                                  id, k > 0);
                 tc::mma_commit(mbar);
             }
-            ok = wait_mma(mbar, phase, err);
+            ok = wait_mma(mbar, phase, err, c.wait_limit);
             if (!ok) break;
             tc::fence_after_sync();
             float z[64];
@@ -505,7 +507,7 @@ __global__ void __launch_bounds__(128, 1) k_rc_train(CacheDev c, TrainBatchDev b
                              tc::sdesc(del_s + 4096 + k * 2 * kDelRg, kDelRg, 128), id4, (!first || k > 0) ? 1u : 0u);
             tc::mma_commit(mbar);
         }
-        ok = wait_mma(mbar, phase, err);
+        ok = wait_mma(mbar, phase, err, c.wait_limit);
         if (!ok) break;
         tc::fence_after_sync();
         first = false;
@@ -1031,7 +1033,9 @@ cudaError_t cache_launch_infer(rbr_ctx* ctx, const float4* records, uint32_t n, 
     o.q_info = q_info;
     const uint32_t tiles = (n + kRcTile - 1) / kRcTile;
     const uint32_t grid = std::max(1u, std::min<uint32_t>(tiles, ctx->num_sms * 4));
-    k_rc_infer<<<grid, 128, kSmemInfer, stream>>>(cs.dev, records, n, n_ptr, o, ctx->d_error);
+    CacheDev dev = cs.dev;
+    dev.wait_limit = ctx->cache_wait_limit;
+    k_rc_infer<<<grid, 128, kSmemInfer, stream>>>(dev, records, n, n_ptr, o, ctx->d_error);
     return cudaGetLastError();
 }
 
@@ -1059,7 +1063,9 @@ cudaError_t cache_launch_step(rbr_ctx* ctx, const TrainBatchDev& b, bool apply, 
     CacheState& cs = ctx->cache;
     const uint32_t tiles = (b.batch + kRcTile - 1) / kRcTile;
     const uint32_t grid = std::max(1u, std::min<uint32_t>(tiles, ctx->num_sms));
-    k_rc_train<<<grid, 128, kSmemTrain, stream>>>(cs.dev, b, as<float>(cs.scalars), ctx->d_error);
+    CacheDev dev = cs.dev;
+    dev.wait_limit = ctx->cache_wait_limit;
+    k_rc_train<<<grid, 128, kSmemTrain, stream>>>(dev, b, as<float>(cs.scalars), ctx->d_error);
     if (!apply) return cudaGetLastError();
     const AdamDev a = adam_dev(cs);
     k_rc_adam_prep<<<1, 1, 0, stream>>>(a, b, as<float>(cs.scalars));

@@ -31,6 +31,9 @@ rbr_status ensure(rbr_ctx* ctx, DevBuf& b, size_t bytes, const char* what) {
     if (b.bytes >= bytes && b.ptr) return RBR_OK;
     release(b);
     if (bytes == 0) return RBR_OK;
+    if (ctx->fail_alloc_countdown > 0 && --ctx->fail_alloc_countdown == 0)
+        return fail(ctx, RBR_ERR_OUT_OF_MEMORY, std::string("cudaMalloc for ") + what + " (" + std::to_string(bytes) +
+                                                    " B): failure injected by debug.fail_alloc");
     cudaError_t e = cudaMalloc(&b.ptr, bytes);
     if (e != cudaSuccess) {
         b.ptr = nullptr;
@@ -184,6 +187,15 @@ rbr_status rbr_param_set(rbr_ctx* ctx, const char* name, int64_t value) {
     } else if (n == "pt.wave_paths") {
         if (value < 1024 || value > (int64_t(1) << 26)) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "pt.wave_paths is 1024..2^26");
         ctx->pt_wave_paths = static_cast<uint32_t>(value);
+    } else if (n == "pt.shade_split") {
+        if (value != 0 && value != 1) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "pt.shade_split is 0 or 1");
+        ctx->pt_shade_split = static_cast<int>(value);
+    } else if (n == "cache.wait_limit") {
+        if (value < 0 || value > (int64_t(1) << 22)) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "cache.wait_limit is 0..2^22");
+        ctx->cache_wait_limit = static_cast<uint32_t>(value);
+    } else if (n == "debug.fail_alloc") {
+        if (value < 0 || value > 1000000) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "debug.fail_alloc is 0..1000000");
+        ctx->fail_alloc_countdown = static_cast<uint32_t>(value);
     } else if (n == "bvh.record_cost_milli") {
         if (value < 1 || value > 100000) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "bvh.record_cost_milli is 1..100000");
         ctx->bvh_record_cost_milli = static_cast<int>(value);
@@ -212,6 +224,9 @@ rbr_status rbr_param_get(const rbr_ctx* ctx, const char* name, int64_t* value) {
     else if (n == "pt.streams") *value = ctx->pt_streams;
     else if (n == "trace.host_chunk") *value = ctx->trace_host_chunk;
     else if (n == "bvh.record_cost_milli") *value = ctx->bvh_record_cost_milli;
+    else if (n == "cache.wait_limit") *value = ctx->cache_wait_limit;
+    else if (n == "pt.shade_split") *value = ctx->pt_shade_split;
+    else if (n == "debug.fail_alloc") *value = ctx->fail_alloc_countdown;
     else return RBR_ERR_INVALID_ARGUMENT;
     return RBR_OK;
 }

@@ -43,8 +43,23 @@ enum : int {
     kCQuery = 12,   // radiance cache: paths ended into the cache in this wave
     kCTrain = 13,   // radiance cache: training vertices gathered in this frame
     kCTrainBase = 14,  // radiance cache: kCTrain at the start of this wave
-    kCWords = 16
+    kCShade = 16,      // 64-bit: hit vertices shaded
+    kCTraffic = 18,    // 4 x 64-bit (RBR_RENDER_COUNT_TRAFFIC): extension nodes, records; shadow nodes, records
+    kCWords = 26
 };
+
+// Adds this warp's node / record counts to two 64-bit counters (every lane of the warp calls it).
+__device__ __forceinline__ void warp_add_counts(uint32_t* counters, int word, uint2 c) {
+    unsigned long long nodes = c.x, recs = c.y;
+    for (int off = 16; off > 0; off >>= 1) {
+        nodes += __shfl_down_sync(0xFFFFFFFFu, nodes, off);
+        recs += __shfl_down_sync(0xFFFFFFFFu, recs, off);
+    }
+    if ((threadIdx.x & 31) == 0 && (nodes | recs) != 0) {
+        atomicAdd(reinterpret_cast<unsigned long long*>(counters + word), nodes);
+        atomicAdd(reinterpret_cast<unsigned long long*>(counters + word + 2), recs);
+    }
+}
 
 struct Wave {
     uint32_t p0;       // first pixel
@@ -203,7 +218,8 @@ __global__ void k_begin(Paths P, uint32_t d) {
 // Register budget for 8 resident blocks per SM (64 registers): the volumetric variant, which
 // also samples the medium and traces point-light shadow rays from scatter points, gains 5 % over
 // the natural 56-register allocation (foggy Cornell box); the surface variant is unchanged.
-template <bool kVol, bool kPacked>
+// kCount (RBR_RENDER_COUNT_TRAFFIC): also counts the nodes and records the traversals fetch.
+template <bool kVol, bool kPacked, bool kCount = false>
 __global__ void __launch_bounds__(kBlock, 8) k_extend(DeviceScene s, Wave w, Paths P, uint32_t d, int* err) {
     const uint32_t n = P.counters[kCQ0 + (d & 1)];
     const uint32_t* q = (d & 1) ? P.q1 : P.q0;
@@ -211,6 +227,7 @@ __global__ void __launch_bounds__(kBlock, 8) k_extend(DeviceScene s, Wave w, Pat
     uint32_t* nextc = P.counters + kCQ0 + ((d + 1) & 1);
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(reinterpret_cast<unsigned long long*>(P.counters + kCExt), n);
     const uint32_t stride = gridDim.x * blockDim.x;
+    uint2 traffic = make_uint2(0u, 0u);
     for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {
         const uint32_t j = base + threadIdx.x;
         const bool valid = j < n;
@@ -224,7 +241,8 @@ __global__ void __launch_bounds__(kBlock, 8) k_extend(DeviceScene s, Wave w, Pat
             float t = 0.0f;
             // A ray with a zero or non-finite direction or origin: no traversal, no hit.
             const uint32_t prim = degenerate(a, b) ? 0xFFFFFFFFu
-                                                   : traverse<false>(s, ld_f3(a), ld_f3(b), __int_as_float(0x7f800000), t, err);
+                                                   : traverse<false, kCount>(s, ld_f3(a), ld_f3(b), __int_as_float(0x7f800000),
+                                                                             t, err, &traffic);
             P.hit[k] = make_uint2(prim, __float_as_uint(t));
             if (kVol && s.has_medium) {
                 const float4 T4 = P.thr[k];
@@ -298,6 +316,7 @@ __global__ void __launch_bounds__(kBlock, 8) k_extend(DeviceScene s, Wave w, Pat
             if (cont) nextq[slot] = k;
         }
     }
+    if (kCount) warp_add_counts(P.counters, kCTraffic, traffic);
 }
 
 // Surface data of a hit, as the primitive's intersect() fills SurfaceInteraction.
@@ -383,15 +402,30 @@ __device__ __forceinline__ bool train_path(const Wave& w, uint64_t seed, uint32_
 // latency-bound on its division and square-root chains, and twice the warps of its natural
 // 124-register allocation hide more of it (GGX scene +5 %, Cornell box +3 %; 5, 6, 10 and 12
 // blocks were measured slower).
-template <int kMode, bool kPacked>
+// kCls < 0: one launch over the four class queues; kCls = a material class: that class's
+// queue only, with the lobe kinds of the class known at compile time (no microfacet code for
+// the diffuse and delta-only classes, no next-event estimation for delta-only and lobeless
+// materials, whose light samples always evaluate to zero).
+constexpr int kShadeDiffuse = static_cast<int>(kClassDiffuse), kShadeGlossy = static_cast<int>(kClassGlossy),
+              kShadeSpecular = static_cast<int>(kClassSpecular), kShadeNone = static_cast<int>(kClassNone);
+template <int kCls>
+__host__ __device__ constexpr uint32_t class_kinds() {
+    return kCls == kShadeDiffuse ? kNoGGXKinds : kCls == kShadeSpecular ? kDeltaKinds : kCls == kShadeNone ? 0u : kAllKinds;
+}
+
+template <int kMode, bool kPacked, int kCls = -1>
 __global__ void __launch_bounds__(kBlock, 8) k_shade(DeviceScene s, Wave w, Paths P, uint32_t d) {
     constexpr bool kCache = kMode == 1, kVolSurface = kMode == 2;
+    constexpr uint32_t kKinds = class_kinds<kCls>();
+    constexpr bool kNoNee = kCls == kShadeSpecular || kCls == kShadeNone;
     uint32_t cnt[kNumClasses + 1];
     cnt[0] = 0;
-    for (int c = 0; c < kNumClasses; ++c) cnt[c + 1] = cnt[c] + P.counters[kCClass + c];
-    const uint32_t n = cnt[kNumClasses];
+    if (kCls < 0)
+        for (int c = 0; c < kNumClasses; ++c) cnt[c + 1] = cnt[c] + P.counters[kCClass + c];
+    const uint32_t n = kCls < 0 ? cnt[kNumClasses] : P.counters[kCClass + (kCls < 0 ? 0 : kCls)];
     uint32_t* nextq = (d & 1) ? P.q0 : P.q1;
     uint32_t* nextc = P.counters + kCQ0 + ((d + 1) & 1);
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(reinterpret_cast<unsigned long long*>(P.counters + kCShade), n);
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {
         const uint32_t j = base + threadIdx.x;
@@ -409,9 +443,13 @@ __global__ void __launch_bounds__(kBlock, 8) k_shade(DeviceScene s, Wave w, Path
         mx.total = 0.0f;
         uint32_t pixel = 0, sample = 0;
         if (valid) {
-            int c = 0;
-            while (j >= cnt[c + 1]) ++c;
-            k = P.classq[c * P.cap + (j - cnt[c])];
+            if (kCls < 0) {
+                int c = 0;
+                while (j >= cnt[c + 1]) ++c;
+                k = P.classq[c * P.cap + (j - cnt[c])];
+            } else {
+                k = P.classq[kCls * P.cap + j];
+            }
             const PathKey key = path_key<kPacked>(w, P, k);
             pixel = key.pixel;
             sample = key.sample;
@@ -436,7 +474,7 @@ __global__ void __launch_bounds__(kBlock, 8) k_shade(DeviceScene s, Wave w, Path
             fr = make_frame(h.outward);
             wo = to_local(fr, xneg(rd));  // isect.wo = -ray.direction
             mx = mixture(bs, wo);
-            nee = key.nee && !bsdf_delta(bs);
+            nee = !kNoNee && key.nee && !bsdf_delta(bs);
             alive = true;
             if (kCache && bs.n > 0 && !bsdf_delta(bs)) {
                 if (train_path(w, seed, pixel, sample)) {
@@ -481,7 +519,7 @@ __global__ void __launch_bounds__(kBlock, 8) k_shade(DeviceScene s, Wave w, Path
             bool emit = false;
             f3 contrib, so, sd;
             float stmax = 0.0f;
-            if (valid && nee) {
+            if (!kNoNee && valid && nee) {
                 const float4 u = draw4(seed, pixel, sample, d, kRngLights + ((l >> 1) << 8));
                 const LightDev& L = s.lights[l];
                 const LSample ls = light_sample(L, h.point, (l & 1) ? u.z : u.x, (l & 1) ? u.w : u.y);
@@ -489,7 +527,7 @@ __global__ void __launch_bounds__(kBlock, 8) k_shade(DeviceScene s, Wave w, Path
                     const f3 wiL = to_local(fr, ls.wi);
                     f3 f;
                     float bpdf;
-                    bsdf_eval_pdf(bs, mx, wo, wiL, f, bpdf);
+                    bsdf_eval_pdf<kKinds>(bs, mx, wo, wiL, f, bpdf);
                     if (!black(f)) {
                         spawn(h, ls.wi, so, sd);
                         stmax = fs(ls.dist, kEpsilon);
@@ -518,7 +556,7 @@ __global__ void __launch_bounds__(kBlock, 8) k_shade(DeviceScene s, Wave w, Path
         bool cont = false;
         if (valid && alive && !last) {
             const float4 u = draw4(seed, pixel, sample, d, kRngBounce);
-            const BSample b = bsdf_sample(bs, mx, wo, u.x, u.y);
+            const BSample b = bsdf_sample<kKinds>(bs, mx, wo, u.x, u.y);
             if (b.pdf > 0.0f && !black(b.f)) {
                 const f3 wiW = to_world(fr, b.wi);
                 const float c = fabsf(xdot(wiW, h.normal));
@@ -543,6 +581,7 @@ __global__ void __launch_bounds__(kBlock, 8) k_shade(DeviceScene s, Wave w, Path
     }
 }
 
+template <bool kCount = false>
 __global__ void __launch_bounds__(kBlock) k_shadow(DeviceScene s, Paths P, int* err) {
     uint32_t n = P.counters[kCShadow];
     if (n > P.shadow_cap) {
@@ -551,11 +590,12 @@ __global__ void __launch_bounds__(kBlock) k_shadow(DeviceScene s, Paths P, int* 
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(reinterpret_cast<unsigned long long*>(P.counters + kCSh), n);
     const uint32_t stride = gridDim.x * blockDim.x;
+    uint2 traffic = make_uint2(0u, 0u);
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
         const float4* e = P.shadow + 3 * static_cast<size_t>(j);
         const float4 a = e[0], b = e[1];
         float t;
-        if (!degenerate(a, b) && !traverse<true>(s, ld_f3(a), ld_f3(b), a.w, t, err)) {
+        if (!degenerate(a, b) && !traverse<true, kCount>(s, ld_f3(a), ld_f3(b), a.w, t, err, &traffic)) {
             const float4 c = e[2];
             float4* L = P.rad + __float_as_uint(b.w);
             atomicAdd(&L->x, c.x);
@@ -563,6 +603,7 @@ __global__ void __launch_bounds__(kBlock) k_shadow(DeviceScene s, Paths P, int* 
             atomicAdd(&L->z, c.z);
         }
     }
+    if (kCount) warp_add_counts(P.counters, kCTraffic + 4, traffic);
 }
 
 __global__ void __launch_bounds__(kBlock) k_film(Wave w, Paths P, float* film_mean, float* film_m2) {
@@ -623,15 +664,22 @@ __global__ void __launch_bounds__(kBlock) k_film_packed(Paths P) {
 
 rbr_status read_render_counters(rbr_ctx* ctx) {
     if (!ctx->pt.counters.ptr) return RBR_OK;
-    ctx->last_render.extension_rays = 0;
-    ctx->last_render.shadow_rays = 0;
+    rbr_render_stats& r = ctx->last_render;
+    r.extension_rays = r.shadow_rays = r.shaded_vertices = 0;
+    r.ext_nodes = r.ext_records = r.shadow_nodes = r.shadow_records = 0;
     for (int b = 0; b < (ctx->pt_last_two ? 2 : 1); ++b) {
         const PathBuffers& pb = b ? ctx->pt2 : ctx->pt;
-        unsigned long long h[2] = {0, 0};
-        const cudaError_t e = cudaMemcpy(h, static_cast<uint32_t*>(pb.counters.ptr) + kCExt, 16, cudaMemcpyDeviceToHost);
+        uint32_t h[kCWords];
+        const cudaError_t e = cudaMemcpy(h, pb.counters.ptr, sizeof(h), cudaMemcpyDeviceToHost);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "reading the render counters");
-        ctx->last_render.extension_rays += h[0];
-        ctx->last_render.shadow_rays += h[1];
+        auto u64 = [&](int word) { return uint64_t(h[word]) | (uint64_t(h[word + 1]) << 32); };
+        r.extension_rays += u64(kCExt);
+        r.shadow_rays += u64(kCSh);
+        r.shaded_vertices += u64(kCShade);
+        r.ext_nodes += u64(kCTraffic);
+        r.ext_records += u64(kCTraffic + 2);
+        r.shadow_nodes += u64(kCTraffic + 4);
+        r.shadow_records += u64(kCTraffic + 6);
     }
     return RBR_OK;
 }
@@ -694,6 +742,7 @@ rbr_status render(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_params* 
         return fail(ctx, RBR_ERR_UNSUPPORTED, "RBR_RENDER_CORRECTED_MIS is not implemented");
     if ((p->flags & RBR_RENDER_SECOND_MOMENT) == 0) film_m2 = nullptr;
     const bool volumetric = (p->flags & RBR_RENDER_VOLUMETRIC) != 0;
+    const bool count = (p->flags & RBR_RENDER_COUNT_TRAFFIC) != 0;
     const uint64_t npix = uint64_t(cam->width) * cam->height;
     const uint32_t spp = static_cast<uint32_t>(p->samples_per_pixel);
     if (npix * spp > 0xFFFFFFFFull || spp > kDefaultCapacity)
@@ -776,13 +825,24 @@ rbr_status render(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_params* 
         for (uint32_t d = 0; d < w.max_depth; ++d) {
             k_begin<<<1, 1, 0, ws>>>(P, d);
             if (volumetric) {
-                k_extend<true, false><<<grid, kBlock, 0, ws>>>(ctx->scene, w, P, d, ctx->d_error);
+                if (count) k_extend<true, false, true><<<grid, kBlock, 0, ws>>>(ctx->scene, w, P, d, ctx->d_error);
+                else k_extend<true, false><<<grid, kBlock, 0, ws>>>(ctx->scene, w, P, d, ctx->d_error);
                 k_shade<2, false><<<grid, kBlock, 0, ws>>>(ctx->scene, w, P, d);
             } else {
-                k_extend<false, false><<<grid, kBlock, 0, ws>>>(ctx->scene, w, P, d, ctx->d_error);
-                k_shade<0, false><<<grid, kBlock, 0, ws>>>(ctx->scene, w, P, d);
+                if (count) k_extend<false, false, true><<<grid, kBlock, 0, ws>>>(ctx->scene, w, P, d, ctx->d_error);
+                else k_extend<false, false><<<grid, kBlock, 0, ws>>>(ctx->scene, w, P, d, ctx->d_error);
+                if (ctx->pt_shade_split) {
+                    k_shade<0, false, kShadeGlossy><<<grid, kBlock, 0, ws>>>(ctx->scene, w, P, d);
+                    k_shade<0, false, kShadeDiffuse><<<grid, kBlock, 0, ws>>>(ctx->scene, w, P, d);
+                    k_shade<0, false, kShadeSpecular><<<grid, kBlock, 0, ws>>>(ctx->scene, w, P, d);
+                    k_shade<0, false, kShadeNone><<<grid, kBlock, 0, ws>>>(ctx->scene, w, P, d);
+                    launches += 3;
+                } else {
+                    k_shade<0, false><<<grid, kBlock, 0, ws>>>(ctx->scene, w, P, d);
+                }
             }
-            k_shadow<<<grid, kBlock, 0, ws>>>(ctx->scene, P, ctx->d_error);
+            if (count) k_shadow<true><<<grid, kBlock, 0, ws>>>(ctx->scene, P, ctx->d_error);
+            else k_shadow<<<grid, kBlock, 0, ws>>>(ctx->scene, P, ctx->d_error);
             launches += 4;
         }
         k_film<<<grid, kBlock, 0, ws>>>(w, P, film_mean, film_m2);  // the wave's own pixels

@@ -433,41 +433,48 @@ __device__ __forceinline__ BSample st_sample(const Bsdf& b, uint32_t k, f3 wo) {
     return r;
 }
 
+// Lobe kinds a BSDF may hold, as a bit set over the kinds above. Code templated on a set
+// compiles only the lobes in it: the path tracer shades each material class (material_class:
+// any GGX lobe -> glossy; else a Lambertian lobe -> diffuse; else delta lobes only) with the
+// set of that class, so the diffuse and delta-only kernels carry no microfacet code.
+constexpr uint32_t kAllKinds = 0xFFu;
+constexpr uint32_t kDeltaKinds = (1u << kCondSpec) | (1u << kDielSpec) | (1u << kTransSpec) | (1u << kPassSpec);
+constexpr uint32_t kNoGGXKinds = kDeltaKinds | (1u << kLambert);
+__host__ __device__ constexpr bool has_kind(uint32_t set, uint32_t k) { return ((set >> k) & 1u) != 0; }
+
 // evaluate() and pdf() of a non-delta lobe (delta lobes give 0 and 0)
+template <uint32_t kKinds = kAllKinds>
 __device__ __forceinline__ void lobe_eval_pdf(const Bsdf& b, uint32_t k, f3 wo, f3 wi, f3& f, float& pdf) {
-    switch (k) {
-        case kLambert: {
-            const bool same = same_hemi(wo, wi);
-            f = same ? xmuls(b.base, kInvPi) : mk(0.0f, 0.0f, 0.0f);
-            pdf = same ? fm(fabsf(wi.z), kInvPi) : 0.0f;
-            return;
-        }
-        case kCondGGX:
-        case kDielGGX: ggxr_eval_pdf(b, k, wo, wi, f, pdf); return;
-        case kTransGGX: ggxt_eval_pdf(b, wo, wi, f, pdf); return;
-        default:
-            f = mk(0.0f, 0.0f, 0.0f);
-            pdf = 0.0f;
+    f = mk(0.0f, 0.0f, 0.0f);
+    pdf = 0.0f;
+    if (has_kind(kKinds, kLambert) && k == kLambert) {
+        const bool same = same_hemi(wo, wi);
+        f = same ? xmuls(b.base, kInvPi) : mk(0.0f, 0.0f, 0.0f);
+        pdf = same ? fm(fabsf(wi.z), kInvPi) : 0.0f;
+    } else if ((has_kind(kKinds, kCondGGX) || has_kind(kKinds, kDielGGX)) && (k == kCondGGX || k == kDielGGX)) {
+        ggxr_eval_pdf(b, k, wo, wi, f, pdf);
+    } else if (has_kind(kKinds, kTransGGX) && k == kTransGGX) {
+        ggxt_eval_pdf(b, wo, wi, f, pdf);
     }
 }
+template <uint32_t kKinds = kAllKinds>
 __device__ __forceinline__ BSample lobe_sample(const Bsdf& b, uint32_t k, f3 wo, float u1, float u2) {
-    switch (k) {
-        case kLambert: {
-            BSample r = none();
-            r.wi = cosine_hemisphere(u1, u2);
-            if (wo.z < 0.0f) r.wi.z = -r.wi.z;
-            r.f = xmuls(b.base, kInvPi);
-            r.pdf = fm(fabsf(r.wi.z), kInvPi);
-            return r;
-        }
-        case kCondSpec:
-        case kDielSpec: return sr_sample(b, k, wo);
-        case kTransSpec:
-        case kPassSpec: return st_sample(b, k, wo);
-        case kCondGGX:
-        case kDielGGX: return ggxr_sample(b, k, wo, u1, u2);
-        default: return ggxt_sample(b, wo, u1, u2);
+    if (has_kind(kKinds, kLambert) && k == kLambert) {
+        BSample r = none();
+        r.wi = cosine_hemisphere(u1, u2);
+        if (wo.z < 0.0f) r.wi.z = -r.wi.z;
+        r.f = xmuls(b.base, kInvPi);
+        r.pdf = fm(fabsf(r.wi.z), kInvPi);
+        return r;
     }
+    if ((has_kind(kKinds, kCondSpec) || has_kind(kKinds, kDielSpec)) && (k == kCondSpec || k == kDielSpec))
+        return sr_sample(b, k, wo);
+    if ((has_kind(kKinds, kTransSpec) || has_kind(kKinds, kPassSpec)) && (k == kTransSpec || k == kPassSpec))
+        return st_sample(b, k, wo);
+    if ((has_kind(kKinds, kCondGGX) || has_kind(kKinds, kDielGGX)) && (k == kCondGGX || k == kDielGGX))
+        return ggxr_sample(b, k, wo, u1, u2);
+    if (has_kind(kKinds, kTransGGX) && k == kTransGGX) return ggxt_sample(b, wo, u1, u2);
+    return none();
 }
 
 // MixtureBSDF
@@ -505,6 +512,7 @@ __device__ __forceinline__ Mix mixture(const Bsdf& b, f3 wo) {
 }
 // MixtureBSDF::evaluate and MixtureBSDF::pdf for one (wo, wi), in one pass over the lobes:
 // f = sum of w_i f_i, pdf = (sum of score_i pdf_i) / total over the non-delta lobes.
+template <uint32_t kKinds = kAllKinds>
 __device__ __forceinline__ void bsdf_eval_pdf(const Bsdf& b, const Mix& m, f3 wo, f3 wi, f3& f, float& pdf) {
     f = mk(0.0f, 0.0f, 0.0f);
     float p = 0.0f;
@@ -513,12 +521,13 @@ __device__ __forceinline__ void bsdf_eval_pdf(const Bsdf& b, const Mix& m, f3 wo
         if (lobe_delta(k)) continue;
         f3 fl;
         float pl;
-        lobe_eval_pdf(b, k, wo, wi, fl, pl);
+        lobe_eval_pdf<kKinds>(b, k, wo, wi, fl, pl);
         f = xadd(f, xmuls(fl, mix_w(m, i)));
         p = fa(p, fm(mix_sc(m, i), pl));
     }
     pdf = m.total <= 0.0f ? 0.0f : fd(p, m.total);
 }
+template <uint32_t kKinds = kAllKinds>
 __device__ __forceinline__ BSample bsdf_sample(const Bsdf& b, const Mix& m, f3 wo, float u1, float u2) {
     if (m.total <= 0.0f) return none();
     float u = fm(u1, m.total);
@@ -536,7 +545,7 @@ __device__ __forceinline__ BSample bsdf_sample(const Bsdf& b, const Mix& m, f3 w
     if (sc <= 0.0f) return none();
     const float v1 = omin(fd(u, sc), 0.99999994f);
     const uint32_t k = kind_of(b, chosen);
-    BSample s = lobe_sample(b, k, wo, v1, u2);
+    BSample s = lobe_sample<kKinds>(b, k, wo, v1, u2);
     if (s.pdf <= 0.0f || black(s.f)) return none();
     const float pChosen = fd(sc, m.total);
     if (lobe_delta(k)) {
@@ -544,7 +553,7 @@ __device__ __forceinline__ BSample bsdf_sample(const Bsdf& b, const Mix& m, f3 w
         s.pdf = fm(s.pdf, pChosen);
         return s;
     }
-    bsdf_eval_pdf(b, m, wo, s.wi, s.f, s.pdf);
+    bsdf_eval_pdf<kKinds>(b, m, wo, s.wi, s.f, s.pdf);
     if (s.pdf <= 0.0f) return none();
     return s;
 }

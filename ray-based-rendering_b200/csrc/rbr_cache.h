@@ -24,6 +24,7 @@ struct CacheDev {
     uint32_t dense_mask;          // bit l: level l indexed densely
     uint32_t log2_table;
     float lo[3], inv_ext[3];      // position -> [0,1]^3: (p - lo) * inv_ext, clamped
+    uint32_t wait_limit;          // polls of a tensor-core completion wait before it gives up
 };
 
 // Adam's per-run constants and device-side step state.

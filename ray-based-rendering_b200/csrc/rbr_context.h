@@ -64,10 +64,13 @@ struct rbr_ctx {
     uint32_t trace_host_chunk = 1u << 20;  // rbr_trace_host: rays per pipelined chunk (0: one piece)
     uint32_t pt_wave_paths = 1u << 23;
     int bvh_record_cost_milli = 1000;      // 8-wide collapse: record test cost / node test cost x1000
+    uint32_t cache_wait_limit = 1u << 22;  // polls of a tensor-core completion wait (cache kernels)
+    uint32_t fail_alloc_countdown = 0;     // > 0: the n-th next device allocation fails (fault injection)
     // path tracer
     rbr::PathBuffers pt;
     rbr::PathBuffers pt2;                  // second wave in flight (rbr_render, pt_streams 2)
     int pt_streams = 2;                    // waves in flight in rbr_render: 1 or 2
+    int pt_shade_split = 0;                // rbr_render: one shading launch per material class
     bool pt_last_two = false;              // the last rbr_render used pt2
     cudaStream_t side_stream = nullptr;    // stream of the second wave
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;

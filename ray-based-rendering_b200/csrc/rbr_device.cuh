@@ -190,7 +190,7 @@ __device__ __forceinline__ float fmin3(float a, float b, float c) {
     return d;
 }
 
-// Mask of (width & 31) bits starting at bit (pos & 31); bits above 31 are dropped.
+// Mask of `width` bits starting at bit `pos` (pos < 32, width < 32); bits above 31 are dropped.
 __device__ __forceinline__ uint32_t bitmask_at(uint32_t pos, uint32_t width) {
     uint32_t d;
     asm("bmsk.wrap.b32 %0, %1, %2;" : "=r"(d) : "r"(pos), "r"(width));
@@ -214,8 +214,8 @@ constexpr float kTHi = 1.0f + 1.0f / 65536.0f;
 struct NodeView {
     float2 ax, bx, ay, by, az, bz;   // (near, far) factors per axis
     uint2 nx, fx, ny, fy, nz, fz;    // near / far plane bytes per axis (8 slots)
-    uint32_t pos_lo, pos_hi;         // meta bytes with internal positions XOR the ray octant
-    uint32_t wid_lo, wid_hi;         // widths of the slots' bit ranges
+    uint32_t pos_lo, pos_hi;         // per slot byte: first bit (internal: 24 + (slot ^ ray octant))
+    uint32_t wid_lo, wid_hi;         // per slot byte: number of bits
     uint32_t imask, child_base, prim_base;
 };
 
@@ -250,8 +250,8 @@ __device__ __forceinline__ NodeView node_view(const uint4* __restrict__ nodes, u
     v.nz = r.nz ? qhiz : qloz;
     v.fz = r.nz ? qloz : qhiz;
     v.imask = w0.w >> 24;
-    v.pos_lo = w1.z ^ inner_oct4(v.imask & 0xFu, r.oct);
-    v.pos_hi = w1.w ^ inner_oct4(v.imask >> 4, r.oct);
+    v.pos_lo = (w1.z ^ inner_oct4(v.imask & 0xFu, r.oct)) & 0x1F1F1F1Fu;
+    v.pos_hi = (w1.w ^ inner_oct4(v.imask >> 4, r.oct)) & 0x1F1F1F1Fu;
     v.wid_lo = (w1.z >> 5) & 0x07070707u;
     v.wid_hi = (w1.w >> 5) & 0x07070707u;
     v.child_base = w1.x;
@@ -271,10 +271,13 @@ __device__ __forceinline__ bool slot_hit(const NodeView& v, int i, float tbest) 
     return fmaxf(tn, 0.0f) <= fminf(tf, tbest);
 }
 
+// Byte k (0..3) of a word, zero-extended.
+__device__ __forceinline__ uint32_t byte_of(uint32_t w, uint32_t k) { return __byte_perm(w, 0u, 0x4440u | k); }
+
 // Bits of slot i in the node's hit mask: its leaf records, or bit 24 + (slot ^ octant).
 __device__ __forceinline__ uint32_t slot_bits(const NodeView& v, int i) {
-    const uint32_t sh = 8u * static_cast<uint32_t>(i & 3);
-    return bitmask_at((i >= 4 ? v.pos_hi : v.pos_lo) >> sh, (i >= 4 ? v.wid_hi : v.wid_lo) >> sh);
+    const uint32_t k = static_cast<uint32_t>(i & 3);
+    return bitmask_at(byte_of(i >= 4 ? v.pos_hi : v.pos_lo, k), byte_of(i >= 4 ? v.wid_hi : v.wid_lo, k));
 }
 
 // Splits a node's hit mask into ngroup = (child_base, internal hit bits << 24 | imask << 16)

@@ -88,10 +88,12 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* mbar, uint32_t parity) {
     return ok != 0;
 }
 
-// Bounded wait for phase `parity` of the mbarrier to complete. Returns false if it did not
-// complete within the limit (the caller records an error and stops issuing work).
-__device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity) {
-    for (uint32_t i = 0; i < (1u << 22); ++i)
+// Bounded wait for phase `parity` of the mbarrier to complete: at most `limit` polls (each a
+// try_wait, which itself suspends for a bounded time). Returns false if it did not complete
+// (the caller records an error and stops issuing work).
+constexpr uint32_t kWaitPolls = 1u << 22;
+__device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, uint32_t limit = kWaitPolls) {
+    for (uint32_t i = 0; i < limit; ++i)
         if (mbar_try_wait(mbar, parity)) return true;
     return false;
 }

@@ -37,6 +37,7 @@ RBR_CAMERA_THIN_LENS = 1
 RBR_RENDER_CORRECTED_MIS = 1 << 0
 RBR_RENDER_SECOND_MOMENT = 1 << 1
 RBR_RENDER_VOLUMETRIC = 1 << 2
+RBR_RENDER_COUNT_TRAFFIC = 1 << 3
 
 _f3 = C.c_float * 3
 _u32p = C.POINTER(C.c_uint32)
@@ -150,6 +151,11 @@ class rbr_render_stats(C.Structure):
         ("waves", C.c_uint32),
         ("launches", C.c_uint32),
         ("milliseconds", C.c_float),
+        ("shaded_vertices", C.c_uint64),
+        ("ext_nodes", C.c_uint64),
+        ("ext_records", C.c_uint64),
+        ("shadow_nodes", C.c_uint64),
+        ("shadow_records", C.c_uint64),
     ]
 
 
