@@ -448,7 +448,7 @@ __global__ void __launch_bounds__(kBlock, 8) k_shade(DeviceScene s, Wave w, Path
                 while (j >= cnt[c + 1]) ++c;
                 k = P.classq[c * P.cap + (j - cnt[c])];
             } else {
-                k = P.classq[kCls * P.cap + j];
+                k = P.classq[static_cast<uint32_t>(kCls < 0 ? 0 : kCls) * P.cap + j];
             }
             const PathKey key = path_key<kPacked>(w, P, k);
             pixel = key.pixel;
