@@ -453,6 +453,13 @@ typedef struct rbr_batch_config {
     int32_t use_graphs;         /* replay each wave shape from a captured CUDA graph (default 1) */
     uint32_t waves_in_flight;   /* 1, or 2 (default; 0 means 2): waves alternate between two
                                    path-buffer sets and streams, each set within the budget */
+    uint32_t persistent;        /* 1: one cooperative launch renders every wave of a run (all
+                                   its stages, grid barriers between them) when no request uses
+                                   the radiance cache and the run has at most 16 scenes; 0 (default):
+                                   one captured graph per wave shape */
+    uint32_t barrier_timeout_us; /* persistent run: longest wait of a block at a grid barrier, in
+                                   microseconds, before the run gives up with RBR_ERR_DEVICE_TIMEOUT
+                                   (default 2,000,000; 0 means the default) */
 } rbr_batch_config;
 
 typedef struct rbr_request {
@@ -463,11 +470,15 @@ typedef struct rbr_request {
     int32_t use_cache;          /* end paths into the scene's radiance cache (rbr_batch_cache_create) */
     int32_t train_cache;        /* with use_cache: also train it on this request's paths */
     float* film;                /* device pointer, width*height*3 floats: per-pixel mean */
+    uint32_t arrival_us;        /* arrival after the start of rbr_batch_run, in microseconds (at
+                                   most 600 s): no wave holding the request starts before it, and
+                                   its latency counts from it. 0: present at the start */
+    uint32_t reserved;          /* 0 */
 } rbr_request;
 
 typedef struct rbr_request_stats {
-    float start_ms;             /* from the start of rbr_batch_run to the start of its first wave */
-    float latency_ms;           /* from the start of rbr_batch_run to the end of its last wave */
+    float start_ms;             /* from its arrival to the start of its first wave (queueing) */
+    float latency_ms;           /* from its arrival to the end of its last wave (device clock) */
     uint32_t waves;             /* waves it was spread over */
     uint32_t segments;
     uint64_t paths;
@@ -478,6 +489,7 @@ typedef struct rbr_batch_stats {
     uint32_t requests, waves, segments;
     uint32_t graphs_captured, graph_launches, kernel_launches;
     uint32_t wave_paths, blocks_per_sm;
+    uint32_t persistent_launches; /* cooperative launches that rendered the run (0 or 1) */
     uint64_t paths;
 } rbr_batch_stats;
 

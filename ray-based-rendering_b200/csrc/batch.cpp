@@ -8,7 +8,16 @@
 // segment table (SegDev) that is copied to a fixed device address before the wave, so the
 // kernels' arguments, and with them the captured graph, are the same for every wave of a
 // given (scene, mode, depth, grid).
+//
+// Requests may carry an arrival time: they are then served in arrival order and no wave
+// starts before its last request has arrived (device clock), which makes the latencies those
+// of a server under staggered arrivals. With `persistent`, one cooperative launch of
+// k_wave_loop renders every wave of the run (all stages, grid barriers between them, bounded
+// waits) instead of one graph launch per wave. Either way the device clock stamps the start of
+// the run and the end of every wave, and a request's latency runs from its arrival to the end
+// of its last wave.
 #include <algorithm>
+#include <numeric>
 #include <cstring>
 #include <map>
 #include <new>
@@ -26,6 +35,8 @@ constexpr uint32_t kMaxSegs = 512;                       // segments per wave
 constexpr size_t kHdrBytes = 64;                         // [paths, segments], padded
 constexpr size_t kTableBytes = kHdrBytes + sizeof(SegDev) * kMaxSegs;
 
+constexpr uint64_t kMaxArrivalUs = 600000000ull;        // 10 minutes
+
 struct Req {
     rbr_request r{};
     uint32_t id = 0;
@@ -39,6 +50,7 @@ struct WavePlan {
     bool train = false;
     uint32_t max_depth = 0;
     uint32_t paths = 0;
+    uint64_t release_ns = 0;  // arrival of its last request
     std::vector<SegDev> segs;
 };
 
@@ -68,6 +80,17 @@ struct rbr_batch {
     std::map<uint32_t, const void*> cache_buffers;  // per cached scene: its query buffer at capture
     rbr_batch_stats stats{};
     bool ran = false;
+    // device clock of the last run: [0] start, [1 + w] end of wave w
+    unsigned long long* d_stamps = nullptr;
+    size_t d_stamps_n = 0;
+    std::vector<unsigned long long> h_stamps;
+    bool stamps_read = false;
+    std::vector<uint64_t> run_release;           // release time of every wave of the last run (ns)
+    bool run_persistent = false;
+    // persistent runs: wave list + segment tables of the whole run, and the grid barrier
+    void* d_loop = nullptr;
+    size_t d_loop_bytes = 0;
+    uint32_t* d_bar = nullptr;
 };
 
 namespace {
@@ -108,16 +131,42 @@ uint32_t wave_capacity(const rbr_batch* b, bool any_cache) {
     return static_cast<uint32_t>(std::max<uint64_t>(1u << 16, std::min<uint64_t>(cap, 1u << 23)));
 }
 
-// Groups the pending requests by (scene, mode, train) in order of first appearance and packs
-// each group's requests, first come first served, into waves of `cap` paths.
+using WaveKey = std::tuple<uint32_t, int, bool>;  // scene, mode, train
+WaveKey key_of(const Req& q) { return std::make_tuple(q.r.scene, mode_of(q.r), q.r.use_cache && q.r.train_cache); }
+
+// Packs the requests into waves of `cap` paths, first come first served. Without arrival
+// times the requests are grouped by (scene, mode, train) in order of first appearance; with
+// them they are taken in arrival order and a wave closes whenever the next request needs
+// another scene or mode. A wave's release time is the arrival of its last request.
 std::vector<WavePlan> plan(rbr_batch* b, std::vector<Req>& reqs, uint32_t cap) {
-    std::vector<std::tuple<uint32_t, int, bool>> keys;
-    for (const Req& q : reqs) {
-        const auto k = std::make_tuple(q.r.scene, mode_of(q.r), q.r.use_cache && q.r.train_cache);
-        if (std::find(keys.begin(), keys.end(), k) == keys.end()) keys.push_back(k);
+    bool arrivals = false;
+    for (const Req& q : reqs) arrivals = arrivals || q.r.arrival_us != 0;
+    std::vector<std::vector<size_t>> groups;  // request indices, packed group by group
+    if (arrivals) {
+        std::vector<size_t> order(reqs.size());
+        std::iota(order.begin(), order.end(), size_t(0));
+        std::stable_sort(order.begin(), order.end(),
+                         [&](size_t x, size_t y) { return reqs[x].r.arrival_us < reqs[y].r.arrival_us; });
+        for (size_t i : order) {
+            if (groups.empty() || key_of(reqs[groups.back().front()]) != key_of(reqs[i])) groups.emplace_back();
+            groups.back().push_back(i);
+        }
+    } else {
+        std::vector<WaveKey> keys;
+        for (size_t i = 0; i < reqs.size(); ++i) {
+            const auto it = std::find(keys.begin(), keys.end(), key_of(reqs[i]));
+            if (it == keys.end()) {
+                keys.push_back(key_of(reqs[i]));
+                groups.emplace_back();
+                groups.back().push_back(i);
+            } else {
+                groups[static_cast<size_t>(it - keys.begin())].push_back(i);
+            }
+        }
     }
     std::vector<WavePlan> waves;
-    for (const auto& k : keys) {
+    for (const auto& group : groups) {
+        const WaveKey k = key_of(reqs[group.front()]);
         WavePlan cur;
         cur.scene = std::get<0>(k);
         cur.mode = std::get<1>(k);
@@ -127,9 +176,10 @@ std::vector<WavePlan> plan(rbr_batch* b, std::vector<Req>& reqs, uint32_t cap) {
             cur.segs.clear();
             cur.paths = 0;
             cur.max_depth = 0;
+            cur.release_ns = 0;
         };
-        for (Req& q : reqs) {
-            if (std::make_tuple(q.r.scene, mode_of(q.r), q.r.use_cache && q.r.train_cache) != k) continue;
+        for (size_t qi : group) {
+            Req& q = reqs[qi];
             const rbr_request& r = q.r;
             const uint32_t spp = static_cast<uint32_t>(r.params.samples_per_pixel);
             const uint32_t npix = static_cast<uint32_t>(r.camera.width) * static_cast<uint32_t>(r.camera.height);
@@ -161,6 +211,7 @@ std::vector<WavePlan> plan(rbr_batch* b, std::vector<Req>& reqs, uint32_t cap) {
                 }
                 ++q.segments;
                 q.paths += g.npaths;
+                cur.release_ns = std::max(cur.release_ns, uint64_t(r.arrival_us) * 1000u);
                 cur.segs.push_back(g);
                 cur.paths += g.npaths;
                 cur.max_depth = std::max(cur.max_depth, g.max_depth);
@@ -203,9 +254,13 @@ rbr_status run(rbr_batch* b, std::vector<Req>& reqs, cudaStream_t stream) {
     for (const Req& q : reqs)
         if (static_cast<uint32_t>(q.r.params.samples_per_pixel) > cap)
             return bfail(b, RBR_ERR_INVALID_ARGUMENT, "request " + std::to_string(q.id) + ": samples per pixel exceed the wave");
+    for (const Req& q : reqs)
+        if (q.r.arrival_us > kMaxArrivalUs)
+            return bfail(b, RBR_ERR_INVALID_ARGUMENT, "request " + std::to_string(q.id) + ": arrival beyond 600 s");
     std::vector<WavePlan> waves = plan(b, reqs, cap);
+    const bool persistent = b->cfg.persistent && !any_cache && !waves.empty() && b->scenes.size() <= 16;
     const uint32_t nl = max_lights(b);
-    rbr_status st = ensure_wave_buffers(eng, cap, cap * nl, slots);
+    rbr_status st = ensure_wave_buffers(eng, cap, cap * nl, persistent ? 1 : slots);
     if (st != RBR_OK) return bfail(b, st, eng->error);
     for (const WavePlan& w : waves) {
         if (w.mode != 1) continue;
@@ -223,7 +278,9 @@ rbr_status run(rbr_batch* b, std::vector<Req>& reqs, cudaStream_t stream) {
         drop_graphs(b);
         b->graph_generation = eng->pt_generation;
     }
-    const size_t need = std::max<size_t>(1, waves.size()) * kTableBytes;
+    // persistent runs upload the wave list and every segment table at once
+    const size_t list_bytes = (waves.size() * sizeof(LoopWave) + 255) & ~size_t(255);
+    const size_t need = (persistent ? list_bytes : 0) + std::max<size_t>(1, waves.size()) * kTableBytes;
     if (b->h_stage_bytes < need) {
         if (b->h_stage) cudaFreeHost(b->h_stage);
         b->h_stage = nullptr;
@@ -234,16 +291,81 @@ rbr_status run(rbr_batch* b, std::vector<Req>& reqs, cudaStream_t stream) {
     }
     st = ensure_events(b, waves.size() + 2);
     if (st != RBR_OK) return st;
+    if (b->d_stamps_n < waves.size() + 1) {
+        if (b->d_stamps) cudaFree(b->d_stamps);
+        b->d_stamps = nullptr;
+        b->d_stamps_n = 0;
+        const cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&b->d_stamps), (waves.size() + 1) * 8);
+        if (e != cudaSuccess) return bcuda(b, e, "wave time stamps");
+        b->d_stamps_n = waves.size() + 1;
+    }
+    b->run_release.clear();
+    for (const WavePlan& w : waves) b->run_release.push_back(w.release_ns);
+    b->stamps_read = false;
     const int grid = eng->num_sms * static_cast<int>(b->cfg.blocks_per_sm ? b->cfg.blocks_per_sm : 8);
     rbr_batch_stats s{};
     s.requests = static_cast<uint32_t>(reqs.size());
     s.wave_paths = cap;
     s.blocks_per_sm = b->cfg.blocks_per_sm ? b->cfg.blocks_per_sm : 8;
+    if (persistent) {
+        // one cooperative launch: the wave list, then every wave's segment table
+        char* host = static_cast<char*>(b->h_stage);
+        for (size_t wi = 0; wi < waves.size(); ++wi) {
+            const WavePlan& w = waves[wi];
+            LoopWave lw{};
+            lw.scene = w.scene;
+            lw.mode = static_cast<uint32_t>(w.mode);
+            lw.max_depth = w.max_depth;
+            lw.table = static_cast<uint32_t>(wi * kTableBytes);
+            lw.release_ns = w.release_ns;
+            std::memcpy(host + wi * sizeof(LoopWave), &lw, sizeof(lw));
+            char* tab = host + list_bytes + wi * kTableBytes;
+            const uint32_t hdr[2] = {w.paths, static_cast<uint32_t>(w.segs.size())};
+            std::memcpy(tab, hdr, sizeof(hdr));
+            std::memcpy(tab + kHdrBytes, w.segs.data(), w.segs.size() * sizeof(SegDev));
+            s.segments += static_cast<uint32_t>(w.segs.size());
+            s.paths += w.paths;
+        }
+        if (b->d_loop_bytes < need) {
+            if (b->d_loop) cudaFree(b->d_loop);
+            b->d_loop = nullptr;
+            b->d_loop_bytes = 0;
+            const cudaError_t e = cudaMalloc(&b->d_loop, need);
+            if (e != cudaSuccess) return bcuda(b, e, "persistent wave list");
+            b->d_loop_bytes = need;
+        }
+        if (!b->d_bar) {
+            const cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&b->d_bar), 2 * sizeof(uint32_t));
+            if (e != cudaSuccess) return bcuda(b, e, "grid barrier");
+        }
+        const uint64_t limit_ns = uint64_t(b->cfg.barrier_timeout_us ? b->cfg.barrier_timeout_us : 2000000u) * 1000ull;
+        int loop_grid = 0;
+        cudaError_t e = cudaEventRecord(b->events[0], stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_loop, host, need, cudaMemcpyHostToDevice, stream);
+        if (e == cudaSuccess)
+            e = launch_wave_loop(eng, b->scenes, static_cast<const LoopWave*>(b->d_loop), static_cast<uint32_t>(waves.size()),
+                                 static_cast<const char*>(b->d_loop) + list_bytes, b->d_stamps, b->d_bar, limit_ns, stream,
+                                 &loop_grid);
+        if (e == cudaSuccess) e = cudaEventRecord(b->events[waves.size() + 1], stream);
+        if (e != cudaSuccess) return bcuda(b, e, "persistent wave loop");
+        s.waves = static_cast<uint32_t>(waves.size());
+        s.kernel_launches = 1;
+        s.persistent_launches = 1;
+        s.blocks_per_sm = static_cast<uint32_t>(loop_grid / std::max(1, eng->num_sms));
+        b->stats = s;
+        b->run_waves = s.waves;
+        b->run_slots = 1;
+        b->run_persistent = true;
+        b->ran = true;
+        return RBR_OK;
+    }
     // Waves alternate between two path-buffer sets, segment tables and streams (slot = wave
     // index & 1), so one wave's latency-bound last bounces run beside the next wave. Waves
     // with the radiance cache share the scene's cache buffers and weights: each waits for the
     // previous one.
     cudaError_t e = cudaEventRecord(b->events[0], stream);
+    if (e == cudaSuccess) e = launch_stamp(b->d_stamps, stream);
+    ++s.kernel_launches;
     if (e == cudaSuccess && slots == 2) e = cudaEventRecord(b->ev_fork, stream);
     if (e == cudaSuccess && slots == 2) e = cudaStreamWaitEvent(b->side, b->ev_fork, 0);
     bool cache_wave = false;
@@ -254,6 +376,11 @@ rbr_status run(rbr_batch* b, std::vector<Req>& reqs, cudaStream_t stream) {
         const cudaStream_t ws = slot ? b->side : stream;
         if (w.mode == 1 && cache_wave && slots == 2) {
             e = cudaStreamWaitEvent(ws, b->ev_cache, 0);
+            if (e != cudaSuccess) break;
+        }
+        if (w.release_ns) {  // admission: not before the arrival of the wave's last request
+            e = launch_release(b->d_stamps, w.release_ns, ws);
+            ++s.kernel_launches;
             if (e != cudaSuccess) break;
         }
         char* dtab = static_cast<char*>(b->d_table) + slot * kTableBytes;
@@ -302,6 +429,8 @@ rbr_status run(rbr_batch* b, std::vector<Req>& reqs, cudaStream_t stream) {
         } else {
             e = launch_packed_wave(eng, scn, pw, ws);
         }
+        if (e == cudaSuccess) e = launch_stamp(b->d_stamps + 1 + wi, ws);
+        ++s.kernel_launches;
         if (e == cudaSuccess) e = cudaEventRecord(b->events[wi + 1], ws);
         if (e == cudaSuccess && w.mode == 1 && slots == 2) {
             e = cudaEventRecord(b->ev_cache, ws);
@@ -316,6 +445,7 @@ rbr_status run(rbr_batch* b, std::vector<Req>& reqs, cudaStream_t stream) {
     b->stats = s;
     b->run_waves = s.waves;
     b->run_slots = slots;
+    b->run_persistent = false;
     b->ran = true;
     return RBR_OK;
 }
@@ -332,6 +462,8 @@ void rbr_batch_config_default(rbr_batch_config* out) {
     out->blocks_per_sm = 8;
     out->use_graphs = 1;
     out->waves_in_flight = 2;
+    out->persistent = 0;
+    out->barrier_timeout_us = 2000000;
 }
 
 rbr_status rbr_batch_create(rbr_ctx* ctx, const rbr_batch_config* config, rbr_batch** out) {
@@ -365,6 +497,9 @@ void rbr_batch_destroy(rbr_batch* b) {
     if (b->ev_cache) cudaEventDestroy(b->ev_cache);
     for (size_t i = b->scenes.size(); i-- > 0;) rbr_ctx_destroy(b->scenes[i]);  // variants before their bases
     if (b->d_table) cudaFree(b->d_table);
+    if (b->d_stamps) cudaFree(b->d_stamps);
+    if (b->d_loop) cudaFree(b->d_loop);
+    if (b->d_bar) cudaFree(b->d_bar);
     if (b->h_stage) cudaFreeHost(b->h_stage);
     delete b;
 }
@@ -429,6 +564,8 @@ rbr_status rbr_batch_submit(rbr_batch* b, const rbr_request* r, uint32_t* reques
         return bfail(b, RBR_ERR_INVALID_ARGUMENT, "the scene has no radiance cache (rbr_batch_cache_create)");
     if (uint64_t(r->camera.width) * r->camera.height * r->params.samples_per_pixel > 0xFFFFFFFFull)
         return bfail(b, RBR_ERR_INVALID_ARGUMENT, "more than 2^32 samples in one request");
+    if (r->arrival_us > kMaxArrivalUs || r->reserved != 0)
+        return bfail(b, RBR_ERR_INVALID_ARGUMENT, "arrival beyond 600 s, or reserved field not 0");
     Req q;
     q.r = *r;
     q.id = b->next_id++;
@@ -457,14 +594,23 @@ rbr_status rbr_batch_request_stats(rbr_batch* b, uint32_t id, rbr_request_stats*
     const Req& q = b->done[it->second];
     const DeviceScope scope(b->eng->device);
     cudaError_t e = cudaEventSynchronize(b->events[b->run_waves + 1]);
-    // a wave starts when the previous wave of its stream has ended
-    const uint32_t prev = b->run_slots == 2 ? (q.first_wave >= 2 ? q.first_wave - 1 : 0) : q.first_wave;
-    float t0 = 0.0f, t1 = 0.0f;
-    if (e == cudaSuccess) e = cudaEventElapsedTime(&t0, b->events[0], b->events[prev]);
-    if (e == cudaSuccess) e = cudaEventElapsedTime(&t1, b->events[0], b->events[q.last_wave + 1]);
+    if (e == cudaSuccess && !b->stamps_read) {
+        b->h_stamps.assign(b->run_waves + 1, 0ull);
+        e = cudaMemcpy(b->h_stamps.data(), b->d_stamps, (b->run_waves + 1) * 8, cudaMemcpyDeviceToHost);
+        b->stamps_read = e == cudaSuccess;
+    }
     if (e != cudaSuccess) return bcuda(b, e, "request timing");
-    out->start_ms = prev == 0 ? 0.0f : t0;
-    out->latency_ms = t1;
+    // device clock, ns: the run's start, the request's arrival, the end of its last wave; its
+    // first wave started at its release time, or when the wave before it on the same path
+    // buffers ended, whichever was later
+    const double t0 = static_cast<double>(b->h_stamps[0]);
+    const double arrival = t0 + 1000.0 * q.r.arrival_us;
+    const double end = static_cast<double>(b->h_stamps[1 + q.last_wave]);
+    const uint32_t fw = q.first_wave, lag = b->run_slots == 2 ? 2u : 1u;
+    double start = fw >= lag ? static_cast<double>(b->h_stamps[1 + fw - lag]) : t0;
+    start = std::max(start, t0 + static_cast<double>(b->run_release[fw]));
+    out->start_ms = static_cast<float>(std::max(0.0, start - arrival) / 1e6);
+    out->latency_ms = static_cast<float>(std::max(0.0, end - arrival) / 1e6);
     out->waves = q.waves;
     out->segments = q.segments;
     out->paths = q.paths;

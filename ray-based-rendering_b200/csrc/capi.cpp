@@ -66,7 +66,7 @@ rbr_status check_device_error(rbr_ctx* ctx, cudaStream_t stream) {
     if (h & kErrStackOverflow) what += " traversal-stack overflow;";
     if (h & kErrQueueOverflow) what += " queue overflow;";
     if (h & kErrDeviceTimeout) {
-        what += " bounded wait for tensor-core completion ran out;";
+        what += " a bounded device wait (tensor-core completion or grid barrier) ran out;";
         return fail(ctx, RBR_ERR_DEVICE_TIMEOUT, "device check failed:" + what);
     }
     return fail(ctx, RBR_ERR_INTERNAL, "device check failed:" + what);

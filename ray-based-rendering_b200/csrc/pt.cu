@@ -30,6 +30,7 @@ namespace rbr {
 namespace {
 
 constexpr int kBlock = 128;
+constexpr int kLoopScenes = 16;  // scenes one persistent batched run can address
 constexpr uint32_t kDefaultCapacity = 1u << 22;  // most samples per pixel in one call (a wave holds a pixel's samples)
 constexpr size_t kShadowBytesLimit = size_t(2) << 30;
 
@@ -163,7 +164,7 @@ __device__ __forceinline__ bool degenerate(float4 o, float4 d) {
 
 // ------------------------------------------------------------------------------------------
 template <bool kPacked>
-__global__ void __launch_bounds__(kBlock) k_raygen(CameraDev cam, Wave w, Paths P) {
+__device__ __forceinline__ void raygen_body(const CameraDev& cam, const Wave& w, const Paths& P) {
     const uint32_t n = kPacked ? P.wave_hdr[0] : w.npaths;
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
@@ -201,12 +202,21 @@ __global__ void __launch_bounds__(kBlock) k_raygen(CameraDev cam, Wave w, Paths 
     }
 }
 
+template <bool kPacked>
+__global__ void __launch_bounds__(kBlock) k_raygen(CameraDev cam, Wave w, Paths P) {
+    raygen_body<kPacked>(cam, w, P);
+}
+
 // Resets the counters depth `d` appends to.
-__global__ void k_begin(Paths P, uint32_t d) {
+__device__ __forceinline__ void begin_body(const Paths& P, uint32_t d) {
     uint32_t* c = P.counters;
     c[kCQ0 + ((d + 1) & 1)] = 0;
     for (int i = 0; i < kNumClasses; ++i) c[kCClass + i] = 0;
     c[kCShadow] = 0;
+}
+
+__global__ void k_begin(Paths P, uint32_t d) {
+    begin_body(P, d);
 }
 
 // Closest hit for the active queue; misses add the background, hits are appended to their
@@ -219,8 +229,8 @@ __global__ void k_begin(Paths P, uint32_t d) {
 // also samples the medium and traces point-light shadow rays from scatter points, gains 5 % over
 // the natural 56-register allocation (foggy Cornell box); the surface variant is unchanged.
 // kCount (RBR_RENDER_COUNT_TRAFFIC): also counts the nodes and records the traversals fetch.
-template <bool kVol, bool kPacked, bool kCount = false>
-__global__ void __launch_bounds__(kBlock, 8) k_extend(DeviceScene s, Wave w, Paths P, uint32_t d, int* err) {
+template <bool kVol, bool kPacked, bool kCount>
+__device__ __forceinline__ void extend_body(const DeviceScene& s, const Wave& w, const Paths& P, uint32_t d, int* err) {
     const uint32_t n = P.counters[kCQ0 + (d & 1)];
     const uint32_t* q = (d & 1) ? P.q1 : P.q0;
     uint32_t* nextq = (d & 1) ? P.q0 : P.q1;
@@ -319,6 +329,11 @@ __global__ void __launch_bounds__(kBlock, 8) k_extend(DeviceScene s, Wave w, Pat
     if (kCount) warp_add_counts(P.counters, kCTraffic, traffic);
 }
 
+template <bool kVol, bool kPacked, bool kCount = false>
+__global__ void __launch_bounds__(kBlock, 8) k_extend(DeviceScene s, Wave w, Paths P, uint32_t d, int* err) {
+    extend_body<kVol, kPacked, kCount>(s, w, P, d, err);
+}
+
 // Surface data of a hit, as the primitive's intersect() fills SurfaceInteraction.
 struct Hit {
     f3 point;
@@ -413,8 +428,8 @@ __host__ __device__ constexpr uint32_t class_kinds() {
     return kCls == kShadeDiffuse ? kNoGGXKinds : kCls == kShadeSpecular ? kDeltaKinds : kCls == kShadeNone ? 0u : kAllKinds;
 }
 
-template <int kMode, bool kPacked, int kCls = -1>
-__global__ void __launch_bounds__(kBlock, 8) k_shade(DeviceScene s, Wave w, Paths P, uint32_t d) {
+template <int kMode, bool kPacked, int kCls>
+__device__ __forceinline__ void shade_body(const DeviceScene& s, const Wave& w, const Paths& P, uint32_t d) {
     constexpr bool kCache = kMode == 1, kVolSurface = kMode == 2;
     constexpr uint32_t kKinds = class_kinds<kCls>();
     constexpr bool kNoNee = kCls == kShadeSpecular || kCls == kShadeNone;
@@ -581,8 +596,13 @@ __global__ void __launch_bounds__(kBlock, 8) k_shade(DeviceScene s, Wave w, Path
     }
 }
 
-template <bool kCount = false>
-__global__ void __launch_bounds__(kBlock) k_shadow(DeviceScene s, Paths P, int* err) {
+template <int kMode, bool kPacked, int kCls = -1>
+__global__ void __launch_bounds__(kBlock, 8) k_shade(DeviceScene s, Wave w, Paths P, uint32_t d) {
+    shade_body<kMode, kPacked, kCls>(s, w, P, d);
+}
+
+template <bool kCount>
+__device__ __forceinline__ void shadow_body(const DeviceScene& s, const Paths& P, int* err) {
     uint32_t n = P.counters[kCShadow];
     if (n > P.shadow_cap) {
         if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(err, kErrQueueOverflow);
@@ -604,6 +624,11 @@ __global__ void __launch_bounds__(kBlock) k_shadow(DeviceScene s, Paths P, int* 
         }
     }
     if (kCount) warp_add_counts(P.counters, kCTraffic + 4, traffic);
+}
+
+template <bool kCount = false>
+__global__ void __launch_bounds__(kBlock) k_shadow(DeviceScene s, Paths P, int* err) {
+    shadow_body<kCount>(s, P, err);
 }
 
 __global__ void __launch_bounds__(kBlock) k_film(Wave w, Paths P, float* film_mean, float* film_m2) {
@@ -643,7 +668,7 @@ __global__ void __launch_bounds__(kBlock) k_film(Wave w, Paths P, float* film_me
 
 // Film of a packed wave: the first path of each pixel sums the pixel's samples into its
 // request's film.
-__global__ void __launch_bounds__(kBlock) k_film_packed(Paths P) {
+__device__ __forceinline__ void film_packed_body(const Paths& P) {
     const uint32_t n = P.wave_hdr[0];
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
@@ -658,6 +683,137 @@ __global__ void __launch_bounds__(kBlock) k_film_packed(Paths P) {
         o[1] = mean.y;
         o[2] = mean.z;
     }
+}
+
+__global__ void __launch_bounds__(kBlock) k_film_packed(Paths P) {
+    film_packed_body(P);
+}
+
+// ------------------------------------------------------------------------------------------
+// Persistent wave loop: one cooperative launch renders every wave of a batched run. The
+// stages of all waves run in the same resident blocks, separated by grid barriers instead of
+// kernel boundaries; a wave starts once its release time (the arrival of its last request)
+// has passed, and the device clock stamps its end.
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Grid-wide barrier of a cooperative launch (every block is resident). bar[0] counts arrivals,
+// bar[1] is the generation the last arrival advances. A wait longer than limit_ns of device
+// time records kErrDeviceTimeout; after that, or when another block recorded it, the barrier
+// reports failure and the caller leaves the kernel, so the blocks still waiting give up in
+// turn and nothing waits without bound.
+__device__ bool grid_barrier(uint32_t* bar, uint32_t& gen, uint64_t limit_ns, int* err) {
+    __shared__ int ok_s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        __threadfence();
+        if (atomicAdd(bar, 1u) + 1u == gridDim.x) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicExch(bar + 1, gen + 1u);
+        } else {
+            const uint64_t t0 = global_ns();
+            while (ld_acquire(bar + 1) == gen) {
+                if (global_ns() - t0 > limit_ns || (*reinterpret_cast<volatile int*>(err) & kErrDeviceTimeout)) {
+                    ok = 0;
+                    atomicOr(err, kErrDeviceTimeout);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        ok_s = ok;
+    }
+    __syncthreads();
+    ++gen;
+    return ok_s != 0;
+}
+
+// The stages as separate (not inlined) functions: each keeps the register allocation of its own
+// kernel instead of the loop kernel holding all of them at once.
+__device__ __noinline__ void loop_raygen(const Paths& P) {
+    const Wave w{};
+    const CameraDev unused{};
+    raygen_body<true>(unused, w, P);
+}
+template <bool kVol>
+__device__ __noinline__ void loop_extend(const DeviceScene& s, const Paths& P, uint32_t d, int* err) {
+    const Wave w{};
+    extend_body<kVol, true, false>(s, w, P, d, err);
+}
+template <int kMode>
+__device__ __noinline__ void loop_shade(const DeviceScene& s, const Paths& P, uint32_t d) {
+    const Wave w{};
+    shade_body<kMode, true, -1>(s, w, P, d);
+}
+__device__ __noinline__ void loop_shadow(const DeviceScene& s, const Paths& P, int* err) { shadow_body<false>(s, P, err); }
+__device__ __noinline__ void loop_film(const Paths& P) { film_packed_body(P); }
+
+struct LoopParams {
+    DeviceScene scenes[kLoopScenes];
+    const LoopWave* waves;
+    uint32_t nwaves;
+    const char* tables;          // segment tables, at LoopWave::table
+    Paths P;                     // path buffers (segments and header set per wave)
+    unsigned long long* stamps;  // [0] start of the run, [1 + w] end of wave w (device ns)
+    uint32_t* bar;               // [0] arrivals, [1] generation (zero at launch)
+    int* err;
+    uint64_t limit_ns;           // longest wait at a barrier
+};
+
+__global__ void __launch_bounds__(kBlock, 8) k_wave_loop(const __grid_constant__ LoopParams p) {
+    uint32_t gen = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) p.stamps[0] = global_ns();
+    if (!grid_barrier(p.bar, gen, p.limit_ns, p.err)) return;
+    const uint64_t t0 = *reinterpret_cast<volatile unsigned long long*>(p.stamps);
+    for (uint32_t wi = 0; wi < p.nwaves; ++wi) {
+        const LoopWave lw = p.waves[wi];
+        // admission: the wave's last request arrives release_ns after the run's start (the host
+        // bounds release_ns, so this wait ends)
+        while (global_ns() - t0 < lw.release_ns) __nanosleep(2048);
+        Paths P = p.P;
+        P.wave_hdr = reinterpret_cast<const uint32_t*>(p.tables + lw.table);
+        P.segs = reinterpret_cast<const SegDev*>(p.tables + lw.table + kSegTableHeader);
+        const DeviceScene& s = p.scenes[lw.scene];
+        if (blockIdx.x == 0)
+            for (uint32_t i = threadIdx.x; i < kCWords; i += blockDim.x) P.counters[i] = 0;
+        if (!grid_barrier(p.bar, gen, p.limit_ns, p.err)) return;
+        loop_raygen(P);
+        if (!grid_barrier(p.bar, gen, p.limit_ns, p.err)) return;
+        for (uint32_t d = 0; d < lw.max_depth; ++d) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) begin_body(P, d);
+            if (!grid_barrier(p.bar, gen, p.limit_ns, p.err)) return;
+            if (lw.mode == 2) loop_extend<true>(s, P, d, p.err);
+            else loop_extend<false>(s, P, d, p.err);
+            if (!grid_barrier(p.bar, gen, p.limit_ns, p.err)) return;
+            if (lw.mode == 2) loop_shade<2>(s, P, d);
+            else loop_shade<0>(s, P, d);
+            if (!grid_barrier(p.bar, gen, p.limit_ns, p.err)) return;
+            loop_shadow(s, P, p.err);
+            if (!grid_barrier(p.bar, gen, p.limit_ns, p.err)) return;
+        }
+        loop_film(P);
+        if (!grid_barrier(p.bar, gen, p.limit_ns, p.err)) return;
+        if (blockIdx.x == 0 && threadIdx.x == 0) p.stamps[1 + wi] = global_ns();
+    }
+}
+
+// Device clock stamps and admission for the graph-replayed waves of a batched run.
+__global__ void k_stamp(unsigned long long* at) { *at = global_ns(); }
+__global__ void k_release(const unsigned long long* start, uint64_t release_ns) {
+    const uint64_t t0 = *start;
+    while (global_ns() - t0 < release_ns) __nanosleep(2048);
 }
 
 }  // namespace
@@ -1128,6 +1284,57 @@ cudaError_t launch_packed_wave(rbr_ctx* eng, rbr_ctx* scn, const PackedWave& pw,
         e = cache_launch_train_frame(scn, P.counters + kCTrain, nullptr, scn->cache.t_cap, 0, stream);
         if (e != cudaSuccess) return e;
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wave_loop(rbr_ctx* eng, const std::vector<rbr_ctx*>& scenes, const LoopWave* waves, uint32_t nwaves,
+                             const char* tables, unsigned long long* stamps, uint32_t* bar, uint64_t limit_ns,
+                             cudaStream_t stream, int* grid_out) {
+    if (scenes.size() > static_cast<size_t>(kLoopScenes)) return cudaErrorInvalidValue;
+    LoopParams lp{};
+    for (size_t i = 0; i < scenes.size(); ++i) lp.scenes[i] = scenes[i]->scene;
+    lp.waves = waves;
+    lp.nwaves = nwaves;
+    lp.tables = tables;
+    PathBuffers& pb = eng->pt;
+    Paths& P = lp.P;
+    P.ray = static_cast<float4*>(pb.ray.ptr);
+    P.thr = static_cast<float4*>(pb.thr.ptr);
+    P.rad = static_cast<float4*>(pb.rad.ptr);
+    P.hit = static_cast<uint2*>(pb.hit.ptr);
+    P.q0 = static_cast<uint32_t*>(pb.queue[0].ptr);
+    P.q1 = static_cast<uint32_t*>(pb.queue[1].ptr);
+    P.classq = static_cast<uint32_t*>(pb.classq.ptr);
+    P.shadow = static_cast<float4*>(pb.shadow.ptr);
+    P.counters = static_cast<uint32_t*>(pb.counters.ptr);
+    P.cap = pb.capacity;
+    P.shadow_cap = pb.shadow_capacity;
+    P.seg_of = static_cast<uint32_t*>(eng->pt_seg_of.ptr);
+    lp.stamps = stamps;
+    lp.bar = bar;
+    lp.err = eng->d_error;
+    lp.limit_ns = limit_ns;
+    int per_sm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_wave_loop, kBlock, 0);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorCooperativeLaunchTooLarge;
+    const int grid = eng->num_sms * per_sm;  // every block resident: the barriers depend on it
+    if (grid_out) *grid_out = grid;
+    e = cudaMemsetAsync(bar, 0, 2 * sizeof(uint32_t), stream);
+    if (e != cudaSuccess) return e;
+    void* args[] = {&lp};
+    return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(k_wave_loop), dim3(grid), dim3(kBlock), args, 0,
+                                       stream);
+}
+
+cudaError_t launch_stamp(unsigned long long* at, cudaStream_t stream) {
+    k_stamp<<<1, 1, 0, stream>>>(at);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_release(const unsigned long long* start, uint64_t release_ns, cudaStream_t stream) {
+    if (release_ns == 0) return cudaSuccess;
+    k_release<<<1, 1, 0, stream>>>(start, release_ns);
     return cudaGetLastError();
 }
 

@@ -72,4 +72,17 @@ struct SegDev {
     uint32_t spp, sample_offset, width, max_depth, use_nee, use_mis;
 };
 
+// Device segment tables of the batched loop: a 64-byte header ([0] paths of the wave, [1]
+// segments) followed by the wave's SegDev entries.
+constexpr uint32_t kSegTableHeader = 64;
+
+// One wave of a persistent batched run (k_wave_loop): its scene, integrator mode (0 path
+// tracer, 2 volumetric), depth iterations, the byte offset of its segment table in the run's
+// table array, and the earliest device time (ns after the run's start) at which it may start:
+// the arrival of its last request.
+struct LoopWave {
+    uint32_t scene, mode, max_depth, table;
+    uint64_t release_ns;
+};
+
 }  // namespace rbr

@@ -473,7 +473,7 @@ class Batch:
         cfg = self.ctx.cache_config(**kw)
         self._check(self.lib.rbr_batch_cache_create(self.h, scene_id, C.byref(cfg)))
 
-    def submit(self, scene_id, camera, params, film_ptr, use_cache=False, train_cache=False) -> int:
+    def submit(self, scene_id, camera, params, film_ptr, use_cache=False, train_cache=False, arrival_us=0) -> int:
         r = abi.rbr_request()
         r.scene = scene_id
         r.camera = camera
@@ -481,6 +481,7 @@ class Batch:
         r.use_cache = int(use_cache)
         r.train_cache = int(train_cache)
         r.film = film_ptr
+        r.arrival_us = int(arrival_us)
         rid = C.c_uint32()
         self._check(self.lib.rbr_batch_submit(self.h, C.byref(r), C.byref(rid)))
         return int(rid.value)

@@ -208,6 +208,8 @@ class rbr_batch_config(C.Structure):
         ("blocks_per_sm", C.c_uint32),
         ("use_graphs", C.c_int32),
         ("waves_in_flight", C.c_uint32),
+        ("persistent", C.c_uint32),
+        ("barrier_timeout_us", C.c_uint32),
     ]
 
 
@@ -219,6 +221,8 @@ class rbr_request(C.Structure):
         ("use_cache", C.c_int32),
         ("train_cache", C.c_int32),
         ("film", C.c_void_p),
+        ("arrival_us", C.c_uint32),
+        ("reserved", C.c_uint32),
     ]
 
 
@@ -243,6 +247,7 @@ class rbr_batch_stats(C.Structure):
         ("kernel_launches", C.c_uint32),
         ("wave_paths", C.c_uint32),
         ("blocks_per_sm", C.c_uint32),
+        ("persistent_launches", C.c_uint32),
         ("paths", C.c_uint64),
     ]
 

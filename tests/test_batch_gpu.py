@@ -1,8 +1,9 @@
 """Batched request loop (rbr_batch_*): requests of several scenes, resolutions, sample counts,
 depths and integrators packed into shared waves give the same images as rendering each request
 alone with rbr_render (the same random numbers per (pixel, sample, seed)), whether the waves
-are replayed from captured CUDA graphs or launched directly, and however a request is split
-over waves; per-request latency and batch statistics are reported."""
+are replayed from captured CUDA graphs, launched directly, or rendered by one persistent
+cooperative launch, however a request is split over waves, and with staggered arrival times;
+per-request latency (from arrival, on the device clock) and batch statistics are reported."""
 import numpy as np
 import pytest
 import torch
@@ -60,17 +61,17 @@ def alone(ctx, key, w, h, p):
     return ctx.render_host(s.camera, p)
 
 
-def batched(ctx, **cfg):
+def batched(ctx, arrivals=None, **cfg):
     b = Batch(ctx, **cfg)
     ids = {}
     for key, fn in build_scenes().items():
         ids[key] = b.add_scene(fn(16, 16))
     films, rids = [], []
-    for key, w, h, p in requests():
+    for i, (key, w, h, p) in enumerate(requests()):
         cam = build_scenes()[key](w, h).camera
         f = torch.zeros(w * h * 3, device="cuda")
         films.append(f)
-        rids.append(b.submit(ids[key], cam, p, f.data_ptr()))
+        rids.append(b.submit(ids[key], cam, p, f.data_ptr(), arrival_us=0 if arrivals is None else arrivals[i]))
     b.run()
     torch.cuda.synchronize()
     stats = [b.request_stats(r) for r in rids]
@@ -78,8 +79,10 @@ def batched(ctx, **cfg):
 
 
 @pytest.mark.parametrize("cfg", [dict(), dict(use_graphs=0), dict(wave_paths=4096), dict(wave_paths=1000, blocks_per_sm=2),
-                                 dict(wave_paths=4096, waves_in_flight=1)],
-                         ids=["graphs", "direct", "small-waves", "split-requests", "one-wave-in-flight"])
+                                 dict(wave_paths=4096, waves_in_flight=1), dict(persistent=1),
+                                 dict(persistent=1, wave_paths=1000)],
+                         ids=["graphs", "direct", "small-waves", "split-requests", "one-wave-in-flight", "persistent",
+                              "persistent-split-requests"])
 def test_packed_requests_equal_single_renders(bctx, cfg):
     b, films, stats = batched(bctx, **cfg)
     for (key, w, h, p), got in zip(requests(), films):
@@ -89,11 +92,13 @@ def test_packed_requests_equal_single_renders(bctx, cfg):
     bs = b.stats()
     assert bs.requests == len(requests()) and bs.waves >= 3  # three scenes x modes at least
     assert bs.paths == sum(w * h * p.samples_per_pixel for _, w, h, p in requests())
-    if cfg.get("use_graphs", 1):
-        assert bs.graph_launches == bs.waves and 1 <= bs.graphs_captured <= bs.waves
+    if cfg.get("persistent"):
+        assert bs.persistent_launches == 1 and bs.kernel_launches == 1 and bs.graph_launches == 0
+    elif cfg.get("use_graphs", 1):
+        assert bs.graph_launches == bs.waves and 1 <= bs.graphs_captured <= bs.waves and bs.persistent_launches == 0
     lat = [s.latency_ms for s in stats]
     assert all(s.latency_ms > 0 and s.start_ms <= s.latency_ms for s in stats)
-    assert max(lat) <= bs.milliseconds * 1.0001
+    assert max(lat) <= bs.milliseconds + 0.01
     if cfg.get("wave_paths") == 1000:
         assert any(s.waves > 1 for s in stats)  # a request spread over several waves
     b.close()
@@ -177,3 +182,50 @@ def test_scene_variants_share_geometry(bctx):
     bctx.upload(base)
     assert not np.allclose(bctx.render_host(cam, p), want)
     b.close()
+
+
+@pytest.mark.parametrize("persistent", [0, 1], ids=["graphs", "persistent"])
+def test_staggered_arrivals(bctx, persistent):
+    """Requests arriving over 30 ms (seeded): the same images; no request's wave starts before
+    it arrives, so the run lasts past the last arrival; latency counts from the arrival."""
+    rng = np.random.default_rng(41)
+    arrivals = np.sort(rng.integers(0, 30000, len(requests()))).tolist()
+    arrivals = list(rng.permutation(arrivals))  # submitted out of arrival order
+    b, films, stats = batched(bctx, arrivals=arrivals, persistent=persistent)
+    for (key, w, h, p), got in zip(requests(), films):
+        np.testing.assert_allclose(got, alone(bctx, key, w, h, p), rtol=2e-5, atol=2e-6, err_msg=key)
+    bs = b.stats()
+    assert bs.milliseconds >= max(arrivals) / 1000.0
+    assert all(s.latency_ms > 0 and 0 <= s.start_ms <= s.latency_ms for s in stats)
+    # a request is done within its arrival plus the whole run
+    assert all(a / 1000.0 + s.latency_ms <= bs.milliseconds + 0.01 for a, s in zip(arrivals, stats))
+    b.close()
+
+
+def test_persistent_barrier_wait_runs_out_and_recovers(bctx):
+    """A grid-barrier limit of 1 us makes the persistent run's barrier waits give up: the run
+    reports RBR_ERR_DEVICE_TIMEOUT (every block leaves the kernel, nothing waits without bound)
+    and the same context renders correctly afterwards."""
+    from rbr_b200 import RbrError
+
+    b = Batch(bctx, persistent=1, barrier_timeout_us=1)
+    sid = b.add_scene(cornell(16, 16))
+    cam = cornell(64, 64).camera
+    f = torch.zeros(64 * 64 * 3, device="cuda")
+    p = render_params(spp=4, max_depth=8, seed=3)
+    b.submit(sid, cam, p, f.data_ptr())
+    b.run()
+    with pytest.raises(RbrError) as e:
+        b.stats()
+    assert e.value.status == abi.RBR_ERR_DEVICE_TIMEOUT
+    b.close()
+    b = Batch(bctx, persistent=1)
+    sid = b.add_scene(cornell(16, 16))
+    b.submit(sid, cam, p, f.data_ptr())
+    b.run()
+    torch.cuda.synchronize()
+    assert b.stats().persistent_launches == 1
+    np.testing.assert_allclose(f.cpu().numpy().reshape(64, 64, 3), alone(bctx, "cornell", 64, 64, p), rtol=2e-5,
+                               atol=2e-6)
+    b.close()
+

@@ -37,7 +37,7 @@ def test_tensor_core_wait_runs_out_and_context_recovers():
         with pytest.raises(RbrError) as e:
             c.cache_infer(recs)
         assert e.value.status == abi.RBR_ERR_DEVICE_TIMEOUT
-        assert "bounded wait" in c.last_error()
+        assert "bounded device wait" in c.last_error()
         with pytest.raises(RbrError) as e:
             c.cache_train(recs, t, apply=False)
         assert e.value.status == abi.RBR_ERR_DEVICE_TIMEOUT
