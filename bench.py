@@ -594,108 +594,144 @@ def run_cache(args, rank, world, local_rank):
         print(json.dumps(line))
 
 
-def run_batch(args, rank, world, local_rank):
+def measure_batch(ctx, local_rank, rank, steps, warmup, e2e=True, autotune=True):
     """Batched request loop (config 5): 64 seeded requests, resolution uniform over {128^2,
     256^2, 512^2, 1024^2}, spp U{1..64}; scenes: 7 seeded material/light variants of the GGX
     scene sharing its geometry and BVH, and the foggy Cornell box (volumetric path, 1 in 8
-    requests); run once with the radiance cache off and once on (GGX variants end paths into
-    their scene's cache and train it). Latency of a request = device time from the start of the
-    run to the end of its last wave (all requests are submitted together). A step is one run of
-    the 64 requests."""
+    requests). Throughput with every request present at the start; then p50/p99 latency under
+    staggered arrivals: a seeded Poisson process whose mean gap is 1.25 x (all-at-once run time
+    / 64), i.e. about 80 % load, for the graph-replayed waves and for the persistent launch
+    (cache off), and for the graph path with the radiance cache on (GGX variants end paths into
+    their scene's cache and train it). Latency of a request = device time from its arrival to
+    the end of its last wave."""
     import torch
 
-    from rbr_b200 import Batch, Context, abi, render_params, scenes
+    from rbr_b200 import Batch, abi, render_params, scenes
 
-    torch.cuda.set_device(local_rank)
     rng = np.random.default_rng(5 + rank)
-    ctx = Context(local_rank)
-    batch = Batch(ctx)
     base = scenes.ggx_scene()
-    ids = [batch.add_scene(base)]
-    for v in range(1, 7):
-        ids.append(batch.add_scene_variant(ids[0], scenes.ggx_variant(base, v)))
+    variants = [scenes.ggx_variant(base, v) for v in range(1, 7)]
     fog = scenes.foggy_cornell_box()
-    fog_id = batch.add_scene(fog)
     sizes = [128, 256, 512, 1024]
     reqs = []
     for i in range(64):
         size = int(rng.choice(sizes))
         spp = int(rng.integers(1, 65))
         if i % 8 == 7:
-            reqs.append((fog_id, scenes.square_camera(fog.camera, size), spp, 8, abi.RBR_RENDER_VOLUMETRIC))
+            reqs.append(("fog", scenes.square_camera(fog.camera, size), spp, 8, abi.RBR_RENDER_VOLUMETRIC))
         else:
-            reqs.append((ids[int(rng.integers(0, len(ids)))], scenes.square_camera(base.camera, size), spp, 16, 0))
+            reqs.append((int(rng.integers(0, 7)), scenes.square_camera(base.camera, size), spp, 16, 0))
     films = [torch.zeros(c.width * c.height * 3, device=f"cuda:{local_rank}") for _, c, _, _, _ in reqs]
     stream = torch.cuda.current_stream().cuda_stream
-    for sid in ids:
-        batch.cache_create(sid, seed=1)
+    total_paths = sum(c.width * c.height * spp for _, c, spp, _, _ in reqs)
 
-    def submit(use_cache, subset=None):
+    def make(**cfg):
+        b = Batch(ctx, **cfg)
+        ids = [b.add_scene(base)] + [None] * 6
+        for v in range(1, 7):
+            ids[v] = b.add_scene_variant(ids[0], variants[v - 1])
+        fid = b.add_scene(fog)
+        for sid in ids:
+            b.cache_create(sid, seed=1)
+        return b, ids, fid
+
+    def submit(b, ids, fid, use_cache, arrivals=None, subset=None):
         rid = []
-        for i, (sid, cam, spp, depth, flags) in enumerate(reqs if subset is None else reqs[:subset]):
+        for i, (sk, cam, spp, depth, flags) in enumerate(reqs if subset is None else reqs[:subset]):
             cache = use_cache and not flags
-            rid.append(batch.submit(sid, cam, render_params(spp=spp, max_depth=depth, seed=1000 + i, flags=flags),
-                                    films[i].data_ptr(), use_cache=cache, train_cache=cache))
+            rid.append(b.submit(fid if sk == "fog" else ids[sk], cam,
+                                render_params(spp=spp, max_depth=depth, seed=1000 + i, flags=flags),
+                                films[i].data_ptr(), use_cache=cache, train_cache=cache,
+                                arrival_us=0 if arrivals is None else int(arrivals[i])))
         return rid
 
-    # autotune wave size and grid on a calibration subset, then warm up (graphs captured)
-    submit(False, subset=8)
-    batch.autotune(stream)
-    batch.run(stream)
-    for _ in range(max(1, args.warmup)):
-        submit(False)
-        batch.run(stream)
-    torch.cuda.synchronize()
-    results = {}
-    clocks = Clocks() if rank == 0 else None
-    if clocks:
-        clocks.start()
-    for mode in ("off", "on"):
-        lat, total_ms, paths, st = [], 0.0, 0, None
-        for step in range(args.steps):
-            rid = submit(mode == "on")
+    def timed(b, ids, fid, use_cache, arrivals, n):
+        lat, qlat, total_ms, paths, st, wall = [], [], 0.0, 0, None, 0.0
+        for _ in range(n):
+            rid = submit(b, ids, fid, use_cache, arrivals)
             t0 = time.perf_counter()
-            batch.run(stream)
-            st = batch.stats()
+            b.run(stream)
+            st = b.stats()
             wall = time.perf_counter() - t0
             total_ms += st.milliseconds
             paths += st.paths
-            lat += [batch.request_stats(r).latency_ms for r in rid]
-        results[mode] = {
-            "mpaths_per_s": paths / (total_ms / 1e3) / 1e6, "ms_per_run": total_ms / args.steps,
-            "latency_ms_p50": float(np.percentile(lat, 50)), "latency_ms_p99": float(np.percentile(lat, 99)),
-            "waves_per_run": st.waves, "segments_per_run": st.segments, "graph_launches_per_run": st.graph_launches,
-            "kernel_launches_per_run": st.kernel_launches, "wave_paths": st.wave_paths,
-            "blocks_per_sm": st.blocks_per_sm, "host_wall_s_last_run": wall}
-    clk = clocks.stop(visible_gpu_indices(local_rank)) if clocks else None
-    # end to end: submit, run and read every film back to the host
-    t0 = time.perf_counter()
-    submit(False)
-    batch.run(stream)
-    host = [f.cpu() for f in films]
-    e2e_s = time.perf_counter() - t0
-    total_paths = sum(c.width * c.height * spp for _, c, spp, _, _ in reqs)
+            rs = [b.request_stats(r) for r in rid]
+            lat += [r.latency_ms for r in rs]
+            qlat += [r.start_ms for r in rs]
+        return {"mpaths_per_s": paths / (total_ms / 1e3) / 1e6, "ms_per_run": total_ms / n,
+                "latency_ms_p50": float(np.percentile(lat, 50)), "latency_ms_p99": float(np.percentile(lat, 99)),
+                "queueing_ms_p50": float(np.percentile(qlat, 50)), "waves_per_run": st.waves,
+                "segments_per_run": st.segments, "graph_launches_per_run": st.graph_launches,
+                "kernel_launches_per_run": st.kernel_launches, "persistent_launches_per_run": st.persistent_launches,
+                "wave_paths": st.wave_paths, "blocks_per_sm": st.blocks_per_sm, "host_wall_s_last_run": wall}
+
+    out = {"workload": "64 seeded requests: resolution uniform over {128^2, 256^2, 512^2, 1024^2}, spp U{1..64}; "
+                       "7 material/light variants of the GGX scene (shared geometry, depth 16) and the foggy Cornell "
+                       "box (volumetric, depth 8, every 8th request)", "paths_per_run": total_paths}
+    clocks = Clocks() if rank == 0 else None
+    b, ids, fid = make()
+    if autotune:  # wave size and grid on a calibration subset, then warm up (graphs captured)
+        submit(b, ids, fid, False, subset=8)
+        b.autotune(stream)
+        b.run(stream)
+    for _ in range(max(1, warmup)):
+        submit(b, ids, fid, False)
+        b.run(stream)
+    torch.cuda.synchronize()
+    if clocks:
+        clocks.start()
+    out["all_at_once"] = timed(b, ids, fid, False, None, steps)
+    gap_us = 1.25 * out["all_at_once"]["ms_per_run"] * 1000.0 / len(reqs)
+    arrivals = np.cumsum(np.random.default_rng(77 + rank).exponential(gap_us, len(reqs))) - gap_us
+    arrivals = np.clip(arrivals, 0, None).astype(np.int64)
+    out["arrivals"] = {"process": "Poisson, seeded", "mean_gap_us": gap_us, "span_ms": float(arrivals[-1] / 1e3),
+                       "load": "about 80 % of the all-at-once throughput"}
+    out["staggered_graphs"] = timed(b, ids, fid, False, arrivals, steps)
+    out["staggered_graphs_cache_on"] = timed(b, ids, fid, True, arrivals, steps)
+    cfg = dict(wave_paths=out["all_at_once"]["wave_paths"], persistent=1)
+    bp, pids, pfid = make(**cfg)
+    submit(bp, pids, pfid, False)
+    bp.run(stream)  # warm-up
+    out["all_at_once_persistent"] = timed(bp, pids, pfid, False, None, steps)
+    out["staggered_persistent"] = timed(bp, pids, pfid, False, arrivals, steps)
+    out["clocks"] = clocks.stop(visible_gpu_indices(local_rank)) if clocks else None
+    if e2e:  # submit, run and read every film back to the host
+        t0 = time.perf_counter()
+        submit(b, ids, fid, False)
+        b.run(stream)
+        host = [f.cpu() for f in films]
+        e2e_s = time.perf_counter() - t0
+        del host
+        out["e2e"] = {"value": total_paths / e2e_s / 1e6, "unit": "Mpaths/s", "h2d_bytes_per_step": 0,
+                      "d2h_bytes_per_step": sum(c.width * c.height * 12 for _, c, _, _, _ in reqs),
+                      "path": "rbr_batch_submit x64 + rbr_batch_run + every film to host"}
+    bp.close()
+    b.close()
+    return out
+
+
+def run_batch(args, rank, world, local_rank):
+    import torch
+
+    from rbr_b200 import Context
+
+    torch.cuda.set_device(local_rank)
+    ctx = Context(local_rank)
+    r = measure_batch(ctx, local_rank, rank, args.steps, args.warmup, e2e=not args.no_e2e)
+    ctx.close()
     if rank == 0:
-        off = results["off"]
+        a = r["all_at_once"]
         print(json.dumps({
             "metric": "Mpaths/s & p50/p99 request latency, batched request loop (64 requests)",
-            "value": off["mpaths_per_s"] * world, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
-            "warmup": max(1, args.warmup), "ms_per_step": off["ms_per_run"], "higher_is_better": True,
+            "value": a["mpaths_per_s"] * world, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(1, args.warmup), "ms_per_step": a["ms_per_run"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-            "config": {"workload": "64 seeded requests: resolution uniform over {128^2, 256^2, 512^2, 1024^2}, spp "
-                                   "U{1..64}; 7 material/light variants of the GGX scene (shared geometry, depth 16) "
-                                   "and the foggy Cornell box (volumetric, depth 8, every 8th request)",
-                       "paths_per_run": total_paths,
+            "config": {"workload": r["workload"], "paths_per_run": r["paths_per_run"], "arrivals": r["arrivals"],
                        "l2": "path state of a wave (up to 8M paths x ~250 B, two waves in flight) larger than L2"},
-            "latency": {"cache_off": off, "cache_on": results["on"]},
-            "e2e": {"value": total_paths / e2e_s / 1e6, "unit": "Mpaths/s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": sum(c.width * c.height * 12 for _, c, _, _, _ in reqs),
-                    "path": "rbr_batch_submit x64 + rbr_batch_run + every film to host"},
-            "clocks": clk, "gpu_launches": off["kernel_launches_per_run"] * args.steps,
+            "latency": {k: r[k] for k in ("all_at_once", "staggered_graphs", "staggered_graphs_cache_on",
+                                          "all_at_once_persistent", "staggered_persistent")},
+            "e2e": r.get("e2e"), "clocks": r["clocks"], "gpu_launches": a["kernel_launches_per_run"] * args.steps,
         }))
-    del host
-    batch.close()
-    ctx.close()
 
 
 def main():

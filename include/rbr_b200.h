@@ -257,6 +257,8 @@ rbr_status rbr_scene_stats_get(const rbr_ctx* ctx, rbr_scene_stats* out);
  *   "pt.shade_split"       rbr_render: 1 shades each material class (glossy, diffuse, delta-only,
  *                          none) in a launch of its own, compiled for that class's lobes; 0 one
  *                          launch for all classes (default)
+ *   "cache.infer_groups"   radiance-cache inference: 128-sample tiles in flight per CTA, 1, 2 or 4
+ *                          (groups of four warps sharing one copy of the weights; default 1)
  *   "cache.wait_limit"     polls of a tensor-core completion wait in the radiance-cache kernels
  *                          before it gives up with RBR_ERR_DEVICE_TIMEOUT (default 2^22; 0
  *                          makes every such wait give up at once, which tests the error path:

@@ -359,6 +359,184 @@ __global__ void __launch_bounds__(128, 4)
 }
 
 // --------------------------------------------------------------------------------------------
+// Inference with several tiles in flight per CTA: G groups of 128 threads (four warps) each own
+// a 128-sample tile and run its chain (encode, five layers of MMA, commit, wait, epilogue)
+// independently of the other groups, with a named barrier per group instead of the CTA
+// barrier; the weights are loaded once per CTA and shared. While one group waits for its MMAs
+// or its hash-grid gathers, the others issue. The encoding and the epilogues stream eight or
+// sixteen features at a time, so that a thread keeps few values live and two CTAs of four
+// groups fit an SM (eight tiles in flight instead of four).
+// --------------------------------------------------------------------------------------------
+__device__ __forceinline__ void group_sync(uint32_t g) { asm volatile("bar.sync %0, 128;" ::"r"(1 + g) : "memory"); }
+// OR of `v` over the group's 128 threads (a barrier of the group).
+__device__ __forceinline__ bool group_any(uint32_t g, bool v) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %2, 0;\n\t"
+        "bar.red.or.pred q, %1, 128, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}\n"
+        : "=r"(r)
+        : "r"(1 + g), "r"(v ? 1u : 0u)
+        : "memory");
+    return r != 0;
+}
+
+// The encoding of `encode`, written as row `row` of the A operand eight features at a time.
+__device__ __forceinline__ void encode_row(const CacheDev& c, const float4* rec, uint8_t* act, uint32_t rg,
+                                           uint32_t row) {
+    const float4 r0 = __ldg(rec), r1 = __ldg(rec + 1), r2 = __ldg(rec + 2), r3 = __ldg(rec + 3);
+    float p[3];
+    unit_position(c, r0, p);
+#pragma unroll 1
+    for (int q = 0; q < 4; ++q) {
+        float v[8];
+#pragma unroll
+        for (int ll = 0; ll < 4; ++ll) {
+            const int l = 4 * q + ll;
+            uint32_t i[3];
+            float w[3];
+            level_cell(c, l, p, i, w);
+            const __half2* tab = c.grid + (static_cast<size_t>(l) << c.log2_table);
+            float f0 = 0.0f, f1 = 0.0f;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const float wt = corner_weight(w, k);
+                const float2 g = __half22float2(__ldg(tab + corner_index(c, l, i, k)));
+                f0 = fa(f0, fm(wt, g.x));
+                f1 = fa(f1, fm(wt, g.y));
+            }
+            v[2 * ll] = f0;
+            v[2 * ll + 1] = f1;
+        }
+        store_row(act, rg, row, 8 * q, v, 1);
+    }
+    float v[32];
+    const float d[3] = {r0.w, r1.x, r1.y};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float t = fm(fa(d[a], 1.0f), 2.0f);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) v[5 * a + k] = fmaxf(0.0f, fs(1.0f, fabsf(fs(t, static_cast<float>(k)))));
+    }
+    v[15] = r1.z;
+    v[16] = r1.w;
+    v[17] = r2.x;
+    v[18] = r2.y;
+    v[19] = r2.z;
+    v[20] = r2.w;
+    v[21] = r3.x;
+    v[22] = r3.y;
+    v[23] = r3.z;
+    v[24] = r3.w;
+    v[25] = 1.0f;
+#pragma unroll
+    for (int k = 26; k < 32; ++k) v[k] = 0.0f;
+    store_row(act, rg, row, 32, v, 4);
+}
+
+template <int G>
+__global__ void __launch_bounds__(128 * G, 8 / G)
+    k_rc_infer_groups(CacheDev c, const float4* records, uint32_t n, const uint32_t* n_ptr, InferOut o, int* err) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint8_t* ws = smem;
+    uint64_t* mbars = reinterpret_cast<uint64_t*>(smem + kWBytes + G * kActBytesInfer);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + kWBytes + G * kActBytesInfer + 8 * G);
+    const uint32_t count = n_ptr ? min(*n_ptr, n) : n;
+    const uint32_t tiles = (count + kRcTile - 1) / kRcTile;
+    if (blockIdx.x * G >= tiles) return;
+    const uint32_t tid = threadIdx.x, warp = tid >> 5;
+    const uint32_t g = tid >> 7, lt = tid & 127u;  // tile group, thread within the group
+    uint8_t* act = smem + kWBytes + g * kActBytesInfer;
+    uint64_t* mbar = mbars + g;
+    if (lt == 0) tc::mbar_init(mbar, 1);
+    load_weights(c.w, ws);
+    if (warp == 0) {
+        tc::tmem_alloc(tslot, 64 * G);
+        tc::tmem_relinquish();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tm = *tslot + 64u * g;                 // the group's 64 accumulator columns
+    const uint32_t tl = tm + (((warp & 3u) * 32u) << 16);  // this warp's 32 lanes
+    const uint32_t act_s = tc::smem_addr(act), w_s = tc::smem_addr(ws);
+    uint32_t phase = 0;
+    bool ok = true;
+    for (uint32_t tile = blockIdx.x * G + g; tile < tiles && ok; tile += gridDim.x * G) {
+        const uint32_t j = tile * kRcTile + lt;
+        const bool valid = j < count;
+        if (valid) {
+            encode_row(c, records + 4 * static_cast<size_t>(j), act, kActRgInfer, lt);
+        } else {
+            float z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+            for (int q = 0; q < 8; ++q) store_row(act, kActRgInfer, lt, 8 * q, z, 1);
+        }
+        float y[16];
+        for (int l = 0; l < 5 && ok; ++l) {
+            tc::fence_smem_async();
+            tc::fence_before_sync();
+            group_sync(g);
+            if (lt == 0) {
+                tc::fence_after_sync();
+                const uint32_t id = tc::idesc_bf16(128, l < 4 ? 64 : 16, 0, 0);
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    tc::mma_bf16(tm, tc::sdesc(act_s + k * 256, 128, kActRgInfer),
+                                 tc::sdesc(w_s + l * 8192 + k * 256, 128, 1024), id, k > 0);
+                tc::mma_commit(mbar);
+            }
+            const bool done = tc::mbar_wait(mbar, phase, c.wait_limit);
+            phase ^= 1u;
+            ok = !group_any(g, !done);
+            if (!ok) {
+                if (lt == 0) atomicOr(err, kErrDeviceTimeout);
+                break;
+            }
+            tc::fence_after_sync();
+            if (l < 4) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    float z[16];
+                    tc::tmem_ld16(tl + 16 * q, z);
+#pragma unroll
+                    for (int k = 0; k < 16; ++k) z[k] = fmaxf(z[k], 0.0f);
+                    store_row(act, kActRgInfer, lt, 16 * q, z, 2);
+                }
+            } else {
+                tc::tmem_ld16(tl, y);
+            }
+        }
+        if (ok && valid) {
+            const float r = fmaxf(y[0], 0.0f), gg = fmaxf(y[1], 0.0f), b = fmaxf(y[2], 0.0f);
+            if (o.rgb) {
+                o.rgb[3 * static_cast<size_t>(j)] = r;
+                o.rgb[3 * static_cast<size_t>(j) + 1] = gg;
+                o.rgb[3 * static_cast<size_t>(j) + 2] = b;
+            } else {
+                const float4 qi = o.q_info[j];
+                float4* L = o.path_rad + __float_as_uint(qi.w);
+                float4 v = *L;
+                v.x = fa(v.x, fm(qi.x, r));
+                v.y = fa(v.y, fm(qi.y, gg));
+                v.z = fa(v.z, fm(qi.z, b));
+                *L = v;
+            }
+        }
+    }
+    if (!ok) tc::mbar_wait(mbar, phase ^ 1u);  // let an overdue MMA drain before freeing TMEM
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        tc::fence_after_sync();
+        tc::tmem_dealloc(*tslot, 64 * G);
+    }
+}
+
+constexpr uint32_t smem_infer_groups(int G) { return kWBytes + G * kActBytesInfer + 8 * G + 8; }
+
+// --------------------------------------------------------------------------------------------
 // Training: forward + loss gradient + backward + weight and grid gradients for one batch.
 // --------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(128, 1) k_rc_train(CacheDev c, TrainBatchDev b, float* scalars, int* err) {
@@ -735,6 +913,12 @@ cudaError_t set_kernel_attributes(int device) {
     cudaError_t e = cudaFuncSetAttribute(k_rc_train, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemTrain);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_rc_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemInfer);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_rc_infer_groups<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 smem_infer_groups(2));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_rc_infer_groups<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 smem_infer_groups(4));
     if (e == cudaSuccess) g_attr_done = device;
     return e;
 }
@@ -1032,9 +1216,17 @@ cudaError_t cache_launch_infer(rbr_ctx* ctx, const float4* records, uint32_t n, 
     o.path_rad = path_rad;
     o.q_info = q_info;
     const uint32_t tiles = (n + kRcTile - 1) / kRcTile;
-    const uint32_t grid = std::max(1u, std::min<uint32_t>(tiles, ctx->num_sms * 4));
     CacheDev dev = cs.dev;
     dev.wait_limit = ctx->cache_wait_limit;
+    const int G = ctx->cache_infer_groups;
+    if (G == 2 || G == 4) {  // G tiles per CTA, 8 / G CTAs per SM
+        const uint32_t ctas = (tiles + G - 1) / G;
+        const uint32_t grid = std::max(1u, std::min<uint32_t>(ctas, ctx->num_sms * (8 / G)));
+        if (G == 2) k_rc_infer_groups<2><<<grid, 256, smem_infer_groups(2), stream>>>(dev, records, n, n_ptr, o, ctx->d_error);
+        else k_rc_infer_groups<4><<<grid, 512, smem_infer_groups(4), stream>>>(dev, records, n, n_ptr, o, ctx->d_error);
+        return cudaGetLastError();
+    }
+    const uint32_t grid = std::max(1u, std::min<uint32_t>(tiles, ctx->num_sms * 4));
     k_rc_infer<<<grid, 128, kSmemInfer, stream>>>(dev, records, n, n_ptr, o, ctx->d_error);
     return cudaGetLastError();
 }

@@ -190,6 +190,9 @@ rbr_status rbr_param_set(rbr_ctx* ctx, const char* name, int64_t value) {
     } else if (n == "pt.shade_split") {
         if (value != 0 && value != 1) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "pt.shade_split is 0 or 1");
         ctx->pt_shade_split = static_cast<int>(value);
+    } else if (n == "cache.infer_groups") {
+        if (value != 1 && value != 2 && value != 4) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "cache.infer_groups is 1, 2 or 4");
+        ctx->cache_infer_groups = static_cast<int>(value);
     } else if (n == "cache.wait_limit") {
         if (value < 0 || value > (int64_t(1) << 22)) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "cache.wait_limit is 0..2^22");
         ctx->cache_wait_limit = static_cast<uint32_t>(value);
@@ -225,6 +228,7 @@ rbr_status rbr_param_get(const rbr_ctx* ctx, const char* name, int64_t* value) {
     else if (n == "trace.host_chunk") *value = ctx->trace_host_chunk;
     else if (n == "bvh.record_cost_milli") *value = ctx->bvh_record_cost_milli;
     else if (n == "cache.wait_limit") *value = ctx->cache_wait_limit;
+    else if (n == "cache.infer_groups") *value = ctx->cache_infer_groups;
     else if (n == "pt.shade_split") *value = ctx->pt_shade_split;
     else if (n == "debug.fail_alloc") *value = ctx->fail_alloc_countdown;
     else return RBR_ERR_INVALID_ARGUMENT;

@@ -158,3 +158,20 @@ def test_training_lowers_loss(cctx):
     t = field(recs)
     rel = np.mean((pred - t) ** 2 / (t ** 2 + 1e-2))
     assert rel < 0.05, rel
+
+
+@pytest.mark.parametrize("groups", [2, 4])
+def test_grouped_inference_equals_one_tile_per_cta(cctx, groups):
+    """cache.infer_groups: several 128-sample tiles in flight per CTA compute each tile with the
+    same MMA sequence and epilogue as one tile per CTA, so the predictions are the same bits;
+    a ragged last tile and more tiles than the grid holds at once are covered."""
+    _, rng = make_cache(cctx, 7)
+    recs = random_records(rng, 5000)
+    cctx.set_param("cache.infer_groups", 1)
+    want = cctx.cache_infer(recs)
+    cctx.set_param("cache.infer_groups", groups)
+    try:
+        got = cctx.cache_infer(recs)
+    finally:
+        cctx.set_param("cache.infer_groups", 1)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
