@@ -187,6 +187,25 @@ rbr_status rbr_param_set(rbr_ctx* ctx, const char* name, int64_t value) {
     } else if (n == "pt.wave_paths") {
         if (value < 1024 || value > (int64_t(1) << 26)) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "pt.wave_paths is 1024..2^26");
         ctx->pt_wave_paths = static_cast<uint32_t>(value);
+    } else if (n == "trace.stream_io") {
+        if (value != 0 && value != 1) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "trace.stream_io is 0 or 1");
+        ctx->trace_stream_io = static_cast<int>(value);
+    } else if (n == "trace.l2_persist") {
+        if (value != 0 && value != 1) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "trace.l2_persist is 0 or 1");
+        const DeviceScope scope(ctx->device);
+        // the set-aside is a limit of this process's context: it ends with the context
+        size_t bytes = 0;
+        if (value) {
+            int max_persist = 0;
+            cudaError_t e = cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, ctx->device);
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "persisting L2 size");
+            bytes = static_cast<size_t>(max_persist);
+        }
+        cudaError_t e = cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, bytes);
+        if (e == cudaSuccess && !value) e = cudaCtxResetPersistingL2Cache();
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "persisting L2 set-aside");
+        ctx->l2_persist_bytes = bytes;
+        ctx->trace_l2_persist = static_cast<int>(value);
     } else if (n == "pt.shade_split") {
         if (value != 0 && value != 1) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "pt.shade_split is 0 or 1");
         ctx->pt_shade_split = static_cast<int>(value);
@@ -230,6 +249,8 @@ rbr_status rbr_param_get(const rbr_ctx* ctx, const char* name, int64_t* value) {
     else if (n == "cache.wait_limit") *value = ctx->cache_wait_limit;
     else if (n == "cache.infer_groups") *value = ctx->cache_infer_groups;
     else if (n == "pt.shade_split") *value = ctx->pt_shade_split;
+    else if (n == "trace.stream_io") *value = ctx->trace_stream_io;
+    else if (n == "trace.l2_persist") *value = ctx->trace_l2_persist;
     else if (n == "debug.fail_alloc") *value = ctx->fail_alloc_countdown;
     else return RBR_ERR_INVALID_ARGUMENT;
     return RBR_OK;

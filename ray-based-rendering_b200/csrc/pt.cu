@@ -596,8 +596,16 @@ __device__ __forceinline__ void shade_body(const DeviceScene& s, const Wave& w, 
     }
 }
 
+// Resident blocks per SM the register budget of a shading kernel allows: the unified kernel and
+// the lobeless and delta-only classes 8 (64 registers); the glossy class 6 (80 registers) and
+// the diffuse class 7 (72), which keeps their spills small (76 / 68 bytes instead of 232 / 156).
+template <int kCls>
+__host__ __device__ constexpr int shade_blocks() {
+    return kCls == kShadeGlossy ? 6 : kCls == kShadeDiffuse ? 7 : 8;
+}
+
 template <int kMode, bool kPacked, int kCls = -1>
-__global__ void __launch_bounds__(kBlock, 8) k_shade(DeviceScene s, Wave w, Paths P, uint32_t d) {
+__global__ void __launch_bounds__(kBlock, shade_blocks<kCls>()) k_shade(DeviceScene s, Wave w, Paths P, uint32_t d) {
     shade_body<kMode, kPacked, kCls>(s, w, P, d);
 }
 

@@ -44,6 +44,8 @@ struct rbr_ctx {
     bool has_scene = false;
     rbr::DeviceScene scene{};
     std::vector<rbr::DevBuf> scene_bufs;
+    const void* bvh_base = nullptr;   // nodes followed by leaf records, one allocation
+    size_t bvh_bytes = 0;
     rbr_scene_stats stats{};
     float bounds_lo[3] = {0, 0, 0}, bounds_hi[3] = {0, 0, 0};
     // host-call staging
@@ -59,6 +61,9 @@ struct rbr_ctx {
     int trace_blocks_per_sm = 0;   // persistent grid per SM (0: occupancy limit)
     int trace_min_blocks = 10;     // kernel 0: register budget for 8, 10 or 12 resident blocks per SM
     int trace_order = 0;           // kernel 0: 0 rays in the given order, 1 sorted by direction octant and origin
+    int trace_stream_io = 1;       // kernel 0: rays read and hits written with evict-first (streaming) hints
+    int trace_l2_persist = 0;      // kernel 0: the BVH's address range marked persisting in L2
+    size_t l2_persist_bytes = 0;   // the context's persisting-L2 set-aside while trace_l2_persist is on
     rbr::DevBuf sort_buf;          // keys, permutation and radix-sort scratch of trace_order 1
     rbr::DevBuf sort_buf2;         // the same for the second stream of a chunked rbr_trace_host
     uint32_t trace_host_chunk = 1u << 20;  // rbr_trace_host: rays per pipelined chunk (0: one piece)

@@ -203,6 +203,8 @@ void free_scene(rbr_ctx* ctx) {
     for (auto& b : ctx->scene_bufs) release(b);
     ctx->scene_bufs.clear();
     ctx->scene = DeviceScene{};
+    ctx->bvh_base = nullptr;
+    ctx->bvh_bytes = 0;
     ctx->has_scene = false;
     ctx->stats = rbr_scene_stats{};
 }
@@ -382,10 +384,19 @@ rbr_status upload_scene(rbr_ctx* ctx, const rbr_scene_desc* d) {
     DeviceScene s{};
     void* p = nullptr;
     rbr_status st;
-    if ((st = upload(ctx, bvh.nodes, "BVH nodes", &p)) != RBR_OK) return free_scene(ctx), st;
-    s.nodes = static_cast<const uint4*>(p);
-    if ((st = upload(ctx, records, "leaf records", &p)) != RBR_OK) return free_scene(ctx), st;
-    s.records = static_cast<const float4*>(p);
+    // nodes and leaf records in one allocation (records right after the nodes, 16-byte aligned
+    // since a node is 80 bytes): the traversal's whole read set is one address range, which an
+    // L2 access-policy window can cover ("trace.l2_persist")
+    {
+        std::vector<uint32_t> bvh_words(bvh.nodes.size() + records.size());
+        std::copy(bvh.nodes.begin(), bvh.nodes.end(), bvh_words.begin());
+        std::copy(records.begin(), records.end(), bvh_words.begin() + static_cast<std::ptrdiff_t>(bvh.nodes.size()));
+        if ((st = upload(ctx, bvh_words, "BVH nodes and leaf records", &p)) != RBR_OK) return free_scene(ctx), st;
+        s.nodes = bvh.nodes.empty() ? nullptr : static_cast<const uint4*>(p);
+        s.records = records.empty() ? nullptr : reinterpret_cast<const float4*>(static_cast<const uint32_t*>(p) + bvh.nodes.size());
+        ctx->bvh_base = p;
+        ctx->bvh_bytes = bvh_words.size() * 4;
+    }
     if ((st = upload(ctx, planes, "planes", &p)) != RBR_OK) return free_scene(ctx), st;
     s.planes = static_cast<const float4*>(p);
     if ((st = upload(ctx, plane_tags, "plane tags", &p)) != RBR_OK) return free_scene(ctx), st;
@@ -455,6 +466,8 @@ rbr_status upload_scene_variant(rbr_ctx* dst, const rbr_ctx* base, const rbr_mat
     s.num_lights = num_lights;
     set_medium(s, medium);
     dst->scene = s;
+    dst->bvh_base = base->bvh_base;
+    dst->bvh_bytes = base->bvh_bytes;
     dst->has_scene = true;
     for (int a = 0; a < 3; ++a) {
         dst->bounds_lo[a] = base->bounds_lo[a];

@@ -3,6 +3,7 @@
 // One thread per ray. Rays are read as two 16 B words (origin+tmax, direction+pad), answers
 // written as one 8 B word (closest) or one byte (any). The traversal itself is in
 // rbr_device.cuh.
+#include <algorithm>
 #include <cmath>
 
 #include <cub/device/device_radix_sort.cuh>
@@ -16,35 +17,70 @@ namespace {
 
 constexpr int kTraceBlock = 128;
 
+// Ray loads and hit stores: with kStream, evict-first (streaming) hints, since every ray and
+// hit is touched once and the L2 is better spent on the BVH.
+template <bool kStream>
+__device__ __forceinline__ float4 ray_word(const float4* p) { return kStream ? __ldcs(p) : __ldg(p); }
+template <bool kStream>
+__device__ __forceinline__ void put_hit(uint2* p, uint2 h) {
+    if (kStream) __stcs(p, h);
+    else *p = h;
+}
+
 // kMinBlocks: resident blocks per SM the register allocation must allow (8: up to 64
 // registers a thread, 10: 48, 12: 40) -- occupancy against register spills, picked by tuning.
-template <int kMinBlocks>
+template <int kMinBlocks, bool kStream>
 __global__ void __launch_bounds__(kTraceBlock, kMinBlocks) k_trace_closest(DeviceScene s, const float4* __restrict__ rays,
                                                                            uint32_t n, uint2* __restrict__ hits, int* err) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const float4 a = __ldg(rays + 2 * static_cast<size_t>(i));
-    const float4 b = __ldg(rays + 2 * static_cast<size_t>(i) + 1);
+    const float4 a = ray_word<kStream>(rays + 2 * static_cast<size_t>(i));
+    const float4 b = ray_word<kStream>(rays + 2 * static_cast<size_t>(i) + 1);
     float t = 0.0f;
     const uint32_t prim = traverse<false>(s, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, t, err);
-    hits[i] = make_uint2(prim, prim == 0xFFFFFFFFu ? 0u : __float_as_uint(t));
+    put_hit<kStream>(hits + i, make_uint2(prim, prim == 0xFFFFFFFFu ? 0u : __float_as_uint(t)));
 }
 
 // The same query on the rays in the order `perm` (a permutation of 0..n-1): rays that start
 // close together with directions of the same octant share warps, so they walk the same nodes.
 // Answers go to the rays' own positions.
-template <int kMinBlocks>
+template <int kMinBlocks, bool kStream>
 __global__ void __launch_bounds__(kTraceBlock, kMinBlocks)
     k_trace_closest_perm(DeviceScene s, const float4* __restrict__ rays, uint32_t n, const uint32_t* __restrict__ perm,
                          uint2* __restrict__ hits, int* err) {
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
-    const uint32_t i = __ldg(perm + j);
-    const float4 a = __ldg(rays + 2 * static_cast<size_t>(i));
-    const float4 b = __ldg(rays + 2 * static_cast<size_t>(i) + 1);
+    const uint32_t i = kStream ? __ldcs(perm + j) : __ldg(perm + j);
+    const float4 a = ray_word<kStream>(rays + 2 * static_cast<size_t>(i));
+    const float4 b = ray_word<kStream>(rays + 2 * static_cast<size_t>(i) + 1);
     float t = 0.0f;
     const uint32_t prim = traverse<false>(s, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, t, err);
-    hits[i] = make_uint2(prim, prim == 0xFFFFFFFFu ? 0u : __float_as_uint(t));
+    put_hit<kStream>(hits + i, make_uint2(prim, prim == 0xFFFFFFFFu ? 0u : __float_as_uint(t)));
+}
+
+// Launches a ray-query kernel; with trace.l2_persist the BVH's address range (nodes and leaf
+// records) is marked persisting in L2 for this launch only (a launch attribute: the caller's
+// stream keeps its own attributes).
+template <typename... Params, typename... Args>
+cudaError_t launch_query(const rbr_ctx* ctx, void (*kernel)(Params...), uint32_t blocks, cudaStream_t stream,
+                         Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(blocks);
+    cfg.blockDim = dim3(kTraceBlock);
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    if (ctx->trace_l2_persist && ctx->bvh_bytes && ctx->l2_persist_bytes) {
+        attr[0].id = cudaLaunchAttributeAccessPolicyWindow;
+        attr[0].val.accessPolicyWindow.base_ptr = const_cast<void*>(ctx->bvh_base);
+        attr[0].val.accessPolicyWindow.num_bytes = ctx->bvh_bytes;
+        attr[0].val.accessPolicyWindow.hitRatio =
+            static_cast<float>(std::min(1.0, double(ctx->l2_persist_bytes) / double(ctx->bvh_bytes)));
+        attr[0].val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+        attr[0].val.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+    }
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<Params>(args)...);
 }
 
 __global__ void __launch_bounds__(kTraceBlock) k_trace_any_perm(DeviceScene s, const float4* __restrict__ rays, uint32_t n,
@@ -440,20 +476,29 @@ cudaError_t launch_trace(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any_
                                                                 ctx->d_error);
         } else {
             auto* h = static_cast<uint2*>(out);
-            if (ctx->trace_min_blocks >= 12)
-                k_trace_closest_perm<12><<<blocks, kTraceBlock, 0, stream>>>(ctx->scene, r, n, perm, h, ctx->d_error);
-            else if (ctx->trace_min_blocks >= 10)
-                k_trace_closest_perm<10><<<blocks, kTraceBlock, 0, stream>>>(ctx->scene, r, n, perm, h, ctx->d_error);
-            else
-                k_trace_closest_perm<8><<<blocks, kTraceBlock, 0, stream>>>(ctx->scene, r, n, perm, h, ctx->d_error);
+            const bool st = ctx->trace_stream_io != 0;
+            const int mb = ctx->trace_min_blocks;
+            auto k = mb >= 12 ? (st ? k_trace_closest_perm<12, true> : k_trace_closest_perm<12, false>)
+                   : mb >= 10 ? (st ? k_trace_closest_perm<10, true> : k_trace_closest_perm<10, false>)
+                              : (st ? k_trace_closest_perm<8, true> : k_trace_closest_perm<8, false>);
+            return launch_query(ctx, k, blocks, stream, ctx->scene, r, n, perm, h, ctx->d_error);
         }
         return cudaGetLastError();
     }
     if (ctx->trace_kernel == 0) {
-        return any_hit ? launch_trace_any(ctx->scene, rays, n, static_cast<uint8_t*>(out), ctx->d_error, ctx->trace_min_blocks,
-                                          stream)
-                       : launch_trace_closest(ctx->scene, rays, n, static_cast<rbr_hit*>(out), ctx->d_error,
-                                              ctx->trace_min_blocks, stream);
+        if (any_hit)
+            return launch_trace_any(ctx->scene, rays, n, static_cast<uint8_t*>(out), ctx->d_error, ctx->trace_min_blocks,
+                                    stream);
+        if (n == 0) return cudaSuccess;
+        const uint32_t blocks = (n + kTraceBlock - 1) / kTraceBlock;
+        const auto* r = reinterpret_cast<const float4*>(rays);
+        auto* h = static_cast<uint2*>(out);
+        const bool st = ctx->trace_stream_io != 0;
+        const int mb = ctx->trace_min_blocks;
+        auto k = mb >= 12 ? (st ? k_trace_closest<12, true> : k_trace_closest<12, false>)
+               : mb >= 10 ? (st ? k_trace_closest<10, true> : k_trace_closest<10, false>)
+                          : (st ? k_trace_closest<8, true> : k_trace_closest<8, false>);
+        return launch_query(ctx, k, blocks, stream, ctx->scene, r, n, h, ctx->d_error);
     }
     const bool coop = ctx->trace_kernel == 2;
     const int per_sm = ctx->trace_blocks_per_sm > 0
@@ -545,9 +590,9 @@ cudaError_t launch_trace_closest(const DeviceScene& s, const rbr_ray* rays, uint
     const uint32_t blocks = (n + kTraceBlock - 1) / kTraceBlock;
     const auto* r = reinterpret_cast<const float4*>(rays);
     auto* h = reinterpret_cast<uint2*>(hits);
-    if (min_blocks >= 12) k_trace_closest<12><<<blocks, kTraceBlock, 0, stream>>>(s, r, n, h, err);
-    else if (min_blocks >= 10) k_trace_closest<10><<<blocks, kTraceBlock, 0, stream>>>(s, r, n, h, err);
-    else k_trace_closest<8><<<blocks, kTraceBlock, 0, stream>>>(s, r, n, h, err);
+    if (min_blocks >= 12) k_trace_closest<12, true><<<blocks, kTraceBlock, 0, stream>>>(s, r, n, h, err);
+    else if (min_blocks >= 10) k_trace_closest<10, true><<<blocks, kTraceBlock, 0, stream>>>(s, r, n, h, err);
+    else k_trace_closest<8, true><<<blocks, kTraceBlock, 0, stream>>>(s, r, n, h, err);
     return cudaGetLastError();
 }
 
