@@ -577,6 +577,9 @@ def run_cache(args, rank, world, local_rank):
         k, v = kv.split("=")
         cache_kw[k] = int(v)
     ctx = Context(local_rank)
+    for kv in args.param:
+        k, v = kv.split("=")
+        ctx.set_param(k, int(v))
     r = measure_cache(ctx, local_rank, rank, args.steps, args.warmup, args.ref_spp, cache_kw,
                       cpu_crop=args.cpu_ref_crop, cpu_spp=args.cpu_ref_spp)
     ctx.close()
