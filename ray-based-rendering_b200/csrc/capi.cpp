@@ -173,7 +173,7 @@ rbr_status rbr_param_set(rbr_ctx* ctx, const char* name, int64_t value) {
         if (value < 0 || value > 32) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "trace.blocks_per_sm is 0..32");
         ctx->trace_blocks_per_sm = static_cast<int>(value);
     } else if (n == "trace.order") {
-        if (value < 0 || value > 3) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "trace.order is 0..3");
+        if (value < 0 || value > 5) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "trace.order is 0..5");
         ctx->trace_order = static_cast<int>(value);
     } else if (n == "trace.min_blocks") {
         if (value != 8 && value != 10 && value != 12) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "trace.min_blocks is 8, 10 or 12");

@@ -99,6 +99,11 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_any_perm(DeviceScene s, c
 // scene box. order 1: octant, then 27-bit Morton code of 512^3 cells (30 key bits); order 2:
 // octant, then 18-bit code of 64^3 cells (21 bits, one radix pass fewer); order 3: the 64^3
 // cell first, octant last (21 bits), so consecutive warps stay in one region of the scene.
+// Orders 4 and 5 bin the direction finely and the origin coarsely (16 bits, two radix passes):
+// the direction's octahedral map onto the unit square in 16 x 8 cells (7 bits) and a Morton
+// code of 8^3 origin cells (9 bits); order 4 direction first, order 5 origin first. Rays of one
+// direction cell from nearby origins diverge less than rays of one octant, whose directions
+// span 90 degrees.
 __device__ __forceinline__ uint32_t spread3(uint32_t x) {  // 9 bits -> every third of 27
     x &= 0x1FFu;
     x = (x | (x << 16)) & 0x030000FFu;
@@ -120,7 +125,25 @@ __global__ void k_ray_keys(const float4* __restrict__ rays, uint32_t n, float3 l
         };
         const uint32_t m = spread3(cell(a.x, lo.x, scale.x)) << 2 | spread3(cell(a.y, lo.y, scale.y)) << 1 |
                            spread3(cell(a.z, lo.z, scale.z));
-        keys[i] = order == 1 ? (oct << 27) | m : order == 2 ? (oct << 18) | (m >> 9) : ((m >> 9) << 3) | oct;
+        uint32_t key;
+        if (order >= 4) {
+            // octahedral map: (x, y) / (|x| + |y| + |z|), the lower hemisphere folded outwards
+            const float l1 = fabsf(b.x) + fabsf(b.y) + fabsf(b.z);
+            float u = l1 > 0.0f ? b.x / l1 : 0.0f, v = l1 > 0.0f ? b.y / l1 : 0.0f;
+            if (b.z < 0.0f) {
+                const float uu = (1.0f - fabsf(v)) * (u < 0.0f ? -1.0f : 1.0f);
+                v = (1.0f - fabsf(u)) * (v < 0.0f ? -1.0f : 1.0f);
+                u = uu;
+            }
+            const uint32_t du = static_cast<uint32_t>(fminf(fmaxf((u + 1.0f) * 8.0f, 0.0f), 15.0f));  // NaN -> 0
+            const uint32_t dv = static_cast<uint32_t>(fminf(fmaxf((v + 1.0f) * 4.0f, 0.0f), 7.0f));
+            const uint32_t dir = (du << 3) | dv;
+            const uint32_t cell = m >> 18;  // 8^3 cells: the top 9 bits of the 27-bit code
+            key = order == 4 ? (dir << 9) | cell : (cell << 7) | dir;
+        } else {
+            key = order == 1 ? (oct << 27) | m : order == 2 ? (oct << 18) | (m >> 9) : ((m >> 9) << 3) | oct;
+        }
+        keys[i] = key;
         idx[i] = i;
     }
 }
@@ -432,7 +455,7 @@ cudaError_t launch_trace_persist(const DeviceScene& s, const rbr_ray* rays, uint
 static cudaError_t sort_rays(rbr_ctx* ctx, DevBuf& sort_buf, const rbr_ray* rays, uint32_t n, const uint32_t** perm,
                              cudaStream_t stream) {
     const int order = ctx->trace_order;
-    const int key_bits = order == 1 ? 30 : 21;
+    const int key_bits = order == 1 ? 30 : order >= 4 ? 16 : 21;
     size_t temp = 0;
     cudaError_t e = cub::DeviceRadixSort::SortPairs(nullptr, temp, static_cast<const uint32_t*>(nullptr),
                                                     static_cast<uint32_t*>(nullptr), static_cast<const uint32_t*>(nullptr),
@@ -518,7 +541,8 @@ rbr_status autotune_trace(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any
         int kernel, min_blocks, per_sm, order;
     };
     const Cand cands[] = {{0, 8, 0, 0}, {0, 10, 0, 0}, {0, 12, 0, 0}, {1, 10, 0, 0}, {2, 10, 0, 0},
-                          {0, 8, 0, 1}, {0, 10, 0, 1}, {0, 12, 0, 1}, {0, 10, 0, 2}, {0, 10, 0, 3}};
+                          {0, 8, 0, 1}, {0, 10, 0, 1}, {0, 12, 0, 1}, {0, 10, 0, 2}, {0, 10, 0, 3},
+                          {0, 8, 0, 4}, {0, 10, 0, 4}, {0, 10, 0, 5}};
     rbr_status st = ensure(ctx, ctx->stage_out, size_t(n) * (any_hit ? 1 : sizeof(rbr_hit)), "autotune output");
     if (st != RBR_OK) return st;
     const Cand saved{ctx->trace_kernel, ctx->trace_min_blocks, ctx->trace_blocks_per_sm, ctx->trace_order};

@@ -29,13 +29,14 @@ def assert_same_closest(got, want):
 
 WORLDS = [(30, 30, False, 1), (400, 1500, False, 2), (60, 200, True, 3)]
 # (trace.kernel, trace.order): one thread per ray, persistent lane refill, warp-cooperative,
-# and one thread per ray on rays sorted by the three key layouts (direction octant and origin
-# cell of 512^3 or 64^3, or cell first)
-KERNELS = [(0, 0), (1, 0), (2, 0), (0, 1), (0, 2), (0, 3)]
+# and one thread per ray on rays sorted by the five key layouts (direction octant and origin
+# cell of 512^3 or 64^3, or cell first; octahedral direction cell and origin cell of 8^3, in
+# either order)
+KERNELS = [(0, 0), (1, 0), (2, 0), (0, 1), (0, 2), (0, 3), (0, 4), (0, 5)]
 
 
 @pytest.fixture(params=KERNELS, ids=["kernel0", "kernel1", "kernel2", "kernel0-sorted", "kernel0-sorted64",
-                                     "kernel0-cellfirst"])
+                                     "kernel0-cellfirst", "kernel0-dirfirst", "kernel0-originfirst"])
 def kctx(ctx, request):
     """The shared context with each traversal variant in turn."""
     ctx.set_param("trace.kernel", request.param[0])
