@@ -462,9 +462,10 @@ typedef struct rbr_batch_config {
     uint32_t waves_in_flight;   /* 1, or 2 (default; 0 means 2): waves alternate between two
                                    path-buffer sets and streams, each set within the budget */
     uint32_t persistent;        /* 1: one cooperative launch renders every wave of a run (all
-                                   its stages, grid barriers between them) when no request uses
-                                   the radiance cache and the run has at most 16 scenes; 0 (default):
-                                   one captured graph per wave shape */
+                                   its stages, grid barriers between them; with two waves in
+                                   flight the grid's halves take alternate waves) when no request
+                                   uses the radiance cache and the run has at most 16 scenes; 0
+                                   (default): one captured graph per wave shape */
     uint32_t barrier_timeout_us; /* persistent run: longest wait of a block at a grid barrier, in
                                    microseconds, before the run gives up with RBR_ERR_DEVICE_TIMEOUT
                                    (default 2,000,000; 0 means the default) */

@@ -260,7 +260,7 @@ rbr_status run(rbr_batch* b, std::vector<Req>& reqs, cudaStream_t stream) {
     std::vector<WavePlan> waves = plan(b, reqs, cap);
     const bool persistent = b->cfg.persistent && !any_cache && !waves.empty() && b->scenes.size() <= 16;
     const uint32_t nl = max_lights(b);
-    rbr_status st = ensure_wave_buffers(eng, cap, cap * nl, persistent ? 1 : slots);
+    rbr_status st = ensure_wave_buffers(eng, cap, cap * nl, slots);
     if (st != RBR_OK) return bfail(b, st, eng->error);
     for (const WavePlan& w : waves) {
         if (w.mode != 1) continue;
@@ -335,7 +335,7 @@ rbr_status run(rbr_batch* b, std::vector<Req>& reqs, cudaStream_t stream) {
             b->d_loop_bytes = need;
         }
         if (!b->d_bar) {
-            const cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&b->d_bar), 2 * sizeof(uint32_t));
+            const cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&b->d_bar), kLoopBarrierWords * sizeof(uint32_t));
             if (e != cudaSuccess) return bcuda(b, e, "grid barrier");
         }
         const uint64_t limit_ns = uint64_t(b->cfg.barrier_timeout_us ? b->cfg.barrier_timeout_us : 2000000u) * 1000ull;
@@ -344,8 +344,8 @@ rbr_status run(rbr_batch* b, std::vector<Req>& reqs, cudaStream_t stream) {
         if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_loop, host, need, cudaMemcpyHostToDevice, stream);
         if (e == cudaSuccess)
             e = launch_wave_loop(eng, b->scenes, static_cast<const LoopWave*>(b->d_loop), static_cast<uint32_t>(waves.size()),
-                                 static_cast<const char*>(b->d_loop) + list_bytes, b->d_stamps, b->d_bar, limit_ns, stream,
-                                 &loop_grid);
+                                 static_cast<const char*>(b->d_loop) + list_bytes, b->d_stamps, b->d_bar, limit_ns, slots,
+                                 stream, &loop_grid);
         if (e == cudaSuccess) e = cudaEventRecord(b->events[waves.size() + 1], stream);
         if (e != cudaSuccess) return bcuda(b, e, "persistent wave loop");
         s.waves = static_cast<uint32_t>(waves.size());
@@ -354,7 +354,7 @@ rbr_status run(rbr_batch* b, std::vector<Req>& reqs, cudaStream_t stream) {
         s.blocks_per_sm = static_cast<uint32_t>(loop_grid / std::max(1, eng->num_sms));
         b->stats = s;
         b->run_waves = s.waves;
-        b->run_slots = 1;
+        b->run_slots = slots;
         b->run_persistent = true;
         b->ran = true;
         return RBR_OK;

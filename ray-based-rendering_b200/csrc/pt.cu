@@ -49,6 +49,13 @@ enum : int {
     kCWords = 26
 };
 
+// The blocks a stage runs on: the whole grid for the wavefront kernels, one half of it for a
+// half of the persistent wave loop. Grid-stride loops start at block `block` of `blocks`.
+struct Span {
+    uint32_t block, blocks;
+};
+__device__ __forceinline__ Span grid_span() { return Span{blockIdx.x, gridDim.x}; }
+
 // Adds this warp's node / record counts to two 64-bit counters (every lane of the warp calls it).
 __device__ __forceinline__ void warp_add_counts(uint32_t* counters, int word, uint2 c) {
     unsigned long long nodes = c.x, recs = c.y;
@@ -164,10 +171,10 @@ __device__ __forceinline__ bool degenerate(float4 o, float4 d) {
 
 // ------------------------------------------------------------------------------------------
 template <bool kPacked>
-__device__ __forceinline__ void raygen_body(const CameraDev& cam, const Wave& w, const Paths& P) {
+__device__ __forceinline__ void raygen_body(const CameraDev& cam, const Wave& w, const Paths& P, Span g) {
     const uint32_t n = kPacked ? P.wave_hdr[0] : w.npaths;
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
+    const uint32_t stride = g.blocks * blockDim.x;
+    for (uint32_t k = g.block * blockDim.x + threadIdx.x; k < n; k += stride) {
         uint32_t width = w.width, seg = 0;
         if (kPacked) {  // the segment holding path k (segments are sorted by first path)
             uint32_t hi = P.wave_hdr[1] - 1;
@@ -193,7 +200,7 @@ __device__ __forceinline__ void raygen_body(const CameraDev& cam, const Wave& w,
         P.rad[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         P.q0[k] = k;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (g.block == 0 && threadIdx.x == 0) {
         P.counters[kCQ0] = n;
         if (w.cache_on) {
             P.counters[kCQuery] = 0;
@@ -204,7 +211,7 @@ __device__ __forceinline__ void raygen_body(const CameraDev& cam, const Wave& w,
 
 template <bool kPacked>
 __global__ void __launch_bounds__(kBlock) k_raygen(CameraDev cam, Wave w, Paths P) {
-    raygen_body<kPacked>(cam, w, P);
+    raygen_body<kPacked>(cam, w, P, grid_span());
 }
 
 // Resets the counters depth `d` appends to.
@@ -230,15 +237,15 @@ __global__ void k_begin(Paths P, uint32_t d) {
 // the natural 56-register allocation (foggy Cornell box); the surface variant is unchanged.
 // kCount (RBR_RENDER_COUNT_TRAFFIC): also counts the nodes and records the traversals fetch.
 template <bool kVol, bool kPacked, bool kCount>
-__device__ __forceinline__ void extend_body(const DeviceScene& s, const Wave& w, const Paths& P, uint32_t d, int* err) {
+__device__ __forceinline__ void extend_body(const DeviceScene& s, const Wave& w, const Paths& P, uint32_t d, int* err, Span g) {
     const uint32_t n = P.counters[kCQ0 + (d & 1)];
     const uint32_t* q = (d & 1) ? P.q1 : P.q0;
     uint32_t* nextq = (d & 1) ? P.q0 : P.q1;
     uint32_t* nextc = P.counters + kCQ0 + ((d + 1) & 1);
-    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(reinterpret_cast<unsigned long long*>(P.counters + kCExt), n);
-    const uint32_t stride = gridDim.x * blockDim.x;
+    if (g.block == 0 && threadIdx.x == 0) atomicAdd(reinterpret_cast<unsigned long long*>(P.counters + kCExt), n);
+    const uint32_t stride = g.blocks * blockDim.x;
     uint2 traffic = make_uint2(0u, 0u);
-    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {
+    for (uint32_t base = g.block * blockDim.x; base < n; base += stride) {
         const uint32_t j = base + threadIdx.x;
         const bool valid = j < n;
         uint32_t k = 0, cls = kNumClasses;
@@ -331,7 +338,7 @@ __device__ __forceinline__ void extend_body(const DeviceScene& s, const Wave& w,
 
 template <bool kVol, bool kPacked, bool kCount = false>
 __global__ void __launch_bounds__(kBlock, 8) k_extend(DeviceScene s, Wave w, Paths P, uint32_t d, int* err) {
-    extend_body<kVol, kPacked, kCount>(s, w, P, d, err);
+    extend_body<kVol, kPacked, kCount>(s, w, P, d, err, grid_span());
 }
 
 // Surface data of a hit, as the primitive's intersect() fills SurfaceInteraction.
@@ -429,7 +436,7 @@ __host__ __device__ constexpr uint32_t class_kinds() {
 }
 
 template <int kMode, bool kPacked, int kCls>
-__device__ __forceinline__ void shade_body(const DeviceScene& s, const Wave& w, const Paths& P, uint32_t d) {
+__device__ __forceinline__ void shade_body(const DeviceScene& s, const Wave& w, const Paths& P, uint32_t d, Span g) {
     constexpr bool kCache = kMode == 1, kVolSurface = kMode == 2;
     constexpr uint32_t kKinds = class_kinds<kCls>();
     constexpr bool kNoNee = kCls == kShadeSpecular || kCls == kShadeNone;
@@ -440,9 +447,9 @@ __device__ __forceinline__ void shade_body(const DeviceScene& s, const Wave& w, 
     const uint32_t n = kCls < 0 ? cnt[kNumClasses] : P.counters[kCClass + (kCls < 0 ? 0 : kCls)];
     uint32_t* nextq = (d & 1) ? P.q0 : P.q1;
     uint32_t* nextc = P.counters + kCQ0 + ((d + 1) & 1);
-    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(reinterpret_cast<unsigned long long*>(P.counters + kCShade), n);
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {
+    if (g.block == 0 && threadIdx.x == 0) atomicAdd(reinterpret_cast<unsigned long long*>(P.counters + kCShade), n);
+    const uint32_t stride = g.blocks * blockDim.x;
+    for (uint32_t base = g.block * blockDim.x; base < n; base += stride) {
         const uint32_t j = base + threadIdx.x;
         const bool valid = j < n;
         uint32_t k = 0;
@@ -606,20 +613,20 @@ __host__ __device__ constexpr int shade_blocks() {
 
 template <int kMode, bool kPacked, int kCls = -1>
 __global__ void __launch_bounds__(kBlock, shade_blocks<kCls>()) k_shade(DeviceScene s, Wave w, Paths P, uint32_t d) {
-    shade_body<kMode, kPacked, kCls>(s, w, P, d);
+    shade_body<kMode, kPacked, kCls>(s, w, P, d, grid_span());
 }
 
 template <bool kCount>
-__device__ __forceinline__ void shadow_body(const DeviceScene& s, const Paths& P, int* err) {
+__device__ __forceinline__ void shadow_body(const DeviceScene& s, const Paths& P, int* err, Span g) {
     uint32_t n = P.counters[kCShadow];
     if (n > P.shadow_cap) {
-        if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(err, kErrQueueOverflow);
+        if (g.block == 0 && threadIdx.x == 0) atomicOr(err, kErrQueueOverflow);
         n = P.shadow_cap;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(reinterpret_cast<unsigned long long*>(P.counters + kCSh), n);
-    const uint32_t stride = gridDim.x * blockDim.x;
+    if (g.block == 0 && threadIdx.x == 0) atomicAdd(reinterpret_cast<unsigned long long*>(P.counters + kCSh), n);
+    const uint32_t stride = g.blocks * blockDim.x;
     uint2 traffic = make_uint2(0u, 0u);
-    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
+    for (uint32_t j = g.block * blockDim.x + threadIdx.x; j < n; j += stride) {
         const float4* e = P.shadow + 3 * static_cast<size_t>(j);
         const float4 a = e[0], b = e[1];
         float t;
@@ -636,7 +643,7 @@ __device__ __forceinline__ void shadow_body(const DeviceScene& s, const Paths& P
 
 template <bool kCount = false>
 __global__ void __launch_bounds__(kBlock) k_shadow(DeviceScene s, Paths P, int* err) {
-    shadow_body<kCount>(s, P, err);
+    shadow_body<kCount>(s, P, err, grid_span());
 }
 
 __global__ void __launch_bounds__(kBlock) k_film(Wave w, Paths P, float* film_mean, float* film_m2) {
@@ -676,10 +683,10 @@ __global__ void __launch_bounds__(kBlock) k_film(Wave w, Paths P, float* film_me
 
 // Film of a packed wave: the first path of each pixel sums the pixel's samples into its
 // request's film.
-__device__ __forceinline__ void film_packed_body(const Paths& P) {
+__device__ __forceinline__ void film_packed_body(const Paths& P, Span g) {
     const uint32_t n = P.wave_hdr[0];
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
+    const uint32_t stride = g.blocks * blockDim.x;
+    for (uint32_t k = g.block * blockDim.x + threadIdx.x; k < n; k += stride) {
         const SegDev& g = P.segs[P.seg_of[k]];
         const uint32_t local = k - g.path0;
         if (local % g.spp != 0) continue;
@@ -694,7 +701,7 @@ __device__ __forceinline__ void film_packed_body(const Paths& P) {
 }
 
 __global__ void __launch_bounds__(kBlock) k_film_packed(Paths P) {
-    film_packed_body(P);
+    film_packed_body(P, grid_span());
 }
 
 // ------------------------------------------------------------------------------------------
@@ -714,18 +721,18 @@ __device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
     return v;
 }
 
-// Grid-wide barrier of a cooperative launch (every block is resident). bar[0] counts arrivals,
-// bar[1] is the generation the last arrival advances. A wait longer than limit_ns of device
-// time records kErrDeviceTimeout; after that, or when another block recorded it, the barrier
-// reports failure and the caller leaves the kernel, so the blocks still waiting give up in
-// turn and nothing waits without bound.
-__device__ bool grid_barrier(uint32_t* bar, uint32_t& gen, uint64_t limit_ns, int* err) {
+// Barrier of `nblocks` blocks of a cooperative launch (every block is resident). bar[0] counts
+// arrivals, bar[1] is the generation the last arrival advances. A wait longer than limit_ns of
+// device time records kErrDeviceTimeout; after that, or when another block recorded it, the
+// barrier reports failure and the caller leaves the kernel, so the blocks still waiting give
+// up in turn and nothing waits without bound.
+__device__ bool grid_barrier(uint32_t* bar, uint32_t& gen, uint32_t nblocks, uint64_t limit_ns, int* err) {
     __shared__ int ok_s;
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
         __threadfence();
-        if (atomicAdd(bar, 1u) + 1u == gridDim.x) {
+        if (atomicAdd(bar, 1u) + 1u == nblocks) {
             atomicExch(bar, 0u);
             __threadfence();
             atomicExch(bar + 1, gen + 1u);
@@ -750,70 +757,82 @@ __device__ bool grid_barrier(uint32_t* bar, uint32_t& gen, uint64_t limit_ns, in
 
 // The stages as separate (not inlined) functions: each keeps the register allocation of its own
 // kernel instead of the loop kernel holding all of them at once.
-__device__ __noinline__ void loop_raygen(const Paths& P) {
+__device__ __noinline__ void loop_raygen(const Paths& P, Span g) {
     const Wave w{};
     const CameraDev unused{};
-    raygen_body<true>(unused, w, P);
+    raygen_body<true>(unused, w, P, g);
 }
 template <bool kVol>
-__device__ __noinline__ void loop_extend(const DeviceScene& s, const Paths& P, uint32_t d, int* err) {
+__device__ __noinline__ void loop_extend(const DeviceScene& s, const Paths& P, uint32_t d, int* err, Span g) {
     const Wave w{};
-    extend_body<kVol, true, false>(s, w, P, d, err);
+    extend_body<kVol, true, false>(s, w, P, d, err, g);
 }
 template <int kMode>
-__device__ __noinline__ void loop_shade(const DeviceScene& s, const Paths& P, uint32_t d) {
+__device__ __noinline__ void loop_shade(const DeviceScene& s, const Paths& P, uint32_t d, Span g) {
     const Wave w{};
-    shade_body<kMode, true, -1>(s, w, P, d);
+    shade_body<kMode, true, -1>(s, w, P, d, g);
 }
-__device__ __noinline__ void loop_shadow(const DeviceScene& s, const Paths& P, int* err) { shadow_body<false>(s, P, err); }
-__device__ __noinline__ void loop_film(const Paths& P) { film_packed_body(P); }
+__device__ __noinline__ void loop_shadow(const DeviceScene& s, const Paths& P, int* err, Span g) {
+    shadow_body<false>(s, P, err, g);
+}
+__device__ __noinline__ void loop_film(const Paths& P, Span g) { film_packed_body(P, g); }
 
 struct LoopParams {
     DeviceScene scenes[kLoopScenes];
     const LoopWave* waves;
     uint32_t nwaves;
+    uint32_t halves;             // 1, or 2: the grid's halves render alternate waves
     const char* tables;          // segment tables, at LoopWave::table
-    Paths P;                     // path buffers (segments and header set per wave)
+    Paths P[2];                  // path buffers of each half (segments and header set per wave)
     unsigned long long* stamps;  // [0] start of the run, [1 + w] end of wave w (device ns)
-    uint32_t* bar;               // [0] arrivals, [1] generation (zero at launch)
+    uint32_t* bar;               // per half [2h] arrivals, [2h + 1] generation; [4], [5] whole grid
     int* err;
     uint64_t limit_ns;           // longest wait at a barrier
 };
 
+// With two halves, blocks [0, G/2) render the even waves on the first path-buffer set and
+// blocks [G/2, G) the odd waves on the second, each half with its own barrier, so that one
+// half's latency-bound last bounces run beside the other half's full stages (what two waves in
+// flight on two streams give the graph-replayed path).
 __global__ void __launch_bounds__(kBlock, 8) k_wave_loop(const __grid_constant__ LoopParams p) {
-    uint32_t gen = 0;
+    uint32_t gen0 = 0;
     if (blockIdx.x == 0 && threadIdx.x == 0) p.stamps[0] = global_ns();
-    if (!grid_barrier(p.bar, gen, p.limit_ns, p.err)) return;
+    if (!grid_barrier(p.bar + 4, gen0, gridDim.x, p.limit_ns, p.err)) return;
     const uint64_t t0 = *reinterpret_cast<volatile unsigned long long*>(p.stamps);
-    for (uint32_t wi = 0; wi < p.nwaves; ++wi) {
+    const uint32_t per = gridDim.x / p.halves;
+    const uint32_t h = min(blockIdx.x / per, p.halves - 1);
+    const Span g{blockIdx.x - h * per, per};
+    uint32_t* bar = p.bar + 2 * h;
+    uint32_t gen = 0;
+    for (uint32_t wi = h; wi < p.nwaves; wi += p.halves) {
         const LoopWave lw = p.waves[wi];
         // admission: the wave's last request arrives release_ns after the run's start (the host
         // bounds release_ns, so this wait ends)
         while (global_ns() - t0 < lw.release_ns) __nanosleep(2048);
-        Paths P = p.P;
+        Paths P = p.P[h];
         P.wave_hdr = reinterpret_cast<const uint32_t*>(p.tables + lw.table);
         P.segs = reinterpret_cast<const SegDev*>(p.tables + lw.table + kSegTableHeader);
         const DeviceScene& s = p.scenes[lw.scene];
-        if (blockIdx.x == 0)
+        if (g.block == 0)
             for (uint32_t i = threadIdx.x; i < kCWords; i += blockDim.x) P.counters[i] = 0;
-        if (!grid_barrier(p.bar, gen, p.limit_ns, p.err)) return;
-        loop_raygen(P);
-        if (!grid_barrier(p.bar, gen, p.limit_ns, p.err)) return;
+        if (!grid_barrier(bar, gen, per, p.limit_ns, p.err)) return;
+        loop_raygen(P, g);
+        if (!grid_barrier(bar, gen, per, p.limit_ns, p.err)) return;
         for (uint32_t d = 0; d < lw.max_depth; ++d) {
-            if (blockIdx.x == 0 && threadIdx.x == 0) begin_body(P, d);
-            if (!grid_barrier(p.bar, gen, p.limit_ns, p.err)) return;
-            if (lw.mode == 2) loop_extend<true>(s, P, d, p.err);
-            else loop_extend<false>(s, P, d, p.err);
-            if (!grid_barrier(p.bar, gen, p.limit_ns, p.err)) return;
-            if (lw.mode == 2) loop_shade<2>(s, P, d);
-            else loop_shade<0>(s, P, d);
-            if (!grid_barrier(p.bar, gen, p.limit_ns, p.err)) return;
-            loop_shadow(s, P, p.err);
-            if (!grid_barrier(p.bar, gen, p.limit_ns, p.err)) return;
+            if (g.block == 0 && threadIdx.x == 0) begin_body(P, d);
+            if (!grid_barrier(bar, gen, per, p.limit_ns, p.err)) return;
+            if (lw.mode == 2) loop_extend<true>(s, P, d, p.err, g);
+            else loop_extend<false>(s, P, d, p.err, g);
+            if (!grid_barrier(bar, gen, per, p.limit_ns, p.err)) return;
+            if (lw.mode == 2) loop_shade<2>(s, P, d, g);
+            else loop_shade<0>(s, P, d, g);
+            if (!grid_barrier(bar, gen, per, p.limit_ns, p.err)) return;
+            loop_shadow(s, P, p.err, g);
+            if (!grid_barrier(bar, gen, per, p.limit_ns, p.err)) return;
         }
-        loop_film(P);
-        if (!grid_barrier(p.bar, gen, p.limit_ns, p.err)) return;
-        if (blockIdx.x == 0 && threadIdx.x == 0) p.stamps[1 + wi] = global_ns();
+        loop_film(P, g);
+        if (!grid_barrier(bar, gen, per, p.limit_ns, p.err)) return;
+        if (g.block == 0 && threadIdx.x == 0) p.stamps[1 + wi] = global_ns();
     }
 }
 
@@ -1297,27 +1316,30 @@ cudaError_t launch_packed_wave(rbr_ctx* eng, rbr_ctx* scn, const PackedWave& pw,
 
 cudaError_t launch_wave_loop(rbr_ctx* eng, const std::vector<rbr_ctx*>& scenes, const LoopWave* waves, uint32_t nwaves,
                              const char* tables, unsigned long long* stamps, uint32_t* bar, uint64_t limit_ns,
-                             cudaStream_t stream, int* grid_out) {
-    if (scenes.size() > static_cast<size_t>(kLoopScenes)) return cudaErrorInvalidValue;
+                             int halves, cudaStream_t stream, int* grid_out) {
+    if (scenes.size() > static_cast<size_t>(kLoopScenes) || (halves != 1 && halves != 2)) return cudaErrorInvalidValue;
     LoopParams lp{};
     for (size_t i = 0; i < scenes.size(); ++i) lp.scenes[i] = scenes[i]->scene;
     lp.waves = waves;
     lp.nwaves = nwaves;
+    lp.halves = static_cast<uint32_t>(halves);
     lp.tables = tables;
-    PathBuffers& pb = eng->pt;
-    Paths& P = lp.P;
-    P.ray = static_cast<float4*>(pb.ray.ptr);
-    P.thr = static_cast<float4*>(pb.thr.ptr);
-    P.rad = static_cast<float4*>(pb.rad.ptr);
-    P.hit = static_cast<uint2*>(pb.hit.ptr);
-    P.q0 = static_cast<uint32_t*>(pb.queue[0].ptr);
-    P.q1 = static_cast<uint32_t*>(pb.queue[1].ptr);
-    P.classq = static_cast<uint32_t*>(pb.classq.ptr);
-    P.shadow = static_cast<float4*>(pb.shadow.ptr);
-    P.counters = static_cast<uint32_t*>(pb.counters.ptr);
-    P.cap = pb.capacity;
-    P.shadow_cap = pb.shadow_capacity;
-    P.seg_of = static_cast<uint32_t*>(eng->pt_seg_of.ptr);
+    for (int h = 0; h < halves; ++h) {
+        PathBuffers& pb = h ? eng->pt2 : eng->pt;
+        Paths& P = lp.P[h];
+        P.ray = static_cast<float4*>(pb.ray.ptr);
+        P.thr = static_cast<float4*>(pb.thr.ptr);
+        P.rad = static_cast<float4*>(pb.rad.ptr);
+        P.hit = static_cast<uint2*>(pb.hit.ptr);
+        P.q0 = static_cast<uint32_t*>(pb.queue[0].ptr);
+        P.q1 = static_cast<uint32_t*>(pb.queue[1].ptr);
+        P.classq = static_cast<uint32_t*>(pb.classq.ptr);
+        P.shadow = static_cast<float4*>(pb.shadow.ptr);
+        P.counters = static_cast<uint32_t*>(pb.counters.ptr);
+        P.cap = pb.capacity;
+        P.shadow_cap = pb.shadow_capacity;
+        P.seg_of = static_cast<uint32_t*>((h ? eng->pt_seg_of2 : eng->pt_seg_of).ptr);
+    }
     lp.stamps = stamps;
     lp.bar = bar;
     lp.err = eng->d_error;
@@ -1326,9 +1348,10 @@ cudaError_t launch_wave_loop(rbr_ctx* eng, const std::vector<rbr_ctx*>& scenes, 
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_wave_loop, kBlock, 0);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorCooperativeLaunchTooLarge;
-    const int grid = eng->num_sms * per_sm;  // every block resident: the barriers depend on it
+    int grid = eng->num_sms * per_sm;  // every block resident: the barriers depend on it
+    grid -= grid % halves;
     if (grid_out) *grid_out = grid;
-    e = cudaMemsetAsync(bar, 0, 2 * sizeof(uint32_t), stream);
+    e = cudaMemsetAsync(bar, 0, kLoopBarrierWords * sizeof(uint32_t), stream);
     if (e != cudaSuccess) return e;
     void* args[] = {&lp};
     return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(k_wave_loop), dim3(grid), dim3(kBlock), args, 0,

@@ -194,11 +194,13 @@ struct PackedWave {
 // Path buffers for packed waves: `slots` (1 or 2) sets of `cap` paths with their segment index.
 rbr_status ensure_wave_buffers(rbr_ctx* ctx, uint32_t cap, uint32_t shadow_cap, int slots = 1);
 cudaError_t launch_packed_wave(rbr_ctx* eng, rbr_ctx* scn, const PackedWave& pw, cudaStream_t stream);
-// One cooperative launch that renders `nwaves` waves (modes 0 and 2) of up to 16 scenes with
-// the context's first path-buffer set; device-clock stamps: [0] start, [1 + w] end of wave w.
+// One cooperative launch that renders `nwaves` waves (modes 0 and 2) of up to 16 scenes; with
+// halves 2 the grid's halves render alternate waves on the context's two path-buffer sets.
+// Device-clock stamps: [0] start, [1 + w] end of wave w. bar: kLoopBarrierWords words.
+constexpr int kLoopBarrierWords = 6;
 cudaError_t launch_wave_loop(rbr_ctx* eng, const std::vector<rbr_ctx*>& scenes, const LoopWave* waves, uint32_t nwaves,
                              const char* tables, unsigned long long* stamps, uint32_t* bar, uint64_t limit_ns,
-                             cudaStream_t stream, int* grid_out);
+                             int halves, cudaStream_t stream, int* grid_out);
 cudaError_t launch_stamp(unsigned long long* at, cudaStream_t stream);
 cudaError_t launch_release(const unsigned long long* start, uint64_t release_ns, cudaStream_t stream);
 uint32_t packed_wave_launches(const PackedWave& pw);
