@@ -244,7 +244,7 @@ rbr_status rbr_scene_stats_get(const rbr_ctx* ctx, rbr_scene_stats* out);
  *                          8 lanes per ray, one child box per lane
  *   "trace.blocks_per_sm"  resident blocks per SM of kernels 1 and 2 (0: occupancy limit)
  *   "trace.min_blocks"     kernel 0's register budget: 8, 10 or 12 resident blocks per SM
- *   "trace.order"          kernel 0: 0 traces the rays in the order given; 1..5 first sort
+ *   "trace.order"          kernels 0 and 1: 0 traces the rays in the order given; 1..5 first sort
  *                          them on the device so that warps hold rays that walk the same nodes:
  *                          1 by direction octant, then origin cell of 512^3; 2 octant, then cell
  *                          of 64^3; 3 cell of 64^3, then octant; 4 direction cell (octahedral

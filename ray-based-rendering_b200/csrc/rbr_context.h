@@ -135,7 +135,7 @@ cudaError_t launch_trace_any(const DeviceScene& s, const rbr_ray* rays, uint32_t
 cudaError_t launch_trace_counts(const DeviceScene& s, const rbr_ray* rays, uint32_t n, int any_hit,
                                 unsigned long long* totals, int* err, cudaStream_t stream);
 cudaError_t launch_trace_persist(const DeviceScene& s, const rbr_ray* rays, uint32_t n, int any_hit, void* out,
-                                 int* err, uint32_t* cursor, int grid, cudaStream_t stream);
+                                 int* err, uint32_t* cursor, int grid, cudaStream_t stream, const uint32_t* perm = nullptr);
 int trace_persist_blocks_per_sm(int any_hit);
 cudaError_t launch_trace_coop(const DeviceScene& s, const rbr_ray* rays, uint32_t n, int any_hit, void* out, int* err,
                               uint32_t* cursor, int grid, cudaStream_t stream);

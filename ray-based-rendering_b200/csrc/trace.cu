@@ -191,14 +191,15 @@ __device__ __forceinline__ uint32_t lane_mask_lt() {
 // (one atomic per chunk) and hands the next ray of its chunk to any lane whose ray is done,
 // so lanes keep working while the warp's other rays are still traversing. Every loop
 // iteration each active lane advances its ray by one step (a leaf-record test or a node test).
+// With `perm` (sorted rays), position j of the cursor's order is ray perm[j].
 constexpr int kPersistBlock = 128;
 constexpr uint32_t kChunk = 256;
 
 template <bool kAny>
 __global__ void __launch_bounds__(kPersistBlock) k_trace_persist(DeviceScene s, const float4* __restrict__ rays,
-                                                                 uint32_t n, uint2* __restrict__ hits,
-                                                                 uint8_t* __restrict__ occ, int* err,
-                                                                 uint32_t* cursor) {
+                                                                 uint32_t n, const uint32_t* __restrict__ perm,
+                                                                 uint2* __restrict__ hits, uint8_t* __restrict__ occ,
+                                                                 int* err, uint32_t* cursor) {
     const uint32_t lane = threadIdx.x & 31u;
     uint32_t chunk_next = 0, chunk_end = 0;  // warp-uniform
     bool exhausted = false;                  // warp-uniform
@@ -223,7 +224,7 @@ __global__ void __launch_bounds__(kPersistBlock) k_trace_persist(DeviceScene s, 
             const uint32_t avail = chunk_end - chunk_next;
             const uint32_t rank = __popc(need & lane_mask_lt());
             if (((need >> lane) & 1u) && rank < avail) {
-                idx = chunk_next + rank;
+                idx = perm ? __ldg(perm + chunk_next + rank) : chunk_next + rank;
                 const float4 a = __ldg(rays + 2 * static_cast<size_t>(idx));
                 const float4 b = __ldg(rays + 2 * static_cast<size_t>(idx) + 1);
                 if (trace_begin<kAny>(s, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, st, anyhit)) {
@@ -437,17 +438,17 @@ int trace_coop_blocks_per_sm(int any_hit) {
 }
 
 cudaError_t launch_trace_persist(const DeviceScene& s, const rbr_ray* rays, uint32_t n, int any_hit, void* out,
-                                 int* err, uint32_t* cursor, int grid, cudaStream_t stream) {
+                                 int* err, uint32_t* cursor, int grid, cudaStream_t stream, const uint32_t* perm) {
     if (n == 0) return cudaSuccess;
     cudaError_t e = cudaMemsetAsync(cursor, 0, sizeof(uint32_t), stream);
     if (e != cudaSuccess) return e;
     const auto* r = reinterpret_cast<const float4*>(rays);
     if (any_hit)
-        k_trace_persist<true><<<grid, kPersistBlock, 0, stream>>>(s, r, n, nullptr, static_cast<uint8_t*>(out), err,
-                                                                  cursor);
+        k_trace_persist<true><<<grid, kPersistBlock, 0, stream>>>(s, r, n, perm, nullptr, static_cast<uint8_t*>(out),
+                                                                  err, cursor);
     else
-        k_trace_persist<false><<<grid, kPersistBlock, 0, stream>>>(s, r, n, static_cast<uint2*>(out), nullptr, err,
-                                                                   cursor);
+        k_trace_persist<false><<<grid, kPersistBlock, 0, stream>>>(s, r, n, perm, static_cast<uint2*>(out), nullptr,
+                                                                   err, cursor);
     return cudaGetLastError();
 }
 
@@ -524,6 +525,11 @@ cudaError_t launch_trace(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any_
         return launch_query(ctx, k, blocks, stream, ctx->scene, r, n, h, ctx->d_error);
     }
     const bool coop = ctx->trace_kernel == 2;
+    const uint32_t* perm = nullptr;  // kernel 1 refills its lanes in sorted order when trace.order is set
+    if (!coop && ctx->trace_order != 0 && n > 0) {
+        cudaError_t e = sort_rays(ctx, slot ? ctx->sort_buf2 : ctx->sort_buf, rays, n, &perm, stream);
+        if (e != cudaSuccess) return e;
+    }
     const int per_sm = ctx->trace_blocks_per_sm > 0
                            ? ctx->trace_blocks_per_sm
                            : (coop ? trace_coop_blocks_per_sm(any_hit) : trace_persist_blocks_per_sm(any_hit));
@@ -532,7 +538,7 @@ cudaError_t launch_trace(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any_
     const int grid = std::max(1, std::min(ctx->num_sms * per_sm, need));
     uint32_t* cursor = ctx->d_cursors + (ctx->cursor_next++ % kCursorRing);
     if (coop) return launch_trace_coop(ctx->scene, rays, n, any_hit, out, ctx->d_error, cursor, grid, stream);
-    return launch_trace_persist(ctx->scene, rays, n, any_hit, out, ctx->d_error, cursor, grid, stream);
+    return launch_trace_persist(ctx->scene, rays, n, any_hit, out, ctx->d_error, cursor, grid, stream, perm);
 }
 
 // Times every traversal variant on the caller's rays (device pointer) and keeps the fastest.
@@ -542,7 +548,7 @@ rbr_status autotune_trace(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any
     };
     const Cand cands[] = {{0, 8, 0, 0}, {0, 10, 0, 0}, {0, 12, 0, 0}, {1, 10, 0, 0}, {2, 10, 0, 0},
                           {0, 8, 0, 1}, {0, 10, 0, 1}, {0, 12, 0, 1}, {0, 10, 0, 2}, {0, 10, 0, 3},
-                          {0, 8, 0, 4}, {0, 10, 0, 4}, {0, 10, 0, 5}};
+                          {0, 8, 0, 4}, {0, 10, 0, 4}, {0, 10, 0, 5}, {1, 10, 0, 2}, {1, 10, 0, 4}};
     rbr_status st = ensure(ctx, ctx->stage_out, size_t(n) * (any_hit ? 1 : sizeof(rbr_hit)), "autotune output");
     if (st != RBR_OK) return st;
     const Cand saved{ctx->trace_kernel, ctx->trace_min_blocks, ctx->trace_blocks_per_sm, ctx->trace_order};
