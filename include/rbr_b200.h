@@ -256,6 +256,8 @@ rbr_status rbr_scene_stats_get(const rbr_ctx* ctx, rbr_scene_stats* out);
  *   "pt.streams"           rbr_render: waves in flight, 1 or 2 (default 2: waves alternate
  *                          between two sets of path buffers on two streams; an image that
  *                          fits one wave is rendered as two half-image waves)
+ *   "trace.node_test"      sorted queries of kernel 0: 0 the packed node test (f32x2 FMAs), 1 a
+ *                          register-lean one (scalar FMAs, fewer live registers)
  *   "trace.stream_io"      kernel 0: rays read and hits written with evict-first hints (default 1)
  *   "trace.l2_persist"     kernel 0: 1 reserves the largest persisting-L2 set-aside this process's
  *                          context allows and marks the BVH (nodes and leaf records) persisting for

@@ -187,6 +187,9 @@ rbr_status rbr_param_set(rbr_ctx* ctx, const char* name, int64_t value) {
     } else if (n == "pt.wave_paths") {
         if (value < 1024 || value > (int64_t(1) << 26)) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "pt.wave_paths is 1024..2^26");
         ctx->pt_wave_paths = static_cast<uint32_t>(value);
+    } else if (n == "trace.node_test") {
+        if (value != 0 && value != 1) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "trace.node_test is 0 or 1");
+        ctx->trace_node_test = static_cast<int>(value);
     } else if (n == "trace.stream_io") {
         if (value != 0 && value != 1) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "trace.stream_io is 0 or 1");
         ctx->trace_stream_io = static_cast<int>(value);
@@ -250,6 +253,7 @@ rbr_status rbr_param_get(const rbr_ctx* ctx, const char* name, int64_t* value) {
     else if (n == "cache.infer_groups") *value = ctx->cache_infer_groups;
     else if (n == "pt.shade_split") *value = ctx->pt_shade_split;
     else if (n == "trace.stream_io") *value = ctx->trace_stream_io;
+    else if (n == "trace.node_test") *value = ctx->trace_node_test;
     else if (n == "trace.l2_persist") *value = ctx->trace_l2_persist;
     else if (n == "debug.fail_alloc") *value = ctx->fail_alloc_countdown;
     else return RBR_ERR_INVALID_ARGUMENT;

@@ -61,6 +61,7 @@ struct rbr_ctx {
     int trace_blocks_per_sm = 0;   // persistent grid per SM (0: occupancy limit)
     int trace_min_blocks = 10;     // kernel 0: register budget for 8, 10 or 12 resident blocks per SM
     int trace_order = 0;           // kernel 0: 0 rays in the given order, 1 sorted by direction octant and origin
+    int trace_node_test = 0;       // sorted ray queries: 0 packed node test, 1 register-lean one
     int trace_stream_io = 1;       // kernel 0: rays read and hits written with evict-first (streaming) hints
     int trace_l2_persist = 0;      // kernel 0: the BVH's address range marked persisting in L2
     size_t l2_persist_bytes = 0;   // the context's persisting-L2 set-aside while trace_l2_persist is on

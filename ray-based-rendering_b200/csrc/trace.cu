@@ -44,7 +44,7 @@ __global__ void __launch_bounds__(kTraceBlock, kMinBlocks) k_trace_closest(Devic
 // The same query on the rays in the order `perm` (a permutation of 0..n-1): rays that start
 // close together with directions of the same octant share warps, so they walk the same nodes.
 // Answers go to the rays' own positions.
-template <int kMinBlocks, bool kStream>
+template <int kMinBlocks, bool kStream, bool kLean = false>
 __global__ void __launch_bounds__(kTraceBlock, kMinBlocks)
     k_trace_closest_perm(DeviceScene s, const float4* __restrict__ rays, uint32_t n, const uint32_t* __restrict__ perm,
                          uint2* __restrict__ hits, int* err) {
@@ -54,7 +54,7 @@ __global__ void __launch_bounds__(kTraceBlock, kMinBlocks)
     const float4 a = ray_word<kStream>(rays + 2 * static_cast<size_t>(i));
     const float4 b = ray_word<kStream>(rays + 2 * static_cast<size_t>(i) + 1);
     float t = 0.0f;
-    const uint32_t prim = traverse<false>(s, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, t, err);
+    const uint32_t prim = traverse<false, false, kLean>(s, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, t, err);
     put_hit<kStream>(hits + i, make_uint2(prim, prim == 0xFFFFFFFFu ? 0u : __float_as_uint(t)));
 }
 
@@ -502,9 +502,12 @@ cudaError_t launch_trace(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any_
             auto* h = static_cast<uint2*>(out);
             const bool st = ctx->trace_stream_io != 0;
             const int mb = ctx->trace_min_blocks;
-            auto k = mb >= 12 ? (st ? k_trace_closest_perm<12, true> : k_trace_closest_perm<12, false>)
-                   : mb >= 10 ? (st ? k_trace_closest_perm<10, true> : k_trace_closest_perm<10, false>)
-                              : (st ? k_trace_closest_perm<8, true> : k_trace_closest_perm<8, false>);
+            auto k = ctx->trace_node_test == 1
+                         ? (mb >= 12 ? k_trace_closest_perm<12, true, true>
+                            : mb >= 10 ? k_trace_closest_perm<10, true, true> : k_trace_closest_perm<8, true, true>)
+                     : mb >= 12 ? (st ? k_trace_closest_perm<12, true> : k_trace_closest_perm<12, false>)
+                     : mb >= 10 ? (st ? k_trace_closest_perm<10, true> : k_trace_closest_perm<10, false>)
+                                : (st ? k_trace_closest_perm<8, true> : k_trace_closest_perm<8, false>);
             return launch_query(ctx, k, blocks, stream, ctx->scene, r, n, perm, h, ctx->d_error);
         }
         return cudaGetLastError();
