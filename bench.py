@@ -782,6 +782,7 @@ def main():
     tuned = ctx.autotune_trace(d_rays.data_ptr(), n) if not args.param else {k: ctx.get_param(k) for k in
                                                                            ("trace.kernel", "trace.min_blocks",
                                                                             "trace.order")}
+    tuned["trace.node_test"] = ctx.get_param("trace.node_test")
 
     def step():
         ctx.trace_closest_dev(d_rays.data_ptr(), n, d_hits.data_ptr(), sp)
@@ -815,10 +816,14 @@ def main():
     avg_launch_s = statistics.mean(launch_ms) / 1e3
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / avg_launch_s / 1e9
+    # DRAM bytes per launch of this very variant from an ncu capture (profiles/traffic.json)
     traffic = None
+    traffic_key = "trace_closest_icosphere8_k{}_b{}_o{}_n{}".format(
+        tuned.get("trace.kernel", 0), ctx.get_param("trace.min_blocks"), tuned.get("trace.order", 0),
+        tuned["trace.node_test"])
     tf = REPO / "profiles" / "traffic.json"
     if tf.exists():
-        traffic = json.loads(tf.read_text()).get("trace_closest_icosphere8")
+        traffic = json.loads(tf.read_text()).get(traffic_key)
 
     # end to end through the host-buffer entry point
     e2e = None
@@ -859,7 +864,7 @@ def main():
                             "peak_source": "read bandwidth of a 32 MiB L2-resident buffer (rbr_l2_read_bandwidth), "
                                            "measured in this run"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
+                         "frac": achieved / peak, "traffic": traffic, "traffic_source": traffic_key,
                          "peak_source": f"{peak_kind} HBM copy bandwidth",
                          "algorithmic_bytes_per_launch": alg_bytes,
                          "per_ray": {"nodes": nodes / n, "leaf_records": recs / n,
