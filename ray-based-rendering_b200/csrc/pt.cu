@@ -341,12 +341,15 @@ __global__ void __launch_bounds__(kBlock, 8) k_extend(DeviceScene s, Wave w, Pat
     extend_body<kVol, kPacked, kCount>(s, w, P, d, err, grid_span());
 }
 
-// Surface data of a hit, as the primitive's intersect() fills SurfaceInteraction.
+// Surface data of a hit, as the primitive's intersect() fills SurfaceInteraction. The normal
+// that faces the incoming ray (setFaceNormal) is the outward normal or its negation, kept as a
+// flag (face_normal) so that a shading thread holds three floats fewer.
 struct Hit {
     f3 point;
-    f3 normal;   // faces the incoming ray (setFaceNormal)
     f3 outward;  // outwardNormal()
+    bool front;  // the ray arrived on the outward side
 };
+__device__ __forceinline__ f3 face_normal(const Hit& h) { return h.front ? h.outward : xneg(h.outward); }
 
 __device__ __forceinline__ Hit surface(const DeviceScene& s, uint32_t prim, float t, f3 o, f3 d) {
     Hit h;
@@ -378,16 +381,16 @@ __device__ __forceinline__ Hit surface(const DeviceScene& s, uint32_t prim, floa
             outward = xnorm(xcross(mk(a.w, b.x, b.y), mk(b.z, b.w, c.x)));  // quad normal
         }
     }
-    const bool front = xdot(d, outward) < 0.0f;
-    h.normal = front ? outward : xneg(outward);
+    h.front = xdot(d, outward) < 0.0f;
     h.outward = outward;
     return h;
 }
 
 // Interaction::spawnRay (interaction.h:22-29); the Ray constructor normalises the direction.
 __device__ __forceinline__ void spawn(const Hit& h, f3 dir, f3& o, f3& d) {
-    f3 off = xmuls(h.normal, kEpsilon);
-    if (xdot(dir, h.normal) < 0.0f) off = xneg(off);
+    const f3 n = face_normal(h);
+    f3 off = xmuls(n, kEpsilon);
+    if (xdot(dir, n) < 0.0f) off = xneg(off);
     o = xadd(h.point, off);
     d = xnorm(dir);
 }
@@ -400,8 +403,9 @@ __device__ __forceinline__ void cache_record(const Hit& h, f3 rd, const Material
     const float kd = fm(fs(1.0f, met), fs(1.0f, tr));
     const float k4 = fm(0.04f, fs(1.0f, met));
     rec[0] = make_float4(h.point.x, h.point.y, h.point.z, -rd.x);
-    rec[1] = make_float4(-rd.y, -rd.z, h.normal.x, h.normal.y);
-    rec[2] = make_float4(h.normal.z, m.roughness, fm(m.base[0], kd), fm(m.base[1], kd));
+    const f3 n = face_normal(h);
+    rec[1] = make_float4(-rd.y, -rd.z, n.x, n.y);
+    rec[2] = make_float4(n.z, m.roughness, fm(m.base[0], kd), fm(m.base[1], kd));
     rec[3] = make_float4(fm(m.base[2], kd), fa(fm(m.base[0], met), k4), fa(fm(m.base[1], met), k4),
                          fa(fm(m.base[2], met), k4));
 }
@@ -458,7 +462,6 @@ __device__ __forceinline__ void shade_body(const DeviceScene& s, const Wave& w, 
         float4 rec[4];
         Hit h;
         f3 T = mk(0.0f, 0.0f, 0.0f), wo = mk(0.0f, 0.0f, 0.0f);
-        Frame fr;
         Bsdf bs;
         bs.n = 0;
         Mix mx;
@@ -493,8 +496,7 @@ __device__ __forceinline__ void shade_body(const DeviceScene& s, const Wave& w, 
                 P.rad[k] = L;
             }
             bs = make_bsdf(m);
-            fr = make_frame(h.outward);
-            wo = to_local(fr, xneg(rd));  // isect.wo = -ray.direction
+            wo = to_local(make_frame(h.outward), xneg(rd));  // isect.wo = -ray.direction
             mx = mixture(bs, wo);
             nee = !kNoNee && key.nee && !bsdf_delta(bs);
             alive = true;
@@ -539,21 +541,24 @@ __device__ __forceinline__ void shade_body(const DeviceScene& s, const Wave& w, 
         // next-event estimation: one shadow ray per light (estimateDirectLighting)
         for (uint32_t l = 0; l < s.num_lights; ++l) {
             bool emit = false;
-            f3 contrib, so, sd;
+            f3 contrib, wi;
             float stmax = 0.0f;
             if (!kNoNee && valid && nee) {
                 const float4 u = draw4(seed, pixel, sample, d, kRngLights + ((l >> 1) << 8));
                 const LightDev& L = s.lights[l];
                 const LSample ls = light_sample(L, h.point, (l & 1) ? u.z : u.x, (l & 1) ? u.w : u.y);
                 if (ls.pdf > 0.0f && !black(ls.Li)) {
-                    const f3 wiL = to_local(fr, ls.wi);
+                    // the shading frame is rebuilt from the outward normal where it is needed
+                    // (the same bits each time) instead of being held across the loop
+                    const f3 wiL = to_local(make_frame(h.outward), ls.wi);
                     f3 f;
                     float bpdf;
                     bsdf_eval_pdf<kKinds>(bs, mx, wo, wiL, f, bpdf);
                     if (!black(f)) {
-                        spawn(h, ls.wi, so, sd);
+                        wi = ls.wi;
                         stmax = fs(ls.dist, kEpsilon);
-                        const float c = fabsf(xdot(ls.wi, h.normal));
+                        // |wi . n| of the face normal: negating n negates every product exactly
+                        const float c = fabsf(xdot(ls.wi, h.outward));
                         f3 ld;
                         if (!kVolSurface && mis && !ls.delta) {
                             const float wgt = power_heuristic(ls.pdf, bpdf);
@@ -568,6 +573,8 @@ __device__ __forceinline__ void shade_body(const DeviceScene& s, const Wave& w, 
             }
             const uint32_t slot = warp_append(P.counters + kCShadow, emit);
             if (emit && slot < P.shadow_cap) {
+                f3 so, sd;
+                spawn(h, wi, so, sd);  // after the append: fewer values live across it
                 float4* e = P.shadow + 3 * static_cast<size_t>(slot);
                 e[0] = make_float4(so.x, so.y, so.z, stmax);
                 e[1] = make_float4(sd.x, sd.y, sd.z, __uint_as_float(k));
@@ -580,8 +587,8 @@ __device__ __forceinline__ void shade_body(const DeviceScene& s, const Wave& w, 
             const float4 u = draw4(seed, pixel, sample, d, kRngBounce);
             const BSample b = bsdf_sample<kKinds>(bs, mx, wo, u.x, u.y);
             if (b.pdf > 0.0f && !black(b.f)) {
-                const f3 wiW = to_world(fr, b.wi);
-                const float c = fabsf(xdot(wiW, h.normal));
+                const f3 wiW = to_world(make_frame(h.outward), b.wi);
+                const float c = fabsf(xdot(wiW, h.outward));
                 T = xmul(T, xmuls(b.f, fd(c, b.pdf)));
                 cont = true;
                 if (d > 3) {

@@ -18,6 +18,7 @@
 
 #include "rbr_b200.h"
 #include "rbr_device.cuh"
+#include "rbr_trig.h"
 
 namespace rbr {
 
@@ -43,17 +44,6 @@ __device__ __forceinline__ float maxc(f3 a) {  // std::max({x, y, z})
 constexpr float kPi = 3.14159265358979323846f;
 constexpr float kTwoPi = 2.0f * kPi;
 constexpr float kInvPi = 1.0f / kPi;
-
-// sin and cos of a float, correctly rounded (double-precision sincos, then one rounding).
-// The sampling formulas that use them (GGX visible normals, cosine hemisphere, concentric
-// disk) amplify an ulp of error near their singular points; correctly rounded inputs keep the
-// GPU within the spread of any two accurate float libraries.
-__device__ __forceinline__ void sincos_cr(float x, float& s, float& c) {
-    double sd, cd;
-    sincos(static_cast<double>(x), &sd, &cd);
-    s = __double2float_rn(sd);
-    c = __double2float_rn(cd);
-}
 
 // ----------------------------------------------------------------------------------------
 // Philox-4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11). Counter = (pixel, sample, depth,
@@ -276,7 +266,7 @@ __device__ __forceinline__ f3 ggx_sample_wh(float alpha, f3 wo, float u1, float 
     const float r = fq(u1);
     const float phi = fm(kTwoPi, u2);
     float sp, cp;
-    sincos_cr(phi, sp, cp);
+    sincos_f(phi, sp, cp);
     const float p1 = fm(r, cp);
     float p2 = fm(r, sp);
     const float s = fm(0.5f, fa(1.0f, vh.z));
@@ -398,7 +388,7 @@ __device__ __forceinline__ f3 cosine_hemisphere(float u1, float u2) {
     const float r = fq(u1);
     const float theta = fm(kTwoPi, u2);
     float st, ct;
-    sincos_cr(theta, st, ct);
+    sincos_f(theta, st, ct);
     return mk(fm(r, ct), fm(r, st), fq(omax(0.0f, fs(1.0f, u1))));
 }
 
@@ -445,35 +435,63 @@ __host__ __device__ constexpr bool has_kind(uint32_t set, uint32_t k) { return (
 // evaluate() and pdf() of a non-delta lobe (delta lobes give 0 and 0)
 template <uint32_t kKinds = kAllKinds>
 __device__ __forceinline__ void lobe_eval_pdf(const Bsdf& b, uint32_t k, f3 wo, f3 wi, f3& f, float& pdf) {
+    // a switch over the kind with each case compiled in only if the set holds it
+    switch (k) {
+        case kLambert:
+            if (has_kind(kKinds, kLambert)) {
+                const bool same = same_hemi(wo, wi);
+                f = same ? xmuls(b.base, kInvPi) : mk(0.0f, 0.0f, 0.0f);
+                pdf = same ? fm(fabsf(wi.z), kInvPi) : 0.0f;
+                return;
+            }
+            break;
+        case kCondGGX:
+        case kDielGGX:
+            if (has_kind(kKinds, kCondGGX) || has_kind(kKinds, kDielGGX)) {
+                ggxr_eval_pdf(b, k, wo, wi, f, pdf);
+                return;
+            }
+            break;
+        case kTransGGX:
+            if (has_kind(kKinds, kTransGGX)) {
+                ggxt_eval_pdf(b, wo, wi, f, pdf);
+                return;
+            }
+            break;
+        default: break;
+    }
     f = mk(0.0f, 0.0f, 0.0f);
     pdf = 0.0f;
-    if (has_kind(kKinds, kLambert) && k == kLambert) {
-        const bool same = same_hemi(wo, wi);
-        f = same ? xmuls(b.base, kInvPi) : mk(0.0f, 0.0f, 0.0f);
-        pdf = same ? fm(fabsf(wi.z), kInvPi) : 0.0f;
-    } else if ((has_kind(kKinds, kCondGGX) || has_kind(kKinds, kDielGGX)) && (k == kCondGGX || k == kDielGGX)) {
-        ggxr_eval_pdf(b, k, wo, wi, f, pdf);
-    } else if (has_kind(kKinds, kTransGGX) && k == kTransGGX) {
-        ggxt_eval_pdf(b, wo, wi, f, pdf);
-    }
 }
 template <uint32_t kKinds = kAllKinds>
 __device__ __forceinline__ BSample lobe_sample(const Bsdf& b, uint32_t k, f3 wo, float u1, float u2) {
-    if (has_kind(kKinds, kLambert) && k == kLambert) {
-        BSample r = none();
-        r.wi = cosine_hemisphere(u1, u2);
-        if (wo.z < 0.0f) r.wi.z = -r.wi.z;
-        r.f = xmuls(b.base, kInvPi);
-        r.pdf = fm(fabsf(r.wi.z), kInvPi);
-        return r;
+    switch (k) {
+        case kLambert:
+            if (has_kind(kKinds, kLambert)) {
+                BSample r = none();
+                r.wi = cosine_hemisphere(u1, u2);
+                if (wo.z < 0.0f) r.wi.z = -r.wi.z;
+                r.f = xmuls(b.base, kInvPi);
+                r.pdf = fm(fabsf(r.wi.z), kInvPi);
+                return r;
+            }
+            break;
+        case kCondSpec:
+        case kDielSpec:
+            if (has_kind(kKinds, kCondSpec) || has_kind(kKinds, kDielSpec)) return sr_sample(b, k, wo);
+            break;
+        case kTransSpec:
+        case kPassSpec:
+            if (has_kind(kKinds, kTransSpec) || has_kind(kKinds, kPassSpec)) return st_sample(b, k, wo);
+            break;
+        case kCondGGX:
+        case kDielGGX:
+            if (has_kind(kKinds, kCondGGX) || has_kind(kKinds, kDielGGX)) return ggxr_sample(b, k, wo, u1, u2);
+            break;
+        default:
+            if (has_kind(kKinds, kTransGGX)) return ggxt_sample(b, wo, u1, u2);
+            break;
     }
-    if ((has_kind(kKinds, kCondSpec) || has_kind(kKinds, kDielSpec)) && (k == kCondSpec || k == kDielSpec))
-        return sr_sample(b, k, wo);
-    if ((has_kind(kKinds, kTransSpec) || has_kind(kKinds, kPassSpec)) && (k == kTransSpec || k == kPassSpec))
-        return st_sample(b, k, wo);
-    if ((has_kind(kKinds, kCondGGX) || has_kind(kKinds, kDielGGX)) && (k == kCondGGX || k == kDielGGX))
-        return ggxr_sample(b, k, wo, u1, u2);
-    if (has_kind(kKinds, kTransGGX) && k == kTransGGX) return ggxt_sample(b, wo, u1, u2);
     return none();
 }
 
@@ -635,7 +653,7 @@ __device__ __forceinline__ f3 hg_sample(float g, f3 wo, float u1, float u2) {
     const float st = fq(omax(0.0f, fs(1.0f, fm(c, c))));
     const float phi = fm(kTwoPi, u2);
     float sp, cp;
-    sincos_cr(phi, sp, cp);
+    sincos_f(phi, sp, cp);
     const Frame f = make_frame(wo);  // coordinateSystem(wo, tangent, bitangent)
     return xadd(xadd(xmuls(f.t, fm(st, cp)), xmuls(f.b, fm(st, sp))), xmuls(wo, c));
 }
@@ -683,7 +701,7 @@ __device__ __forceinline__ void concentric_disk(float u1, float u2, float& ox, f
         theta = fs(kPi / 2.0f, fm(kPi / 4.0f, fd(sx, sy)));
     }
     float st, ct;
-    sincos_cr(theta, st, ct);
+    sincos_f(theta, st, ct);
     ox = fm(r, ct);
     oy = fm(r, st);
 }
