@@ -588,8 +588,8 @@ def run_cache(args, rank, world, local_rank):
                 "warmup": r["warmup"], "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "bf16 (MLP) / f32 (path tracer)", "data": "synthetic (seeded)",
                 "config": {"workload": r["workload"], "reference": r["reference"],
-                           "l2": "path state per frame (2M paths x ~100 B) and hash grid (32 MB) + Adam state "
-                                 "(224 MB) exceed L2"}}
+                           "l2": "path state per frame (2M paths x ~100 B) and hash grid (34 MB FP16) + Adam state "
+                                 "and gradients (268 + 67 MB) exceed L2"}}
         for k in ("relmse", "relmse_noise_corrected", "relmse_cpu_reference", "cache", "e2e", "clocks",
                   "gpu_launches"):
             if k in r:
@@ -870,11 +870,14 @@ def main():
                          "per_ray": {"nodes": nodes / n, "leaf_records": recs / n,
                                      "bytes": alg_bytes / n},
                          "kernel": "k_trace_closest" if not tuned.get("trace.order") else
-                         "k_trace_closest_perm (timed with its k_ray_keys + radix sort: the whole call)",
+                         "k_trace_closest_perm (timed with its ray sort: the whole call)",
                          "avg_launch_ms": avg_launch_s * 1e3},
             "cpu_baseline": base,
             "clocks": clk,
-            "gpu_launches": args.steps * (2 if tuned.get("trace.order") else 1),
+            # the traversal, plus the sort's own kernels: keys, offsets and scatter of the
+            # counting sort (orders 4, 5); the key kernel before CUB's radix sort (orders 1-3)
+            "gpu_launches": args.steps * (1 + (0 if not tuned.get("trace.order") else
+                                               3 if tuned.get("trace.order") >= 4 else 1)),
             "tuning": tuned,
             "bvh": {"wide_nodes": stats.num_wide_nodes, "leaf_records": stats.num_leaf_records,
                     "depth": stats.max_depth, "build_s": stats.build_seconds,

@@ -249,7 +249,8 @@ rbr_status rbr_scene_stats_get(const rbr_ctx* ctx, rbr_scene_stats* out);
  *                          1 by direction octant, then origin cell of 512^3; 2 octant, then cell
  *                          of 64^3; 3 cell of 64^3, then octant; 4 direction cell (octahedral
  *                          16 x 8), then origin cell of 8^3; 5 origin cell of 8^3, then direction
- *                          cell
+ *                          cell. Orders 4 and 5 (16-bit keys) use the library's counting sort;
+ *                          1-3 (21- and 30-bit keys) CUB's radix sort
  *   "trace.host_chunk"     rbr_trace_host: rays per chunk of its upload / trace / download
  *                          pipeline over two streams (default 2^20; 0: one piece)
  *   "pt.wave_paths"        camera samples per path-tracer wave (default 2^23)
@@ -279,10 +280,10 @@ rbr_status rbr_scene_stats_get(const rbr_ctx* ctx, rbr_scene_stats* out);
  * Results do not depend on them; only speed and memory do. rbr_autotune picks them. */
 rbr_status rbr_param_set(rbr_ctx* ctx, const char* name, int64_t value);
 rbr_status rbr_param_get(const rbr_ctx* ctx, const char* name, int64_t* value);
-/* Autotuner (no reference counterpart): times every traversal variant ("trace.kernel",
- * "trace.min_blocks", "trace.order") on n rays of the caller's own workload (device pointer) against the
- * uploaded scene, keeps the fastest in the context and returns its time per launch in
- * microseconds (out_us may be NULL). Waits for the timings. */
+/* Autotuner (no reference counterpart): times the traversal variants ("trace.kernel",
+ * "trace.min_blocks", "trace.order" 0, 4 and 5, "trace.node_test") on n rays of the caller's own
+ * workload (device pointer) against the uploaded scene, keeps the fastest in the context and
+ * returns its time per launch in microseconds (out_us may be NULL). Waits for the timings. */
 rbr_status rbr_autotune_trace(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any_hit, int64_t* out_us);
 /* World bounds of the bounded primitives (Accelerator::worldBounds, accelerator.h:33).
  * An empty scene gives min = +FLT_MAX, max = -FLT_MAX (an empty BoundingBox). */

@@ -769,9 +769,23 @@ __global__ void k_rc_adam_mlp(AdamDev a, float* master, float* m, float* v, floa
 }
 
 // Adam over the hash-grid entries that received a gradient (entries with a zero gradient keep
-// their parameters and moments); clears the gradients it consumed.
-__global__ void k_rc_adam_grid(AdamDev a, float2* master, float2* m, float2* v, float2* grad, __half2* h, uint32_t count,
-                               const float* scalars) {
+// their parameters and moments); clears the gradients it consumed. The scan reads the dense
+// gradient array; a touched entry's master copy and moments are one 32-byte sector
+// (interleaved state), so an update reads and writes one sector of state plus its FP16 copy.
+__device__ __forceinline__ void adam_entry(const AdamDev& a, float4* state, __half2* h, uint32_t i, float2 g,
+                                           float c1, float c2) {
+    float4* st = state + 2 * static_cast<size_t>(i);
+    float4 pm = st[0];  // master.xy, m.xy
+    const float4 vv = st[1];
+    float vx = vv.x, vy = vv.y;
+    pm.x = adam_update(pm.x, pm.z, vx, g.x, a, c1, c2);
+    pm.y = adam_update(pm.y, pm.w, vy, g.y, a, c1, c2);
+    st[0] = pm;
+    st[1] = make_float4(vx, vy, 0.0f, 0.0f);
+    h[i] = __floats2half2_rn(pm.x, pm.y);
+}
+
+__global__ void k_rc_adam_grid(AdamDev a, float4* state, float2* grad, __half2* h, uint32_t count, const float* scalars) {
     const float c1 = scalars[kRcBias], c2 = scalars[kRcBias + 1];
     if (c1 == 0.0f) return;
     // Four entries per thread and pass, their gradients loaded together (two 16-byte loads), so
@@ -788,13 +802,7 @@ __global__ void k_rc_adam_grid(AdamDev a, float2* master, float2* m, float2* v, 
             if (g.x == 0.0f && g.y == 0.0f) continue;
             const uint32_t i = 4 * q + e;
             grad[i] = make_float2(0.0f, 0.0f);
-            float2 mi = m[i], vi = v[i], p = master[i];
-            p.x = adam_update(p.x, mi.x, vi.x, g.x, a, c1, c2);
-            p.y = adam_update(p.y, mi.y, vi.y, g.y, a, c1, c2);
-            m[i] = mi;
-            v[i] = vi;
-            master[i] = p;
-            h[i] = __floats2half2_rn(p.x, p.y);
+            adam_entry(a, state, h, i, g, c1, c2);
         }
     }
     // entries past the last full group of four
@@ -802,13 +810,7 @@ __global__ void k_rc_adam_grid(AdamDev a, float2* master, float2* m, float2* v, 
         const float2 g = grad[i];
         if (g.x == 0.0f && g.y == 0.0f) continue;
         grad[i] = make_float2(0.0f, 0.0f);
-        float2 mi = m[i], vi = v[i], p = master[i];
-        p.x = adam_update(p.x, mi.x, vi.x, g.x, a, c1, c2);
-        p.y = adam_update(p.y, mi.y, vi.y, g.y, a, c1, c2);
-        m[i] = mi;
-        v[i] = vi;
-        master[i] = p;
-        h[i] = __floats2half2_rn(p.x, p.y);
+        adam_entry(a, state, h, i, g, c1, c2);
     }
 }
 
@@ -824,15 +826,30 @@ __device__ __forceinline__ uint32_t mix32(uint32_t x) {  // integer finaliser (s
     return x;
 }
 
-__global__ void k_rc_init_grid(float2* master, __half2* h, uint32_t count, uint32_t seed) {
+// Sets the FP32 master copy of entry i (the first two floats of its Adam state) to its FP16 value.
+__device__ __forceinline__ void set_master(float4* state, uint32_t i, __half2 q) {
+    const float2 f = __half22float2(q);
+    float4 s = state[2 * static_cast<size_t>(i)];
+    s.x = f.x;
+    s.y = f.y;
+    state[2 * static_cast<size_t>(i)] = s;
+}
+
+__global__ void k_rc_init_grid(float4* state, __half2* h, uint32_t count, uint32_t seed) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
         const uint32_t a = mix32(2 * i + 1 + seed * 0x9E3779B9u), b = mix32(2 * i + 2 + seed * 0x9E3779B9u);
         const float x = (static_cast<float>(a >> 8) * (1.0f / 16777216.0f) * 2.0f - 1.0f) * 1e-4f;
         const float y = (static_cast<float>(b >> 8) * (1.0f / 16777216.0f) * 2.0f - 1.0f) * 1e-4f;
         const __half2 q = __floats2half2_rn(x, y);
         h[i] = q;
-        master[i] = __half22float2(q);
+        set_master(state, i, q);
     }
+}
+
+// Master copies of caller-given FP16 parameters.
+__global__ void k_rc_master_from_h(float4* state, const __half2* h, uint32_t count) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
+        set_master(state, i, h[i]);
 }
 
 __global__ void k_rc_encode(CacheDev c, const float4* records, uint32_t n, float* out) {
@@ -944,9 +961,7 @@ size_t grid_entries(const CacheState& cs) { return size_t(kRcLevels) * cs.table;
 // The cache's parameters and optimiser state.
 static void free_cache_params(CacheState& cs) {
     free_dev(cs.grid_h);
-    free_dev(cs.grid_master);
-    free_dev(cs.grid_m);
-    free_dev(cs.grid_v);
+    free_dev(cs.grid_state);
     free_dev(cs.grid_grad);
     free_dev(cs.w_bf16);
     free_dev(cs.w_master);
@@ -1015,18 +1030,20 @@ static rbr_status reset_params(rbr_ctx* ctx, const uint16_t* mlp_bf16, const uin
     cudaError_t e = cudaMemcpy(cs.w_bf16, w16.data(), kRcWeights * 2, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(cs.w_master, master.data(), kRcWeights * 4, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(as<float>(cs.w_master) + kRcWeights, 0, size_t(kRcWeights) * 12);  // m, v, grad
-    if (e == cudaSuccess) e = cudaMemset(cs.grid_m, 0, ng * 8);
-    if (e == cudaSuccess) e = cudaMemset(cs.grid_v, 0, ng * 8);
+    if (e == cudaSuccess) e = cudaMemset(cs.grid_state, 0, ng * 32);  // master (set below), m, v
     if (e == cudaSuccess) e = cudaMemset(cs.grid_grad, 0, ng * 8);
     if (e == cudaSuccess) e = cudaMemset(cs.scalars, 0, kRcScalarWords * 4);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "radiance cache: setting parameters");
-    if (grid_f16) {
-        std::vector<float> gm(ng * 2);
-        for (size_t i = 0; i < ng * 2; ++i) gm[i] = __half2float(__ushort_as_half(grid_f16[i]));
-        e = cudaMemcpy(cs.grid_h, grid_f16, ng * 4, cudaMemcpyHostToDevice);
-        if (e == cudaSuccess) e = cudaMemcpy(cs.grid_master, gm.data(), ng * 8, cudaMemcpyHostToDevice);
-    } else if (!mlp_bf16) {
-        k_rc_init_grid<<<ctx->num_sms * 8, 256>>>(as<float2>(cs.grid_master), as<__half2>(cs.grid_h),
+    if (grid_f16 || mlp_bf16) {
+        // caller-given grid, or the grid left as it is: the master copy restarts from the FP16 values
+        if (grid_f16) e = cudaMemcpy(cs.grid_h, grid_f16, ng * 4, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) {
+            k_rc_master_from_h<<<ctx->num_sms * 8, 256>>>(as<float4>(cs.grid_state), as<__half2>(cs.grid_h),
+                                                          static_cast<uint32_t>(ng));
+            e = cudaGetLastError();
+        }
+    } else {
+        k_rc_init_grid<<<ctx->num_sms * 8, 256>>>(as<float4>(cs.grid_state), as<__half2>(cs.grid_h),
                                                   static_cast<uint32_t>(ng), static_cast<uint32_t>(cs.cfg.seed));
         e = cudaGetLastError();
     }
@@ -1093,8 +1110,7 @@ rbr_status cache_create(rbr_ctx* ctx, const rbr_cache_config* cfg_in) {
         if (n1 * n1 * n1 <= cs.table) cs.dev.dense_mask |= 1u << l;
     }
     const size_t ng = grid_entries(cs);
-    if ((e = alloc_dev(cs.grid_h, ng * 4)) != cudaSuccess || (e = alloc_dev(cs.grid_master, ng * 8)) != cudaSuccess ||
-        (e = alloc_dev(cs.grid_m, ng * 8)) != cudaSuccess || (e = alloc_dev(cs.grid_v, ng * 8)) != cudaSuccess ||
+    if ((e = alloc_dev(cs.grid_h, ng * 4)) != cudaSuccess || (e = alloc_dev(cs.grid_state, ng * 32)) != cudaSuccess ||
         (e = alloc_dev(cs.grid_grad, ng * 8)) != cudaSuccess || (e = alloc_dev(cs.w_bf16, kRcWeights * 2)) != cudaSuccess ||
         (e = alloc_dev(cs.w_master, size_t(kRcWeights) * 16)) != cudaSuccess ||
         (e = alloc_dev(cs.scalars, kRcScalarWords * 4)) != cudaSuccess) {
@@ -1265,8 +1281,7 @@ cudaError_t cache_launch_step(rbr_ctx* ctx, const TrainBatchDev& b, bool apply, 
     k_rc_adam_mlp<<<(kRcWeights + 255) / 256, 256, 0, stream>>>(a, wm, wm + kRcWeights, wm + 2 * kRcWeights,
                                                                  wm + 3 * kRcWeights, as<__nv_bfloat16>(cs.w_bf16),
                                                                  as<float>(cs.scalars));
-    k_rc_adam_grid<<<ctx->num_sms * 8, 256, 0, stream>>>(a, as<float2>(cs.grid_master), as<float2>(cs.grid_m),
-                                                        as<float2>(cs.grid_v), as<float2>(cs.grid_grad),
+    k_rc_adam_grid<<<ctx->num_sms * 8, 256, 0, stream>>>(a, as<float4>(cs.grid_state), as<float2>(cs.grid_grad),
                                                         as<__half2>(cs.grid_h), static_cast<uint32_t>(grid_entries(cs)),
                                                         as<float>(cs.scalars));
     return cudaGetLastError();

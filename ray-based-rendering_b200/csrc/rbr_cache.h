@@ -58,9 +58,7 @@ struct CacheState {
     uint32_t table = 0;
     // parameters (device)
     void* grid_h = nullptr;       // __half2 [L*T]
-    void* grid_master = nullptr;  // float2 [L*T]
-    void* grid_m = nullptr;       // float2
-    void* grid_v = nullptr;       // float2
+    void* grid_state = nullptr;   // Adam state, 32 B per entry: float4 (master.xy, m.xy), float4 (v.xy, 0, 0)
     void* grid_grad = nullptr;    // float2
     void* w_bf16 = nullptr;       // bf16 [kRcWeights]
     void* w_master = nullptr;     // float [kRcWeights] x4: master, m, v, grad

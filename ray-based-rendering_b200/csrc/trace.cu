@@ -113,38 +113,138 @@ __device__ __forceinline__ uint32_t spread3(uint32_t x) {  // 9 bits -> every th
     return x;
 }
 
+// Sort key of one ray (a = origin and tmax, b = direction). Orders 1-3: direction octant and
+// Morton code of the origin cell (64^3 or 512^3 cells); orders 4 and 5: octahedral direction
+// cell of 16 x 8 and origin cell of 8^3, 16 bits.
+__device__ __forceinline__ uint32_t ray_key(float4 a, float4 b, float3 lo, float3 scale, int order) {
+    const uint32_t oct = (signbit(b.x) ? 4u : 0u) | (signbit(b.y) ? 2u : 0u) | (signbit(b.z) ? 1u : 0u);
+    auto cell = [](float v, float l, float sc) {
+        const float c = (v - l) * sc;  // NaN and out-of-box origins clamp to the box
+        return static_cast<uint32_t>(fminf(fmaxf(c, 0.0f), 511.0f));
+    };
+    const uint32_t m = spread3(cell(a.x, lo.x, scale.x)) << 2 | spread3(cell(a.y, lo.y, scale.y)) << 1 |
+                       spread3(cell(a.z, lo.z, scale.z));
+    if (order >= 4) {
+        // octahedral map: (x, y) / (|x| + |y| + |z|), the lower hemisphere folded outwards
+        const float l1 = fabsf(b.x) + fabsf(b.y) + fabsf(b.z);
+        float u = l1 > 0.0f ? b.x / l1 : 0.0f, v = l1 > 0.0f ? b.y / l1 : 0.0f;
+        if (b.z < 0.0f) {
+            const float uu = (1.0f - fabsf(v)) * (u < 0.0f ? -1.0f : 1.0f);
+            v = (1.0f - fabsf(u)) * (v < 0.0f ? -1.0f : 1.0f);
+            u = uu;
+        }
+        const uint32_t du = static_cast<uint32_t>(fminf(fmaxf((u + 1.0f) * 8.0f, 0.0f), 15.0f));  // NaN -> 0
+        const uint32_t dv = static_cast<uint32_t>(fminf(fmaxf((v + 1.0f) * 4.0f, 0.0f), 7.0f));
+        const uint32_t dir = (du << 3) | dv;
+        const uint32_t c = m >> 18;  // 8^3 cells: the top 9 bits of the 27-bit code
+        return order == 4 ? (dir << 9) | c : (c << 7) | dir;
+    }
+    return order == 1 ? (oct << 27) | m : order == 2 ? (oct << 18) | (m >> 9) : ((m >> 9) << 3) | oct;
+}
+
 __global__ void k_ray_keys(const float4* __restrict__ rays, uint32_t n, float3 lo, float3 scale, int order,
                            uint32_t* keys, uint32_t* idx) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float4 a = __ldg(rays + 2 * static_cast<size_t>(i));
         const float4 b = __ldg(rays + 2 * static_cast<size_t>(i) + 1);
-        const uint32_t oct = (signbit(b.x) ? 4u : 0u) | (signbit(b.y) ? 2u : 0u) | (signbit(b.z) ? 1u : 0u);
-        auto cell = [](float v, float l, float sc) {
-            const float c = (v - l) * sc;  // NaN and out-of-box origins clamp to the box
-            return static_cast<uint32_t>(fminf(fmaxf(c, 0.0f), 511.0f));
-        };
-        const uint32_t m = spread3(cell(a.x, lo.x, scale.x)) << 2 | spread3(cell(a.y, lo.y, scale.y)) << 1 |
-                           spread3(cell(a.z, lo.z, scale.z));
-        uint32_t key;
-        if (order >= 4) {
-            // octahedral map: (x, y) / (|x| + |y| + |z|), the lower hemisphere folded outwards
-            const float l1 = fabsf(b.x) + fabsf(b.y) + fabsf(b.z);
-            float u = l1 > 0.0f ? b.x / l1 : 0.0f, v = l1 > 0.0f ? b.y / l1 : 0.0f;
-            if (b.z < 0.0f) {
-                const float uu = (1.0f - fabsf(v)) * (u < 0.0f ? -1.0f : 1.0f);
-                v = (1.0f - fabsf(u)) * (v < 0.0f ? -1.0f : 1.0f);
-                u = uu;
-            }
-            const uint32_t du = static_cast<uint32_t>(fminf(fmaxf((u + 1.0f) * 8.0f, 0.0f), 15.0f));  // NaN -> 0
-            const uint32_t dv = static_cast<uint32_t>(fminf(fmaxf((v + 1.0f) * 4.0f, 0.0f), 7.0f));
-            const uint32_t dir = (du << 3) | dv;
-            const uint32_t cell = m >> 18;  // 8^3 cells: the top 9 bits of the 27-bit code
-            key = order == 4 ? (dir << 9) | cell : (cell << 7) | dir;
-        } else {
-            key = order == 1 ? (oct << 27) | m : order == 2 ? (oct << 18) | (m >> 9) : ((m >> 9) << 3) | oct;
-        }
-        keys[i] = key;
+        keys[i] = ray_key(a, b, lo, scale, order);
         idx[i] = i;
+    }
+}
+
+// Counting sort of the 16-bit keys (orders 4 and 5) in three passes: every ray's key and a
+// count per key value (global atomics on 65,536 counters); 64 blocks turn the counts into each
+// key's first slot within its chunk of 1,024 keys, plus the chunk totals; every ray takes the
+// next slot of its key (an atomic on the same counters, plus the slots of the chunks before)
+// and writes its index there. Lanes of a warp with equal keys share one atomic (match.any), so
+// coherent rays (few distinct keys) do not serialise on one counter. The order within one key
+// is the atomics' order, so it can differ between runs; each ray's result does not depend on
+// it.
+constexpr uint32_t kKeyValues = 1u << 16;
+constexpr int kScanThreads = 1024;
+
+constexpr uint32_t kNoKey = 0xFFFFFFFFu;  // lanes past the end (real keys are below 2^16)
+
+// The whole warp walks the grid-stride loop together (its base is a multiple of the block), so
+// every lane takes part in the match.
+__global__ void k_ray_keys16(const float4* __restrict__ rays, uint32_t n, float3 lo, float3 scale, int order,
+                             uint16_t* __restrict__ keys, uint32_t* __restrict__ counts) {
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        uint32_t k = kNoKey;
+        if (i < n) {
+            const float4 a = __ldg(rays + 2 * static_cast<size_t>(i));
+            const float4 b = __ldg(rays + 2 * static_cast<size_t>(i) + 1);
+            k = ray_key(a, b, lo, scale, order);
+            keys[i] = static_cast<uint16_t>(k);
+        }
+        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, k);
+        if (k != kNoKey && lane == static_cast<uint32_t>(__ffs(peers) - 1)) atomicAdd(counts + k, __popc(peers));
+    }
+}
+
+// Exclusive prefix sums of the counts within each chunk of 1,024 keys, in place, one block of
+// 1,024 threads per chunk (64 blocks); the chunk totals go to `chunk_sum`. The scatter adds
+// the totals of the chunks before a key's chunk.
+constexpr uint32_t kScanChunks = kKeyValues / kScanThreads;
+__global__ void __launch_bounds__(kScanThreads) k_key_offsets(uint32_t* counts, uint32_t* chunk_sum) {
+    __shared__ uint32_t warp_sum[kScanThreads / 32];
+    const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+    uint32_t* c = counts + blockIdx.x * kScanThreads;
+    const uint32_t v = c[t];
+    uint32_t incl = v;  // inclusive scan over the warp
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= static_cast<uint32_t>(o)) incl += y;
+    }
+    if (lane == 31) warp_sum[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t w = warp_sum[lane];
+        uint32_t wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, wi, o);
+            if (lane >= static_cast<uint32_t>(o)) wi += y;
+        }
+        warp_sum[lane] = wi - w;  // exclusive over the warps
+        if (lane == 31) chunk_sum[blockIdx.x] = wi;
+    }
+    __syncthreads();
+    c[t] = warp_sum[warp] + incl - v;
+}
+
+__global__ void k_ray_scatter16(const uint16_t* __restrict__ keys, uint32_t n, uint32_t* __restrict__ offsets,
+                                const uint32_t* __restrict__ chunk_sum, uint32_t* __restrict__ perm) {
+    // first slot of each chunk of keys: exclusive sum of the chunk totals (64 of them)
+    __shared__ uint32_t chunk_first[kScanChunks];
+    if (threadIdx.x < 32) {
+        const uint32_t l = threadIdx.x;
+        const uint32_t a = chunk_sum[2 * l], b = chunk_sum[2 * l + 1];
+        uint32_t incl = a + b;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (l >= static_cast<uint32_t>(o)) incl += y;
+        }
+        chunk_first[2 * l] = incl - a - b;
+        chunk_first[2 * l + 1] = incl - b;
+    }
+    __syncthreads();
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t lt;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        const uint32_t k = i < n ? keys[i] : kNoKey;
+        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, k);
+        const uint32_t leader = static_cast<uint32_t>(__ffs(peers) - 1);
+        uint32_t first = 0;
+        if (k != kNoKey && lane == leader) first = chunk_first[k / kScanThreads] + atomicAdd(offsets + k, __popc(peers));
+        first = __shfl_sync(0xFFFFFFFFu, first, leader);
+        if (k != kNoKey) perm[first + __popc(peers & lt)] = i;
     }
 }
 
@@ -452,20 +552,11 @@ cudaError_t launch_trace_persist(const DeviceScene& s, const rbr_ray* rays, uint
     return cudaGetLastError();
 }
 
-// Sorts the rays by (direction octant, origin cell) on `stream` and returns the permutation.
+// Sorts the rays by their key of order ctx->trace_order on `stream` and returns the permutation:
+// orders 4 and 5 by the counting sort above, orders 1-3 (21- and 30-bit keys) by CUB's radix sort.
 static cudaError_t sort_rays(rbr_ctx* ctx, DevBuf& sort_buf, const rbr_ray* rays, uint32_t n, const uint32_t** perm,
                              cudaStream_t stream) {
     const int order = ctx->trace_order;
-    const int key_bits = order == 1 ? 30 : order >= 4 ? 16 : 21;
-    size_t temp = 0;
-    cudaError_t e = cub::DeviceRadixSort::SortPairs(nullptr, temp, static_cast<const uint32_t*>(nullptr),
-                                                    static_cast<uint32_t*>(nullptr), static_cast<const uint32_t*>(nullptr),
-                                                    static_cast<uint32_t*>(nullptr), static_cast<int>(n), 0, key_bits, stream);
-    if (e != cudaSuccess) return e;
-    if (ensure(ctx, sort_buf, size_t(n) * 16 + temp + 256, "ray sort") != RBR_OK) return cudaErrorMemoryAllocation;
-    uint32_t* base = static_cast<uint32_t*>(sort_buf.ptr);
-    uint32_t *keys = base, *keys2 = base + n, *idx = base + 2 * size_t(n), *idx2 = base + 3 * size_t(n);
-    void* tmp = reinterpret_cast<char*>(base + 4 * size_t(n)) + (256 - (reinterpret_cast<uintptr_t>(base + 4 * size_t(n)) & 255));
     float3 lo = make_float3(0.0f, 0.0f, 0.0f), sc = make_float3(0.0f, 0.0f, 0.0f);
     const float* blo = ctx->bounds_lo;
     const float* bhi = ctx->bounds_hi;
@@ -479,6 +570,34 @@ static cudaError_t sort_rays(rbr_ctx* ctx, DevBuf& sort_buf, const rbr_ray* rays
         }
     }
     const int grid = std::min<int>((n + 255) / 256, ctx->num_sms * 8);
+    if (order >= 4) {  // 16-bit keys: the counting sort above
+        const size_t perm_bytes = (size_t(n) * 4 + 255) & ~size_t(255);
+        const size_t key_bytes = (size_t(n) * 2 + 255) & ~size_t(255);
+        if (ensure(ctx, sort_buf, perm_bytes + key_bytes + (kKeyValues + kScanChunks) * 4, "ray sort") != RBR_OK)
+            return cudaErrorMemoryAllocation;
+        char* base = static_cast<char*>(sort_buf.ptr);
+        auto* pm = reinterpret_cast<uint32_t*>(base);
+        auto* keys = reinterpret_cast<uint16_t*>(base + perm_bytes);
+        auto* counts = reinterpret_cast<uint32_t*>(base + perm_bytes + key_bytes);
+        uint32_t* chunk_sum = counts + kKeyValues;
+        cudaError_t e = cudaMemsetAsync(counts, 0, kKeyValues * 4, stream);
+        if (e != cudaSuccess) return e;
+        k_ray_keys16<<<grid, 256, 0, stream>>>(reinterpret_cast<const float4*>(rays), n, lo, sc, order, keys, counts);
+        k_key_offsets<<<kScanChunks, kScanThreads, 0, stream>>>(counts, chunk_sum);
+        k_ray_scatter16<<<grid, 256, 0, stream>>>(keys, n, counts, chunk_sum, pm);
+        *perm = pm;
+        return cudaGetLastError();
+    }
+    const int key_bits = order == 1 ? 30 : 21;
+    size_t temp = 0;
+    cudaError_t e = cub::DeviceRadixSort::SortPairs(nullptr, temp, static_cast<const uint32_t*>(nullptr),
+                                                    static_cast<uint32_t*>(nullptr), static_cast<const uint32_t*>(nullptr),
+                                                    static_cast<uint32_t*>(nullptr), static_cast<int>(n), 0, key_bits, stream);
+    if (e != cudaSuccess) return e;
+    if (ensure(ctx, sort_buf, size_t(n) * 16 + temp + 256, "ray sort") != RBR_OK) return cudaErrorMemoryAllocation;
+    uint32_t* base = static_cast<uint32_t*>(sort_buf.ptr);
+    uint32_t *keys = base, *keys2 = base + n, *idx = base + 2 * size_t(n), *idx2 = base + 3 * size_t(n);
+    void* tmp = reinterpret_cast<char*>(base + 4 * size_t(n)) + (256 - (reinterpret_cast<uintptr_t>(base + 4 * size_t(n)) & 255));
     k_ray_keys<<<grid, 256, 0, stream>>>(reinterpret_cast<const float4*>(rays), n, lo, sc, order, keys, idx);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -547,14 +666,18 @@ cudaError_t launch_trace(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any_
 // Times every traversal variant on the caller's rays (device pointer) and keeps the fastest.
 rbr_status autotune_trace(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any_hit, int64_t* chosen_ms_x1000) {
     struct Cand {
-        int kernel, min_blocks, per_sm, order;
+        int kernel, min_blocks, per_sm, order, node_test;
     };
-    const Cand cands[] = {{0, 8, 0, 0}, {0, 10, 0, 0}, {0, 12, 0, 0}, {1, 10, 0, 0}, {2, 10, 0, 0},
-                          {0, 8, 0, 1}, {0, 10, 0, 1}, {0, 12, 0, 1}, {0, 10, 0, 2}, {0, 10, 0, 3},
-                          {0, 8, 0, 4}, {0, 10, 0, 4}, {0, 10, 0, 5}, {1, 10, 0, 2}, {1, 10, 0, 4}};
+    // Unsorted variants, and sorted ones with the 16-bit keys of orders 4 and 5 (the counting
+    // sort of this file) and either node test. Orders 1-3 (CUB's radix sort) stay selectable
+    // by parameter; measured slower than orders 4 and 5, they are not candidates.
+    const Cand cands[] = {{0, 8, 0, 0, 0},  {0, 10, 0, 0, 0}, {0, 12, 0, 0, 0}, {1, 10, 0, 0, 0}, {2, 10, 0, 0, 0},
+                          {0, 8, 0, 4, 0},  {0, 10, 0, 4, 0}, {0, 10, 0, 5, 0}, {0, 12, 0, 5, 0}, {0, 8, 0, 5, 1},
+                          {0, 10, 0, 4, 1}, {0, 10, 0, 5, 1}, {0, 12, 0, 5, 1}, {1, 10, 0, 5, 0}};
     rbr_status st = ensure(ctx, ctx->stage_out, size_t(n) * (any_hit ? 1 : sizeof(rbr_hit)), "autotune output");
     if (st != RBR_OK) return st;
-    const Cand saved{ctx->trace_kernel, ctx->trace_min_blocks, ctx->trace_blocks_per_sm, ctx->trace_order};
+    const Cand saved{ctx->trace_kernel, ctx->trace_min_blocks, ctx->trace_blocks_per_sm, ctx->trace_order,
+                     ctx->trace_node_test};
     float best_ms = 1e30f;
     Cand best = saved;
     cudaEvent_t a, b;
@@ -565,6 +688,7 @@ rbr_status autotune_trace(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any
         ctx->trace_min_blocks = c.min_blocks;
         ctx->trace_blocks_per_sm = c.per_sm;
         ctx->trace_order = c.order;
+        ctx->trace_node_test = c.node_test;
         cudaError_t e = launch_trace(ctx, rays, n, any_hit, ctx->stage_out.ptr, ctx->stream);  // warm-up
         float ms = 0.0f, total = 0.0f;
         for (int k = 0; k < 3 && e == cudaSuccess; ++k) {
@@ -582,6 +706,7 @@ rbr_status autotune_trace(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any
             ctx->trace_min_blocks = saved.min_blocks;
             ctx->trace_blocks_per_sm = saved.per_sm;
             ctx->trace_order = saved.order;
+            ctx->trace_node_test = saved.node_test;
             return cuda_fail(ctx, e, "autotune launch");
         }
         if (total < best_ms) {
@@ -595,6 +720,7 @@ rbr_status autotune_trace(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any
     ctx->trace_min_blocks = best.min_blocks;
     ctx->trace_blocks_per_sm = best.per_sm;
     ctx->trace_order = best.order;
+    ctx->trace_node_test = best.node_test;
     if (chosen_ms_x1000) *chosen_ms_x1000 = static_cast<int64_t>(best_ms / 3.0f * 1000.0f);
     return check_device_error(ctx, ctx->stream);
 }

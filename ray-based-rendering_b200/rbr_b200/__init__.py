@@ -222,7 +222,8 @@ class Context:
         us = C.c_int64()
         self._check(self.lib.rbr_autotune_trace(self.h, C.c_void_p(rays_ptr), n, int(any_hit), C.byref(us)))
         return {"trace.kernel": self.get_param("trace.kernel"), "trace.min_blocks": self.get_param("trace.min_blocks"),
-                "trace.order": self.get_param("trace.order"), "us_per_launch": us.value}
+                "trace.order": self.get_param("trace.order"), "trace.node_test": self.get_param("trace.node_test"),
+                "us_per_launch": us.value}
 
     def l2_read_bandwidth(self, nbytes: int = 32 << 20, passes: int = 50) -> float:
         """Read bandwidth (GB/s) of an L2-resident buffer: the traversal roofline's denominator."""
