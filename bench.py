@@ -308,6 +308,15 @@ def cpu_render_baseline(scene, cam, spp, max_depth, volumetric, row_frac):
                       f"{dt:.1f} s"}
 
 
+def set_params(ctx, params, bvh=False):
+    """Applies NAME=INT context parameters: only the BVH build ones (bvh.*, read at the next
+    upload) with bvh=True, all of them otherwise."""
+    for kv in params:
+        k, v = kv.split("=")
+        if not bvh or k.startswith("bvh."):
+            ctx.set_param(k, int(v))
+
+
 def measure_render(which, ctx, local_rank, rank, world, steps, warmup, e2e_steps, cpu_row_frac, params=()):
     """Mpaths/s of the path tracer on one configuration: device-timed steps (one rbr_render of the
     whole image each), end to end through rbr_render_host, the reference CPU integrator on a band
@@ -320,10 +329,9 @@ def measure_render(which, ctx, local_rank, rank, world, steps, warmup, e2e_steps
     scene = render_scene(which)
     cam = scene.camera
     W, H = cam.width, cam.height
+    set_params(ctx, params, bvh=True)  # build parameters apply at the upload
     ctx.upload(scene)
-    for kv in params:
-        k, v = kv.split("=")
-        ctx.set_param(k, int(v))
+    set_params(ctx, params)
     film = torch.empty(W * H * 3, dtype=torch.float32, device=f"cuda:{local_rank}")
     stream = torch.cuda.current_stream()
     paths = W * H * cfg["spp"]
@@ -577,9 +585,7 @@ def run_cache(args, rank, world, local_rank):
         k, v = kv.split("=")
         cache_kw[k] = int(v)
     ctx = Context(local_rank)
-    for kv in args.param:
-        k, v = kv.split("=")
-        ctx.set_param(k, int(v))
+    set_params(ctx, args.param)
     r = measure_cache(ctx, local_rank, rank, args.steps, args.warmup, args.ref_spp, cache_kw,
                       cpu_crop=args.cpu_ref_crop, cpu_spp=args.cpu_ref_spp)
     ctx.close()
@@ -769,10 +775,9 @@ def main():
 
     scene, rays = workload(rank)
     ctx = Context(local_rank)
+    set_params(ctx, args.param, bvh=True)  # build parameters apply at the upload
     stats = ctx.upload(scene)
-    for kv in args.param:
-        k, v = kv.split("=")
-        ctx.set_param(k, int(v))
+    set_params(ctx, args.param)
     n = len(rays)
     d_rays = torch.from_numpy(rays.view(np.uint8)).to(f"cuda:{local_rank}")
     d_hits = torch.empty(n * 8, dtype=torch.uint8, device=f"cuda:{local_rank}")

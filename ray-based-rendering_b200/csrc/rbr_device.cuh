@@ -190,7 +190,9 @@ __device__ __forceinline__ float fmin3(float a, float b, float c) {
     return d;
 }
 
-// Mask of `width` bits starting at bit `pos` (pos < 32, width < 32); bits above 31 are dropped.
+// Mask of (width mod 32) bits starting at bit (pos mod 32); bits above 31 are dropped. PTX's
+// bmsk.wrap uses the low five bits of both operands, so a word whose low byte holds a slot's
+// field (and whose other bits hold anything) can be passed as it is.
 __device__ __forceinline__ uint32_t bitmask_at(uint32_t pos, uint32_t width) {
     uint32_t d;
     asm("bmsk.wrap.b32 %0, %1, %2;" : "=r"(d) : "r"(pos), "r"(width));
@@ -214,7 +216,7 @@ constexpr float kTHi = 1.0f + 1.0f / 65536.0f;
 struct NodeView {
     float2 ax, bx, ay, by, az, bz;   // (near, far) factors per axis
     uint2 nx, fx, ny, fy, nz, fz;    // near / far plane bytes per axis (8 slots)
-    uint32_t pos_lo, pos_hi;         // per slot byte: first bit (internal: 24 + (slot ^ ray octant))
+    uint32_t pos_lo, pos_hi;         // per slot byte: first bit in bits 0-4 (internal: 24 + (slot ^ octant))
     uint32_t wid_lo, wid_hi;         // per slot byte: number of bits
     uint32_t imask, child_base, prim_base;
 };
@@ -250,8 +252,8 @@ __device__ __forceinline__ NodeView node_view(const uint4* __restrict__ nodes, u
     v.nz = r.nz ? qhiz : qloz;
     v.fz = r.nz ? qloz : qhiz;
     v.imask = w0.w >> 24;
-    v.pos_lo = (w1.z ^ inner_oct4(v.imask & 0xFu, r.oct)) & 0x1F1F1F1Fu;
-    v.pos_hi = (w1.w ^ inner_oct4(v.imask >> 4, r.oct)) & 0x1F1F1F1Fu;
+    v.pos_lo = w1.z ^ inner_oct4(v.imask & 0xFu, r.oct);  // bits 5-7 of each byte (the width) are
+    v.pos_hi = w1.w ^ inner_oct4(v.imask >> 4, r.oct);    // dropped by bmsk.wrap
     v.wid_lo = (w1.z >> 5) & 0x07070707u;
     v.wid_hi = (w1.w >> 5) & 0x07070707u;
     v.child_base = w1.x;
@@ -271,13 +273,12 @@ __device__ __forceinline__ bool slot_hit(const NodeView& v, int i, float tbest) 
     return fmaxf(tn, 0.0f) <= fminf(tf, tbest);
 }
 
-// Byte k (0..3) of a word, zero-extended.
-__device__ __forceinline__ uint32_t byte_of(uint32_t w, uint32_t k) { return __byte_perm(w, 0u, 0x4440u | k); }
-
-// Bits of slot i in the node's hit mask: its leaf records, or bit 24 + (slot ^ octant).
+// Bits of slot i in the node's hit mask: its leaf records, or bit 24 + (slot ^ octant). The
+// slot's position and width bytes are shifted to the bottom; bmsk.wrap ignores the rest (the
+// widths are at most 7, so the next byte's bits start above bit 4).
 __device__ __forceinline__ uint32_t slot_bits(const NodeView& v, int i) {
-    const uint32_t k = static_cast<uint32_t>(i & 3);
-    return bitmask_at(byte_of(i >= 4 ? v.pos_hi : v.pos_lo, k), byte_of(i >= 4 ? v.wid_hi : v.wid_lo, k));
+    const uint32_t sh = 8u * static_cast<uint32_t>(i & 3);
+    return bitmask_at((i >= 4 ? v.pos_hi : v.pos_lo) >> sh, (i >= 4 ? v.wid_hi : v.wid_lo) >> sh);
 }
 
 // Splits a node's hit mask into ngroup = (child_base, internal hit bits << 24 | imask << 16)
@@ -322,13 +323,13 @@ __device__ __forceinline__ void intersect_node_lean(const uint4* __restrict__ no
     const uint2 ny = r.ny ? qhiy : qloy, fy = r.ny ? qloy : qhiy;
     const uint2 nz = r.nz ? qhiz : qloz, fz = r.nz ? qloz : qhiz;
     const uint32_t imask = w0.w >> 24;
-    const uint32_t pos_lo = (w1.z ^ inner_oct4(imask & 0xFu, r.oct)) & 0x1F1F1F1Fu;
-    const uint32_t pos_hi = (w1.w ^ inner_oct4(imask >> 4, r.oct)) & 0x1F1F1F1Fu;
+    const uint32_t pos_lo = w1.z ^ inner_oct4(imask & 0xFu, r.oct);
+    const uint32_t pos_hi = w1.w ^ inner_oct4(imask >> 4, r.oct);
     const uint32_t wid_lo = (w1.z >> 5) & 0x07070707u, wid_hi = (w1.w >> 5) & 0x07070707u;
     uint32_t bits = 0;
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-        const uint32_t k = static_cast<uint32_t>(i & 3);
+        const uint32_t k = static_cast<uint32_t>(i & 3), sh = 8u * k;
         const bool h = i >= 4;
         const float tnx = fmaf(qplane(h ? nx.y : nx.x, k), ax, bx), tfx = fmaf(qplane(h ? fx.y : fx.x, k), ax, bx);
         const float tny = fmaf(qplane(h ? ny.y : ny.x, k), ay, by), tfy = fmaf(qplane(h ? fy.y : fy.x, k), ay, by);
@@ -336,7 +337,7 @@ __device__ __forceinline__ void intersect_node_lean(const uint4* __restrict__ no
         const float tn = fmax3(tnx, tny, fmaxf(tnz, 0.0f)) * kTLo;
         const float tf = fmin3(tfx, tfy, tfz) * kTHi;
         if (tn <= fminf(tf, tbest))
-            bits |= bitmask_at(byte_of(h ? pos_hi : pos_lo, k), byte_of(h ? wid_hi : wid_lo, k));
+            bits |= bitmask_at((h ? pos_hi : pos_lo) >> sh, (h ? wid_hi : wid_lo) >> sh);
     }
     const uint32_t inner = imask ? 0xFF000000u : 0u;
     ngroup = make_uint2(w1.x, (bits & inner) | (imask << 16));
