@@ -263,7 +263,8 @@ rbr_status rbr_scene_stats_get(const rbr_ctx* ctx, rbr_scene_stats* out);
  *   "trace.l2_persist"     kernel 0: 1 reserves the largest persisting-L2 set-aside this process's
  *                          context allows and marks the BVH (nodes and leaf records) persisting for
  *                          each ray-query launch; 0 (default) releases it
- *   "pt.shade_split"       rbr_render: 1 shades each material class (glossy, diffuse, delta-only,
+ *   "pt.shade_split"       rbr_render: 1 shades each material class (Lambertian, GGX with a
+ *                          Lambertian lobe, GGX reflection only, GGX transmission, delta-only,
  *                          none) in a launch of its own, compiled for that class's lobes; 0 one
  *                          launch for all classes (default)
  *   "cache.infer_groups"   radiance-cache inference: 128-sample tiles in flight per CTA, 1, 2 or 4

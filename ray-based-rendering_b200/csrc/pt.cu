@@ -38,16 +38,18 @@ constexpr size_t kShadowBytesLimit = size_t(2) << 30;
 enum : int {
     kCQ0 = 0,       // active queue counts, ping-pong by depth parity
     kCClass = 2,    // kNumClasses class-queue counts
-    kCShadow = 6,   // shadow queue count
-    kCExt = 8,      // 64-bit: extension rays traced
-    kCSh = 10,      // 64-bit: shadow rays traced
-    kCQuery = 12,   // radiance cache: paths ended into the cache in this wave
-    kCTrain = 13,   // radiance cache: training vertices gathered in this frame
-    kCTrainBase = 14,  // radiance cache: kCTrain at the start of this wave
-    kCShade = 16,      // 64-bit: hit vertices shaded
-    kCTraffic = 18,    // 4 x 64-bit (RBR_RENDER_COUNT_TRAFFIC): extension nodes, records; shadow nodes, records
-    kCWords = 26
+    kCShadow = 8,   // shadow queue count
+    kCExt = 10,     // 64-bit: extension rays traced
+    kCSh = 12,      // 64-bit: shadow rays traced
+    kCQuery = 14,   // radiance cache: paths ended into the cache in this wave
+    kCTrain = 15,   // radiance cache: training vertices gathered in this frame
+    kCTrainBase = 16,  // radiance cache: kCTrain at the start of this wave
+    kCShade = 18,      // 64-bit: hit vertices shaded
+    kCTraffic = 20,    // 4 x 64-bit (RBR_RENDER_COUNT_TRAFFIC): extension nodes, records; shadow nodes, records
+    kCWords = 28
 };
+static_assert(kCClass + static_cast<int>(kNumClasses) <= kCShadow, "class-queue counts overlap the shadow count");
+static_assert(kCExt % 2 == 0 && kCSh % 2 == 0 && kCShade % 2 == 0 && kCTraffic % 2 == 0, "64-bit counters");
 
 // The blocks a stage runs on: the whole grid for the wavefront kernels, one half of it for a
 // half of the persistent wave loop. Grid-stride loops start at block `block` of `blocks`.
@@ -291,10 +293,16 @@ __device__ __forceinline__ void extend_body(const DeviceScene& s, const Wave& w,
                 }
             }
         }
-#pragma unroll
-        for (uint32_t c = 0; c < kNumClasses; ++c) {
-            const uint32_t slot = warp_append(P.counters + kCClass + c, cls == c);
-            if (cls == c) P.classq[c * P.cap + slot] = k;
+        {
+            // append to the class queue: lanes of one class share an atomic (match.any), one
+            // per class present in the warp; kNumClasses marks a lane with nothing to shade
+            const uint32_t peers = __match_any_sync(0xFFFFFFFFu, cls);
+            const int leader = __ffs(peers) - 1;
+            uint32_t first = 0;
+            if (cls < kNumClasses && static_cast<int>(threadIdx.x & 31) == leader)
+                first = atomicAdd(P.counters + kCClass + cls, __popc(peers));
+            first = __shfl_sync(0xFFFFFFFFu, first, leader);
+            if (cls < kNumClasses) P.classq[cls * P.cap + first + __popc(peers & lanemask_lt())] = k;
         }
         if (kVol) {
             // next-event estimation from the scatter point: point lights only, unoccluded
@@ -433,10 +441,19 @@ __device__ __forceinline__ bool train_path(const Wave& w, uint64_t seed, uint32_
 // the diffuse and delta-only classes, no next-event estimation for delta-only and lobeless
 // materials, whose light samples always evaluate to zero).
 constexpr int kShadeDiffuse = static_cast<int>(kClassDiffuse), kShadeGlossy = static_cast<int>(kClassGlossy),
-              kShadeSpecular = static_cast<int>(kClassSpecular), kShadeNone = static_cast<int>(kClassNone);
+              kShadeSpecular = static_cast<int>(kClassSpecular), kShadeNone = static_cast<int>(kClassNone),
+              kShadeGlossyRefl = static_cast<int>(kClassGlossyRefl),
+              kShadeGlossyTrans = static_cast<int>(kClassGlossyTrans);
+constexpr uint32_t kGGXReflKinds = (1u << kCondGGX) | (1u << kDielGGX);
 template <int kCls>
 __host__ __device__ constexpr uint32_t class_kinds() {
-    return kCls == kShadeDiffuse ? kNoGGXKinds : kCls == kShadeSpecular ? kDeltaKinds : kCls == kShadeNone ? 0u : kAllKinds;
+    return kCls == kShadeDiffuse       ? kNoGGXKinds
+           : kCls == kShadeSpecular    ? kDeltaKinds
+           : kCls == kShadeNone        ? 0u
+           : kCls == kShadeGlossy      ? kGGXReflKinds | (1u << kLambert)
+           : kCls == kShadeGlossyRefl  ? kGGXReflKinds
+           : kCls == kShadeGlossyTrans ? kGGXReflKinds | (1u << kTransGGX) | (1u << kLambert)
+                                       : kAllKinds;
 }
 
 template <int kMode, bool kPacked, int kCls>
@@ -615,7 +632,7 @@ __device__ __forceinline__ void shade_body(const DeviceScene& s, const Wave& w, 
 // the diffuse class 7 (72), which keeps their spills small (76 / 68 bytes instead of 232 / 156).
 template <int kCls>
 __host__ __device__ constexpr int shade_blocks() {
-    return kCls == kShadeGlossy ? 6 : kCls == kShadeDiffuse ? 7 : 8;
+    return kCls == kShadeGlossy || kCls == kShadeGlossyRefl || kCls == kShadeGlossyTrans ? 6 : kCls == kShadeDiffuse ? 7 : 8;
 }
 
 template <int kMode, bool kPacked, int kCls = -1>
@@ -1023,6 +1040,8 @@ rbr_status render(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_params* 
                 else k_extend<false, false><<<grid, kBlock, 0, ws>>>(ctx->scene, w, P, d, ctx->d_error);
                 if (ctx->pt_shade_split) {
                     k_shade<0, false, kShadeGlossy><<<grid, kBlock, 0, ws>>>(ctx->scene, w, P, d);
+                    k_shade<0, false, kShadeGlossyRefl><<<grid, kBlock, 0, ws>>>(ctx->scene, w, P, d);
+                    k_shade<0, false, kShadeGlossyTrans><<<grid, kBlock, 0, ws>>>(ctx->scene, w, P, d);
                     k_shade<0, false, kShadeDiffuse><<<grid, kBlock, 0, ws>>>(ctx->scene, w, P, d);
                     k_shade<0, false, kShadeSpecular><<<grid, kBlock, 0, ws>>>(ctx->scene, w, P, d);
                     k_shade<0, false, kShadeNone><<<grid, kBlock, 0, ws>>>(ctx->scene, w, P, d);
@@ -1421,9 +1440,10 @@ rbr_status render_noalloc(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_
     const uint32_t spp = static_cast<uint32_t>(p->samples_per_pixel);
     if (npix * spp > 0xFFFFFFFFull)
         return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "more than 2^32 camera samples in one render call");
-    // wave capacity that fits the fixed array: 96 B of path state + 48 B per light and path
+    // wave capacity that fits the fixed array: 88 B of path state, 4 B per class queue and 48 B
+    // per light and path
     const uint32_t nl = std::max(1u, ctx->scene.num_lights);
-    const size_t per_path = 96 + 48 * size_t(nl);
+    const size_t per_path = 88 + 4 * size_t(kNumClasses) + 48 * size_t(nl);
     const size_t fixed = 9 * 256;  // counters + alignment of the eight arrays
     uint64_t cap = (RBR_NOALLOC_SCRATCH_BYTES - fixed) / per_path;
     cap = std::min<uint64_t>(cap, npix * spp);

@@ -8,7 +8,19 @@ namespace rbr {
 
 // Shading classes: paths are bucketed by the class of the material they hit so that one
 // warp shades one kind of BSDF.
-enum : uint32_t { kClassDiffuse = 0, kClassGlossy = 1, kClassSpecular = 2, kClassNone = 3, kNumClasses = 4 };
+// Shading classes of a material, by the lobes Material::createBSDF gives it: Lambertian (and
+// delta) lobes only; GGX reflection with a Lambertian lobe (plastics); delta lobes only; no
+// lobes; GGX reflection only (metals); GGX with GGX transmission (rough glass). The path tracer
+// queues hits per class, so that a warp of the shading kernel runs one lobe combination.
+enum : uint32_t {
+    kClassDiffuse = 0,
+    kClassGlossy = 1,
+    kClassSpecular = 2,
+    kClassNone = 3,
+    kClassGlossyRefl = 4,
+    kClassGlossyTrans = 5,
+    kNumClasses = 6
+};
 
 struct MaterialDev {
     float base[3];

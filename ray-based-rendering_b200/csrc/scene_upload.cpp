@@ -56,20 +56,24 @@ uint32_t material_class(const rbr_material& m) {
     const bool smooth = m.roughness < 0.03f;
     const bool iface = std::fabs(m.ior - 1.0f) > 1e-3f;
     const bool tinted = !(m.base_color[0] <= 0.0f && m.base_color[1] <= 0.0f && m.base_color[2] <= 0.0f);
-    bool ggx = false, lambert = false, delta = false;
+    bool ggx = false, ggx_trans = false, lambert = false, delta = false;
     auto lobe = [&](bool is_delta) { (is_delta ? delta : ggx) = true; };
     if (met > 0.0f && tinted) lobe(smooth);
     if (diel > 0.0f) {
         if (iface) {
             lobe(smooth);
-            if (t > 0.0f && tinted) lobe(smooth);
+            if (t > 0.0f && tinted) {
+                lobe(smooth);
+                ggx_trans = !smooth;
+            }
             if (t < 1.0f && tinted) lambert = true;
         } else {
             if (t > 0.0f && tinted) delta = true;
             if (t < 1.0f && tinted) lambert = true;
         }
     }
-    if (ggx) return kClassGlossy;
+    if (ggx_trans) return kClassGlossyTrans;
+    if (ggx) return lambert ? kClassGlossy : kClassGlossyRefl;
     if (lambert) return kClassDiffuse;
     if (delta) return kClassSpecular;
     return kClassNone;
