@@ -10,6 +10,7 @@
 #include <memory>
 #include <random>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "gpu_accelerator.h"
@@ -168,6 +169,54 @@ int main() {
         const bool refHit = bruteForce(small.prims, probe, b);
         const bool hit = accel.intersect(probe, a);
         check(hit == refHit && (!hit || a.primitive == b.primitive), "rebuild");
+    }
+    {  // micro-batched per-ray queries from concurrent threads: the answers of single queries
+        World w = randomWorld(rng, 200, 800, 50, true);
+        accel.build(w.prims);
+        std::uniform_real_distribution<float> pos(-14.0f, 14.0f), dir(-1.0f, 1.0f);
+        std::vector<Ray> rays;
+        while (rays.size() < 4000) {
+            const Vec3 d(dir(rng), dir(rng), dir(rng));
+            if (d.length() > 1e-3f) rays.push_back(Ray(Vec3(pos(rng), pos(rng), pos(rng)), d));
+        }
+        std::vector<int> refHit(rays.size()), refP(rays.size());
+        std::vector<const Primitive*> refPrim(rays.size(), nullptr);
+        std::vector<float> refT(rays.size(), 0.0f);
+        for (size_t i = 0; i < rays.size(); ++i) {
+            SurfaceInteraction is;
+            refHit[i] = bruteForce(w.prims, rays[i], is);
+            if (refHit[i]) refPrim[i] = is.primitive, refT[i] = is.t;
+            for (const Primitive* q : w.prims)
+                if (q->intersectP(rays[i])) {
+                    refP[i] = 1;
+                    break;
+                }
+        }
+        accel.setMicroBatching(8, 200);
+        const int kThreads = 8;
+        std::vector<int> bad(kThreads, 0);
+        std::vector<std::thread> pool;
+        for (int t = 0; t < kThreads; ++t)
+            pool.emplace_back([&, t] {
+                for (size_t i = t; i < rays.size(); i += kThreads) {
+                    Ray r = rays[i];
+                    SurfaceInteraction is;
+                    const bool hit = accel.intersect(r, is);
+                    if (hit != static_cast<bool>(refHit[i]) || (hit && (is.primitive != refPrim[i] || !bits_equal(is.t, refT[i]))))
+                        ++bad[t];
+                    if (accel.intersectP(rays[i]) != static_cast<bool>(refP[i])) ++bad[t];
+                }
+            });
+        for (auto& th : pool) th.join();
+        int total = 0;
+        for (int b : bad) total += b;
+        const double per_launch = static_cast<double>(accel.perRayRays()) / std::max<uint64_t>(1, accel.perRayLaunches());
+        std::cout << "micro-batched queries: " << accel.perRayRays() << " rays in " << accel.perRayLaunches()
+                  << " launches (" << per_launch << " per launch), " << total << " mismatches\n";
+        check(total == 0, "micro-batched per-ray queries equal brute force");
+        check(accel.perRayRays() == 2 * rays.size(), "every micro-batched query was traced once");
+        check(per_launch > 1.0, "micro-batching gathers queries of several threads");
+        accel.setMicroBatching(1, 0);
     }
     {  // unsupported primitive: reported, no CPU fallback
         World odd;
