@@ -252,7 +252,8 @@ rbr_status rbr_scene_stats_get(const rbr_ctx* ctx, rbr_scene_stats* out);
  *                          cell. Orders 4 and 5 (16-bit keys) use the library's counting sort;
  *                          1-3 (21- and 30-bit keys) CUB's radix sort
  *   "trace.host_chunk"     rbr_trace_host: rays per chunk of its upload / trace / download
- *                          pipeline over two streams (default 2^20; 0: one piece)
+ *                          pipeline (default 2^19; 0: one piece)
+ *   "trace.host_streams"   rbr_trace_host: streams the chunks rotate over, 2, 3 or 4 (default 3)
  *   "pt.wave_paths"        camera samples per path-tracer wave (default 2^23)
  *   "pt.streams"           rbr_render: waves in flight, 1 or 2 (default 2: waves alternate
  *                          between two sets of path buffers on two streams; an image that

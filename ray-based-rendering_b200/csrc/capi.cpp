@@ -143,12 +143,18 @@ void rbr_ctx_destroy(rbr_ctx* ctx) {
     release(ctx->stage_out);
     release(ctx->sort_buf);
     release(ctx->sort_buf2);
+    release(ctx->sort_more[0]);
+    release(ctx->sort_more[1]);
     if (ctx->d_error) cudaFree(ctx->d_error);
     if (ctx->d_cursors) cudaFree(ctx->d_cursors);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
     if (ctx->ev_stop) cudaEventDestroy(ctx->ev_stop);
     if (ctx->side_stream) cudaStreamDestroy(ctx->side_stream);
+    for (int i = 0; i < 2; ++i) {
+        if (ctx->host_streams[i]) cudaStreamDestroy(ctx->host_streams[i]);
+        if (ctx->host_join[i]) cudaEventDestroy(ctx->host_join[i]);
+    }
     if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
     if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
     delete ctx;
@@ -181,6 +187,9 @@ rbr_status rbr_param_set(rbr_ctx* ctx, const char* name, int64_t value) {
     } else if (n == "trace.host_chunk") {
         if (value < 0 || value > 0xFFFFFFFFll) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "trace.host_chunk is 0..2^32-1");
         ctx->trace_host_chunk = static_cast<uint32_t>(value);
+    } else if (n == "trace.host_streams") {
+        if (value < 2 || value > 4) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "trace.host_streams is 2, 3 or 4");
+        ctx->trace_host_streams = static_cast<int>(value);
     } else if (n == "pt.streams") {
         if (value != 1 && value != 2) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "pt.streams is 1 or 2");
         ctx->pt_streams = static_cast<int>(value);
@@ -248,6 +257,7 @@ rbr_status rbr_param_get(const rbr_ctx* ctx, const char* name, int64_t* value) {
     else if (n == "pt.wave_paths") *value = ctx->pt_wave_paths;
     else if (n == "pt.streams") *value = ctx->pt_streams;
     else if (n == "trace.host_chunk") *value = ctx->trace_host_chunk;
+    else if (n == "trace.host_streams") *value = ctx->trace_host_streams;
     else if (n == "bvh.record_cost_milli") *value = ctx->bvh_record_cost_milli;
     else if (n == "cache.wait_limit") *value = ctx->cache_wait_limit;
     else if (n == "cache.infer_groups") *value = ctx->cache_infer_groups;
@@ -307,34 +317,45 @@ rbr_status rbr_trace_host(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any
     if ((st = ensure(ctx, ctx->stage_in, in_bytes, "ray staging")) != RBR_OK) return st;
     if ((st = ensure(ctx, ctx->stage_out, out_bytes, "hit staging")) != RBR_OK) return st;
     cudaStream_t s = ctx->stream;
-    // Chunks alternate between two streams, so that the upload of one chunk, the traversal
-    // of another and the download of a third overlap (copies in each direction and kernels
-    // run on separate engines).
+    // Chunks rotate over `trace.host_streams` streams (upload, traversal and download of a
+    // chunk in order on its stream), so that the upload of one chunk, the traversal of another
+    // and the download of a third overlap: copies in each direction and kernels run on
+    // separate engines, and a chunk's upload waits only for the download of the chunk that
+    // used its stream before.
     const uint32_t chunk = ctx->trace_host_chunk && n > ctx->trace_host_chunk ? ctx->trace_host_chunk : n;
     const bool two = chunk < n;
+    const int ns = two ? std::max(2, std::min(4, ctx->trace_host_streams)) : 1;
     if (two && (st = ensure_side_stream(ctx)) != RBR_OK) return st;
-    const size_t osz = any_hit ? 1 : sizeof(rbr_hit);
     cudaError_t e = cudaSuccess;
+    for (int i = 0; i + 2 < ns && e == cudaSuccess; ++i) {
+        if (!ctx->host_streams[i]) e = cudaStreamCreateWithFlags(&ctx->host_streams[i], cudaStreamNonBlocking);
+        if (e == cudaSuccess && !ctx->host_join[i]) e = cudaEventCreateWithFlags(&ctx->host_join[i], cudaEventDisableTiming);
+    }
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "trace streams");
+    const cudaStream_t streams[4] = {s, ctx->side_stream, ctx->host_streams[0], ctx->host_streams[1]};
+    const cudaEvent_t joins[4] = {nullptr, ctx->ev_join, ctx->host_join[0], ctx->host_join[1]};
+    const size_t osz = any_hit ? 1 : sizeof(rbr_hit);
     if (two) {
         e = cudaEventRecord(ctx->ev_fork, s);
-        if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->side_stream, ctx->ev_fork, 0);
+        for (int i = 1; i < ns && e == cudaSuccess; ++i) e = cudaStreamWaitEvent(streams[i], ctx->ev_fork, 0);
     }
     uint32_t k = 0;
     for (uint32_t off = 0; off < n && e == cudaSuccess; off += chunk, ++k) {
         const uint32_t m = std::min(chunk, n - off);
-        const cudaStream_t cs = (k & 1) ? ctx->side_stream : s;
+        const int slot = static_cast<int>(k % static_cast<uint32_t>(ns));
+        const cudaStream_t cs = streams[slot];
         rbr_ray* din = static_cast<rbr_ray*>(ctx->stage_in.ptr) + off;
         char* dout = static_cast<char*>(ctx->stage_out.ptr) + size_t(off) * osz;
         e = cudaMemcpyAsync(din, rays + off, size_t(m) * sizeof(rbr_ray), cudaMemcpyHostToDevice, cs);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "ray upload");
-        e = launch_trace(ctx, din, m, any_hit, dout, cs, static_cast<int>(k & 1));
+        e = launch_trace(ctx, din, m, any_hit, dout, cs, slot);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "trace launch");
         e = cudaMemcpyAsync(static_cast<char*>(out) + size_t(off) * osz, dout, size_t(m) * osz, cudaMemcpyDeviceToHost, cs);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "hit download");
     }
-    if (e == cudaSuccess && two) {
-        e = cudaEventRecord(ctx->ev_join, ctx->side_stream);
-        if (e == cudaSuccess) e = cudaStreamWaitEvent(s, ctx->ev_join, 0);
+    for (int i = 1; i < ns && e == cudaSuccess; ++i) {
+        e = cudaEventRecord(joins[i], streams[i]);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(s, joins[i], 0);
     }
     if (e != cudaSuccess) return cuda_fail(ctx, e, "trace pipeline");
     return check_device_error(ctx, s);

@@ -67,7 +67,11 @@ struct rbr_ctx {
     size_t l2_persist_bytes = 0;   // the context's persisting-L2 set-aside while trace_l2_persist is on
     rbr::DevBuf sort_buf;          // keys, permutation and radix-sort scratch of trace_order 1
     rbr::DevBuf sort_buf2;         // the same for the second stream of a chunked rbr_trace_host
-    uint32_t trace_host_chunk = 1u << 20;  // rbr_trace_host: rays per pipelined chunk (0: one piece)
+    rbr::DevBuf sort_more[2];      // the same for its third and fourth streams
+    uint32_t trace_host_chunk = 1u << 19;  // rbr_trace_host: rays per pipelined chunk (0: one piece)
+    int trace_host_streams = 3;    // rbr_trace_host: streams the chunks rotate over (2-4)
+    cudaStream_t host_streams[2] = {nullptr, nullptr};  // rbr_trace_host's third and fourth streams
+    cudaEvent_t host_join[2] = {nullptr, nullptr};
     uint32_t pt_wave_paths = 1u << 23;
     int bvh_record_cost_milli = 1000;      // 8-wide collapse: record test cost / node test cost x1000
     uint32_t cache_wait_limit = 1u << 22;  // polls of a tensor-core completion wait (cache kernels)

@@ -552,6 +552,11 @@ cudaError_t launch_trace_persist(const DeviceScene& s, const rbr_ray* rays, uint
     return cudaGetLastError();
 }
 
+// The sort buffers of the streams of a chunked rbr_trace_host (slot 0: the context's stream).
+static DevBuf& sort_slot(rbr_ctx* ctx, int slot) {
+    return slot <= 0 ? ctx->sort_buf : slot == 1 ? ctx->sort_buf2 : ctx->sort_more[slot == 2 ? 0 : 1];
+}
+
 // Sorts the rays by their key of order ctx->trace_order on `stream` and returns the permutation:
 // orders 4 and 5 by the counting sort above, orders 1-3 (21- and 30-bit keys) by CUB's radix sort.
 static cudaError_t sort_rays(rbr_ctx* ctx, DevBuf& sort_buf, const rbr_ray* rays, uint32_t n, const uint32_t** perm,
@@ -610,7 +615,7 @@ cudaError_t launch_trace(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any_
                          int slot) {
     if (ctx->trace_kernel == 0 && ctx->trace_order != 0 && n > 0) {
         const uint32_t* perm = nullptr;
-        cudaError_t e = sort_rays(ctx, slot ? ctx->sort_buf2 : ctx->sort_buf, rays, n, &perm, stream);
+        cudaError_t e = sort_rays(ctx, sort_slot(ctx, slot), rays, n, &perm, stream);
         if (e != cudaSuccess) return e;
         const uint32_t blocks = (n + kTraceBlock - 1) / kTraceBlock;
         const auto* r = reinterpret_cast<const float4*>(rays);
@@ -649,7 +654,7 @@ cudaError_t launch_trace(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any_
     const bool coop = ctx->trace_kernel == 2;
     const uint32_t* perm = nullptr;  // kernel 1 refills its lanes in sorted order when trace.order is set
     if (!coop && ctx->trace_order != 0 && n > 0) {
-        cudaError_t e = sort_rays(ctx, slot ? ctx->sort_buf2 : ctx->sort_buf, rays, n, &perm, stream);
+        cudaError_t e = sort_rays(ctx, sort_slot(ctx, slot), rays, n, &perm, stream);
         if (e != cudaSuccess) return e;
     }
     const int per_sm = ctx->trace_blocks_per_sm > 0

@@ -65,22 +65,29 @@ def test_closest_and_any_match_bruteforce(kctx, restatement, ns, nt, plane, seed
 
 
 def test_chunked_host_pipeline_matches(kctx, restatement):
-    """rbr_trace_host in chunks of 500 rays over two streams (trace.host_chunk) gives the
-    answers of one piece, with a last chunk shorter than the others."""
+    """rbr_trace_host in chunks of 500 rays rotating over 2, 3 or 4 streams (trace.host_chunk,
+    trace.host_streams) gives the answers of one piece, with a last chunk shorter than the
+    others."""
     ctx = kctx
     w = scenes.random_world(400, 1500, False, seed=9)
     rays = scenes.random_test_rays(6500, seed=109)
     ctx.upload(w)
     h = restatement.scene(w)
     want = restatement.trace_closest(h, rays)
-    chunk = ctx.get_param("trace.host_chunk")
+    want_any = restatement.trace_any(h, rays)
+    chunk, streams = ctx.get_param("trace.host_chunk"), ctx.get_param("trace.host_streams")
     try:
-        for c in (500, 0):
+        for c, ns in ((500, 2), (500, 3), (500, 4), (0, 2)):
             ctx.set_param("trace.host_chunk", c)
+            ctx.set_param("trace.host_streams", ns)
             assert_same_closest(ctx.trace_host(rays), want)
-            assert np.array_equal(ctx.trace_host(rays, any_hit=True), restatement.trace_any(h, rays))
+            assert np.array_equal(ctx.trace_host(rays, any_hit=True), want_any)
+        for bad in (1, 5):
+            with pytest.raises(RbrError):
+                ctx.set_param("trace.host_streams", bad)
     finally:
         ctx.set_param("trace.host_chunk", chunk)
+        ctx.set_param("trace.host_streams", streams)
 
 
 @pytest.mark.parametrize("ns,nt,plane,seed", WORLDS)
