@@ -243,6 +243,8 @@ rbr_status rbr_scene_stats_get(const rbr_ctx* ctx, rbr_scene_stats* out);
  *                          finished lane the next ray of the warp's chunk; 2: warp-cooperative,
  *                          8 lanes per ray, one child box per lane
  *   "trace.blocks_per_sm"  resident blocks per SM of kernels 1 and 2 (0: occupancy limit)
+ *   "trace.refill_min"     kernel 1: idle lanes a warp waits for before it fetches new rays,
+ *                          1..32 (default 1: refill after every step with an idle lane)
  *   "trace.min_blocks"     kernel 0's register budget: 8, 10 or 12 resident blocks per SM
  *   "trace.order"          kernels 0 and 1: 0 traces the rays in the order given; 1..5 first sort
  *                          them on the device so that warps hold rays that walk the same nodes:

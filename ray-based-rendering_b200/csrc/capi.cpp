@@ -187,6 +187,9 @@ rbr_status rbr_param_set(rbr_ctx* ctx, const char* name, int64_t value) {
     } else if (n == "trace.host_chunk") {
         if (value < 0 || value > 0xFFFFFFFFll) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "trace.host_chunk is 0..2^32-1");
         ctx->trace_host_chunk = static_cast<uint32_t>(value);
+    } else if (n == "trace.refill_min") {
+        if (value < 1 || value > 32) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "trace.refill_min is 1..32");
+        ctx->trace_refill_min = static_cast<int>(value);
     } else if (n == "trace.host_streams") {
         if (value < 2 || value > 4) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "trace.host_streams is 2, 3 or 4");
         ctx->trace_host_streams = static_cast<int>(value);
@@ -258,6 +261,7 @@ rbr_status rbr_param_get(const rbr_ctx* ctx, const char* name, int64_t* value) {
     else if (n == "pt.streams") *value = ctx->pt_streams;
     else if (n == "trace.host_chunk") *value = ctx->trace_host_chunk;
     else if (n == "trace.host_streams") *value = ctx->trace_host_streams;
+    else if (n == "trace.refill_min") *value = ctx->trace_refill_min;
     else if (n == "bvh.record_cost_milli") *value = ctx->bvh_record_cost_milli;
     else if (n == "cache.wait_limit") *value = ctx->cache_wait_limit;
     else if (n == "cache.infer_groups") *value = ctx->cache_infer_groups;

@@ -70,6 +70,7 @@ struct rbr_ctx {
     rbr::DevBuf sort_more[2];      // the same for its third and fourth streams
     uint32_t trace_host_chunk = 1u << 19;  // rbr_trace_host: rays per pipelined chunk (0: one piece)
     int trace_host_streams = 3;    // rbr_trace_host: streams the chunks rotate over (2-4)
+    int trace_refill_min = 1;      // kernel 1: idle lanes of a warp before it fetches new rays (1-32)
     cudaStream_t host_streams[2] = {nullptr, nullptr};  // rbr_trace_host's third and fourth streams
     cudaEvent_t host_join[2] = {nullptr, nullptr};
     uint32_t pt_wave_paths = 1u << 23;
@@ -140,7 +141,8 @@ cudaError_t launch_trace_any(const DeviceScene& s, const rbr_ray* rays, uint32_t
 cudaError_t launch_trace_counts(const DeviceScene& s, const rbr_ray* rays, uint32_t n, int any_hit,
                                 unsigned long long* totals, int* err, cudaStream_t stream);
 cudaError_t launch_trace_persist(const DeviceScene& s, const rbr_ray* rays, uint32_t n, int any_hit, void* out,
-                                 int* err, uint32_t* cursor, int grid, cudaStream_t stream, const uint32_t* perm = nullptr);
+                                 int* err, uint32_t* cursor, int grid, cudaStream_t stream, const uint32_t* perm = nullptr,
+                                 uint32_t refill_min = 1);
 int trace_persist_blocks_per_sm(int any_hit);
 cudaError_t launch_trace_coop(const DeviceScene& s, const rbr_ray* rays, uint32_t n, int any_hit, void* out, int* err,
                               uint32_t* cursor, int grid, cudaStream_t stream);

@@ -299,7 +299,7 @@ template <bool kAny>
 __global__ void __launch_bounds__(kPersistBlock) k_trace_persist(DeviceScene s, const float4* __restrict__ rays,
                                                                  uint32_t n, const uint32_t* __restrict__ perm,
                                                                  uint2* __restrict__ hits, uint8_t* __restrict__ occ,
-                                                                 int* err, uint32_t* cursor) {
+                                                                 int* err, uint32_t* cursor, uint32_t refill_min) {
     const uint32_t lane = threadIdx.x & 31u;
     uint32_t chunk_next = 0, chunk_end = 0;  // warp-uniform
     bool exhausted = false;                  // warp-uniform
@@ -309,7 +309,9 @@ __global__ void __launch_bounds__(kPersistBlock) k_trace_persist(DeviceScene s, 
     uint2 stack[kStackSize];
     while (true) {
         uint32_t need = __ballot_sync(0xFFFFFFFFu, idx == 0xFFFFFFFFu);
-        while (need != 0 && !exhausted) {
+        // refill once at least refill_min lanes are idle (or all of them): a refill costs the
+        // whole warp a few ballots and a ray load, so lanes may idle for a few steps first
+        while (need != 0 && !exhausted && (static_cast<uint32_t>(__popc(need)) >= refill_min || need == 0xFFFFFFFFu)) {
             if (chunk_next == chunk_end) {
                 uint32_t b = 0;
                 if (lane == 0) b = atomicAdd(cursor, kChunk);
@@ -538,17 +540,18 @@ int trace_coop_blocks_per_sm(int any_hit) {
 }
 
 cudaError_t launch_trace_persist(const DeviceScene& s, const rbr_ray* rays, uint32_t n, int any_hit, void* out,
-                                 int* err, uint32_t* cursor, int grid, cudaStream_t stream, const uint32_t* perm) {
+                                 int* err, uint32_t* cursor, int grid, cudaStream_t stream, const uint32_t* perm,
+                                 uint32_t refill_min) {
     if (n == 0) return cudaSuccess;
     cudaError_t e = cudaMemsetAsync(cursor, 0, sizeof(uint32_t), stream);
     if (e != cudaSuccess) return e;
     const auto* r = reinterpret_cast<const float4*>(rays);
     if (any_hit)
         k_trace_persist<true><<<grid, kPersistBlock, 0, stream>>>(s, r, n, perm, nullptr, static_cast<uint8_t*>(out),
-                                                                  err, cursor);
+                                                                  err, cursor, refill_min);
     else
         k_trace_persist<false><<<grid, kPersistBlock, 0, stream>>>(s, r, n, perm, static_cast<uint2*>(out), nullptr,
-                                                                   err, cursor);
+                                                                   err, cursor, refill_min);
     return cudaGetLastError();
 }
 
@@ -665,7 +668,8 @@ cudaError_t launch_trace(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any_
     const int grid = std::max(1, std::min(ctx->num_sms * per_sm, need));
     uint32_t* cursor = ctx->d_cursors + (ctx->cursor_next++ % kCursorRing);
     if (coop) return launch_trace_coop(ctx->scene, rays, n, any_hit, out, ctx->d_error, cursor, grid, stream);
-    return launch_trace_persist(ctx->scene, rays, n, any_hit, out, ctx->d_error, cursor, grid, stream, perm);
+    return launch_trace_persist(ctx->scene, rays, n, any_hit, out, ctx->d_error, cursor, grid, stream, perm,
+                                static_cast<uint32_t>(ctx->trace_refill_min));
 }
 
 // Times every traversal variant on the caller's rays (device pointer) and keeps the fastest.
