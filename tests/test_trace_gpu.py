@@ -33,22 +33,25 @@ WORLDS = [(30, 30, False, 1), (400, 1500, False, 2), (60, 200, True, 3)]
 # cell of 512^3 or 64^3, or cell first; octahedral direction cell and origin cell of 8^3, in
 # either order)
 # (trace.kernel, trace.order, trace.node_test): the last case is the register-lean node test
-KERNELS = [(0, 0, 0), (1, 0, 0), (2, 0, 0), (0, 1, 0), (0, 2, 0), (0, 3, 0), (0, 4, 0), (0, 5, 0), (1, 4, 0),
-           (0, 5, 1)]
+# (trace.kernel, trace.order, trace.node_test, trace.refill_min)
+KERNELS = [(0, 0, 0, 1), (1, 0, 0, 1), (2, 0, 0, 1), (0, 1, 0, 1), (0, 2, 0, 1), (0, 3, 0, 1), (0, 4, 0, 1),
+           (0, 5, 0, 1), (1, 4, 0, 1), (0, 5, 1, 1), (1, 5, 0, 12)]
 
 
 @pytest.fixture(params=KERNELS, ids=["kernel0", "kernel1", "kernel2", "kernel0-sorted", "kernel0-sorted64",
                                      "kernel0-cellfirst", "kernel0-dirfirst", "kernel0-originfirst",
-                                     "kernel1-dirfirst", "kernel0-originfirst-lean"])
+                                     "kernel1-dirfirst", "kernel0-originfirst-lean", "kernel1-originfirst-refill12"])
 def kctx(ctx, request):
     """The shared context with each traversal variant in turn."""
     ctx.set_param("trace.kernel", request.param[0])
     ctx.set_param("trace.order", request.param[1])
     ctx.set_param("trace.node_test", request.param[2])
+    ctx.set_param("trace.refill_min", request.param[3])
     yield ctx
     ctx.set_param("trace.kernel", 0)
     ctx.set_param("trace.order", 0)
     ctx.set_param("trace.node_test", 0)
+    ctx.set_param("trace.refill_min", 1)
 
 
 @pytest.mark.parametrize("ns,nt,plane,seed", WORLDS)
