@@ -359,6 +359,158 @@ __global__ void __launch_bounds__(128, 4)
 }
 
 // --------------------------------------------------------------------------------------------
+// Inference with eight warps per 128-sample tile: thread t and thread t + 128 share row t & 127.
+// The first half encodes hash levels 0-7 (features 0-15), the second levels 8-15 and the other
+// 32 features; in the epilogues warp w reads the accumulator lanes of quarter w % 4 and the
+// column half w / 4. A thread then holds half the values of the four-warp kernel, so four CTAs
+// of 256 threads fit an SM (twice the warps to hide the hash-grid gathers), and each thread
+// issues half the gathers. Same arithmetic per feature, so the same results as k_rc_infer.
+// --------------------------------------------------------------------------------------------
+// Part `part` (0 or 1) of the encoding of `rec`, written into row `row` of the A operand.
+__device__ __forceinline__ void encode_part(const CacheDev& c, const float4* rec, uint8_t* act, uint32_t rg,
+                                            uint32_t row, uint32_t part) {
+    const float4 r0 = __ldg(rec);
+    float p[3];
+    unit_position(c, r0, p);
+#pragma unroll 1
+    for (int q = 0; q < 2; ++q) {
+        float v[8];
+#pragma unroll
+        for (int ll = 0; ll < 4; ++ll) {
+            const int l = 8 * static_cast<int>(part) + 4 * q + ll;
+            uint32_t i[3];
+            float w[3];
+            level_cell(c, l, p, i, w);
+            const __half2* tab = c.grid + (static_cast<size_t>(l) << c.log2_table);
+            float f0 = 0.0f, f1 = 0.0f;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const float wt = corner_weight(w, k);
+                const float2 g = __half22float2(__ldg(tab + corner_index(c, l, i, k)));
+                f0 = fa(f0, fm(wt, g.x));
+                f1 = fa(f1, fm(wt, g.y));
+            }
+            v[2 * ll] = f0;
+            v[2 * ll + 1] = f1;
+        }
+        store_row(act, rg, row, 16 * part + 8 * q, v, 1);
+    }
+    if (part == 0) return;
+    const float4 r1 = __ldg(rec + 1), r2 = __ldg(rec + 2), r3 = __ldg(rec + 3);
+    float v[32];
+    const float d[3] = {r0.w, r1.x, r1.y};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float t = fm(fa(d[a], 1.0f), 2.0f);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) v[5 * a + k] = fmaxf(0.0f, fs(1.0f, fabsf(fs(t, static_cast<float>(k)))));
+    }
+    v[15] = r1.z;
+    v[16] = r1.w;
+    v[17] = r2.x;
+    v[18] = r2.y;
+    v[19] = r2.z;
+    v[20] = r2.w;
+    v[21] = r3.x;
+    v[22] = r3.y;
+    v[23] = r3.z;
+    v[24] = r3.w;
+    v[25] = 1.0f;
+#pragma unroll
+    for (int k = 26; k < 32; ++k) v[k] = 0.0f;
+    store_row(act, rg, row, 32, v, 4);
+}
+
+__global__ void __launch_bounds__(256, 4)
+    k_rc_infer8(CacheDev c, const float4* records, uint32_t n, const uint32_t* n_ptr, InferOut o, int* err) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint8_t* ws = smem;
+    uint8_t* act = smem + kWBytes;
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + kWBytes + kActBytesInfer);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + kWBytes + kActBytesInfer + 8);
+    const uint32_t count = n_ptr ? min(*n_ptr, n) : n;
+    const uint32_t tiles = (count + kRcTile - 1) / kRcTile;
+    if (blockIdx.x >= tiles) return;
+    const uint32_t tid = threadIdx.x, warp = tid >> 5;
+    const uint32_t row = tid & 127u, part = tid >> 7;  // part: encoding half and column half
+    if (tid == 0) tc::mbar_init(mbar, 1);
+    load_weights(c.w, ws);
+    if (warp == 0) {
+        tc::tmem_alloc(tslot, kTmemInfer);
+        tc::tmem_relinquish();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tm = *tslot;
+    const uint32_t tl = tm + (((warp & 3u) * 32u) << 16) + 32u * part;  // lane quarter, column half
+    const uint32_t act_s = tc::smem_addr(act), w_s = tc::smem_addr(ws);
+    uint32_t phase = 0;
+    bool ok = true;
+    for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+        const uint32_t j = tile * kRcTile + row;
+        const bool valid = j < count;
+        if (valid) {
+            encode_part(c, records + 4 * static_cast<size_t>(j), act, kActRgInfer, row, part);
+        } else {
+            float z[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) z[k] = 0.0f;
+            for (uint32_t q = 2 * part; q < (part ? 8u : 2u); ++q) store_row(act, kActRgInfer, row, 8 * q, z, 1);
+        }
+        float y[16];
+        for (int l = 0; l < 5 && ok; ++l) {
+            publish();
+            if (tid == 0) {
+                tc::fence_after_sync();
+                const uint32_t id = tc::idesc_bf16(128, l < 4 ? 64 : 16, 0, 0);
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    tc::mma_bf16(tm, tc::sdesc(act_s + k * 256, 128, kActRgInfer),
+                                 tc::sdesc(w_s + l * 8192 + k * 256, 128, 1024), id, k > 0);
+                tc::mma_commit(mbar);
+            }
+            ok = wait_mma(mbar, phase, err, c.wait_limit);
+            if (!ok) break;
+            tc::fence_after_sync();
+            if (l < 4) {
+                float z[32];
+                tc::tmem_ld16(tl, z);
+                tc::tmem_ld16(tl + 16, z + 16);
+#pragma unroll
+                for (int k = 0; k < 32; ++k) z[k] = fmaxf(z[k], 0.0f);
+                store_row(act, kActRgInfer, row, 32 * part, z, 4);
+            } else if (part == 0) {
+                tc::tmem_ld16(tl, y);
+            }
+        }
+        if (ok && valid && part == 0) {
+            const float r = fmaxf(y[0], 0.0f), g = fmaxf(y[1], 0.0f), b = fmaxf(y[2], 0.0f);
+            if (o.rgb) {
+                o.rgb[3 * static_cast<size_t>(j)] = r;
+                o.rgb[3 * static_cast<size_t>(j) + 1] = g;
+                o.rgb[3 * static_cast<size_t>(j) + 2] = b;
+            } else {
+                const float4 q = o.q_info[j];
+                float4* L = o.path_rad + __float_as_uint(q.w);
+                float4 v = *L;
+                v.x = fa(v.x, fm(q.x, r));
+                v.y = fa(v.y, fm(q.y, g));
+                v.z = fa(v.z, fm(q.z, b));
+                *L = v;
+            }
+        }
+    }
+    if (!ok) tc::mbar_wait(mbar, phase ^ 1u);  // let an overdue MMA drain before freeing TMEM
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        tc::fence_after_sync();
+        tc::tmem_dealloc(tm, kTmemInfer);
+    }
+}
+
+// --------------------------------------------------------------------------------------------
 // Inference with several tiles in flight per CTA: G groups of 128 threads (four warps) each own
 // a 128-sample tile and run its chain (encode, five layers of MMA, commit, wait, epilogue)
 // independently of the other groups, with a named barrier per group instead of the CTA
@@ -931,6 +1083,8 @@ cudaError_t set_kernel_attributes(int device) {
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_rc_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemInfer);
     if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_rc_infer8, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemInfer);
+    if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_rc_infer_groups<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  smem_infer_groups(2));
     if (e == cudaSuccess)
@@ -1243,7 +1397,8 @@ cudaError_t cache_launch_infer(rbr_ctx* ctx, const float4* records, uint32_t n, 
         return cudaGetLastError();
     }
     const uint32_t grid = std::max(1u, std::min<uint32_t>(tiles, ctx->num_sms * 4));
-    k_rc_infer<<<grid, 128, kSmemInfer, stream>>>(dev, records, n, n_ptr, o, ctx->d_error);
+    if (ctx->cache_infer_warps == 8) k_rc_infer8<<<grid, 256, kSmemInfer, stream>>>(dev, records, n, n_ptr, o, ctx->d_error);
+    else k_rc_infer<<<grid, 128, kSmemInfer, stream>>>(dev, records, n, n_ptr, o, ctx->d_error);
     return cudaGetLastError();
 }
 

@@ -224,6 +224,9 @@ rbr_status rbr_param_set(rbr_ctx* ctx, const char* name, int64_t value) {
     } else if (n == "pt.shade_split") {
         if (value != 0 && value != 1) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "pt.shade_split is 0 or 1");
         ctx->pt_shade_split = static_cast<int>(value);
+    } else if (n == "cache.infer_warps") {
+        if (value != 4 && value != 8) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "cache.infer_warps is 4 or 8");
+        ctx->cache_infer_warps = static_cast<int>(value);
     } else if (n == "cache.infer_groups") {
         if (value != 1 && value != 2 && value != 4) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "cache.infer_groups is 1, 2 or 4");
         ctx->cache_infer_groups = static_cast<int>(value);
@@ -265,6 +268,7 @@ rbr_status rbr_param_get(const rbr_ctx* ctx, const char* name, int64_t* value) {
     else if (n == "bvh.record_cost_milli") *value = ctx->bvh_record_cost_milli;
     else if (n == "cache.wait_limit") *value = ctx->cache_wait_limit;
     else if (n == "cache.infer_groups") *value = ctx->cache_infer_groups;
+    else if (n == "cache.infer_warps") *value = ctx->cache_infer_warps;
     else if (n == "pt.shade_split") *value = ctx->pt_shade_split;
     else if (n == "trace.stream_io") *value = ctx->trace_stream_io;
     else if (n == "trace.node_test") *value = ctx->trace_node_test;

@@ -77,6 +77,7 @@ struct rbr_ctx {
     int bvh_record_cost_milli = 1000;      // 8-wide collapse: record test cost / node test cost x1000
     uint32_t cache_wait_limit = 1u << 22;  // polls of a tensor-core completion wait (cache kernels)
     int cache_infer_groups = 1;            // tiles in flight per inference CTA: 1, 2 or 4
+    int cache_infer_warps = 4;             // warps per tile of the one-tile inference kernel: 4 or 8
     uint32_t fail_alloc_countdown = 0;     // > 0: the n-th next device allocation fails (fault injection)
     // path tracer
     rbr::PathBuffers pt;

@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 import radiance_cache as rc
-from rbr_b200 import Context
+from rbr_b200 import Context, RbrError
 
 pytestmark = pytest.mark.gpu
 
@@ -175,3 +175,22 @@ def test_grouped_inference_equals_one_tile_per_cta(cctx, groups):
     finally:
         cctx.set_param("cache.infer_groups", 1)
     assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+def test_eight_warp_inference_equals_four_warp(cctx):
+    """cache.infer_warps 8: two threads per sample row (hash levels 0-7, and levels 8-15 with the
+    other inputs; the epilogues split by accumulator column half) feed the same operands to the
+    same MMA sequence as four warps, so the predictions are the same bits; a ragged last tile
+    and more tiles than the grid holds at once are covered."""
+    _, rng = make_cache(cctx, 11)
+    recs = random_records(rng, 150_000)
+    cctx.set_param("cache.infer_warps", 4)
+    want = cctx.cache_infer(recs)
+    cctx.set_param("cache.infer_warps", 8)
+    try:
+        got = cctx.cache_infer(recs)
+    finally:
+        cctx.set_param("cache.infer_warps", 4)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    with pytest.raises(RbrError):
+        cctx.set_param("cache.infer_warps", 6)
