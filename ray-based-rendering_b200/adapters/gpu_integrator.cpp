@@ -86,7 +86,7 @@ void GpuPathIntegrator::render(const Scene& scene, const Camera& camera, Film& f
     p.use_nee = config.useNEE ? 1 : 0;
     p.use_mis = config.useMIS ? 1 : 0;
     p.seed = seed_;
-    p.flags = volumetric_ ? RBR_RENDER_VOLUMETRIC : 0u;
+    p.flags = volumetric_ ? static_cast<uint32_t>(RBR_RENDER_VOLUMETRIC) : 0u;
     std::vector<float> mean(static_cast<size_t>(film.width) * film.height * 3);
     status_ = rbr_render_host(ctx_, &cam, &p, mean.data(), nullptr);
     if (status_ != RBR_OK) {
