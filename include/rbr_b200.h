@@ -255,7 +255,8 @@ rbr_status rbr_scene_stats_get(const rbr_ctx* ctx, rbr_scene_stats* out);
  *                          1-3 (21- and 30-bit keys) CUB's radix sort
  *   "trace.host_chunk"     rbr_trace_host: rays per chunk of its upload / trace / download
  *                          pipeline (default 2^19; 0: one piece)
- *   "trace.host_streams"   rbr_trace_host: streams the chunks rotate over, 2, 3 or 4 (default 3)
+ *   "trace.host_streams"   rbr_trace_host: streams the chunks rotate over, 2, 3 or 4 (default 4);
+ *                          the last full chunk is split into halving pieces (shorter tail)
  *   "pt.wave_paths"        camera samples per path-tracer wave (default 2^23)
  *   "pt.streams"           rbr_render: waves in flight, 1 or 2 (default 2: waves alternate
  *                          between two sets of path buffers on two streams; an image that
@@ -523,6 +524,11 @@ rbr_status rbr_batch_add_scene_variant(rbr_batch* batch, uint32_t base_scene, co
 rbr_status rbr_batch_cache_create(rbr_batch* batch, uint32_t scene_id, const rbr_cache_config* config);
 /* Queues a request; it is rendered by the next rbr_batch_run. */
 rbr_status rbr_batch_submit(rbr_batch* batch, const rbr_request* request, uint32_t* request_id);
+/* Optional, for a queued request: the next rbr_batch_run also copies its film to `host_film`
+ * (width*height*3 floats; page-locked memory for the copy to run asynchronously) on the stream
+ * of its last wave, right after that wave, so the copy overlaps the waves after it. The copy is
+ * complete when the stream given to rbr_batch_run is. */
+rbr_status rbr_batch_set_host_film(rbr_batch* batch, uint32_t request_id, float* host_film);
 /* Renders every queued request (asynchronous on `stream`); the queue is then empty. */
 rbr_status rbr_batch_run(rbr_batch* batch, void* stream);
 /* Per-request and whole-run timings of the last run (wait for it). */

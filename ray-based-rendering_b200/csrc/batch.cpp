@@ -39,6 +39,7 @@ constexpr uint64_t kMaxArrivalUs = 600000000ull;        // 10 minutes
 
 struct Req {
     rbr_request r{};
+    float* host_film = nullptr;  // rbr_batch_set_host_film: copied there after the last wave
     uint32_t id = 0;
     uint32_t first_wave = 0, last_wave = 0, waves = 0, segments = 0;
     uint64_t paths = 0;
@@ -55,6 +56,8 @@ struct WavePlan {
 };
 
 using GraphKey = std::tuple<uint32_t, int, uint32_t, int, bool, uint32_t, int>;  // scene, mode, depth, grid, train, capacity, slot
+
+size_t film_bytes(const rbr_request& r) { return size_t(r.camera.width) * size_t(r.camera.height) * 3 * sizeof(float); }
 
 }  // namespace
 
@@ -346,6 +349,9 @@ rbr_status run(rbr_batch* b, std::vector<Req>& reqs, cudaStream_t stream) {
             e = launch_wave_loop(eng, b->scenes, static_cast<const LoopWave*>(b->d_loop), static_cast<uint32_t>(waves.size()),
                                  static_cast<const char*>(b->d_loop) + list_bytes, b->d_stamps, b->d_bar, limit_ns, slots,
                                  stream, &loop_grid);
+        for (const Req& q : reqs)
+            if (e == cudaSuccess && q.host_film)
+                e = cudaMemcpyAsync(q.host_film, q.r.film, film_bytes(q.r), cudaMemcpyDeviceToHost, stream);
         if (e == cudaSuccess) e = cudaEventRecord(b->events[waves.size() + 1], stream);
         if (e != cudaSuccess) return bcuda(b, e, "persistent wave loop");
         s.waves = static_cast<uint32_t>(waves.size());
@@ -369,6 +375,11 @@ rbr_status run(rbr_batch* b, std::vector<Req>& reqs, cudaStream_t stream) {
     if (e == cudaSuccess && slots == 2) e = cudaEventRecord(b->ev_fork, stream);
     if (e == cudaSuccess && slots == 2) e = cudaStreamWaitEvent(b->side, b->ev_fork, 0);
     bool cache_wave = false;
+    // requests whose film goes to the host, by their last wave: the copy follows that wave on
+    // its stream and overlaps the waves after it
+    std::vector<std::vector<const Req*>> to_host(waves.size());
+    for (const Req& q : reqs)
+        if (q.host_film && q.waves > 0) to_host[q.last_wave].push_back(&q);
     for (size_t wi = 0; wi < waves.size() && e == cudaSuccess; ++wi) {
         const WavePlan& w = waves[wi];
         rbr_ctx* scn = b->scenes[w.scene];
@@ -431,6 +442,12 @@ rbr_status run(rbr_batch* b, std::vector<Req>& reqs, cudaStream_t stream) {
         }
         if (e == cudaSuccess) e = launch_stamp(b->d_stamps + 1 + wi, ws);
         ++s.kernel_launches;
+        for (const Req* q : to_host[wi]) {
+            // a request spread over several waves also has pixels from waves of the other slot:
+            // wait for that stream's last wave before this one (it holds every earlier one)
+            if (e == cudaSuccess && slots == 2 && q->first_wave < wi) e = cudaStreamWaitEvent(ws, b->events[wi], 0);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(q->host_film, q->r.film, film_bytes(q->r), cudaMemcpyDeviceToHost, ws);
+        }
         if (e == cudaSuccess) e = cudaEventRecord(b->events[wi + 1], ws);
         if (e == cudaSuccess && w.mode == 1 && slots == 2) {
             e = cudaEventRecord(b->ev_cache, ws);
@@ -572,6 +589,16 @@ rbr_status rbr_batch_submit(rbr_batch* b, const rbr_request* r, uint32_t* reques
     b->pending.push_back(q);
     if (request_id) *request_id = q.id;
     return RBR_OK;
+}
+
+rbr_status rbr_batch_set_host_film(rbr_batch* b, uint32_t request_id, float* host_film) {
+    if (!b) return RBR_ERR_INVALID_ARGUMENT;
+    for (Req& q : b->pending)
+        if (q.id == request_id) {
+            q.host_film = host_film;
+            return RBR_OK;
+        }
+    return bfail(b, RBR_ERR_INVALID_ARGUMENT, "request not queued (rbr_batch_set_host_film before rbr_batch_run)");
 }
 
 rbr_status rbr_batch_run(rbr_batch* b, void* stream) {

@@ -348,8 +348,13 @@ rbr_status rbr_trace_host(rbr_ctx* ctx, const rbr_ray* rays, uint32_t n, int any
         for (int i = 1; i < ns && e == cudaSuccess; ++i) e = cudaStreamWaitEvent(streams[i], ctx->ev_fork, 0);
     }
     uint32_t k = 0;
-    for (uint32_t off = 0; off < n && e == cudaSuccess; off += chunk, ++k) {
-        const uint32_t m = std::min(chunk, n - off);
+    // The last chunk's traversal and download run after the last upload, so the rays of the
+    // last full chunk are split into halving pieces (down to a quarter chunk): a shorter tail.
+    const uint32_t min_piece = std::max(1u, chunk / 4);
+    uint32_t m = 0;
+    for (uint32_t off = 0; off < n && e == cudaSuccess; off += m, ++k) {
+        const uint32_t rest = n - off;
+        m = !two || rest > chunk ? std::min(chunk, rest) : rest > min_piece ? rest - rest / 2 : rest;
         const int slot = static_cast<int>(k % static_cast<uint32_t>(ns));
         const cudaStream_t cs = streams[slot];
         rbr_ray* din = static_cast<rbr_ray*>(ctx->stage_in.ptr) + off;

@@ -69,7 +69,7 @@ struct rbr_ctx {
     rbr::DevBuf sort_buf2;         // the same for the second stream of a chunked rbr_trace_host
     rbr::DevBuf sort_more[2];      // the same for its third and fourth streams
     uint32_t trace_host_chunk = 1u << 19;  // rbr_trace_host: rays per pipelined chunk (0: one piece)
-    int trace_host_streams = 3;    // rbr_trace_host: streams the chunks rotate over (2-4)
+    int trace_host_streams = 4;    // rbr_trace_host: streams the chunks rotate over (2-4)
     int trace_refill_min = 1;      // kernel 1: idle lanes of a warp before it fetches new rays (1-32)
     cudaStream_t host_streams[2] = {nullptr, nullptr};  // rbr_trace_host's third and fourth streams
     cudaEvent_t host_join[2] = {nullptr, nullptr};

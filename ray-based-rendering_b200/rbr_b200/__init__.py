@@ -103,6 +103,7 @@ def load_library() -> C.CDLL:
                                                   C.POINTER(C.c_uint32)]),
         "rbr_batch_submit": (C.c_int, [P, C.POINTER(abi.rbr_request), C.POINTER(C.c_uint32)]),
         "rbr_batch_run": (C.c_int, [P, P]),
+        "rbr_batch_set_host_film": (C.c_int, [P, C.c_uint32, P]),
         "rbr_batch_request_stats": (C.c_int, [P, C.c_uint32, C.POINTER(abi.rbr_request_stats)]),
         "rbr_batch_stats_get": (C.c_int, [P, C.POINTER(abi.rbr_batch_stats)]),
         "rbr_batch_autotune": (C.c_int, [P, P]),
@@ -486,6 +487,11 @@ class Batch:
         rid = C.c_uint32()
         self._check(self.lib.rbr_batch_submit(self.h, C.byref(r), C.byref(rid)))
         return int(rid.value)
+
+    def set_host_film(self, rid: int, host_ptr: int):
+        """The next run also copies request `rid`'s film to host memory at `host_ptr` (page-locked
+        for an asynchronous copy) right after the request's last wave."""
+        self._check(self.lib.rbr_batch_set_host_film(self.h, rid, C.c_void_p(host_ptr)))
 
     def run(self, stream: int = 0):
         self._check(self.lib.rbr_batch_run(self.h, C.c_void_p(stream)))

@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 import torch
 
-from rbr_b200 import Batch, Context, abi, render_params, scenes
+from rbr_b200 import Batch, Context, RbrError, abi, render_params, scenes
 
 pytestmark = pytest.mark.gpu
 
@@ -229,3 +229,53 @@ def test_persistent_barrier_wait_runs_out_and_recovers(bctx):
                                atol=2e-6)
     b.close()
 
+
+
+@pytest.mark.parametrize("cfg", [dict(), dict(wave_paths=1000), dict(persistent=1)],
+                         ids=["graphs", "split-requests", "persistent"])
+def test_host_films_arrive_after_the_run(bctx, cfg):
+    """rbr_batch_set_host_film: the run copies each registered request's film to its
+    page-locked host buffer after the request's last wave; the host copy equals the device
+    film, requests without a host buffer are untouched, and an unknown request id is rejected."""
+    b = Batch(bctx, **cfg)
+    ids = {key: b.add_scene(fn(16, 16)) for key, fn in build_scenes().items()}
+    films, hosts, rids = [], [], []
+    for i, (key, w, h, p) in enumerate(requests()):
+        cam = build_scenes()[key](w, h).camera
+        f = torch.zeros(w * h * 3, device="cuda")
+        films.append(f)
+        rid = b.submit(ids[key], cam, p, f.data_ptr())
+        rids.append(rid)
+        if i % 2 == 0:  # every other request gets a host buffer
+            hb = torch.full((w * h * 3,), -1.0).pin_memory()
+            b.set_host_film(rid, hb.data_ptr())
+            hosts.append(hb)
+        else:
+            hosts.append(None)
+    with pytest.raises(RbrError):
+        b.set_host_film(max(rids) + 100, hosts[0].data_ptr())
+    b.run()
+    torch.cuda.synchronize()
+    for f, hb in zip(films, hosts):
+        if hb is not None:
+            assert torch.equal(hb, f.cpu())
+    b.close()
+
+
+def test_host_film_of_a_request_over_many_waves(bctx):
+    """A request spread over many waves on both stream slots: its host copy waits for the waves
+    of the other slot too, so it equals the device film (and a single render)."""
+    b = Batch(bctx, wave_paths=1 << 15)
+    sid = b.add_scene(cornell(16, 16))
+    w, h, p = 192, 160, render_params(spp=8, max_depth=8, seed=21)
+    cam = cornell(w, h).camera
+    f = torch.zeros(w * h * 3, device="cuda")
+    rid = b.submit(sid, cam, p, f.data_ptr())
+    hb = torch.full((w * h * 3,), -1.0).pin_memory()
+    b.set_host_film(rid, hb.data_ptr())
+    b.run()
+    torch.cuda.synchronize()
+    assert b.request_stats(rid).waves >= 6
+    assert torch.equal(hb, f.cpu())
+    np.testing.assert_allclose(hb.numpy().reshape(h, w, 3), alone(bctx, "cornell", w, h, p), rtol=2e-5, atol=2e-6)
+    b.close()
