@@ -93,6 +93,35 @@ def test_chunked_host_pipeline_matches(kctx, restatement):
         ctx.set_param("trace.host_streams", streams)
 
 
+def test_sorted_queries_with_few_distinct_keys(ctx, restatement):
+    """The counting sort of orders 4 and 5 with heavily repeated keys: rays from one point into a
+    narrow cone (one origin cell, one or two direction cells), plus rays whose origins lie far
+    outside the scene box (clamped into the boundary cells). Whole warps share a key and take
+    their slots from one aggregated atomic; the answers equal brute force."""
+    w = scenes.random_world(400, 1500, False, seed=31)
+    ctx.upload(w)
+    h = restatement.scene(w)
+    rng = np.random.default_rng(131)
+    n = 70_000
+    o = np.tile(np.array([[0.5, 0.3, 13.0]], np.float32), (n, 1))
+    o[n // 2:, 0] = 1e6  # far outside the box in x
+    d = np.stack([rng.uniform(-0.02, 0.02, n), rng.uniform(-0.02, 0.02, n), -np.ones(n)], 1).astype(np.float32)
+    d[n // 2:] = np.array([-1.0, 0.0, 0.0], np.float32)
+    rays = abi.make_rays(o, d)
+    want = restatement.trace_closest(h, rays)
+    want_any = restatement.trace_any(h, rays)
+    try:
+        for order, lean in ((4, 0), (5, 0), (5, 1)):
+            ctx.set_param("trace.kernel", 0)
+            ctx.set_param("trace.order", order)
+            ctx.set_param("trace.node_test", lean)
+            assert_same_closest(ctx.trace_host(rays), want)
+            assert np.array_equal(ctx.trace_host(rays, any_hit=True), want_any)
+    finally:
+        ctx.set_param("trace.order", 0)
+        ctx.set_param("trace.node_test", 0)
+
+
 @pytest.mark.parametrize("ns,nt,plane,seed", WORLDS)
 def test_matches_reference_bvh_and_bruteforce(ctx, reference, ns, nt, plane, seed):
     """The same worlds through the reference library itself: its brute-force loop and its BVH."""
