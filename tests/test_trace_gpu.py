@@ -95,18 +95,19 @@ def test_chunked_host_pipeline_matches(kctx, restatement):
 
 def test_sorted_queries_with_few_distinct_keys(ctx, restatement):
     """The counting sort of orders 4 and 5 with heavily repeated keys: rays from one point into a
-    narrow cone (one origin cell, one or two direction cells), plus rays whose origins lie far
-    outside the scene box (clamped into the boundary cells). Whole warps share a key and take
-    their slots from one aggregated atomic; the answers equal brute force."""
+    narrow cone from outside the scene box (one boundary origin cell, one or two direction cells),
+    from two such points. Whole warps share a key and take their slots from one aggregated
+    atomic; the answers equal brute force."""
     w = scenes.random_world(400, 1500, False, seed=31)
     ctx.upload(w)
     h = restatement.scene(w)
     rng = np.random.default_rng(131)
     n = 70_000
     o = np.tile(np.array([[0.5, 0.3, 13.0]], np.float32), (n, 1))
-    o[n // 2:, 0] = 1e6  # far outside the box in x
     d = np.stack([rng.uniform(-0.02, 0.02, n), rng.uniform(-0.02, 0.02, n), -np.ones(n)], 1).astype(np.float32)
-    d[n // 2:] = np.array([-1.0, 0.0, 0.0], np.float32)
+    # the second half from beside the box in x (the world spans about +-11.4), towards -x
+    o[n // 2:] = np.array([14.0, 0.3, 0.5], np.float32)
+    d[n // 2:] = np.stack([-np.ones(n - n // 2), d[n // 2:, 0], d[n // 2:, 1]], 1)
     rays = abi.make_rays(o, d)
     want = restatement.trace_closest(h, rays)
     want_any = restatement.trace_any(h, rays)
