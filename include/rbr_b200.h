@@ -273,6 +273,9 @@ rbr_status rbr_scene_stats_get(const rbr_ctx* ctx, rbr_scene_stats* out);
  *                          launch for all classes (default)
  *   "cache.infer_groups"   radiance-cache inference: 128-sample tiles in flight per CTA, 1, 2 or 4
  *                          (groups of four warps sharing one copy of the weights; default 1)
+ *   "cache.infer_warps"    one-tile inference: 4 or 8 warps per 128-sample tile (default 4)
+ *   "cache.sort_queries"   1: inference serves the queries in spatial order (a counting sort of
+ *                          their cells on a 32^3 grid); 0: in the order given (default 0)
  *   "cache.wait_limit"     polls of a tensor-core completion wait in the radiance-cache kernels
  *                          before it gives up with RBR_ERR_DEVICE_TIMEOUT (default 2^22; 0
  *                          makes every such wait give up at once, which tests the error path:

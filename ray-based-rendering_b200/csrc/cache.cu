@@ -34,6 +34,7 @@
 #include "rbr_bsdf.cuh"
 #include "rbr_cache.h"
 #include "rbr_context.h"
+#include "rbr_sort.cuh"
 #include "rbr_tc.cuh"
 
 namespace rbr {
@@ -269,6 +270,7 @@ struct InferOut {
     float* rgb;
     float4* path_rad;
     const float4* q_info;  // throughput rgb, path index bits
+    const uint32_t* perm;  // optional: tile slot j serves query perm[j] (queries sorted by cell)
 };
 
 __global__ void __launch_bounds__(128, 4)
@@ -299,9 +301,10 @@ __global__ void __launch_bounds__(128, 4)
     for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
         const uint32_t j = tile * kRcTile + tid;
         const bool valid = j < count;
+        const uint32_t src = valid && o.perm ? __ldg(o.perm + j) : j;  // the query this slot serves
         {
             float in[64];
-            if (valid) encode(c, records + 4 * static_cast<size_t>(j), in);
+            if (valid) encode(c, records + 4 * static_cast<size_t>(src), in);
             else
 #pragma unroll
                 for (int k = 0; k < 64; ++k) in[k] = 0.0f;
@@ -335,11 +338,11 @@ __global__ void __launch_bounds__(128, 4)
         if (ok && valid) {
             const float r = fmaxf(y[0], 0.0f), g = fmaxf(y[1], 0.0f), b = fmaxf(y[2], 0.0f);
             if (o.rgb) {
-                o.rgb[3 * static_cast<size_t>(j)] = r;
-                o.rgb[3 * static_cast<size_t>(j) + 1] = g;
-                o.rgb[3 * static_cast<size_t>(j) + 2] = b;
+                o.rgb[3 * static_cast<size_t>(src)] = r;
+                o.rgb[3 * static_cast<size_t>(src) + 1] = g;
+                o.rgb[3 * static_cast<size_t>(src) + 2] = b;
             } else {
-                const float4 q = o.q_info[j];
+                const float4 q = o.q_info[src];
                 float4* L = o.path_rad + __float_as_uint(q.w);
                 float4 v = *L;
                 v.x = fa(v.x, fm(q.x, r));
@@ -450,8 +453,9 @@ __global__ void __launch_bounds__(256, 4)
     for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
         const uint32_t j = tile * kRcTile + row;
         const bool valid = j < count;
+        const uint32_t src = valid && o.perm ? __ldg(o.perm + j) : j;  // the query this slot serves
         if (valid) {
-            encode_part(c, records + 4 * static_cast<size_t>(j), act, kActRgInfer, row, part);
+            encode_part(c, records + 4 * static_cast<size_t>(src), act, kActRgInfer, row, part);
         } else {
             float z[8];
 #pragma unroll
@@ -487,11 +491,11 @@ __global__ void __launch_bounds__(256, 4)
         if (ok && valid && part == 0) {
             const float r = fmaxf(y[0], 0.0f), g = fmaxf(y[1], 0.0f), b = fmaxf(y[2], 0.0f);
             if (o.rgb) {
-                o.rgb[3 * static_cast<size_t>(j)] = r;
-                o.rgb[3 * static_cast<size_t>(j) + 1] = g;
-                o.rgb[3 * static_cast<size_t>(j) + 2] = b;
+                o.rgb[3 * static_cast<size_t>(src)] = r;
+                o.rgb[3 * static_cast<size_t>(src) + 1] = g;
+                o.rgb[3 * static_cast<size_t>(src) + 2] = b;
             } else {
-                const float4 q = o.q_info[j];
+                const float4 q = o.q_info[src];
                 float4* L = o.path_rad + __float_as_uint(q.w);
                 float4 v = *L;
                 v.x = fa(v.x, fm(q.x, r));
@@ -618,8 +622,9 @@ __global__ void __launch_bounds__(128 * G, 8 / G)
     for (uint32_t tile = blockIdx.x * G + g; tile < tiles && ok; tile += gridDim.x * G) {
         const uint32_t j = tile * kRcTile + lt;
         const bool valid = j < count;
+        const uint32_t src = valid && o.perm ? __ldg(o.perm + j) : j;  // the query this slot serves
         if (valid) {
-            encode_row(c, records + 4 * static_cast<size_t>(j), act, kActRgInfer, lt);
+            encode_row(c, records + 4 * static_cast<size_t>(src), act, kActRgInfer, lt);
         } else {
             float z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
@@ -663,11 +668,11 @@ __global__ void __launch_bounds__(128 * G, 8 / G)
         if (ok && valid) {
             const float r = fmaxf(y[0], 0.0f), gg = fmaxf(y[1], 0.0f), b = fmaxf(y[2], 0.0f);
             if (o.rgb) {
-                o.rgb[3 * static_cast<size_t>(j)] = r;
-                o.rgb[3 * static_cast<size_t>(j) + 1] = gg;
-                o.rgb[3 * static_cast<size_t>(j) + 2] = b;
+                o.rgb[3 * static_cast<size_t>(src)] = r;
+                o.rgb[3 * static_cast<size_t>(src) + 1] = gg;
+                o.rgb[3 * static_cast<size_t>(src) + 2] = b;
             } else {
-                const float4 qi = o.q_info[j];
+                const float4 qi = o.q_info[src];
                 float4* L = o.path_rad + __float_as_uint(qi.w);
                 float4 v = *L;
                 v.x = fa(v.x, fm(qi.x, r));
@@ -1127,6 +1132,7 @@ void cache_destroy(rbr_ctx* ctx) {
     CacheState& cs = ctx->cache;
     free_cache_params(cs);
     free_dev(cs.q_rec);  // render buffers (queries, training vertices)
+    free_dev(cs.q_sort);
     free_dev(cs.q_info);
     free_dev(cs.t_rec);
     free_dev(cs.t_aux);
@@ -1378,16 +1384,76 @@ rbr_status cache_encode_host(rbr_ctx* ctx, uint32_t n, const rbr_cache_record* r
     return RBR_OK;
 }
 
+// Spatial order of the queries (cache.sort_queries): key = Morton code of the query's cell on
+// a 32^3 grid over the cache's box (15 bits, 32 chunks of 1,024 keys, the counting sort of
+// rbr_sort.cuh); inference then serves the queries cell by cell, so that the samples of a tile
+// read nearby hash-grid entries. Scratch: counts and chunk totals, permutation, keys.
+constexpr uint32_t kQueryKeys = 1u << 15;
+constexpr uint32_t kQueryChunks = kQueryKeys / kScanThreads;
+
+static constexpr size_t round256(size_t b) { return (b + 255) & ~size_t(255); }
+size_t query_sort_bytes(uint32_t n) {
+    return round256((kQueryKeys + kQueryChunks) * 4) + round256(size_t(n) * 4) + round256(size_t(n) * 2);
+}
+
+namespace {
+__device__ __forceinline__ uint32_t spread5(uint32_t x) {  // 5 bits -> every third of 15
+    uint32_t r = 0;
+#pragma unroll
+    for (int i = 0; i < 5; ++i) r |= ((x >> i) & 1u) << (3 * i);
+    return r;
+}
+
+__global__ void k_rc_query_keys(CacheDev c, const float4* __restrict__ records, uint32_t n, const uint32_t* n_ptr,
+                                uint16_t* __restrict__ keys, uint32_t* __restrict__ counts) {
+    const uint32_t count = n_ptr ? min(*n_ptr, n) : n;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += gridDim.x * blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        uint32_t k = kNoKey;
+        if (i < count) {
+            float p[3];
+            unit_position(c, __ldg(records + 4 * static_cast<size_t>(i)), p);
+            k = 0;
+#pragma unroll
+            for (int a = 0; a < 3; ++a) k |= spread5(min(static_cast<uint32_t>(p[a] * 32.0f), 31u)) << (2 - a);
+            keys[i] = static_cast<uint16_t>(k);
+        }
+        count_key(counts, k);
+    }
+}
+
+__global__ void k_rc_query_scatter(const uint16_t* __restrict__ keys, uint32_t n, const uint32_t* n_ptr,
+                                   uint32_t* __restrict__ offsets, const uint32_t* __restrict__ chunk_sum,
+                                   uint32_t* __restrict__ perm) {
+    scatter_keys<kQueryChunks>(keys, n_ptr ? min(*n_ptr, n) : n, offsets, chunk_sum, perm);
+}
+}  // namespace
+
 cudaError_t cache_launch_infer(rbr_ctx* ctx, const float4* records, uint32_t n, const uint32_t* n_ptr, float* rgb,
-                               float4* path_rad, const float4* q_info, cudaStream_t stream) {
+                               float4* path_rad, const float4* q_info, cudaStream_t stream, void* sort_scratch) {
     CacheState& cs = ctx->cache;
     InferOut o;
     o.rgb = rgb;
     o.path_rad = path_rad;
     o.q_info = q_info;
+    o.perm = nullptr;
     const uint32_t tiles = (n + kRcTile - 1) / kRcTile;
     CacheDev dev = cs.dev;
     dev.wait_limit = ctx->cache_wait_limit;
+    if (ctx->cache_sort_queries && sort_scratch && n > 0) {
+        char* base = static_cast<char*>(sort_scratch);
+        auto* counts = reinterpret_cast<uint32_t*>(base);
+        uint32_t* chunk_sum = counts + kQueryKeys;
+        auto* perm = reinterpret_cast<uint32_t*>(base + round256((kQueryKeys + kQueryChunks) * 4));
+        auto* keys = reinterpret_cast<uint16_t*>(base + round256((kQueryKeys + kQueryChunks) * 4) + round256(size_t(n) * 4));
+        cudaError_t e = cudaMemsetAsync(counts, 0, kQueryKeys * 4, stream);
+        if (e != cudaSuccess) return e;
+        const uint32_t sgrid = std::max(1u, std::min<uint32_t>((n + 255) / 256, ctx->num_sms * 8));
+        k_rc_query_keys<<<sgrid, 256, 0, stream>>>(dev, records, n, n_ptr, keys, counts);
+        k_key_offsets<<<kQueryChunks, kScanThreads, 0, stream>>>(counts, chunk_sum);
+        k_rc_query_scatter<<<sgrid, 256, 0, stream>>>(keys, n, n_ptr, counts, chunk_sum, perm);
+        o.perm = perm;
+    }
     const int G = ctx->cache_infer_groups;
     if (G == 2 || G == 4) {  // G tiles per CTA, 8 / G CTAs per SM
         const uint32_t ctas = (tiles + G - 1) / G;
@@ -1410,8 +1476,9 @@ rbr_status cache_infer_host(rbr_ctx* ctx, uint32_t n, const rbr_cache_record* re
     rbr_status st = stage_records(ctx, n, records, nullptr);
     if (st == RBR_OK) st = ensure(ctx, ctx->stage_out, size_t(n) * 12, "cache staging");
     if (st != RBR_OK) return st;
+    if ((st = ensure(ctx, ctx->sort_buf, query_sort_bytes(n), "query sort")) != RBR_OK) return st;
     cudaError_t e = cache_launch_infer(ctx, as<float4>(ctx->stage_in.ptr), n, nullptr, as<float>(ctx->stage_out.ptr),
-                                       nullptr, nullptr, 0);
+                                       nullptr, nullptr, 0, ctx->sort_buf.ptr);
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return cuda_fail(ctx, e, "radiance cache: inference");
     st = check_device_error(ctx, 0);
@@ -1484,9 +1551,12 @@ rbr_status cache_ensure_render(rbr_ctx* ctx, uint32_t paths, uint32_t train_cap)
     if (cs.q_cap < paths) {
         free_dev(cs.q_rec);
         free_dev(cs.q_info);
+        free_dev(cs.q_sort);
         cs.q_cap = 0;
+        cs.q_sort_stride = query_sort_bytes(paths);
         if ((e = alloc_dev(cs.q_rec, size_t(paths) * 64)) == cudaSuccess &&
-            (e = alloc_dev(cs.q_info, size_t(paths) * 16)) == cudaSuccess)
+            (e = alloc_dev(cs.q_info, size_t(paths) * 16)) == cudaSuccess &&
+            (e = alloc_dev(cs.q_sort, 2 * cs.q_sort_stride)) == cudaSuccess)
             cs.q_cap = paths;
     }
     if (e == cudaSuccess && cs.t_cap < train_cap) {

@@ -224,6 +224,9 @@ rbr_status rbr_param_set(rbr_ctx* ctx, const char* name, int64_t value) {
     } else if (n == "pt.shade_split") {
         if (value != 0 && value != 1) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "pt.shade_split is 0 or 1");
         ctx->pt_shade_split = static_cast<int>(value);
+    } else if (n == "cache.sort_queries") {
+        if (value != 0 && value != 1) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "cache.sort_queries is 0 or 1");
+        ctx->cache_sort_queries = static_cast<int>(value);
     } else if (n == "cache.infer_warps") {
         if (value != 4 && value != 8) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "cache.infer_warps is 4 or 8");
         ctx->cache_infer_warps = static_cast<int>(value);
@@ -269,6 +272,7 @@ rbr_status rbr_param_get(const rbr_ctx* ctx, const char* name, int64_t* value) {
     else if (n == "cache.wait_limit") *value = ctx->cache_wait_limit;
     else if (n == "cache.infer_groups") *value = ctx->cache_infer_groups;
     else if (n == "cache.infer_warps") *value = ctx->cache_infer_warps;
+    else if (n == "cache.sort_queries") *value = ctx->cache_sort_queries;
     else if (n == "pt.shade_split") *value = ctx->pt_shade_split;
     else if (n == "trace.stream_io") *value = ctx->trace_stream_io;
     else if (n == "trace.node_test") *value = ctx->trace_node_test;

@@ -103,6 +103,7 @@ struct Paths {
     // radiance cache
     float4* q_rec = nullptr;   // 4 per query (rbr_cache_record)
     float4* q_info = nullptr;  // per query: throughput rgb, path index bits
+    void* q_sort = nullptr;    // scratch of the queries' spatial sort (host side only)
     float4* t_rec = nullptr;   // 4 per training vertex
     float4* t_aux = nullptr;   // 2 per training vertex: (throughput rgb, path index bits), (radiance before, -)
     uint32_t t_cap = 0;
@@ -1168,6 +1169,7 @@ rbr_status render_cached(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_p
         P.shadow_cap = pb.shadow_capacity;
         P.q_rec = static_cast<float4*>(cs.q_rec) + 4 * size_t(b) * cap;
         P.q_info = static_cast<float4*>(cs.q_info) + size_t(b) * cap;
+        P.q_sort = static_cast<char*>(cs.q_sort) + size_t(b) * cs.q_sort_stride;
         P.t_rec = static_cast<float4*>(cs.t_rec) + 4 * size_t(b) * t_half;
         P.t_aux = static_cast<float4*>(cs.t_aux) + 2 * size_t(b) * t_half;
         P.t_cap = train ? t_half : 0;
@@ -1222,7 +1224,7 @@ rbr_status render_cached(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_p
                 k_shadow<<<grid, kBlock, 0, ws>>>(ctx->scene, P, ctx->d_error);
                 launches += 4;
             }
-            e = cache_launch_infer(ctx, P.q_rec, w.npaths, P.counters + kCQuery, nullptr, P.rad, P.q_info, ws);
+            e = cache_launch_infer(ctx, P.q_rec, w.npaths, P.counters + kCQuery, nullptr, P.rad, P.q_info, ws, P.q_sort);
             ++launches;
             if (e == cudaSuccess && train) {
                 e = cache_launch_finalize(ctx, P.rad, P.t_aux, P.counters, kCTrainBase, kCTrain, t_half, ws);
@@ -1301,6 +1303,7 @@ cudaError_t launch_packed_wave(rbr_ctx* eng, rbr_ctx* scn, const PackedWave& pw,
         CacheState& cs = scn->cache;
         P.q_rec = static_cast<float4*>(cs.q_rec);
         P.q_info = static_cast<float4*>(cs.q_info);
+        P.q_sort = cs.q_sort;
         P.t_rec = static_cast<float4*>(cs.t_rec);
         P.t_aux = static_cast<float4*>(cs.t_aux);
         P.t_cap = pw.train ? cs.t_cap : 0;
@@ -1327,7 +1330,7 @@ cudaError_t launch_packed_wave(rbr_ctx* eng, rbr_ctx* scn, const PackedWave& pw,
         k_shadow<<<grid, kBlock, 0, stream>>>(scn->scene, P, eng->d_error);
     }
     if (pw.mode == 1) {
-        e = cache_launch_infer(scn, P.q_rec, pw.capacity, P.counters + kCQuery, nullptr, P.rad, P.q_info, stream);
+        e = cache_launch_infer(scn, P.q_rec, pw.capacity, P.counters + kCQuery, nullptr, P.rad, P.q_info, stream, P.q_sort);
         if (e == cudaSuccess && pw.train)
             e = cache_launch_finalize(scn, P.rad, P.t_aux, P.counters, kCTrainBase, kCTrain, scn->cache.t_cap, stream);
         if (e != cudaSuccess) return e;

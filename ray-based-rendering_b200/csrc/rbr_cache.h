@@ -66,6 +66,8 @@ struct CacheState {
     // render-time buffers
     void* q_rec = nullptr;        // float4 x4 per query
     void* q_info = nullptr;       // float4 per query: throughput rgb, path index bits
+    void* q_sort = nullptr;       // two query-sort scratch areas (one per wave slot), q_sort_stride apart
+    size_t q_sort_stride = 0;
     uint32_t q_cap = 0;
     void* t_rec = nullptr;        // float4 x4 per training vertex
     void* t_aux = nullptr;        // float4 x2 per training vertex: (T, path), (radiance before, -)

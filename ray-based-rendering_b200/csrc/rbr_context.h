@@ -78,6 +78,7 @@ struct rbr_ctx {
     uint32_t cache_wait_limit = 1u << 22;  // polls of a tensor-core completion wait (cache kernels)
     int cache_infer_groups = 1;            // tiles in flight per inference CTA: 1, 2 or 4
     int cache_infer_warps = 4;             // warps per tile of the one-tile inference kernel: 4 or 8
+    int cache_sort_queries = 0;            // inference serves the queries in spatial order (0 or 1)
     uint32_t fail_alloc_countdown = 0;     // > 0: the n-th next device allocation fails (fault injection)
     // path tracer
     rbr::PathBuffers pt;
@@ -176,8 +177,12 @@ rbr_status cache_infer_host(rbr_ctx* ctx, uint32_t n, const rbr_cache_record* re
 rbr_status cache_train_host(rbr_ctx* ctx, uint32_t n, const rbr_cache_record* records, const float* targets, int apply,
                             float* loss);
 rbr_status cache_ensure_render(rbr_ctx* ctx, uint32_t paths, uint32_t train_cap);
+// sort_scratch (optional, query_sort_bytes(n) bytes): with cache.sort_queries the queries are
+// served in spatial order (a counting sort of their cells) instead of the order given.
 cudaError_t cache_launch_infer(rbr_ctx* ctx, const float4* records, uint32_t n, const uint32_t* n_ptr, float* rgb,
-                               float4* path_rad, const float4* q_info, cudaStream_t stream);
+                               float4* path_rad, const float4* q_info, cudaStream_t stream,
+                               void* sort_scratch = nullptr);
+size_t query_sort_bytes(uint32_t n);
 cudaError_t cache_launch_finalize(rbr_ctx* ctx, const float4* path_rad, const float4* t_aux, const uint32_t* counters,
                                   int base_word, int count_word, uint32_t cap, cudaStream_t stream);
 cudaError_t cache_launch_train_frame(rbr_ctx* ctx, const uint32_t* count_ptr, const uint32_t* count2_ptr, uint32_t cap,

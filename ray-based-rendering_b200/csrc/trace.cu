@@ -10,6 +10,7 @@
 
 #include "rbr_context.h"
 #include "rbr_device.cuh"
+#include "rbr_sort.cuh"
 
 namespace rbr {
 
@@ -152,24 +153,13 @@ __global__ void k_ray_keys(const float4* __restrict__ rays, uint32_t n, float3 l
     }
 }
 
-// Counting sort of the 16-bit keys (orders 4 and 5) in three passes: every ray's key and a
-// count per key value (global atomics on 65,536 counters); 64 blocks turn the counts into each
-// key's first slot within its chunk of 1,024 keys, plus the chunk totals; every ray takes the
-// next slot of its key (an atomic on the same counters, plus the slots of the chunks before)
-// and writes its index there. Lanes of a warp with equal keys share one atomic (match.any), so
-// coherent rays (few distinct keys) do not serialise on one counter. The order within one key
-// is the atomics' order, so it can differ between runs; each ray's result does not depend on
-// it.
+// Orders 4 and 5 (16-bit keys) use the counting sort of rbr_sort.cuh: 65,536 key values in 64
+// chunks.
 constexpr uint32_t kKeyValues = 1u << 16;
-constexpr int kScanThreads = 1024;
+constexpr uint32_t kScanChunks = kKeyValues / kScanThreads;
 
-constexpr uint32_t kNoKey = 0xFFFFFFFFu;  // lanes past the end (real keys are below 2^16)
-
-// The whole warp walks the grid-stride loop together (its base is a multiple of the block), so
-// every lane takes part in the match.
 __global__ void k_ray_keys16(const float4* __restrict__ rays, uint32_t n, float3 lo, float3 scale, int order,
                              uint16_t* __restrict__ keys, uint32_t* __restrict__ counts) {
-    const uint32_t lane = threadIdx.x & 31u;
     for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
         const uint32_t i = base + threadIdx.x;
         uint32_t k = kNoKey;
@@ -179,73 +169,13 @@ __global__ void k_ray_keys16(const float4* __restrict__ rays, uint32_t n, float3
             k = ray_key(a, b, lo, scale, order);
             keys[i] = static_cast<uint16_t>(k);
         }
-        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, k);
-        if (k != kNoKey && lane == static_cast<uint32_t>(__ffs(peers) - 1)) atomicAdd(counts + k, __popc(peers));
+        count_key(counts, k);
     }
-}
-
-// Exclusive prefix sums of the counts within each chunk of 1,024 keys, in place, one block of
-// 1,024 threads per chunk (64 blocks); the chunk totals go to `chunk_sum`. The scatter adds
-// the totals of the chunks before a key's chunk.
-constexpr uint32_t kScanChunks = kKeyValues / kScanThreads;
-__global__ void __launch_bounds__(kScanThreads) k_key_offsets(uint32_t* counts, uint32_t* chunk_sum) {
-    __shared__ uint32_t warp_sum[kScanThreads / 32];
-    const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
-    uint32_t* c = counts + blockIdx.x * kScanThreads;
-    const uint32_t v = c[t];
-    uint32_t incl = v;  // inclusive scan over the warp
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-        if (lane >= static_cast<uint32_t>(o)) incl += y;
-    }
-    if (lane == 31) warp_sum[warp] = incl;
-    __syncthreads();
-    if (warp == 0) {
-        const uint32_t w = warp_sum[lane];
-        uint32_t wi = w;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, wi, o);
-            if (lane >= static_cast<uint32_t>(o)) wi += y;
-        }
-        warp_sum[lane] = wi - w;  // exclusive over the warps
-        if (lane == 31) chunk_sum[blockIdx.x] = wi;
-    }
-    __syncthreads();
-    c[t] = warp_sum[warp] + incl - v;
 }
 
 __global__ void k_ray_scatter16(const uint16_t* __restrict__ keys, uint32_t n, uint32_t* __restrict__ offsets,
                                 const uint32_t* __restrict__ chunk_sum, uint32_t* __restrict__ perm) {
-    // first slot of each chunk of keys: exclusive sum of the chunk totals (64 of them)
-    __shared__ uint32_t chunk_first[kScanChunks];
-    if (threadIdx.x < 32) {
-        const uint32_t l = threadIdx.x;
-        const uint32_t a = chunk_sum[2 * l], b = chunk_sum[2 * l + 1];
-        uint32_t incl = a + b;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-            if (l >= static_cast<uint32_t>(o)) incl += y;
-        }
-        chunk_first[2 * l] = incl - a - b;
-        chunk_first[2 * l + 1] = incl - b;
-    }
-    __syncthreads();
-    const uint32_t lane = threadIdx.x & 31u;
-    uint32_t lt;
-    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
-    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
-        const uint32_t i = base + threadIdx.x;
-        const uint32_t k = i < n ? keys[i] : kNoKey;
-        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, k);
-        const uint32_t leader = static_cast<uint32_t>(__ffs(peers) - 1);
-        uint32_t first = 0;
-        if (k != kNoKey && lane == leader) first = chunk_first[k / kScanThreads] + atomicAdd(offsets + k, __popc(peers));
-        first = __shfl_sync(0xFFFFFFFFu, first, leader);
-        if (k != kNoKey) perm[first + __popc(peers & lt)] = i;
-    }
+    scatter_keys<kScanChunks>(keys, n, offsets, chunk_sum, perm);
 }
 
 __global__ void __launch_bounds__(kTraceBlock) k_trace_any(DeviceScene s, const float4* __restrict__ rays, uint32_t n,

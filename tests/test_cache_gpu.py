@@ -194,3 +194,19 @@ def test_eight_warp_inference_equals_four_warp(cctx):
     assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
     with pytest.raises(RbrError):
         cctx.set_param("cache.infer_warps", 6)
+
+
+def test_spatially_sorted_inference_equals_given_order(cctx):
+    """cache.sort_queries 1: the queries are served in the order of their cells (a counting sort
+    on a 32^3 grid, many queries sharing a cell); each query's prediction is the same bits."""
+    _, rng = make_cache(cctx, 13)
+    recs = random_records(rng, 120_000)
+    recs[:20_000, 0:3] = recs[0, 0:3]  # a sixth of them in one cell
+    cctx.set_param("cache.sort_queries", 0)
+    want = cctx.cache_infer(recs)
+    cctx.set_param("cache.sort_queries", 1)
+    try:
+        got = cctx.cache_infer(recs)
+    finally:
+        cctx.set_param("cache.sort_queries", 0)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))

@@ -98,3 +98,22 @@ def test_self_training_suffix(ctx):
     (a, q0, t0), (b, q2, t2) = out[0], out[2]
     assert t2 < t0 and q2 > q0, (t0, t2, q0, q2)
     assert np.isfinite(b).all() and abs(b.mean() / a.mean() - 1.0) < 0.05
+
+
+def test_spatially_sorted_queries_render_the_same_frame(ctx):
+    """cache.sort_queries: the inference serves a wave's queries cell by cell; each query's
+    prediction and its path's radiance are the same, so frames rendered without training agree
+    (up to the order of the shadow rays' atomic sums)."""
+    s = small_ggx()
+    ctx.upload(s)
+    ctx.cache_create(train_paths=(192 * 108) // 8, seed=3)
+    cached_render(ctx, s.camera, 4, 16, 7)  # train a little first
+    try:
+        ctx.set_param("cache.sort_queries", 0)
+        a = cached_render(ctx, s.camera, 2, 16, 8, train=False)
+        ctx.set_param("cache.sort_queries", 1)
+        b = cached_render(ctx, s.camera, 2, 16, 8, train=False)
+    finally:
+        ctx.set_param("cache.sort_queries", 0)
+    assert np.isfinite(b).all()
+    np.testing.assert_allclose(b, a, rtol=1e-4, atol=1e-5)
