@@ -731,6 +731,7 @@ def run_batch(args, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     ctx = Context(local_rank)
+    set_params(ctx, args.param)
     r = measure_batch(ctx, local_rank, rank, args.steps, args.warmup, e2e=not args.no_e2e)
     ctx.close()
     if rank == 0:

@@ -271,6 +271,11 @@ rbr_status rbr_scene_stats_get(const rbr_ctx* ctx, rbr_scene_stats* out);
  *                          Lambertian lobe, GGX reflection only, GGX transmission, delta-only,
  *                          none) in a launch of its own, compiled for that class's lobes; 0 one
  *                          launch for all classes (default)
+ *   "pt.fetch"             path tracer: 1 (default) the extension, shading and shadow launches
+ *                          hand out a queue of four grid rounds or more in claims of 32 to 256
+ *                          entries to whichever warp is free (one atomic per claim), so warps
+ *                          that drew short traversals take more; 0 a fixed grid-stride share
+ *                          per warp
  *   "cache.infer_groups"   radiance-cache inference: 128-sample tiles in flight per CTA, 1, 2 or 4
  *                          (groups of four warps sharing one copy of the weights; default 1)
  *   "cache.infer_warps"    one-tile inference: 4 or 8 warps per 128-sample tile (default 4)

@@ -224,6 +224,10 @@ rbr_status rbr_param_set(rbr_ctx* ctx, const char* name, int64_t value) {
     } else if (n == "pt.shade_split") {
         if (value != 0 && value != 1) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "pt.shade_split is 0 or 1");
         ctx->pt_shade_split = static_cast<int>(value);
+    } else if (n == "pt.fetch") {
+        if (value != 0 && value != 1) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "pt.fetch is 0 or 1");
+        if (ctx->pt_fetch != static_cast<int>(value)) ++ctx->pt_generation;  // captured wave graphs hold the old value
+        ctx->pt_fetch = static_cast<int>(value);
     } else if (n == "cache.sort_queries") {
         if (value != 0 && value != 1) return fail(ctx, RBR_ERR_INVALID_ARGUMENT, "cache.sort_queries is 0 or 1");
         ctx->cache_sort_queries = static_cast<int>(value);
@@ -274,6 +278,7 @@ rbr_status rbr_param_get(const rbr_ctx* ctx, const char* name, int64_t* value) {
     else if (n == "cache.infer_warps") *value = ctx->cache_infer_warps;
     else if (n == "cache.sort_queries") *value = ctx->cache_sort_queries;
     else if (n == "pt.shade_split") *value = ctx->pt_shade_split;
+    else if (n == "pt.fetch") *value = ctx->pt_fetch;
     else if (n == "trace.stream_io") *value = ctx->trace_stream_io;
     else if (n == "trace.node_test") *value = ctx->trace_node_test;
     else if (n == "trace.l2_persist") *value = ctx->trace_l2_persist;

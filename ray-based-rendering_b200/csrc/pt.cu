@@ -46,10 +46,12 @@ enum : int {
     kCTrainBase = 16,  // radiance cache: kCTrain at the start of this wave
     kCShade = 18,      // 64-bit: hit vertices shaded
     kCTraffic = 20,    // 4 x 64-bit (RBR_RENDER_COUNT_TRAFFIC): extension nodes, records; shadow nodes, records
-    kCWords = 28
+    kCCursor = 28,     // 3 claim cursors of one depth (Paths::fetch): extension, shading, shadow queue
+    kCWords = 32
 };
 static_assert(kCClass + static_cast<int>(kNumClasses) <= kCShadow, "class-queue counts overlap the shadow count");
 static_assert(kCExt % 2 == 0 && kCSh % 2 == 0 && kCShade % 2 == 0 && kCTraffic % 2 == 0, "64-bit counters");
+static_assert(kCTraffic + 8 <= kCCursor && kCCursor + 3 <= kCWords, "claim cursors overlap");
 
 // The blocks a stage runs on: the whole grid for the wavefront kernels, one half of it for a
 // half of the persistent wave loop. Grid-stride loops start at block `block` of `blocks`.
@@ -57,6 +59,57 @@ struct Span {
     uint32_t block, blocks;
 };
 __device__ __forceinline__ Span grid_span() { return Span{blockIdx.x, gridDim.x}; }
+
+// Work distribution of a stage over the n entries of a queue. A stage's cost per entry varies
+// widely (a traversal that leaves the scene at once beside one that walks deep into the mesh),
+// so with a fixed grid-stride share per warp the warps that drew the long traversals keep the
+// launch alive while the others have exited. With a claim cursor (a queue counter reset at the
+// start of each depth), a warp done with its entries instead claims the next ones by one atomic
+// on the cursor, so warps that drew short traversals take more. Claims shrink as the queue
+// drains (guided self-scheduling): a quarter of the entries left per warp, in multiples of 32
+// from 256 down to 32, so that early claims are few and the last ones leave no warp with a
+// long run of work behind the others. Atomics on the one cursor are served one after another
+// (about 1.3 ns apart, measured), so a short queue of cheap entries would wait on its claims:
+// queues of fewer than kClaimRounds grid-stride rounds go out in the grid-stride order.
+// take() returns this thread's entry (entries >= n are lanes without work) and sets `live`
+// (warp-uniform) while the warp has entries: `for (j = c.take(); c.live; j = c.take())`.
+constexpr uint32_t kClaimRounds = 8;
+struct Claim {
+    uint32_t* cursor;          // nullptr: grid-stride order
+    uint32_t n, next, stride;  // grid-stride order: this block's next base
+    uint32_t cb = 0, ce = 0;   // the warp's claimed range (warp-uniform)
+    bool live = true;
+    __device__ __forceinline__ Claim(uint32_t* cur, uint32_t count, Span g)
+        : cursor(nullptr), n(count), next(g.block * blockDim.x), stride(g.blocks * blockDim.x) {
+        if (cur && n / stride >= kClaimRounds) cursor = cur;
+    }
+    __device__ __forceinline__ uint32_t take() {
+        const uint32_t lane = threadIdx.x & 31u;
+        uint32_t j;
+        if (!cursor) {
+            j = next + threadIdx.x;
+            next += stride;
+        } else {
+            if (cb >= ce) {
+                uint32_t b = 0, r = 0;
+                if (lane == 0) {
+                    // the cursor as it stands (a plain load: this warp's own last claim can be far
+                    // behind it, and sizing by that would hand out long runs near the end)
+                    const uint32_t at = *reinterpret_cast<volatile uint32_t*>(cursor);
+                    const uint32_t left = at < n ? n - at : 0u;
+                    r = min(256u, max(32u, (left / (stride / 8u)) & ~31u));  // left / (4 x warps)
+                    b = atomicAdd(cursor, r);
+                }
+                cb = __shfl_sync(0xFFFFFFFFu, b, 0);
+                ce = cb + __shfl_sync(0xFFFFFFFFu, r, 0);
+            }
+            j = cb + lane;
+            cb += 32u;
+        }
+        live = j - lane < n;
+        return j;
+    }
+};
 
 // Adds this warp's node / record counts to two 64-bit counters (every lane of the warp calls it).
 __device__ __forceinline__ void warp_add_counts(uint32_t* counters, int word, uint2 c) {
@@ -100,6 +153,7 @@ struct Paths {
     uint32_t* counters;
     uint32_t cap;
     uint32_t shadow_cap;
+    uint32_t fetch = 0;  // 1: the extension, shading and shadow stages hand out long queues by claims
     // radiance cache
     float4* q_rec = nullptr;   // 4 per query (rbr_cache_record)
     float4* q_info = nullptr;  // per query: throughput rgb, path index bits
@@ -223,6 +277,7 @@ __device__ __forceinline__ void begin_body(const Paths& P, uint32_t d) {
     c[kCQ0 + ((d + 1) & 1)] = 0;
     for (int i = 0; i < kNumClasses; ++i) c[kCClass + i] = 0;
     c[kCShadow] = 0;
+    for (int i = 0; i < 3; ++i) c[kCCursor + i] = 0;
 }
 
 __global__ void k_begin(Paths P, uint32_t d) {
@@ -246,10 +301,9 @@ __device__ __forceinline__ void extend_body(const DeviceScene& s, const Wave& w,
     uint32_t* nextq = (d & 1) ? P.q0 : P.q1;
     uint32_t* nextc = P.counters + kCQ0 + ((d + 1) & 1);
     if (g.block == 0 && threadIdx.x == 0) atomicAdd(reinterpret_cast<unsigned long long*>(P.counters + kCExt), n);
-    const uint32_t stride = g.blocks * blockDim.x;
     uint2 traffic = make_uint2(0u, 0u);
-    for (uint32_t base = g.block * blockDim.x; base < n; base += stride) {
-        const uint32_t j = base + threadIdx.x;
+    Claim cl(P.fetch ? P.counters + kCCursor : nullptr, n, g);
+    for (uint32_t j = cl.take(); cl.live; j = cl.take()) {
         const bool valid = j < n;
         uint32_t k = 0, cls = kNumClasses;
         bool scatter = false, last = true, nee = false;
@@ -470,9 +524,9 @@ __device__ __forceinline__ void shade_body(const DeviceScene& s, const Wave& w, 
     uint32_t* nextq = (d & 1) ? P.q0 : P.q1;
     uint32_t* nextc = P.counters + kCQ0 + ((d + 1) & 1);
     if (g.block == 0 && threadIdx.x == 0) atomicAdd(reinterpret_cast<unsigned long long*>(P.counters + kCShade), n);
-    const uint32_t stride = g.blocks * blockDim.x;
-    for (uint32_t base = g.block * blockDim.x; base < n; base += stride) {
-        const uint32_t j = base + threadIdx.x;
+    // one cursor per depth: the per-class launches keep the grid-stride order
+    Claim cl(P.fetch && kCls < 0 ? P.counters + kCCursor + 1 : nullptr, n, g);
+    for (uint32_t j = cl.take(); cl.live; j = cl.take()) {
         const bool valid = j < n;
         uint32_t k = 0;
         bool alive = false, nee = false, to_cache = false, to_train = false, last = true, mis = false;
@@ -649,18 +703,20 @@ __device__ __forceinline__ void shadow_body(const DeviceScene& s, const Paths& P
         n = P.shadow_cap;
     }
     if (g.block == 0 && threadIdx.x == 0) atomicAdd(reinterpret_cast<unsigned long long*>(P.counters + kCSh), n);
-    const uint32_t stride = g.blocks * blockDim.x;
     uint2 traffic = make_uint2(0u, 0u);
-    for (uint32_t j = g.block * blockDim.x + threadIdx.x; j < n; j += stride) {
-        const float4* e = P.shadow + 3 * static_cast<size_t>(j);
-        const float4 a = e[0], b = e[1];
-        float t;
-        if (!degenerate(a, b) && !traverse<true, kCount>(s, ld_f3(a), ld_f3(b), a.w, t, err, &traffic)) {
-            const float4 c = e[2];
-            float4* L = P.rad + __float_as_uint(b.w);
-            atomicAdd(&L->x, c.x);
-            atomicAdd(&L->y, c.y);
-            atomicAdd(&L->z, c.z);
+    Claim cl(P.fetch ? P.counters + kCCursor + 2 : nullptr, n, g);
+    for (uint32_t j = cl.take(); cl.live; j = cl.take()) {
+        if (j < n) {  // lanes past the end claim again with their warp
+            const float4* e = P.shadow + 3 * static_cast<size_t>(j);
+            const float4 a = e[0], b = e[1];
+            float t;
+            if (!degenerate(a, b) && !traverse<true, kCount>(s, ld_f3(a), ld_f3(b), a.w, t, err, &traffic)) {
+                const float4 c = e[2];
+                float4* L = P.rad + __float_as_uint(b.w);
+                atomicAdd(&L->x, c.x);
+                atomicAdd(&L->y, c.y);
+                atomicAdd(&L->z, c.z);
+            }
         }
     }
     if (kCount) warp_add_counts(P.counters, kCTraffic + 4, traffic);
@@ -987,6 +1043,7 @@ rbr_status render(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_params* 
         P.counters = static_cast<uint32_t*>(pb.counters.ptr);
         P.cap = pb.capacity;
         P.shadow_cap = pb.shadow_capacity;
+        P.fetch = static_cast<uint32_t>(ctx->pt_fetch);
     }
     const cudaStream_t streams[2] = {stream, two ? ctx->side_stream : stream};
 
@@ -1167,6 +1224,7 @@ rbr_status render_cached(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_p
         P.counters = static_cast<uint32_t*>(pb.counters.ptr);
         P.cap = pb.capacity;
         P.shadow_cap = pb.shadow_capacity;
+        P.fetch = static_cast<uint32_t>(ctx->pt_fetch);
         P.q_rec = static_cast<float4*>(cs.q_rec) + 4 * size_t(b) * cap;
         P.q_info = static_cast<float4*>(cs.q_info) + size_t(b) * cap;
         P.q_sort = static_cast<char*>(cs.q_sort) + size_t(b) * cs.q_sort_stride;
@@ -1295,6 +1353,7 @@ cudaError_t launch_packed_wave(rbr_ctx* eng, rbr_ctx* scn, const PackedWave& pw,
     P.counters = static_cast<uint32_t*>(pb.counters.ptr);
     P.cap = pb.capacity;
     P.shadow_cap = pb.shadow_capacity;
+    P.fetch = static_cast<uint32_t>(eng->pt_fetch);
     P.segs = pw.segs;
     P.seg_of = static_cast<uint32_t*>((pw.slot ? eng->pt_seg_of2 : eng->pt_seg_of).ptr);
     P.wave_hdr = pw.hdr;
@@ -1367,6 +1426,7 @@ cudaError_t launch_wave_loop(rbr_ctx* eng, const std::vector<rbr_ctx*>& scenes, 
         P.counters = static_cast<uint32_t*>(pb.counters.ptr);
         P.cap = pb.capacity;
         P.shadow_cap = pb.shadow_capacity;
+        P.fetch = static_cast<uint32_t>(eng->pt_fetch);
         P.seg_of = static_cast<uint32_t*>((h ? eng->pt_seg_of2 : eng->pt_seg_of).ptr);
     }
     lp.stamps = stamps;
@@ -1480,6 +1540,7 @@ rbr_status render_noalloc(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_
     if (off > RBR_NOALLOC_SCRATCH_BYTES) return fail(ctx, RBR_ERR_INTERNAL, "scratch layout exceeds the array");
     P.cap = static_cast<uint32_t>(cap);
     P.shadow_cap = static_cast<uint32_t>(cap * nl);
+    P.fetch = static_cast<uint32_t>(ctx->pt_fetch);
 
     CameraDev cd;
     cd.width = cam->width;

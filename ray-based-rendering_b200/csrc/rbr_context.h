@@ -85,6 +85,7 @@ struct rbr_ctx {
     rbr::PathBuffers pt2;                  // second wave in flight (rbr_render, pt_streams 2)
     int pt_streams = 2;                    // waves in flight in rbr_render: 1 or 2
     int pt_shade_split = 0;                // rbr_render: one shading launch per material class
+    int pt_fetch = 1;                      // wavefront stages hand out long queues by claims on cursors (0: grid stride)
     bool pt_last_two = false;              // the last rbr_render used pt2
     cudaStream_t side_stream = nullptr;    // stream of the second wave
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;

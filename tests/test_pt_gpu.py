@@ -106,6 +106,42 @@ def test_two_waves_in_flight_match_one(ctx):
         ctx.set_param("pt.streams", 3)
 
 
+@pytest.mark.parametrize("split", [0, 1])
+def test_claimed_work_matches_grid_stride(ctx, split):
+    """pt.fetch 1 (long queues handed out by claims on per-depth cursors) traces, shades
+    and counts exactly the work of the fixed grid-stride order (pt.fetch 0): the same rays, nodes
+    and records, and the same film up to the order of the shadow rays' atomic additions. Three
+    lights and GGX materials; 5.2 M paths in two waves of up to 2^22, so the queues of the first
+    depths are long enough for claims (eight grid rounds and more) and the later ones are not,
+    and the cursors are reset between depths and waves; with pt.shade_split 1 the per-class
+    shading launches keep the grid-stride order beside claimed extension and shadow launches."""
+    s = scenes.ggx_scene(1024, 640, n_spheres=24, mesh_n=400, seed=3)
+    ctx.upload(s)
+    wave_paths = ctx.get_param("pt.wave_paths")
+    ctx.set_param("pt.wave_paths", 1 << 22)
+    ctx.set_param("pt.shade_split", split)
+    films, stats = {}, {}
+    try:
+        for fetch in (0, 1):
+            ctx.set_param("pt.fetch", fetch)
+            p = render_params(spp=8, max_depth=12, seed=17, flags=abi.RBR_RENDER_COUNT_TRAFFIC)
+            films[fetch] = ctx.render_host(s.camera, p)
+            stats[fetch] = ctx.render_stats()
+    finally:
+        ctx.set_param("pt.fetch", 1)
+        ctx.set_param("pt.shade_split", 0)
+        ctx.set_param("pt.wave_paths", wave_paths)
+    a, b = stats[0], stats[1]
+    assert a.waves == b.waves == 2 and a.ext_nodes > 0 and a.shadow_nodes > 0
+    for f in ("extension_rays", "shadow_rays", "shaded_vertices", "ext_nodes", "ext_records", "shadow_nodes",
+              "shadow_records"):
+        assert getattr(a, f) == getattr(b, f), f
+    assert np.isfinite(films[1]).all()
+    np.testing.assert_allclose(films[1], films[0], rtol=1e-5, atol=1e-6)
+    with pytest.raises(RbrError):
+        ctx.set_param("pt.fetch", 2)
+
+
 def test_edge_parameters(ctx, restatement):
     s = small_cornell(16, 16)
     s.background = (0.25, 0.5, 1.0)  # camera rays leaving through the open front see it
