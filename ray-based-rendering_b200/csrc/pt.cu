@@ -68,9 +68,10 @@ __device__ __forceinline__ Span grid_span() { return Span{blockIdx.x, gridDim.x}
 // on the cursor, so warps that drew short traversals take more. Claims shrink as the queue
 // drains (guided self-scheduling): a quarter of the entries left per warp, in multiples of 32
 // from 256 down to 32, so that early claims are few and the last ones leave no warp with a
-// long run of work behind the others. Atomics on the one cursor are served one after another
-// (about 1.3 ns apart, measured), so a short queue of cheap entries would wait on its claims:
-// queues of fewer than kClaimRounds grid-stride rounds go out in the grid-stride order.
+// long run of work behind the others. Atomics on the one cursor are served one after another,
+// so a short queue of cheap entries would wait on its claims (claims from four rounds up made
+// the foggy Cornell box 12 % slower): queues of fewer than kClaimRounds grid-stride rounds go
+// out in the grid-stride order.
 // take() returns this thread's entry (entries >= n are lanes without work) and sets `live`
 // (warp-uniform) while the warp has entries: `for (j = c.take(); c.live; j = c.take())`.
 constexpr uint32_t kClaimRounds = 8;
