@@ -272,7 +272,7 @@ rbr_status rbr_scene_stats_get(const rbr_ctx* ctx, rbr_scene_stats* out);
  *                          none) in a launch of its own, compiled for that class's lobes; 0 one
  *                          launch for all classes (default)
  *   "pt.fetch"             path tracer: 1 (default) the extension, shading and shadow launches
- *                          hand out a queue of four grid rounds or more in claims of 32 to 256
+ *                          hand out a queue of eight grid rounds or more in claims of 32 to 256
  *                          entries to whichever warp is free (one atomic per claim), so warps
  *                          that drew short traversals take more; 0 a fixed grid-stride share
  *                          per warp

@@ -723,8 +723,10 @@ __device__ __forceinline__ void shadow_body(const DeviceScene& s, const Paths& P
     if (kCount) warp_add_counts(P.counters, kCTraffic + 4, traffic);
 }
 
+// 8 resident blocks per SM (64 registers), the grid's blocks per SM: with more registers a
+// launch would run in two waves of blocks.
 template <bool kCount = false>
-__global__ void __launch_bounds__(kBlock) k_shadow(DeviceScene s, Paths P, int* err) {
+__global__ void __launch_bounds__(kBlock, 8) k_shadow(DeviceScene s, Paths P, int* err) {
     shadow_body<kCount>(s, P, err, grid_span());
 }
 
