@@ -68,3 +68,24 @@ def test_no_cpu_fallback_without_a_device():
         lib.rbr_ctx_destroy(h)
         pytest.skip("a CUDA device is present")
     assert st == abi.RBR_ERR_CUDA and not h.value
+
+
+def test_every_tunable_is_documented_and_accepted():
+    """The tunables rbr_param_set and rbr_param_get accept (capi.cpp) are exactly the ones the
+    header documents, each accepted by both calls."""
+    import re
+    from pathlib import Path
+
+    root = Path(__file__).resolve().parents[1]
+    header = (root / "include" / "rbr_b200.h").read_text()
+    block = header[header.index("Tunables of a context"):header.index("Results do not depend on them")]
+    documented = set(re.findall(r'^ \*   "([a-z_0-9.]+)"', block, re.M))
+    src = (root / "ray-based-rendering_b200" / "csrc" / "capi.cpp").read_text()
+    setter = src[src.index("rbr_status rbr_param_set("):src.index("rbr_status rbr_param_get(")]
+    getter = src[src.index("rbr_status rbr_param_get("):]
+    getter = getter[:getter.index("\n}\n")]
+    accepted_set = set(re.findall(r'n == "([a-z_0-9.]+)"', setter))
+    accepted_get = set(re.findall(r'n == "([a-z_0-9.]+)"', getter))
+    assert "pt.fetch" in documented and "trace.order" in documented
+    assert accepted_set == documented, (accepted_set ^ documented)
+    assert accepted_get == documented, (accepted_get ^ documented)
