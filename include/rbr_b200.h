@@ -260,7 +260,8 @@ rbr_status rbr_scene_stats_get(const rbr_ctx* ctx, rbr_scene_stats* out);
  *   "pt.wave_paths"        camera samples per path-tracer wave (default 2^23)
  *   "pt.streams"           rbr_render: waves in flight, 1 or 2 (default 2: waves alternate
  *                          between two sets of path buffers on two streams; an image that
- *                          fits one wave is rendered as two half-image waves)
+ *                          fits one wave is rendered as two half-image waves; when the second
+ *                          set cannot be allocated, the waves run one at a time in the first)
  *   "trace.node_test"      sorted queries of kernel 0: 0 the packed node test (f32x2 FMAs), 1 a
  *                          register-lean one (scalar FMAs, fewer live registers)
  *   "trace.stream_io"      kernel 0: rays read and hits written with evict-first hints (default 1)

@@ -1020,14 +1020,20 @@ rbr_status render(rbr_ctx* ctx, const rbr_camera* cam, const rbr_render_params* 
     cap = std::max(spp, cap / spp * spp);
     // Two waves in flight (a second path-buffer set on a second stream): the latency-bound
     // launches at the end of one wave's bounces, which occupy few SMs, run beside the full
-    // launches of the next wave. An image that fits one wave is split into two halves.
-    const bool two = ctx->pt_streams == 2 && npix >= 2;
+    // launches of the next wave. An image that fits one wave is split into two halves. When
+    // the second set cannot be allocated, the waves run one at a time in the first.
+    bool two = ctx->pt_streams == 2 && npix >= 2;
     if (two && npix * spp <= cap) cap = static_cast<uint32_t>((npix + 1) / 2) * spp;
     rbr_status st = ensure_paths(ctx, cap, cap * nl);
     if (st != RBR_OK) return st;
     if (two) {
-        st = ensure_paths(ctx, cap, cap * nl, &ctx->pt2);
-        if (st == RBR_OK) st = ensure_side_stream(ctx);
+        st = ensure_paths(ctx, cap, cap * nl, &ctx->pt2);  // frees what it allocated on failure
+        if (st == RBR_ERR_OUT_OF_MEMORY) {
+            two = false;
+            st = RBR_OK;
+        } else if (st == RBR_OK) {
+            st = ensure_side_stream(ctx);
+        }
         if (st != RBR_OK) return st;
     }
     ctx->pt_last_two = two;
