@@ -5,14 +5,15 @@
 // belong to one wave, path k of a wave is sample (k % spp) of pixel (p0 + k / spp). Per wave:
 //   raygen                         camera rays for every path (counter-RNG jitter and lens)
 //   for depth = 0 .. maxDepth-1:
-//     begin    reset the per-depth queue counters
+//     begin    reset the per-depth queue counters and claim cursors
 //     extend   closest hit for the active queue; misses add background; hits are appended
-//              to one of four material-class queues (warp ballot + one atomic per warp)
+//              to one of six material-class queues (match.any + one atomic per class and warp)
 //     shade    per class queue: emission, next-event estimation over ALL lights (one shadow
 //              ray per light with a non-black BSDF value, appended to the shadow queue with
 //              its MIS-weighted contribution), BSDF sampling, Russian roulette after depth 3;
 //              surviving paths are appended to the next active queue
 //     shadow   any hit for the shadow queue; unoccluded contributions are added to the path
+//   (extend, shade and shadow hand out a long queue by claims: see Claim)
 //   film     per pixel, the sum of its samples' radiance in sample order / spp (what
 //            Film::addSample(x, y, sum / spp) stores), plus the sum of squares on request
 // The reference's estimator is reproduced, quirks included: emission only at depth 0 or after
@@ -492,7 +493,7 @@ __device__ __forceinline__ bool train_path(const Wave& w, uint64_t seed, uint32_
 // latency-bound on its division and square-root chains, and twice the warps of its natural
 // 124-register allocation hide more of it (GGX scene +5 %, Cornell box +3 %; 5, 6, 10 and 12
 // blocks were measured slower).
-// kCls < 0: one launch over the four class queues; kCls = a material class: that class's
+// kCls < 0: one launch over the six class queues; kCls = a material class: that class's
 // queue only, with the lobe kinds of the class known at compile time (no microfacet code for
 // the diffuse and delta-only classes, no next-event estimation for delta-only and lobeless
 // materials, whose light samples always evaluate to zero).
